@@ -1,0 +1,1368 @@
+// hg_index.cu -- host side of the B200 Hercules index: tree construction with
+// GPU-side routing and envelopes, the reference's on-disk format, and the
+// query orchestration behind the C ABI of include/hercules_gpu.h.
+#include <cuda_runtime.h>
+#include <float.h>
+#include <limits.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "hg_arith.cuh"
+#include "hg_breakpoints.h"
+#include "hg_gen.cuh"
+#include "hg_internal.h"
+#include "hg_kernels.h"
+
+using hg::Node;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+
+static thread_local char g_last_error[512] = "";
+
+static hg_status set_error(hg_status s, const char* what) {
+  snprintf(g_last_error, sizeof g_last_error, "%s", what);
+  return s;
+}
+
+static hg_status cuda_fail(cudaError_t e, const char* where) {
+  char buf[512];
+  snprintf(buf, sizeof buf, "%s: %s", where, cudaGetErrorString(e));
+  return set_error(e == cudaErrorMemoryAllocation ? HG_ERR_NOMEM : HG_ERR_CUDA, buf);
+}
+
+#define CK(call)                                          \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+  } while (0)
+
+#define HCK(call)                    \
+  do {                               \
+    hg_status s_ = (call);           \
+    if (s_ != HG_OK) return s_;      \
+  } while (0)
+
+template <class T>
+static cudaError_t dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void**)p, sizeof(T) * count);
+}
+
+template <class T>
+static void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// tree algorithm (host, float arithmetic compiled with -ffp-contract=off)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+int seg_start(const std::vector<short>& p, int i) { return i == 0 ? 0 : p[i - 1]; }
+int seg_len(const std::vector<short>& p, int i) { return i == 0 ? p[0] : p[i] - p[i - 1]; }
+
+// calc_hs_split_points, hercules_node_split.c:371-396 (min_length = 1)
+std::vector<short> hs_points_of(const std::vector<short>& points) {
+  std::vector<short> hs;
+  for (size_t i = 0; i < points.size(); ++i) {
+    short length = points[i];
+    if (i > 0) length = (short)(points[i] - points[i - 1]);
+    if (length >= 2) {
+      int start = i > 0 ? points[i - 1] : 0;
+      hs.push_back((short)(start + (length / 2)));
+    }
+    hs.push_back(points[i]);
+  }
+  return hs;
+}
+
+// create_hercules_node_filename, hercules_node.c:441-486
+std::string filename_of(const Node& n, const Node* parent) {
+  char buf[256];
+  int l = snprintf(buf, sizeof buf, "%02d", (int)n.points.size());
+  if (n.level) {
+    l += snprintf(buf + l, sizeof buf - l, "%s", n.is_left ? "_L" : "_R");
+    l += snprintf(buf + l, sizeof buf - l, "%s", parent->split_idx ? "_1" : "_0");
+    l += snprintf(buf + l, sizeof buf - l, "_(%d,%d,%g)", parent->split_from, parent->split_to,
+                  (double)parent->split_value);
+  }
+  snprintf(buf + l, sizeof buf - l, "_%d", n.level);
+  return buf;
+}
+
+void init_sketch(std::vector<float>& s, size_t nseg) {
+  s.assign(4 * nseg, 0.0f);
+  for (size_t i = 0; i < nseg; ++i) {
+    s[4 * i + 0] = -FLT_MAX;
+    s[4 * i + 1] = FLT_MAX;
+    s[4 * i + 2] = -FLT_MAX;
+    s[4 * i + 3] = FLT_MAX;
+  }
+}
+
+Node make_leaf(const std::vector<short>& points) {
+  Node n;
+  n.points = points;
+  n.hs_points = hs_points_of(points);
+  init_sketch(n.sk, points.size());
+  return n;
+}
+
+// range_calc, hercules_node_split.c:337-345
+float range_calc(const float* ind, int len) {
+  float mean_width = ind[0] - ind[1];
+  float stdev_upper = ind[2];
+  return (float)len * (mean_width * mean_width + stdev_upper * stdev_upper);
+}
+
+// mean/stdev split policies (hercules_node_split.c:22-71) for one segment
+// sketch: the splitting benefit QoS(N) - mean(QoS children) and the value.
+float policy_diff(const float* ind, int len, int policy, float* value) {
+  float c0[4], c1[4];
+  memcpy(c0, ind, sizeof c0);
+  memcpy(c1, ind, sizeof c1);
+  float v;
+  if (policy == 0) {
+    v = (ind[0] + ind[1]) / 2;
+    c0[1] = v;
+    c1[0] = v;
+  } else {
+    v = (ind[2] + ind[3]) / 2;
+    c0[2] = v;
+    c1[3] = v;
+  }
+  *value = v;
+  float r0 = range_calc(c0, len), r1 = range_calc(c1, len);
+  float mean = 0.0f;  // calc_mean, calc_utils.c:165-188
+  mean = mean + r0;
+  mean = mean + r1;
+  mean = mean / (float)2;
+  return range_calc(ind, len) - mean;
+}
+
+// The split decision of hercules_index_split_node (hercules_node_split.c:
+// 1043-1252): best vertical policy, then horizontal candidates that must
+// beat twice the best vertical benefit.  Returns the child segment ends.
+std::vector<short> choose_split(Node& n, const std::vector<float>& hs_sk) {
+  float max_diff = -FLT_MAX;
+  int hs_split_point = -1;
+  short from = 0, to = 0;
+  int idx = 0;
+  float value = 0.0f;
+  for (size_t i = 0; i < n.points.size(); ++i) {
+    int len = seg_len(n.points, (int)i);
+    for (int j = 0; j < 2; ++j) {
+      float v;
+      float diff = policy_diff(&n.sk[4 * i], len, j, &v);
+      if (diff > max_diff) {
+        max_diff = diff;
+        from = (short)seg_start(n.points, (int)i);
+        to = n.points[i];
+        idx = j;
+        value = v;
+      }
+    }
+  }
+  max_diff = max_diff * 2;
+  for (size_t i = 0; i < n.hs_points.size(); ++i) {
+    int len = seg_len(n.hs_points, (int)i);
+    for (int j = 0; j < 2; ++j) {
+      float v;
+      float diff = policy_diff(&hs_sk[4 * i], len, j, &v);
+      if (diff > max_diff) {
+        max_diff = diff;
+        from = (short)seg_start(n.hs_points, (int)i);
+        to = n.hs_points[i];
+        idx = j;
+        value = v;
+        // get_hs_split_point, hercules_node_split.c:296-313
+        bool found = std::find(n.points.begin(), n.points.end(), to) != n.points.end();
+        hs_split_point = found ? from : to;
+      }
+    }
+  }
+  n.split_from = from;
+  n.split_to = to;
+  n.split_idx = idx;
+  n.split_value = value;
+  std::vector<short> cp = n.points;
+  if (hs_split_point >= 0) {
+    cp.push_back((short)hs_split_point);
+    std::stable_sort(cp.begin(), cp.end());
+  }
+  return cp;
+}
+
+// Sketch keys (order-preserving ints, as the kernel writes them) to the
+// envelope of node_segment_sketch_update_sketch_parallel: fmaxf/fminf of
+// the initial -FLT_MAX / FLT_MAX with the members' extremes.
+float key_to_float(int k) {
+  int b = k >= 0 ? k : k ^ 0x7fffffff;
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+}
+
+void keys_to_sketch(const int* keys, size_t nseg, float* sk) {
+  for (size_t i = 0; i < nseg; ++i) {
+    const int* k = keys + 4 * i;
+    sk[4 * i + 0] = k[0] == INT_MIN ? -FLT_MAX : fmaxf(-FLT_MAX, key_to_float(k[0]));
+    sk[4 * i + 1] = k[1] == INT_MAX ? FLT_MAX : fminf(FLT_MAX, key_to_float(k[1]));
+    sk[4 * i + 2] = k[2] == INT_MIN ? -FLT_MAX : fmaxf(-FLT_MAX, key_to_float(k[2]));
+    sk[4 * i + 3] = k[3] == INT_MAX ? FLT_MAX : fminf(FLT_MAX, key_to_float(k[3]));
+  }
+}
+
+// update_node_ancestors_statistics_for_non_split_segments,
+// hercules_node.c:613-657: with split_segment = -1 (never set by the
+// parallel build) segment i of a parent is merged with segment i of the child.
+void merge_ancestors(std::vector<Node>& nodes, int leaf) {
+  int cn = leaf, cp = nodes[leaf].parent;
+  while (cp >= 0) {
+    Node& p = nodes[cp];
+    const Node& c = nodes[cn];
+    for (size_t i = 0; i < p.points.size(); ++i) {
+      p.sk[4 * i + 0] = fmaxf(p.sk[4 * i + 0], c.sk[4 * i + 0]);
+      p.sk[4 * i + 1] = fminf(p.sk[4 * i + 1], c.sk[4 * i + 1]);
+      p.sk[4 * i + 2] = fmaxf(p.sk[4 * i + 2], c.sk[4 * i + 2]);
+      p.sk[4 * i + 3] = fminf(p.sk[4 * i + 3], c.sk[4 * i + 3]);
+    }
+    cn = cp;
+    cp = p.parent;
+  }
+}
+
+void collect_leaves(const std::vector<Node>& nodes, int n, std::vector<int>& out) {
+  // iterative DFS, left first
+  std::vector<int> st{n};
+  while (!st.empty()) {
+    int x = st.back();
+    st.pop_back();
+    if (nodes[x].is_leaf) out.push_back(x);
+    else {
+      st.push_back(nodes[x].right);
+      st.push_back(nodes[x].left);
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// device index assembly
+// ---------------------------------------------------------------------------
+
+static void free_device(hg_index* ix) {
+  hg::DeviceIndex& d = ix->d;
+  dfree(d.rows);
+  dfree(d.rows_rm);
+  dfree(d.ids);
+  dfree(d.sax);
+  dfree(d.bp);
+  dfree(d.leaf_start);
+  dfree(d.leaf_size);
+  dfree(d.leaf_seg_off);
+  dfree(d.leaf_points);
+  dfree(d.leaf_sk);
+  dfree(d.nodes);
+  hg::QueryScratch& s = ix->s;
+  dfree(s.q);
+  dfree(s.lb);
+  dfree(s.approx_leaf);
+  dfree(s.cand);
+  dfree(s.cand_lb);
+  dfree(s.cand_count);
+  dfree(s.unit_prefix);
+  dfree(s.counters);
+  dfree(s.bound);
+  dfree(s.parts);
+  dfree(s.part_count);
+  dfree(s.topk);
+  dfree(s.topk_count);
+  dfree(s.topk_row);
+  dfree(s.paa);
+  dfree(s.stats);
+  dfree(s.err);
+  s.kmax = 0;
+}
+
+// Routing tree in the final encoding: internal nodes renumbered densely,
+// leaf children as ~leaf_index (DFS).
+static std::vector<hg::DNode> routing_nodes(const hg_index* ix, int* root) {
+  std::vector<int> dense(ix->nodes.size(), -1);
+  int cnt = 0;
+  for (size_t i = 0; i < ix->nodes.size(); ++i)
+    if (!ix->nodes[i].is_leaf) dense[i] = cnt++;
+  std::vector<hg::DNode> out(cnt > 0 ? cnt : 1);
+  auto enc = [&](int nid) { return ix->nodes[nid].is_leaf ? ~ix->nodes[nid].leaf_index : dense[nid]; };
+  for (size_t i = 0; i < ix->nodes.size(); ++i) {
+    const Node& n = ix->nodes[i];
+    if (n.is_leaf) continue;
+    hg::DNode& d = out[dense[i]];
+    d.left = enc(n.left);
+    d.right = enc(n.right);
+    d.value = n.split_value;
+    d.from = n.split_from;
+    d.to = n.split_to;
+    d.idx = n.split_idx;
+    d.pad = 0;
+  }
+  *root = enc(0);
+  return out;
+}
+
+// Leaf tables and routing tree to the device (rows, ids, sax already there).
+static hg_status upload_tables(hg_index* ix) {
+  hg::DeviceIndex& d = ix->d;
+  const size_t nl = ix->leaves.size();
+  std::vector<uint64_t> start(nl);
+  std::vector<uint32_t> size(nl);
+  std::vector<int> off(nl + 1, 0);
+  std::vector<short> pts;
+  std::vector<float> sk;
+  int max_seg = 0;
+  for (size_t i = 0; i < nl; ++i) {
+    const Node& n = ix->nodes[ix->leaves[i]];
+    start[i] = n.file_pos;
+    size[i] = n.node_size;
+    off[i + 1] = off[i] + (int)n.points.size();
+    pts.insert(pts.end(), n.points.begin(), n.points.end());
+    sk.insert(sk.end(), n.sk.begin(), n.sk.end());
+    max_seg = std::max(max_seg, (int)n.points.size());
+  }
+  ix->max_seg = max_seg;
+  CK(dalloc(&d.leaf_start, nl));
+  CK(dalloc(&d.leaf_size, nl));
+  CK(dalloc(&d.leaf_seg_off, nl + 1));
+  CK(dalloc(&d.leaf_points, pts.size()));
+  CK(dalloc(&d.leaf_sk, sk.size()));
+  CK(cudaMemcpy(d.leaf_start, start.data(), sizeof(uint64_t) * nl, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d.leaf_size, size.data(), sizeof(uint32_t) * nl, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d.leaf_seg_off, off.data(), sizeof(int) * (nl + 1), cudaMemcpyHostToDevice));
+  if (!pts.empty()) CK(cudaMemcpy(d.leaf_points, pts.data(), sizeof(short) * pts.size(), cudaMemcpyHostToDevice));
+  if (!sk.empty()) CK(cudaMemcpy(d.leaf_sk, sk.data(), sizeof(float) * sk.size(), cudaMemcpyHostToDevice));
+  int root;
+  std::vector<hg::DNode> rn = routing_nodes(ix, &root);
+  CK(dalloc(&d.nodes, rn.size()));
+  CK(cudaMemcpy(d.nodes, rn.data(), sizeof(hg::DNode) * rn.size(), cudaMemcpyHostToDevice));
+  d.root = root;
+  if (!d.bp) {
+    CK(dalloc(&d.bp, 256));
+    CK(cudaMemcpy(d.bp, kHgBreakpoints, sizeof(float) * 255, cudaMemcpyHostToDevice));
+  }
+  return HG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// build
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct BuildCtx {
+  hg_index* ix;
+  const float* X;  // device, n x L row-major, original order
+  cudaStream_t st;
+  // device build scratch
+  hg::DNode* d_tree = nullptr;
+  size_t tree_cap = 0;
+  int* d_leaf_of = nullptr;
+  uint32_t* d_members = nullptr;
+  uint8_t* d_flags = nullptr;
+  int* d_keys = nullptr;
+  short* d_seg = nullptr;  // from[MAXS], to[MAXS]
+  int* h_leaf_of = nullptr;  // pinned
+  uint32_t members_cap = 0;
+  std::vector<hg::DNode> h_tree;  // node id -> routing entry (internal nodes)
+  int root_enc = ~0;
+  static constexpr uint32_t kWindow = 65536;
+  static constexpr int kMaxSegs = 4096;
+
+  ~BuildCtx() {
+    dfree(d_tree);
+    dfree(d_leaf_of);
+    dfree(d_members);
+    dfree(d_flags);
+    dfree(d_keys);
+    dfree(d_seg);
+    if (h_leaf_of) cudaFreeHost(h_leaf_of);
+  }
+
+  // During the build a leaf child is encoded ~node_id.
+  hg_status sync_tree() {
+    if (h_tree.size() > tree_cap) {
+      dfree(d_tree);
+      tree_cap = std::max<size_t>(h_tree.size() * 2, 1024);
+      CK(dalloc(&d_tree, tree_cap));
+    }
+    CK(cudaMemcpyAsync(d_tree, h_tree.data(), sizeof(hg::DNode) * h_tree.size(), cudaMemcpyHostToDevice, st));
+    return HG_OK;
+  }
+
+  hg::Tree tree() const { return hg::Tree{d_tree, root_enc}; }
+
+  // min/max envelopes of segments [from_i, to_i) over the members
+  hg_status sketches(const uint32_t* d_mem, uint32_t count, const std::vector<short>& from,
+                     const std::vector<short>& to, std::vector<float>& out) {
+    const int ns = (int)from.size();
+    if (ns > kMaxSegs) return set_error(HG_ERR_LIMIT, "too many EAPCA segments in one node");
+    std::vector<int> init(4 * ns);
+    for (int i = 0; i < ns; ++i) {
+      init[4 * i + 0] = INT_MIN;
+      init[4 * i + 1] = INT_MAX;
+      init[4 * i + 2] = INT_MIN;
+      init[4 * i + 3] = INT_MAX;
+    }
+    CK(cudaMemcpyAsync(d_keys, init.data(), sizeof(int) * 4 * ns, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_seg, from.data(), sizeof(short) * ns, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_seg + kMaxSegs, to.data(), sizeof(short) * ns, cudaMemcpyHostToDevice, st));
+    CK(hg::launch_sketch_members(X, ix->L, d_mem, count, d_seg, d_seg + kMaxSegs, ns, d_keys, st));
+    CK(cudaMemcpyAsync(init.data(), d_keys, sizeof(int) * 4 * ns, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    out.resize(4 * ns);
+    keys_to_sketch(init.data(), ns, out.data());
+    return HG_OK;
+  }
+
+  // hercules_index_split_node (hercules_node_split.c:1043-1345) for leaf nid
+  hg_status split(int nid) {
+    std::vector<Node>& nodes = ix->nodes;
+    const uint32_t count = nodes[nid].node_size;
+    // a leaf that received every row of its parent's split holds more than
+    // leaf_size rows when it splits in turn
+    if (count > members_cap) {
+      CK(cudaStreamSynchronize(st));
+      dfree(d_members);
+      dfree(d_flags);
+      members_cap = std::max(count, members_cap * 2);
+      CK(dalloc(&d_members, members_cap));
+      CK(dalloc(&d_flags, members_cap));
+    }
+    CK(cudaMemcpyAsync(d_members, nodes[nid].members.data(), sizeof(uint32_t) * count, cudaMemcpyHostToDevice,
+                       st));
+    // vertical + horizontal sketches of the leaf over its members
+    std::vector<short> from, to;
+    for (size_t i = 0; i < nodes[nid].points.size(); ++i) {
+      from.push_back((short)seg_start(nodes[nid].points, (int)i));
+      to.push_back(nodes[nid].points[i]);
+    }
+    for (size_t i = 0; i < nodes[nid].hs_points.size(); ++i) {
+      from.push_back((short)seg_start(nodes[nid].hs_points, (int)i));
+      to.push_back(nodes[nid].hs_points[i]);
+    }
+    std::vector<float> all;
+    HCK(sketches(d_members, count, from, to, all));
+    const size_t nv = nodes[nid].points.size();
+    nodes[nid].sk.assign(all.begin(), all.begin() + 4 * nv);
+    std::vector<float> hs_sk(all.begin() + 4 * nv, all.end());
+    std::vector<short> cp = choose_split(nodes[nid], hs_sk);
+    // children (split_node_create_children, hercules_node_split.c:197-262)
+    Node l = make_leaf(cp), r = make_leaf(cp);
+    l.parent = r.parent = nid;
+    l.level = r.level = nodes[nid].level + 1;
+    l.is_left = true;
+    l.filename = filename_of(l, &nodes[nid]);
+    r.filename = filename_of(r, &nodes[nid]);
+    const int lid = (int)nodes.size(), rid = lid + 1;
+    nodes.push_back(std::move(l));
+    nodes.push_back(std::move(r));
+    Node& n = nodes[nid];
+    n.left = lid;
+    n.right = rid;
+    // redistribution in insertion order (:1294-1333)
+    CK(hg::launch_route_flags(X, ix->L, d_members, count, n.split_from, n.split_to, n.split_idx, n.split_value,
+                              d_flags, st));
+    std::vector<uint8_t> flags(count);
+    CK(cudaMemcpyAsync(flags.data(), d_flags, count, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    Node& L = nodes[lid];
+    Node& R = nodes[rid];
+    for (uint32_t m = 0; m < count; ++m) {
+      Node& c = flags[m] ? L : R;
+      c.members.push_back(n.members[m]);
+      ++c.node_size;
+    }
+    std::vector<uint32_t>().swap(n.members);
+    n.is_leaf = false;
+    // routing entries: this node becomes internal, its parent points to it
+    if (h_tree.size() < nodes.size()) h_tree.resize(nodes.size());
+    hg::DNode& d = h_tree[nid];
+    d.left = ~lid;
+    d.right = ~rid;
+    d.value = n.split_value;
+    d.from = n.split_from;
+    d.to = n.split_to;
+    d.idx = n.split_idx;
+    d.pad = 0;
+    if (n.parent < 0) root_enc = nid;
+    else {
+      hg::DNode& p = h_tree[n.parent];
+      if (p.left == ~nid) p.left = nid;
+      else p.right = nid;
+    }
+    return sync_tree();
+  }
+
+  hg_status run() {
+    std::vector<Node>& nodes = ix->nodes;
+    const uint64_t n = ix->n;
+    const uint32_t S = ix->leaf_size;
+    CK(dalloc(&d_leaf_of, kWindow));
+    members_cap = S + 1;
+    CK(dalloc(&d_members, members_cap));
+    CK(dalloc(&d_flags, members_cap));
+    CK(dalloc(&d_keys, 4 * kMaxSegs));
+    CK(dalloc(&d_seg, 2 * kMaxSegs));
+    CK(cudaMallocHost((void**)&h_leaf_of, sizeof(int) * kWindow));
+    h_tree.resize(1);
+    HCK(sync_tree());
+    uint64_t c = 0;
+    while (c < n) {
+      const uint32_t w = (uint32_t)std::min<uint64_t>(kWindow, n - c);
+      CK(hg::launch_route_rows(X, ix->L, nullptr, c, w, tree(), d_leaf_of, st));
+      CK(cudaMemcpyAsync(h_leaf_of, d_leaf_of, sizeof(int) * w, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      uint64_t next = c + w;
+      for (uint32_t j = 0; j < w; ++j) {
+        const int nid = ~h_leaf_of[j];
+        Node& leaf = nodes[nid];
+        leaf.members.push_back((uint32_t)(c + j));
+        ++leaf.node_size;
+        if (leaf.node_size >= S) {
+          HCK(split(nid));
+          next = c + j + 1;  // the rest of the window routes through the new tree
+          break;
+        }
+      }
+      c = next;
+    }
+    return HG_OK;
+  }
+};
+
+}  // namespace
+
+// Leaf order, file positions, leaf envelopes, the leaf-ordered tiles, iSAX
+// words and the merged internal envelopes of the written index.
+static hg_status finalize_build(hg_index* ix, const float* X, cudaStream_t st) {
+  std::vector<Node>& nodes = ix->nodes;
+  ix->leaves.clear();
+  collect_leaves(nodes, 0, ix->leaves);
+  std::vector<uint32_t> perm;
+  perm.reserve(ix->n);
+  uint64_t pos = 0;
+  for (size_t i = 0; i < ix->leaves.size(); ++i) {
+    Node& lf = nodes[ix->leaves[i]];
+    lf.leaf_index = (int)i;
+    lf.file_pos = pos;
+    pos += lf.node_size;
+    perm.insert(perm.end(), lf.members.begin(), lf.members.end());
+  }
+  if (pos != ix->n) return set_error(HG_ERR_ARG, "internal: leaf sizes do not add up");
+  uint32_t* d_perm = nullptr;
+  CK(dalloc(&d_perm, ix->n));
+  std::unique_ptr<uint32_t, void (*)(uint32_t*)> guard(d_perm, [](uint32_t* p) { cudaFree(p); });
+  CK(cudaMemcpyAsync(d_perm, perm.data(), sizeof(uint32_t) * ix->n, cudaMemcpyHostToDevice, st));
+  // leaf envelopes: vertical sketches over each leaf's members
+  int* d_keys = nullptr;
+  size_t total_segs = 0;
+  std::vector<size_t> koff(ix->leaves.size() + 1, 0);
+  for (size_t i = 0; i < ix->leaves.size(); ++i) {
+    total_segs += nodes[ix->leaves[i]].points.size();
+    koff[i + 1] = total_segs;
+  }
+  std::vector<int> keys(4 * total_segs);
+  std::vector<short> from, to;
+  for (size_t i = 0; i < ix->leaves.size(); ++i) {
+    const Node& lf = nodes[ix->leaves[i]];
+    for (size_t s = 0; s < lf.points.size(); ++s) {
+      from.push_back((short)seg_start(lf.points, (int)s));
+      to.push_back(lf.points[s]);
+      keys[4 * (koff[i] + s) + 0] = INT_MIN;
+      keys[4 * (koff[i] + s) + 1] = INT_MAX;
+      keys[4 * (koff[i] + s) + 2] = INT_MIN;
+      keys[4 * (koff[i] + s) + 3] = INT_MAX;
+    }
+  }
+  short* d_seg = nullptr;
+  CK(dalloc(&d_keys, keys.size()));
+  CK(dalloc(&d_seg, 2 * total_segs));
+  std::unique_ptr<int, void (*)(int*)> g2(d_keys, [](int* p) { cudaFree(p); });
+  std::unique_ptr<short, void (*)(short*)> g3(d_seg, [](short* p) { cudaFree(p); });
+  CK(cudaMemcpyAsync(d_keys, keys.data(), sizeof(int) * keys.size(), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_seg, from.data(), sizeof(short) * total_segs, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_seg + total_segs, to.data(), sizeof(short) * total_segs, cudaMemcpyHostToDevice, st));
+  for (size_t i = 0; i < ix->leaves.size(); ++i) {
+    const Node& lf = nodes[ix->leaves[i]];
+    if (lf.node_size == 0) continue;
+    CK(hg::launch_sketch_members(X, ix->L, d_perm + lf.file_pos, lf.node_size, d_seg + koff[i],
+                                 d_seg + total_segs + koff[i], (int)lf.points.size(), d_keys + 4 * koff[i], st));
+  }
+  CK(cudaMemcpyAsync(keys.data(), d_keys, sizeof(int) * keys.size(), cudaMemcpyDeviceToHost, st));
+  // tiles, ids, iSAX words
+  hg::DeviceIndex& d = ix->d;
+  ix->ntiles = (uint32_t)((ix->n + 31) / 32);
+  CK(dalloc(&d.rows, (size_t)ix->ntiles * 32 * ix->L));
+  CK(hg::launch_gather_tiles(X, ix->L, d_perm, ix->n, d.rows, st));
+  ix->ids.assign(perm.begin(), perm.end());
+  ix->has_ids = true;
+  CK(dalloc(&d.ids, ix->n));
+  CK(cudaMemcpyAsync(d.ids, ix->ids.data(), sizeof(int64_t) * ix->n, cudaMemcpyHostToDevice, st));
+  CK(dalloc(&d.bp, 256));
+  CK(cudaMemcpyAsync(d.bp, kHgBreakpoints, sizeof(float) * 255, cudaMemcpyHostToDevice, st));
+  CK(dalloc(&d.sax, (size_t)ix->n * 16));
+  CK(hg::launch_sax_rows(d.rows, ix->L, ix->n, d.bp, d.sax, st));
+  CK(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < ix->leaves.size(); ++i) {
+    Node& lf = nodes[ix->leaves[i]];
+    if (lf.node_size == 0) continue;  // an empty leaf keeps the initial envelope
+    keys_to_sketch(&keys[4 * koff[i]], lf.points.size(), lf.sk.data());
+  }
+  for (size_t i = 0; i < ix->leaves.size(); ++i) std::vector<uint32_t>().swap(nodes[ix->leaves[i]].members);
+  // internal envelopes as the sequential writer leaves them
+  for (size_t i = 0; i < ix->leaves.size(); ++i) merge_ancestors(nodes, ix->leaves[i]);
+  return upload_tables(ix);
+}
+
+static hg_status build_impl(const float* data, int on_device, uint64_t n, uint32_t L, uint32_t S, int device,
+                            hg_index** out) {
+  if (!out || !data || n == 0 || L == 0 || L % 16 != 0 || L > 32752 || S == 0)
+    return set_error(HG_ERR_ARG, "hg_index_build: need data, n > 0, L a multiple of 16 (<= 32752), leaf size > 0");
+  if (n > 0xffffffffull) return set_error(HG_ERR_LIMIT, "hg_index_build: at most 2^32-1 series");
+  CK(cudaSetDevice(device));
+  std::unique_ptr<hg_index> ix(new hg_index());
+  ix->device = device;
+  ix->L = L;
+  ix->leaf_size = S;
+  ix->n = n;
+  CK(cudaStreamCreateWithFlags(&ix->stream, cudaStreamNonBlocking));
+  const float* X = data;
+  float* owned = nullptr;
+  if (!on_device) {
+    CK(dalloc(&owned, n * L));
+    // staged copy from pageable memory in 256 MiB pieces
+    const size_t piece = (256u << 20) / (sizeof(float) * L) * L;
+    for (size_t o = 0; o < n * L; o += piece) {
+      size_t cnt = std::min(piece, (size_t)(n * L - o));
+      CK(cudaMemcpyAsync(owned + o, data + o, sizeof(float) * cnt, cudaMemcpyHostToDevice, ix->stream));
+    }
+    X = owned;
+  }
+  std::unique_ptr<float, void (*)(float*)> g(owned, [](float* p) {
+    if (p) cudaFree(p);
+  });
+  // root (hercules_root_node_init, hercules_node.c:27-78): one segment [0, L)
+  Node root = make_leaf(std::vector<short>{(short)L});
+  root.filename = filename_of(root, nullptr);
+  ix->nodes.push_back(std::move(root));
+  {
+    BuildCtx ctx;
+    ctx.ix = ix.get();
+    ctx.X = X;
+    ctx.st = ix->stream;
+    hg_status s = ctx.run();
+    if (s != HG_OK) {
+      free_device(ix.get());
+      cudaStreamDestroy(ix->stream);
+      return s;
+    }
+  }
+  hg_status s = finalize_build(ix.get(), X, ix->stream);
+  if (s != HG_OK) {
+    free_device(ix.get());
+    cudaStreamDestroy(ix->stream);
+    return s;
+  }
+  *out = ix.release();
+  return HG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// on-disk format (App. A of the format: root.idx, leaves_raw.idx, leaves_sims.idx)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct Writer {
+  FILE* f;
+  bool ok = true;
+  template <class T>
+  void put(const T& v) { ok = ok && fwrite(&v, sizeof(T), 1, f) == 1; }
+  void bytes(const void* p, size_t n) { ok = ok && (n == 0 || fwrite(p, 1, n, f) == n); }
+};
+
+// hercules_node_write, hercules_index.c:1967-2077
+void write_node(const hg_index* ix, int nid, Writer& w) {
+  const Node& n = ix->nodes[nid];
+  w.put<uint8_t>(n.is_leaf ? 1 : 0);
+  w.put<uint32_t>(n.level);
+  if (!n.is_leaf) {
+    write_node(ix, n.left, w);
+    write_node(ix, n.right, w);
+    w.put<uint32_t>(n.node_size);
+    w.put<int16_t>(-1);  // split_segment, never set by the parallel build
+    // struct node_split_policy (48 bytes, hercules_node_split.h:21-34): the
+    // trailing padding and pointer bytes carry no information; zeros here.
+    uint8_t pol[48];
+    memset(pol, 0, sizeof pol);
+    memcpy(pol + 0, &n.split_from, 2);
+    memcpy(pol + 2, &n.split_to, 2);
+    memcpy(pol + 4, &n.split_value, 4);
+    memcpy(pol + 8, &n.split_idx, 4);
+    memcpy(pol + 12, &n.split_idx, 4);
+    memcpy(pol + 16, &n.split_value, 4);
+    w.bytes(pol, 48);
+  } else {
+    w.put<uint32_t>(n.node_size);
+    w.put<int32_t>((int32_t)n.filename.size());
+    w.bytes(n.filename.data(), n.filename.size());
+  }
+  w.put<int16_t>((int16_t)n.points.size());
+  w.bytes(n.points.data(), sizeof(short) * n.points.size());
+  for (size_t i = 0; i < n.points.size(); ++i) {
+    w.put<int32_t>(4);
+    w.bytes(&n.sk[4 * i], 16);
+  }
+  if (n.is_leaf) w.put<uint64_t>(n.file_pos);
+}
+
+struct Reader {
+  FILE* f;
+  bool ok = true;
+  template <class T>
+  T get() {
+    T v{};
+    ok = ok && fread(&v, sizeof(T), 1, f) == 1;
+    return v;
+  }
+  void bytes(void* p, size_t n) { ok = ok && (n == 0 || fread(p, 1, n, f) == n); }
+};
+
+// hercules_node_read, hercules_index.c:2188-2340
+int read_node(hg_index* ix, Reader& r, int parent, int depth) {
+  if (!r.ok || depth > 10000) return -1;
+  const int nid = (int)ix->nodes.size();
+  ix->nodes.emplace_back();
+  const uint8_t is_leaf = r.get<uint8_t>();
+  const uint32_t level = r.get<uint32_t>();
+  ix->nodes[nid].parent = parent;
+  ix->nodes[nid].level = level;
+  ix->nodes[nid].is_leaf = is_leaf != 0;
+  if (!is_leaf) {
+    int l = read_node(ix, r, nid, depth + 1);
+    int rr = read_node(ix, r, nid, depth + 1);
+    if (l < 0 || rr < 0) return -1;
+    Node& n = ix->nodes[nid];
+    n.left = l;
+    n.right = rr;
+    ix->nodes[l].is_left = true;
+    n.node_size = r.get<uint32_t>();
+    (void)r.get<int16_t>();
+    uint8_t pol[48];
+    r.bytes(pol, 48);
+    memcpy(&n.split_from, pol + 0, 2);
+    memcpy(&n.split_to, pol + 2, 2);
+    memcpy(&n.split_idx, pol + 12, 4);
+    memcpy(&n.split_value, pol + 16, 4);
+  } else {
+    Node& n = ix->nodes[nid];
+    n.node_size = r.get<uint32_t>();
+    const int32_t len = r.get<int32_t>();
+    if (len <= 0) {
+      n.node_size = 0;  // a leaf written without a file name holds nothing
+      return r.ok ? nid : -1;
+    }
+    if (len > 65536) return -1;
+    n.filename.resize(len);
+    r.bytes(&n.filename[0], len);
+  }
+  Node& n = ix->nodes[nid];
+  const int16_t np = r.get<int16_t>();
+  if (np < 0 || np > 32767) return -1;
+  n.points.resize(np);
+  r.bytes(n.points.data(), sizeof(short) * np);
+  n.sk.resize(4 * np);
+  for (int i = 0; i < np; ++i) {
+    if (r.get<int32_t>() != 4) return -1;
+    r.bytes(&n.sk[4 * i], 16);
+  }
+  if (n.is_leaf) n.file_pos = r.get<uint64_t>();
+  return r.ok ? nid : -1;
+}
+
+std::string join(const char* dir, const char* name) {
+  std::string s(dir);
+  return s + name;
+}
+
+}  // namespace
+
+static hg_status write_impl(hg_index* ix, const char* dir, double buffer_mb) {
+  if (!ix || !dir) return set_error(HG_ERR_ARG, "hg_index_write: null argument");
+  CK(cudaSetDevice(ix->device));
+  FILE* f = fopen(join(dir, "root.idx").c_str(), "wb");
+  FILE* raw = fopen(join(dir, "leaves_raw.idx").c_str(), "wb");
+  FILE* sims = fopen(join(dir, "leaves_sims.idx").c_str(), "wb");
+  FILE* idf = fopen(join(dir, "leaves_ids.idx").c_str(), "wb");
+  auto close_all = [&]() {
+    if (f) fclose(f);
+    if (raw) fclose(raw);
+    if (sims) fclose(sims);
+    if (idf) fclose(idf);
+  };
+  if (!f || !raw || !sims || !idf) {
+    close_all();
+    return set_error(HG_ERR_IO, "hg_index_write: cannot create the index files");
+  }
+  // header (hercules_index.c:1671-1682)
+  Writer w{f};
+  w.put<uint64_t>((uint64_t)ix->leaves.size());
+  w.put<double>(buffer_mb);
+  w.put<uint32_t>(ix->L);
+  w.put<uint32_t>(1u);
+  w.put<int32_t>(16);
+  w.put<int32_t>(8);
+  w.put<uint32_t>(ix->leaf_size);
+  w.put<int32_t>(1);
+  w.put<int32_t>(1);
+  write_node(ix, 0, w);
+  // leaf-ordered raw rows and iSAX words, in pieces
+  const uint64_t piece = std::max<uint64_t>(1, (64u << 20) / (sizeof(float) * ix->L));
+  float* d_rm = nullptr;
+  CK(dalloc(&d_rm, piece * ix->L));
+  std::vector<float> h_rm(piece * ix->L);
+  std::vector<uint8_t> h_sax(piece * 16);
+  bool ok = w.ok;
+  for (uint64_t r0 = 0; r0 < ix->n && ok; r0 += piece) {
+    const uint64_t cnt = std::min(piece, ix->n - r0);
+    cudaError_t e = hg::launch_rowmajor_from_tiles(ix->d.rows, ix->L, r0, cnt, d_rm, ix->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_rm.data(), d_rm, sizeof(float) * cnt * ix->L, cudaMemcpyDeviceToHost, ix->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_sax.data(), ix->d.sax + r0 * 16, cnt * 16, cudaMemcpyDeviceToHost, ix->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
+    if (e != cudaSuccess) {
+      cudaFree(d_rm);
+      close_all();
+      return cuda_fail(e, "hg_index_write");
+    }
+    ok = fwrite(h_rm.data(), sizeof(float) * ix->L, cnt, raw) == cnt && fwrite(h_sax.data(), 16, cnt, sims) == cnt;
+  }
+  cudaFree(d_rm);
+  std::vector<uint64_t> ids64(ix->n);
+  for (uint64_t i = 0; i < ix->n; ++i) ids64[i] = ix->has_ids ? (uint64_t)ix->ids[i] : i;
+  ok = ok && fwrite(ids64.data(), 8, ix->n, idf) == ix->n;
+  close_all();
+  return ok ? HG_OK : set_error(HG_ERR_IO, "hg_index_write: short write");
+}
+
+static hg_status read_impl(const char* dir, int device, hg_index** out) {
+  if (!dir || !out) return set_error(HG_ERR_ARG, "hg_index_read: null argument");
+  FILE* f = fopen(join(dir, "root.idx").c_str(), "rb");
+  if (!f) return set_error(HG_ERR_IO, "hg_index_read: cannot open root.idx");
+  std::unique_ptr<hg_index> ix(new hg_index());
+  Reader r{f};
+  const uint64_t nleaves_hdr = r.get<uint64_t>();
+  ix->buffer_mb = r.get<double>();
+  ix->L = r.get<uint32_t>();
+  const uint32_t init_segments = r.get<uint32_t>();
+  const int32_t paa = r.get<int32_t>();
+  const int32_t card = r.get<int32_t>();
+  ix->leaf_size = r.get<uint32_t>();
+  const int32_t serial = r.get<int32_t>();
+  (void)r.get<int32_t>();
+  (void)init_segments;
+  if (!r.ok || paa != 16 || card != 8 || ix->L == 0 || ix->L % 16 != 0 || !serial) {
+    fclose(f);
+    return set_error(HG_ERR_FORMAT, "hg_index_read: root.idx header is not a serial 16x8-bit Hercules index");
+  }
+  if (read_node(ix.get(), r, -1, 0) != 0) {
+    fclose(f);
+    return set_error(HG_ERR_FORMAT, "hg_index_read: malformed node records in root.idx");
+  }
+  fclose(f);
+  collect_leaves(ix->nodes, 0, ix->leaves);
+  uint64_t pos = 0;
+  for (size_t i = 0; i < ix->leaves.size(); ++i) {
+    Node& lf = ix->nodes[ix->leaves[i]];
+    lf.leaf_index = (int)i;
+    if (lf.node_size > 0 && lf.file_pos != pos)
+      return set_error(HG_ERR_FORMAT, "hg_index_read: leaves are not stored in DFS order in leaves_raw.idx");
+    lf.file_pos = pos;
+    pos += lf.node_size;
+  }
+  (void)nleaves_hdr;
+  ix->n = pos;
+  ix->device = device;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&ix->stream, cudaStreamNonBlocking));
+  hg::DeviceIndex& d = ix->d;
+  ix->ntiles = (uint32_t)((ix->n + 31) / 32);
+  FILE* raw = fopen(join(dir, "leaves_raw.idx").c_str(), "rb");
+  if (!raw) return set_error(HG_ERR_IO, "hg_index_read: cannot open leaves_raw.idx");
+  const uint64_t piece = std::max<uint64_t>(32, ((64u << 20) / (sizeof(float) * ix->L)) / 32 * 32);
+  std::vector<float> h_rm(piece * ix->L);
+  float* d_rm = nullptr;
+  cudaError_t e = dalloc(&d.rows, (size_t)ix->ntiles * 32 * ix->L);
+  if (e == cudaSuccess) e = cudaMemset(d.rows, 0, sizeof(float) * (size_t)ix->ntiles * 32 * ix->L);
+  if (e == cudaSuccess) e = dalloc(&d_rm, piece * ix->L);
+  for (uint64_t r0 = 0; r0 < ix->n && e == cudaSuccess; r0 += piece) {
+    const uint64_t cnt = std::min(piece, ix->n - r0);
+    if (fread(h_rm.data(), sizeof(float) * ix->L, cnt, raw) != cnt) {
+      fclose(raw);
+      cudaFree(d_rm);
+      free_device(ix.get());
+      return set_error(HG_ERR_IO, "hg_index_read: leaves_raw.idx is shorter than the leaves");
+    }
+    e = cudaMemcpyAsync(d_rm, h_rm.data(), sizeof(float) * cnt * ix->L, cudaMemcpyHostToDevice, ix->stream);
+    if (e == cudaSuccess) e = hg::launch_tiles_from_rowmajor(d_rm, ix->L, r0, cnt, d.rows, ix->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
+  }
+  fclose(raw);
+  if (d_rm) cudaFree(d_rm);
+  if (e != cudaSuccess) {
+    free_device(ix.get());
+    return cuda_fail(e, "hg_index_read");
+  }
+  // dataset ids: leaves_ids.idx when present, else the row number
+  ix->ids.resize(ix->n);
+  FILE* idf = fopen(join(dir, "leaves_ids.idx").c_str(), "rb");
+  ix->has_ids = false;
+  if (idf) {
+    std::vector<uint64_t> ids64(ix->n);
+    if (fread(ids64.data(), 8, ix->n, idf) == ix->n) {
+      for (uint64_t i = 0; i < ix->n; ++i) ix->ids[i] = (int64_t)ids64[i];
+      ix->has_ids = true;
+    }
+    fclose(idf);
+  }
+  if (!ix->has_ids)
+    for (uint64_t i = 0; i < ix->n; ++i) ix->ids[i] = (int64_t)i;
+  CK(dalloc(&d.ids, ix->n));
+  CK(cudaMemcpy(d.ids, ix->ids.data(), sizeof(int64_t) * ix->n, cudaMemcpyHostToDevice));
+  CK(dalloc(&d.bp, 256));
+  CK(cudaMemcpy(d.bp, kHgBreakpoints, sizeof(float) * 255, cudaMemcpyHostToDevice));
+  CK(dalloc(&d.sax, (size_t)ix->n * 16));
+  CK(hg::launch_sax_rows(d.rows, ix->L, ix->n, d.bp, d.sax, ix->stream));
+  CK(cudaStreamSynchronize(ix->stream));
+  HCK(upload_tables(ix.get()));
+  *out = ix.release();
+  return HG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// queries
+// ---------------------------------------------------------------------------
+
+static hg_status ensure_scratch(hg_index* ix, int k) {
+  hg::QueryScratch& s = ix->s;
+  if (s.kmax >= k && s.q) return HG_OK;
+  const int nl = (int)ix->leaves.size();
+  dfree(s.q);
+  dfree(s.lb);
+  dfree(s.approx_leaf);
+  dfree(s.cand);
+  dfree(s.cand_lb);
+  dfree(s.cand_count);
+  dfree(s.unit_prefix);
+  dfree(s.bound);
+  dfree(s.parts);
+  dfree(s.part_count);
+  dfree(s.topk);
+  dfree(s.topk_count);
+  dfree(s.paa);
+  dfree(s.stats);
+  dfree(s.err);
+  const int blocks = hg::scan_grid_blocks(ix->device);
+  s.nparts = blocks * hg::kScanWarps;
+  CK(dalloc(&s.lb, nl));
+  CK(dalloc(&s.approx_leaf, 1));
+  CK(dalloc(&s.cand, nl + 1));
+  CK(dalloc(&s.cand_lb, nl + 1));
+  CK(dalloc(&s.cand_count, 1));
+  CK(dalloc(&s.unit_prefix, nl + 2));
+  CK(dalloc(&s.bound, 1));
+  CK(dalloc(&s.parts, (size_t)s.nparts * hg::kWarpListCap));
+  CK(dalloc(&s.part_count, s.nparts));
+  CK(dalloc(&s.topk, hg::kMaxK));
+  CK(dalloc(&s.topk_count, 1));
+  CK(dalloc(&s.paa, 16));
+  CK(dalloc(&s.stats, 4));
+  CK(dalloc(&s.err, 1));
+  CK(dalloc(&s.q, 1));
+  s.kmax = hg::kMaxK;
+  return HG_OK;
+}
+
+static hg::Tree index_tree(const hg_index* ix) { return hg::Tree{ix->d.nodes, ix->d.root}; }
+
+// One query through the plain path: approximate leaf, LB_EAPCA of every
+// leaf, scan of the approximate leaf, candidates by LB, scan, merge.
+static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opts& o, float* d_dist,
+                         int64_t* d_id, cudaStream_t st) {
+  hg::QueryScratch& s = ix->s;
+  hg::DeviceIndex& d = ix->d;
+  const int nl = (int)ix->leaves.size();
+  const int blocks = hg::scan_grid_blocks(ix->device);
+  hg::ScanArgs a{};
+  a.rows = d.rows;
+  a.ids = d.ids;
+  a.sax = d.sax;
+  a.bp = d.bp;
+  a.L = (int)ix->L;
+  a.nrows = ix->n;
+  a.leaf_start = d.leaf_start;
+  a.leaf_size = d.leaf_size;
+  a.cand = s.cand;
+  a.cand_lb = s.cand_lb;
+  a.cand_count = s.cand_count;
+  a.unit_prefix = s.unit_prefix;
+  a.q = d_q;
+  a.paa = s.paa;
+  a.k = k;
+  a.bound = s.bound;
+  a.parts = s.parts;
+  a.part_count = s.part_count;
+  a.stats = s.stats;
+  if (o.mode == HG_MODE_PSCAN) {
+    CK(hg::launch_pscan_prep(ix->n, s.cand_count, s.unit_prefix, s.bound, s.topk_count, st));
+    a.pscan = 1;
+    a.use_lbsax = 0;
+    CK(hg::launch_scan(a, blocks, st));
+    CK(hg::launch_merge(s.parts, s.part_count, s.nparts, k, s.topk, s.topk_count, s.bound, s.err, st));
+  } else {
+    a.pscan = 0;
+    a.use_lbsax = o.use_lb_sax ? 1 : 0;
+    CK(hg::launch_query_prep(d_q, a.L, index_tree(ix), d.leaf_start, d.leaf_size, s.approx_leaf, s.paa, s.cand,
+                             s.cand_lb, s.cand_count, s.unit_prefix, s.bound, s.topk_count, st));
+    CK(hg::launch_leaf_lb(d_q, a.L, nl, d.leaf_seg_off, d.leaf_points, d.leaf_sk, s.lb, st));
+    CK(hg::launch_scan(a, blocks, st));
+    CK(hg::launch_merge(s.parts, s.part_count, s.nparts, k, s.topk, s.topk_count, s.bound, s.err, st));
+    CK(hg::launch_select_sort(s.lb, nl, s.bound, s.approx_leaf, d.leaf_start, d.leaf_size, s.cand, s.cand_lb,
+                              s.cand_count, s.unit_prefix, st));
+    CK(hg::launch_scan(a, blocks, st));
+    CK(hg::launch_merge(s.parts, s.part_count, s.nparts, k, s.topk, s.topk_count, s.bound, s.err, st));
+  }
+  CK(hg::launch_emit(s.topk, s.topk_count, k, d_dist, d_id, st));
+  return HG_OK;
+}
+
+static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t nq, uint32_t k,
+                                 const hg_knn_opts* opts, float* d_dist, int64_t* d_id, cudaStream_t st,
+                                 hg_query_stats* stats) {
+  if (!ix || (!d_queries && nq)) return set_error(HG_ERR_ARG, "hg_knn: null argument");
+  if (k == 0) return set_error(HG_ERR_ARG, "hg_knn: k must be positive");
+  if ((int)k > hg::kMaxK) return set_error(HG_ERR_LIMIT, "hg_knn: k above 224");
+  if (ix->leaves.size() > (size_t)hg::kMaxLeavesSort)
+    return set_error(HG_ERR_LIMIT, "hg_knn: more than 8192 leaves");
+  hg_knn_opts o{};
+  if (opts) o = *opts;
+  CK(cudaSetDevice(ix->device));
+  HCK(ensure_scratch(ix, (int)k));
+  if (!st) st = ix->stream;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaMemsetAsync(ix->s.stats, 0, sizeof(unsigned long long) * 4, st));
+  CK(cudaEventRecord(e0, st));
+  for (uint32_t i = 0; i < nq; ++i)
+    HCK(knn_one(ix, d_queries + (uint64_t)i * ix->L, (int)k, o, d_dist ? d_dist + (uint64_t)i * k : nullptr,
+                d_id ? d_id + (uint64_t)i * k : nullptr, st));
+  CK(cudaEventRecord(e1, st));
+  unsigned long long hs[4];
+  CK(cudaMemcpyAsync(hs, ix->s.stats, sizeof hs, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (stats) {
+    memset(stats, 0, sizeof *stats);
+    stats->queries = nq;
+    stats->rows_visited = hs[0];
+    stats->chunks_loaded = hs[1];
+    stats->rows_lbsax_pruned = hs[2];
+    stats->leaves_scanned = hs[3];
+    stats->device_ms = ms;
+  }
+  return HG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host generators (same bits as the kernels)
+// ---------------------------------------------------------------------------
+
+template <class F>
+static void parallel_for(uint64_t n, F f) {
+  unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  if (n < 64) nt = 1;
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nt; ++t)
+    th.emplace_back([=]() {
+      for (uint64_t i = t; i < n; i += nt) f(i);
+    });
+  for (auto& x : th) x.join();
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+const char* hg_status_string(hg_status s) {
+  switch (s) {
+    case HG_OK: return "ok";
+    case HG_ERR_ARG: return "invalid argument";
+    case HG_ERR_IO: return "i/o error";
+    case HG_ERR_FORMAT: return "index format error";
+    case HG_ERR_CUDA: return "CUDA error";
+    case HG_ERR_NOMEM: return "out of memory";
+    case HG_ERR_TIMEOUT: return "device wait timed out";
+    case HG_ERR_LIMIT: return "size limit exceeded";
+    default: return "unknown status";
+  }
+}
+
+const char* hg_last_error(void) { return g_last_error; }
+
+hg_status hg_index_build(const float* data, int data_on_device, uint64_t n, uint32_t L, uint32_t leaf_size,
+                         int device, hg_index** out) {
+  return build_impl(data, data_on_device, n, L, leaf_size, device, out);
+}
+
+hg_status hg_index_build_file(const char* dataset, uint64_t n, uint32_t L, uint32_t leaf_size, int device,
+                              hg_index** out) {
+  if (!dataset || !out || L == 0) return set_error(HG_ERR_ARG, "hg_index_build_file: null argument");
+  FILE* f = fopen(dataset, "rb");
+  if (!f) return set_error(HG_ERR_IO, "hg_index_build_file: dataset not found");
+  fseek(f, 0, SEEK_END);
+  const uint64_t sz = (uint64_t)ftell(f);
+  fseek(f, 0, SEEK_SET);
+  if (sz / (sizeof(float) * L) < n) {
+    fclose(f);
+    return set_error(HG_ERR_IO, "hg_index_build_file: the file holds fewer series than requested");
+  }
+  std::vector<float> buf;
+  try {
+    buf.resize((size_t)n * L);
+  } catch (...) {
+    fclose(f);
+    return set_error(HG_ERR_NOMEM, "hg_index_build_file: host allocation");
+  }
+  const size_t got = fread(buf.data(), sizeof(float) * L, n, f);
+  fclose(f);
+  if (got != n) return set_error(HG_ERR_IO, "hg_index_build_file: short read");
+  return build_impl(buf.data(), 0, n, L, leaf_size, device, out);
+}
+
+hg_status hg_index_write(hg_index* ix, const char* dir, double buffer_mb) { return write_impl(ix, dir, buffer_mb); }
+
+hg_status hg_index_read(const char* dir, int device, hg_index** out) { return read_impl(dir, device, out); }
+
+void hg_index_destroy(hg_index* ix) {
+  if (!ix) return;
+  cudaSetDevice(ix->device);
+  free_device(ix);
+  if (ix->stream) cudaStreamDestroy(ix->stream);
+  delete ix;
+}
+
+hg_status hg_index_info_get(const hg_index* ix, hg_index_info* info) {
+  if (!ix || !info) return set_error(HG_ERR_ARG, "hg_index_info_get: null argument");
+  info->num_series = ix->n;
+  info->ts_length = ix->L;
+  info->leaf_size = ix->leaf_size;
+  info->num_leaves = (uint32_t)ix->leaves.size();
+  info->num_nodes = (uint32_t)ix->nodes.size();
+  info->max_segments = (uint32_t)ix->max_seg;
+  info->has_ids = ix->has_ids ? 1 : 0;
+  info->device_bytes = (uint64_t)ix->ntiles * 32 * ix->L * 4 + ix->n * (8 + 16);
+  return HG_OK;
+}
+
+hg_status hg_index_leaf(const hg_index* ix, uint32_t i, uint64_t* file_pos, uint32_t* size, uint32_t* nseg) {
+  if (!ix || i >= ix->leaves.size()) return set_error(HG_ERR_ARG, "hg_index_leaf: bad leaf");
+  const Node& n = ix->nodes[ix->leaves[i]];
+  if (file_pos) *file_pos = n.file_pos;
+  if (size) *size = n.node_size;
+  if (nseg) *nseg = (uint32_t)n.points.size();
+  return HG_OK;
+}
+
+hg_status hg_index_leaf_envelope(const hg_index* ix, uint32_t i, short* points, float* env) {
+  if (!ix || i >= ix->leaves.size()) return set_error(HG_ERR_ARG, "hg_index_leaf_envelope: bad leaf");
+  const Node& n = ix->nodes[ix->leaves[i]];
+  if (points) memcpy(points, n.points.data(), sizeof(short) * n.points.size());
+  if (env) memcpy(env, n.sk.data(), sizeof(float) * n.sk.size());
+  return HG_OK;
+}
+
+hg_status hg_index_row_ids(const hg_index* ix, int64_t* ids) {
+  if (!ix || !ids) return set_error(HG_ERR_ARG, "hg_index_row_ids: null argument");
+  memcpy(ids, ix->ids.data(), sizeof(int64_t) * ix->n);
+  return HG_OK;
+}
+
+hg_status hg_index_rows(const hg_index* ix, uint64_t first, uint64_t count, float* rows, uint8_t* sax) {
+  if (!ix || first + count > ix->n) return set_error(HG_ERR_ARG, "hg_index_rows: range outside the index");
+  if (count == 0) return HG_OK;
+  CK(cudaSetDevice(ix->device));
+  if (rows) {
+    float* d_rm = nullptr;
+    CK(dalloc(&d_rm, count * ix->L));
+    cudaError_t e = hg::launch_rowmajor_from_tiles(ix->d.rows, ix->L, first, count, d_rm, ix->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rows, d_rm, sizeof(float) * count * ix->L, cudaMemcpyDeviceToHost, ix->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
+    cudaFree(d_rm);
+    if (e != cudaSuccess) return cuda_fail(e, "hg_index_rows");
+  }
+  if (sax) CK(cudaMemcpy(sax, ix->d.sax + first * 16, count * 16, cudaMemcpyDeviceToHost));
+  return HG_OK;
+}
+
+hg_status hg_knn_device(hg_index* ix, const float* d_queries, uint32_t nq, uint32_t k, const hg_knn_opts* opts,
+                        float* d_dist_out, int64_t* d_id_out, void* stream, hg_query_stats* stats) {
+  return knn_device_impl(ix, d_queries, nq, k, opts, d_dist_out, d_id_out, (cudaStream_t)stream, stats);
+}
+
+hg_status hg_knn(hg_index* ix, const float* queries, uint32_t nq, uint32_t k, const hg_knn_opts* opts,
+                 float* dist_out, int64_t* id_out, uint64_t* leaf_pos_out, hg_query_stats* stats) {
+  if (!ix || (!queries && nq)) return set_error(HG_ERR_ARG, "hg_knn: null argument");
+  if (nq == 0) return HG_OK;
+  CK(cudaSetDevice(ix->device));
+  float* d_q = nullptr;
+  float* d_dist = nullptr;
+  int64_t* d_id = nullptr;
+  CK(dalloc(&d_q, (size_t)nq * ix->L));
+  cudaError_t e = dalloc(&d_dist, (size_t)nq * k);
+  if (e == cudaSuccess) e = dalloc(&d_id, (size_t)nq * k);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_q, queries, sizeof(float) * nq * ix->L, cudaMemcpyHostToDevice, ix->stream);
+  hg_status s = e == cudaSuccess ? HG_OK : cuda_fail(e, "hg_knn");
+  if (s == HG_OK) s = knn_device_impl(ix, d_q, nq, k, opts, d_dist, d_id, ix->stream, stats);
+  std::vector<int64_t> ids((size_t)nq * k);
+  if (s == HG_OK) {
+    e = cudaMemcpyAsync(ids.data(), d_id, sizeof(int64_t) * nq * k, cudaMemcpyDeviceToHost, ix->stream);
+    if (e == cudaSuccess && dist_out)
+      e = cudaMemcpyAsync(dist_out, d_dist, sizeof(float) * nq * k, cudaMemcpyDeviceToHost, ix->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
+    if (e != cudaSuccess) s = cuda_fail(e, "hg_knn");
+  }
+  cudaFree(d_q);
+  cudaFree(d_dist);
+  cudaFree(d_id);
+  if (s != HG_OK) return s;
+  if (id_out) memcpy(id_out, ids.data(), sizeof(int64_t) * nq * k);
+  if (leaf_pos_out) {
+    // answer id -> leaf-ordered row -> its leaf's file_pos
+    std::vector<uint64_t> row_of_id;
+    if (ix->has_ids) {
+      row_of_id.assign(ix->n, 0);
+      for (uint64_t r = 0; r < ix->n; ++r)
+        if ((uint64_t)ix->ids[r] < ix->n) row_of_id[ix->ids[r]] = r;
+    }
+    std::vector<uint64_t> starts(ix->leaves.size());
+    for (size_t i = 0; i < ix->leaves.size(); ++i) starts[i] = ix->nodes[ix->leaves[i]].file_pos;
+    for (size_t j = 0; j < (size_t)nq * k; ++j) {
+      if (ids[j] < 0) {
+        leaf_pos_out[j] = UINT64_MAX;
+        continue;
+      }
+      const uint64_t row = ix->has_ids ? row_of_id[ids[j]] : (uint64_t)ids[j];
+      size_t li = std::upper_bound(starts.begin(), starts.end(), row) - starts.begin();
+      // skip empty leaves sharing the start position
+      while (li > 0 && ix->nodes[ix->leaves[li - 1]].node_size == 0) --li;
+      leaf_pos_out[j] = li > 0 ? starts[li - 1] : 0;
+    }
+  }
+  return HG_OK;
+}
+
+hg_status hg_route(hg_index* ix, const float* queries, uint32_t nq, int32_t* leaf_out) {
+  if (!ix || !queries || !leaf_out) return set_error(HG_ERR_ARG, "hg_route: null argument");
+  if (nq == 0) return HG_OK;
+  CK(cudaSetDevice(ix->device));
+  float* d_q = nullptr;
+  int* d_l = nullptr;
+  CK(dalloc(&d_q, (size_t)nq * ix->L));
+  cudaError_t e = dalloc(&d_l, nq);
+  if (e == cudaSuccess) e = cudaMemcpy(d_q, queries, sizeof(float) * nq * ix->L, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = hg::launch_route_queries(d_q, (int)nq, (int)ix->L, index_tree(ix), d_l, ix->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(leaf_out, d_l, sizeof(int) * nq, cudaMemcpyDeviceToHost, ix->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
+  cudaFree(d_q);
+  if (d_l) cudaFree(d_l);
+  return e == cudaSuccess ? HG_OK : cuda_fail(e, "hg_route");
+}
+
+hg_status hg_leaf_lower_bounds(hg_index* ix, const float* query, float* lb_out) {
+  if (!ix || !query || !lb_out) return set_error(HG_ERR_ARG, "hg_leaf_lower_bounds: null argument");
+  CK(cudaSetDevice(ix->device));
+  const int nl = (int)ix->leaves.size();
+  float* d_q = nullptr;
+  float* d_lb = nullptr;
+  CK(dalloc(&d_q, ix->L));
+  cudaError_t e = dalloc(&d_lb, nl);
+  if (e == cudaSuccess) e = cudaMemcpy(d_q, query, sizeof(float) * ix->L, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = hg::launch_leaf_lb(d_q, (int)ix->L, nl, ix->d.leaf_seg_off, ix->d.leaf_points, ix->d.leaf_sk, d_lb, ix->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(lb_out, d_lb, sizeof(float) * nl, cudaMemcpyDeviceToHost, ix->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
+  cudaFree(d_q);
+  if (d_lb) cudaFree(d_lb);
+  return e == cudaSuccess ? HG_OK : cuda_fail(e, "hg_leaf_lower_bounds");
+}
+
+hg_status hg_generate_walks(uint64_t seed, uint64_t first, uint64_t n, uint32_t L, float* out, int on_device,
+                            int device) {
+  if (!out || L == 0 || L % 4 != 0) return set_error(HG_ERR_ARG, "hg_generate_walks: L must be a multiple of 4");
+  if (on_device) {
+    CK(cudaSetDevice(device));
+    CK(hg::launch_generate_walks(seed, first, n, (int)L, out, 0));
+    CK(cudaStreamSynchronize(0));
+    return HG_OK;
+  }
+  parallel_for(n, [=](uint64_t i) { hg::random_walk(seed, first + i, (int)L, out + i * L); });
+  return HG_OK;
+}
+
+hg_status hg_generate_queries(uint64_t seed, const float* data, uint64_t n, uint32_t L, uint32_t nq,
+                              const double* sigma2, float* out, uint64_t* base_ids, int on_device, int device) {
+  if (!data || !out || !sigma2 || n == 0 || L == 0 || L % 4 != 0)
+    return set_error(HG_ERR_ARG, "hg_generate_queries: bad argument");
+  if (on_device) {
+    CK(cudaSetDevice(device));
+    double* d_s = nullptr;
+    CK(dalloc(&d_s, nq));
+    cudaError_t e = cudaMemcpy(d_s, sigma2, sizeof(double) * nq, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = hg::launch_generate_queries(seed, data, n, (int)L, (int)nq, d_s, out, base_ids, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    cudaFree(d_s);
+    return e == cudaSuccess ? HG_OK : cuda_fail(e, "hg_generate_queries");
+  }
+  parallel_for(nq, [=](uint64_t j) {
+    const uint64_t b = hg::pick_row(seed, j, n);
+    if (base_ids) base_ids[j] = b;
+    hg::noisy_query(seed, j, data + b * L, (int)L, sigma2[j], out + j * L);
+  });
+  return HG_OK;
+}
+
+hg_status hg_sax_breakpoints(float* out255) {
+  if (!out255) return set_error(HG_ERR_ARG, "hg_sax_breakpoints: null argument");
+  memcpy(out255, kHgBreakpoints, sizeof(float) * 255);
+  return HG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,93 @@
+// hg_internal.h -- host-side structures of the B200 Hercules index.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/hercules_gpu.h"
+#include "hg_kernels.h"
+
+namespace hg {
+
+// One node of the EAPCA tree (struct hercules_node, hercules_node.h:19-64,
+// reduced to what the build, the query path and root.idx need).
+struct Node {
+  int parent = -1, left = -1, right = -1;
+  bool is_leaf = true, is_left = false;
+  uint32_t level = 0;
+  std::vector<short> points;     // vertical segment ends
+  std::vector<short> hs_points;  // horizontal-split candidate ends
+  std::vector<float> sk;         // points.size() x {mean max, mean min, stdev max, stdev min}
+  // split policy of an internal node (hercules_node_split.h:21-34)
+  short split_from = 0, split_to = 0;
+  int split_idx = 0;
+  float split_value = 0.0f;
+  uint32_t node_size = 0;
+  std::vector<uint32_t> members;  // dataset rows of a leaf, insertion order
+  std::string filename;
+  uint64_t file_pos = 0;
+  int leaf_index = -1;
+};
+
+// Device buffers sized by an index (one GPU per handle).
+struct DeviceIndex {
+  float* rows = nullptr;      // leaf-ordered rows, 32-row chunk-interleaved tiles
+  float* rows_rm = nullptr;   // optional row-major copy (write/export), may be null
+  int64_t* ids = nullptr;     // dataset id of each leaf-ordered row
+  uint8_t* sax = nullptr;     // iSAX word (16 symbols) of each leaf-ordered row
+  float* bp = nullptr;        // 255 breakpoints of cardinality 256
+  // leaves (DFS order)
+  uint64_t* leaf_start = nullptr;
+  uint32_t* leaf_size = nullptr;
+  int* leaf_seg_off = nullptr;  // CSR offsets into leaf_points / leaf_sk
+  short* leaf_points = nullptr;
+  float* leaf_sk = nullptr;
+  // routing tree (internal nodes; a child < 0 is the leaf ~child, DFS index)
+  DNode* nodes = nullptr;
+  int root = 0;
+};
+
+// Per-query scratch for the plain path (sized for the largest k).
+struct QueryScratch {
+  int kmax = 0;
+  int nparts = 0;
+  float* q = nullptr;             // L
+  float* lb = nullptr;            // leaves
+  int* approx_leaf = nullptr;     // 1
+  int* cand = nullptr;            // leaves
+  float* cand_lb = nullptr;       // leaves
+  int* cand_count = nullptr;      // 1
+  uint32_t* unit_prefix = nullptr;  // leaves + 1 (tiles per candidate, exclusive scan)
+  uint32_t* counters = nullptr;   // work counter, misc
+  uint32_t* bound = nullptr;      // float bits of the current k-th distance bound
+  unsigned long long* parts = nullptr;  // nparts x kmax keys (d bits << 32 | id)
+  int* part_count = nullptr;      // nparts
+  unsigned long long* topk = nullptr;   // kmax keys
+  int* topk_count = nullptr;
+  uint64_t* topk_row = nullptr;   // kmax leaf-ordered rows of the answers
+  float* paa = nullptr;           // 16
+  unsigned long long* stats = nullptr;  // counters: rows visited, chunks loaded, rows lbsax-pruned, leaves scanned
+  int* err = nullptr;             // device error flag
+};
+
+}  // namespace hg
+
+struct hg_index {
+  int device = 0;
+  uint32_t L = 0;
+  uint32_t leaf_size = 0;
+  uint64_t n = 0;
+  double buffer_mb = 0.0;
+  std::vector<hg::Node> nodes;  // nodes[0] is the root
+  std::vector<int> leaves;      // node id of each leaf, DFS order
+  std::vector<int64_t> ids;     // host copy of the row -> dataset id map
+  bool has_ids = false;         // false for an index built by the reference
+  hg::DeviceIndex d;
+  hg::QueryScratch s;
+  cudaStream_t stream = nullptr;
+  uint32_t ntiles = 0;
+  int max_seg = 0;
+};

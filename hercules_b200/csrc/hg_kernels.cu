@@ -1,0 +1,961 @@
+// hg_kernels.cu -- sm_100a kernels of the Hercules exact k-NN path.
+//
+// Data layout in HBM: the leaf-ordered rows (leaves_raw.idx order) are held
+// in 32-row tiles, chunk-interleaved: element (row r, column j) lives at
+//   ((r/32) * (L/8) + j/8) * 256 + (r%32) * 8 + j%8
+// so one 8-float chunk (32 bytes, one DRAM sector) of 32 consecutive rows
+// is a contiguous 1 KiB block.  A warp scanning 32 rows chunk by chunk reads
+// fully coalesced 1 KiB blocks, and a row that abandons stops requesting its
+// sectors.  Distances follow the reference's summation order exactly
+// (hg_arith.cuh).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hg_arith.cuh"
+#include "hg_gen.cuh"
+#include "hg_kernels.h"
+
+namespace hg {
+
+#define HG_FULL 0xffffffffu
+
+__device__ __forceinline__ uint64_t tile_off(uint64_t row, int chunk, int nchunks) {
+  return ((((row >> 5) * (uint64_t)nchunks + (uint64_t)chunk) << 5) + (row & 31)) << 3;
+}
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
+  return *(const volatile uint32_t*)p;
+}
+
+// Mean and stdev of v[from, to) in the order of calc_mean_stdev_SIMD: the
+// lanes compute the 8-chunk sums in parallel, then every lane accumulates
+// them in chunk order (identical warp-uniform result).
+__device__ void warp_mean_stdev(const float* v, int from, int to, float* mean, float* stdev) {
+  const int lane = threadIdx.x & 31;
+  const int count = to - from;
+  if (count <= 0) {
+    *mean = 0.0f;
+    *stdev = 0.0f;
+    return;
+  }
+  const int nch = (count + 7) >> 3;
+  float sum = 0.0f, sumsq = 0.0f;
+  for (int base = 0; base < nch; base += 32) {
+    const int c = base + lane;
+    float cs = 0.0f, cq = 0.0f;
+    if (c < nch) {
+      float x[8], x2[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int i = c * 8 + j;
+        x[j] = i < count ? v[from + i] : 0.0f;
+        x2[j] = __fmul_rn(x[j], x[j]);
+      }
+      cs = hg_hsum8(x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7]);
+      cq = hg_hsum8(x2[0], x2[1], x2[2], x2[3], x2[4], x2[5], x2[6], x2[7]);
+    }
+    const int lim = min(32, nch - base);
+    for (int j = 0; j < lim; ++j) {
+      sum = __fadd_rn(sum, __shfl_sync(HG_FULL, cs, j));
+      sumsq = __fadd_rn(sumsq, __shfl_sync(HG_FULL, cq, j));
+    }
+  }
+  const float fc = (float)count;
+  *mean = __fdiv_rn(sum, fc);
+  sumsq = __fsub_rn(sumsq, __fdiv_rn(__fmul_rn(sum, sum), fc));
+  *stdev = __fsqrt_rn(__fdiv_rn(sumsq, fc));
+}
+
+// Walks the tree from the root (node_split_policy_route_to_left,
+// hercules_node_split.c:172-193).  Returns the leaf index.
+__device__ int warp_route(const float* q, const Tree& t) {
+  int node = t.root;
+  while (node >= 0) {
+    const DNode n = t.nodes[node];
+    float m, s;
+    warp_mean_stdev(q, n.from, n.to, &m, &s);
+    const float v = n.idx ? s : m;
+    node = (v < n.value) ? n.left : n.right;
+  }
+  return ~node;
+}
+
+__device__ __forceinline__ uint32_t tiles_of_leaf(uint64_t start, uint32_t size) {
+  if (size == 0) return 0;
+  return (uint32_t)(((start + size - 1) >> 5) - (start >> 5) + 1);
+}
+
+// ---------------------------------------------------------------------------
+// block-wide helpers
+// ---------------------------------------------------------------------------
+
+template <int THREADS>
+__device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* tmp /* THREADS/32 + 1 */, uint32_t* total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(HG_FULL, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) tmp[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t s = lane < THREADS / 32 ? tmp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(HG_FULL, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < THREADS / 32) tmp[lane] = s;
+    if (lane == THREADS / 32 - 1) tmp[THREADS / 32] = s;
+  }
+  __syncthreads();
+  const uint32_t excl = x - v + (w > 0 ? tmp[w - 1] : 0);
+  if (total) *total = tmp[THREADS / 32];
+  __syncthreads();
+  return excl;
+}
+
+// ---------------------------------------------------------------------------
+// build kernels
+// ---------------------------------------------------------------------------
+
+// One series per thread: walk the current tree to a leaf.
+__global__ void k_route_rows(const float* __restrict__ X, int L, const uint32_t* __restrict__ rows, uint64_t first,
+                             uint32_t count, Tree t, int* __restrict__ leaf_out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const uint64_t r = rows ? rows[i] : first + i;
+  const float* x = X + r * (uint64_t)L;
+  int node = t.root;
+  while (node >= 0) {
+    const DNode n = t.nodes[node];
+    float m, s;
+    hg_mean_stdev(x, n.from, n.to, &m, &s);
+    const float v = n.idx ? s : m;
+    node = (v < n.value) ? n.left : n.right;
+  }
+  leaf_out[i] = ~node;
+}
+
+// Order-preserving int image of a float for atomicMax/atomicMin.
+__device__ __forceinline__ int fkey(float f) {
+  int b = __float_as_int(f);
+  return b >= 0 ? b : b ^ 0x7fffffff;
+}
+
+// Segment sketches (min/max of per-series segment mean and stdev) over a
+// member list: node_segment_sketch_update_sketch_parallel applied to every
+// member (hercules_node_split.c:86-120).  Min/max are order independent and
+// fmaxf/fminf ignore NaN, so skipping NaN gives the same envelope.
+// keys_out: nsegs x 4 ints {max mean, min mean, max stdev, min stdev}.
+__global__ void k_sketch_members(const float* __restrict__ X, int L, const uint32_t* __restrict__ members,
+                                 uint32_t count, const short* __restrict__ seg_from,
+                                 const short* __restrict__ seg_to, int nsegs, int* __restrict__ keys_out) {
+  extern __shared__ int sk[];  // nsegs x 4
+  for (int i = threadIdx.x; i < nsegs; i += blockDim.x) {
+    sk[4 * i + 0] = INT_MIN;
+    sk[4 * i + 1] = INT_MAX;
+    sk[4 * i + 2] = INT_MIN;
+    sk[4 * i + 3] = INT_MAX;
+  }
+  __syncthreads();
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < count; m += gridDim.x * blockDim.x) {
+    const float* x = X + (uint64_t)members[m] * L;
+    for (int s = 0; s < nsegs; ++s) {
+      float mean, sd;
+      hg_mean_stdev(x, seg_from[s], seg_to[s], &mean, &sd);
+      if (mean == mean) {
+        atomicMax(&sk[4 * s + 0], fkey(mean));
+        atomicMin(&sk[4 * s + 1], fkey(mean));
+      }
+      if (sd == sd) {
+        atomicMax(&sk[4 * s + 2], fkey(sd));
+        atomicMin(&sk[4 * s + 3], fkey(sd));
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nsegs; i += blockDim.x) {
+    atomicMax(&keys_out[4 * i + 0], sk[4 * i + 0]);
+    atomicMin(&keys_out[4 * i + 1], sk[4 * i + 1]);
+    atomicMax(&keys_out[4 * i + 2], sk[4 * i + 2]);
+    atomicMin(&keys_out[4 * i + 3], sk[4 * i + 3]);
+  }
+}
+
+__global__ void k_route_flags(const float* __restrict__ X, int L, const uint32_t* __restrict__ members,
+                              uint32_t count, short from, short to, int idx, float value,
+                              uint8_t* __restrict__ flags) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  float m, s;
+  hg_mean_stdev(X + (uint64_t)members[i] * L, from, to, &m, &s);
+  flags[i] = ((idx ? s : m) < value) ? 1 : 0;
+}
+
+// tiles[row] = X[perm[row]]; one thread per (row, chunk), rows fastest so
+// that a warp writes one contiguous 1 KiB tile block.
+__global__ void k_gather_tiles(const float* __restrict__ X, int L, const uint32_t* __restrict__ perm, uint64_t n,
+                               float* __restrict__ tiles) {
+  const int nch = L >> 3;
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t tile = t / (32ull * nch);
+  const int within = (int)(t % (32ull * nch));
+  const int chunk = within >> 5, lane = within & 31;
+  const uint64_t row = tile * 32 + lane;
+  if (tile * 32 >= n) return;
+  float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+  if (row < n) {
+    const float4* src = reinterpret_cast<const float4*>(X + (uint64_t)perm[row] * L + chunk * 8);
+    a = src[0];
+    b = src[1];
+  }
+  float4* dst = reinterpret_cast<float4*>(tiles + tile_off(row, chunk, nch));
+  dst[0] = a;
+  dst[1] = b;
+}
+
+__global__ void k_tiles_from_rowmajor(const float* __restrict__ rm, int L, uint64_t first, uint64_t count,
+                                      float* __restrict__ tiles) {
+  // rm holds rows [first, first+count); first is a multiple of 32
+  const int nch = L >> 3;
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t tl = t / (32ull * nch);
+  const int within = (int)(t % (32ull * nch));
+  const int chunk = within >> 5, lane = within & 31;
+  const uint64_t local = tl * 32 + lane;
+  if (tl * 32 >= count) return;
+  float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+  if (local < count) {
+    const float4* src = reinterpret_cast<const float4*>(rm + local * L + chunk * 8);
+    a = src[0];
+    b = src[1];
+  }
+  float4* dst = reinterpret_cast<float4*>(tiles + tile_off(first + local, chunk, nch));
+  dst[0] = a;
+  dst[1] = b;
+}
+
+__global__ void k_rowmajor_from_tiles(const float* __restrict__ tiles, int L, uint64_t first, uint64_t count,
+                                      float* __restrict__ rm) {
+  const int nch = L >> 3;
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t local = t / nch;
+  const int chunk = (int)(t % nch);
+  if (local >= count) return;
+  const float4* src = reinterpret_cast<const float4*>(tiles + tile_off(first + local, chunk, nch));
+  float4* dst = reinterpret_cast<float4*>(rm + local * L + chunk * 8);
+  dst[0] = src[0];
+  dst[1] = src[1];
+}
+
+// iSAX word of every leaf-ordered row (sax_from_ts, sax.c:86-135).
+__global__ void k_sax_rows(const float* __restrict__ tiles, int L, uint64_t n, const float* __restrict__ bp,
+                           uint8_t* __restrict__ sax) {
+  __shared__ float sbp[256];
+  for (int i = threadIdx.x; i < 255; i += blockDim.x) sbp[i] = bp[i];
+  __syncthreads();
+  const uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  const int nch = L >> 3;
+  const int per = L / HG_PAA_SEGMENTS;
+  uint8_t w[16];
+  float acc = 0.0f;
+  int seg = 0, in_seg = 0;
+  for (int c = 0; c < nch; ++c) {
+    const float4* p = reinterpret_cast<const float4*>(tiles + tile_off(row, c, nch));
+    const float4 a = p[0], b = p[1];
+    const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      acc = __fadd_rn(acc, v[j]);
+      if (++in_seg == per) {
+        w[seg++] = (uint8_t)hg_sax_symbol(__fdiv_rn(acc, (float)per), sbp);
+        acc = 0.0f;
+        in_seg = 0;
+      }
+    }
+  }
+  uint4 out;
+  out.x = w[0] | (w[1] << 8) | (w[2] << 16) | ((uint32_t)w[3] << 24);
+  out.y = w[4] | (w[5] << 8) | (w[6] << 16) | ((uint32_t)w[7] << 24);
+  out.z = w[8] | (w[9] << 8) | (w[10] << 16) | ((uint32_t)w[11] << 24);
+  out.w = w[12] | (w[13] << 8) | (w[14] << 16) | ((uint32_t)w[15] << 24);
+  reinterpret_cast<uint4*>(sax)[row] = out;
+}
+
+// ---------------------------------------------------------------------------
+// query kernels
+// ---------------------------------------------------------------------------
+
+// One warp: route the query (approximate_knn_search's traversal), compute
+// its PAA, and set the first scan phase to the approximate leaf with an
+// unbounded k-th distance.
+__global__ void k_query_prep(const float* __restrict__ q, int L, Tree t, const uint64_t* __restrict__ leaf_start,
+                             const uint32_t* __restrict__ leaf_size, int* approx_leaf, float* paa, int* cand,
+                             float* cand_lb, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
+                             int* topk_count) {
+  const int lane = threadIdx.x & 31;
+  const int leaf = warp_route(q, t);
+  if (lane < HG_PAA_SEGMENTS) {
+    const int per = L / HG_PAA_SEGMENTS;
+    float acc = 0.0f;
+    for (int i = 0; i < per; ++i) acc = __fadd_rn(acc, q[lane * per + i]);
+    paa[lane] = __fdiv_rn(acc, (float)per);
+  }
+  if (lane == 0) {
+    *approx_leaf = leaf;
+    cand[0] = leaf;
+    cand_lb[0] = 0.0f;
+    *cand_count = 1;
+    unit_prefix[0] = 0;
+    unit_prefix[1] = tiles_of_leaf(leaf_start[leaf], leaf_size[leaf]);
+    *bound = 0x7f800000u;  // +inf
+    *topk_count = 0;
+  }
+}
+
+__global__ void k_route_queries(const float* __restrict__ Q, int nq, int L, Tree t, int* __restrict__ leaf_out) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nq) return;
+  const int leaf = warp_route(Q + (uint64_t)w * L, t);
+  if ((threadIdx.x & 31) == 0) leaf_out[w] = leaf;
+}
+
+// LB_EAPCA of the query against every leaf, one warp per leaf.
+__global__ void k_leaf_lb(const float* __restrict__ q, int L, int nleaves, const int* __restrict__ seg_off,
+                          const short* __restrict__ points, const float* __restrict__ sk, float* __restrict__ lb) {
+  extern __shared__ float qs[];
+  for (int i = threadIdx.x; i < L; i += blockDim.x) qs[i] = q[i];
+  __syncthreads();
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nleaves) return;
+  const int off = seg_off[w], nseg = seg_off[w + 1] - off;
+  float sum = 0.0f;
+  int start = 0;
+  for (int s = 0; s < nseg; ++s) {
+    const int end = points[off + s];
+    float m, sd;
+    warp_mean_stdev(qs, start, end, &m, &sd);
+    sum = __fadd_rn(sum, hg_eapca_term(m, sd, sk + 4 * (off + s), end - start));
+    start = end;
+  }
+  if ((threadIdx.x & 31) == 0) lb[w] = sum;
+}
+
+// Candidate leaves: LB_EAPCA <= current bound, not the approximate leaf, not
+// empty; ordered by LB with a stable LSD radix sort (4-bit digits, 8 passes)
+// in one CTA; then the exclusive prefix of their tile counts.
+constexpr int kSortThreads = 1024;
+__global__ void __launch_bounds__(kSortThreads) k_select_sort(const float* __restrict__ lb, int nleaves,
+                                                              const uint32_t* bound, const int* approx_leaf,
+                                                              const uint64_t* __restrict__ leaf_start,
+                                                              const uint32_t* __restrict__ leaf_size, int* cand,
+                                                              float* cand_lb, int* cand_count,
+                                                              uint32_t* unit_prefix) {
+  extern __shared__ uint32_t sm[];
+  uint32_t* keys0 = sm;
+  uint32_t* vals0 = keys0 + kMaxLeavesSort;
+  uint32_t* keys1 = vals0 + kMaxLeavesSort;
+  uint32_t* vals1 = keys1 + kMaxLeavesSort;
+  uint16_t* cnt = reinterpret_cast<uint16_t*>(vals1 + kMaxLeavesSort);  // 16 x kSortThreads
+  __shared__ uint32_t tmp[kSortThreads / 32 + 1];
+  __shared__ uint32_t total;
+  const int t = threadIdx.x;
+  const float B = __int_as_float((int)ld_volatile(bound));
+  const int approx = *approx_leaf;
+  // 1. select (order preserving compaction)
+  const int per = (nleaves + kSortThreads - 1) / kSortThreads;
+  const int b0 = min(nleaves, t * per), b1 = min(nleaves, b0 + per);
+  uint32_t mine = 0;
+  for (int i = b0; i < b1; ++i) {
+    const float l = lb[i];
+    if (leaf_size[i] > 0 && i != approx && !(l > B)) ++mine;
+  }
+  uint32_t pos = block_exclusive_scan<kSortThreads>(mine, tmp, &total);
+  const int n = (int)total;
+  for (int i = b0; i < b1; ++i) {
+    const float l = lb[i];
+    if (leaf_size[i] > 0 && i != approx && !(l > B)) {
+      keys0[pos] = (l == l) ? __float_as_uint(l) : 0u;  // NaN bound: never pruned, scanned first
+      vals0[pos] = (uint32_t)i;
+      ++pos;
+    }
+  }
+  __syncthreads();
+  // 2. radix sort, stable, each thread owning a contiguous run of keys
+  const int per2 = (n + kSortThreads - 1) / kSortThreads;
+  const int r0 = min(n, t * per2), r1 = min(n, r0 + per2);
+  uint32_t *ki = keys0, *vi = vals0, *ko = keys1, *vo = vals1;
+  for (int pass = 0; pass < 8; ++pass) {
+    const int shift = pass * 4;
+    uint32_t c[16];
+#pragma unroll
+    for (int d = 0; d < 16; ++d) c[d] = 0;
+    for (int i = r0; i < r1; ++i) ++c[(ki[i] >> shift) & 15];
+    // flattened digit-major counts: index d * kSortThreads + t; scan them in
+    // that order (thread t owns the 16 entries t*16 .. t*16+15 of the flat array)
+#pragma unroll
+    for (int d = 0; d < 16; ++d) cnt[d * kSortThreads + t] = (uint16_t)c[d];
+    __syncthreads();
+    uint32_t s = 0;
+    uint32_t loc[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      loc[j] = s;
+      s += cnt[t * 16 + j];
+    }
+    const uint32_t base = block_exclusive_scan<kSortThreads>(s, tmp, nullptr);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) cnt[t * 16 + j] = (uint16_t)(base + loc[j]);
+    __syncthreads();
+    uint32_t off[16];
+#pragma unroll
+    for (int d = 0; d < 16; ++d) off[d] = cnt[d * kSortThreads + t];
+    for (int i = r0; i < r1; ++i) {
+      const int d = (ki[i] >> shift) & 15;
+      const uint32_t p = off[d]++;
+      ko[p] = ki[i];
+      vo[p] = vi[i];
+    }
+    __syncthreads();
+    uint32_t* x = ki;
+    ki = ko;
+    ko = x;
+    x = vi;
+    vi = vo;
+    vo = x;
+  }
+  // 3. outputs and tile prefix
+  uint32_t tiles = 0;
+  for (int i = r0; i < r1; ++i) {
+    const int leaf = (int)vi[i];
+    cand[i] = leaf;
+    cand_lb[i] = __uint_as_float(ki[i]);
+    tiles += tiles_of_leaf(leaf_start[leaf], leaf_size[leaf]);
+  }
+  uint32_t tp = block_exclusive_scan<kSortThreads>(tiles, tmp, &total);
+  for (int i = r0; i < r1; ++i) {
+    const int leaf = (int)vi[i];
+    unit_prefix[i] = tp;
+    tp += tiles_of_leaf(leaf_start[leaf], leaf_size[leaf]);
+  }
+  if (t == 0) {
+    unit_prefix[n] = total;
+    *cand_count = n;
+  }
+}
+
+__global__ void k_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
+                             int* topk_count) {
+  if (threadIdx.x == 0) {
+    *cand_count = 1;
+    unit_prefix[0] = 0;
+    unit_prefix[1] = (uint32_t)((nrows + 31) >> 5);
+    *bound = 0x7f800000u;
+    *topk_count = 0;
+  }
+}
+
+// --- warp candidate list -----------------------------------------------------
+// A warp keeps its candidates as 64-bit keys (distance bits << 32 | id) in a
+// shared buffer of kWarpListCap entries.  Compaction sorts the buffer
+// (bitonic), keeps the first entry of each distinct distance (the lowest id,
+// the tie rule) and the k smallest distances.
+
+__device__ void warp_sort(unsigned long long* a, int n) {
+  const int lane = threadIdx.x & 31;
+  for (int size = 2; size <= n; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = lane; i < (n >> 1); i += 32) {
+        const int pos = 2 * i - (i & (stride - 1));
+        const int partner = pos + stride;
+        const bool asc = (pos & size) == 0;
+        const unsigned long long x = a[pos], y = a[partner];
+        if ((x > y) == asc) {
+          a[pos] = y;
+          a[partner] = x;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Sorts list[0..cnt), dedups by distance, keeps at most k; returns the new
+// count (warp-uniform).  Entries beyond cnt must be ~0ull on entry.
+__device__ int warp_compact(unsigned long long* list, int cnt, int k) {
+  const int lane = threadIdx.x & 31;
+  int n = 32;
+  while (n < cnt) n <<= 1;
+  warp_sort(list, n);
+  int out = 0;
+  uint32_t prev_d = 0xffffffffu;
+  bool have_prev = false;
+  for (int base = 0; base < cnt && out < k; base += 32) {
+    const int i = base + lane;
+    const unsigned long long v = i < cnt ? list[i] : ~0ull;
+    const uint32_t d = (uint32_t)(v >> 32);
+    uint32_t dprev = __shfl_up_sync(HG_FULL, d, 1);
+    if (lane == 0) dprev = have_prev ? prev_d : ~d;
+    const bool keep = i < cnt && d != dprev;
+    const uint32_t m = __ballot_sync(HG_FULL, keep);
+    const int r = __popc(m & ((1u << lane) - 1));
+    __syncwarp();
+    if (keep && out + r < k) list[out + r] = v;
+    prev_d = __shfl_sync(HG_FULL, d, 31);
+    have_prev = true;
+    out = min(k, out + __popc(m));
+    __syncwarp();
+  }
+  for (int i = out + lane; i < kWarpListCap; i += 32) list[i] = ~0ull;
+  __syncwarp();
+  return out;
+}
+
+// The leaf scan: every warp takes 32-row tiles of the candidate leaves in
+// LB order (grid-stride), computes each row's reference-order squared
+// distance chunk by chunk and abandons a row as soon as its partial sum
+// exceeds the running k-th bound.  Finished rows within the bound enter the
+// warp's list; whenever the list holds k distances its k-th lowers the
+// global bound (atomicMin on the float bits).
+__global__ void __launch_bounds__(kScanThreads, 4) k_scan(ScanArgs a) {
+  __shared__ unsigned long long lists[kScanWarps][kWarpListCap];
+  __shared__ float sbp[256];
+  __shared__ float spaa[16];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  unsigned long long* list = lists[wib];
+  for (int i = lane; i < kWarpListCap; i += 32) list[i] = ~0ull;
+  if (a.use_lbsax) {
+    for (int i = threadIdx.x; i < 255; i += blockDim.x) sbp[i] = a.bp[i];
+    if (threadIdx.x < 16) spaa[threadIdx.x] = a.paa[threadIdx.x];
+  }
+  __syncthreads();
+  const int nch = a.L >> 3;
+  const int ncand = *a.cand_count;
+  const uint32_t total = a.unit_prefix[ncand];
+  const uint32_t nwarps = gridDim.x * kScanWarps;
+  const uint32_t gw = blockIdx.x * kScanWarps + wib;
+  // this lane's query chunk is re-read from L1 each iteration
+  const float* q = a.q;
+  int cnt = 0;
+  float T = __int_as_float(0x7f800000);  // the warp's own k-th (when full)
+  unsigned long long n_rows = 0, n_chunks = 0, n_pruned = 0, n_leaves = 0;
+  int c = 0;
+  for (uint32_t unit = gw; unit < total; unit += nwarps) {
+    uint64_t lstart;
+    uint32_t lsize;
+    float lbv;
+    uint32_t tile_in;
+    if (a.pscan) {
+      lstart = 0;
+      lsize = (uint32_t)(a.nrows < 0xffffffffull ? a.nrows : 0xffffffffull);
+      lbv = 0.0f;
+      tile_in = unit;
+    } else {
+      // candidate index: largest c with unit_prefix[c] <= unit (c only grows)
+      int lo = c, hi = ncand - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.unit_prefix[mid] <= unit) lo = mid;
+        else hi = mid - 1;
+      }
+      c = lo;
+      const int leaf = a.cand[c];
+      lstart = a.leaf_start[leaf];
+      lsize = a.leaf_size[leaf];
+      lbv = a.cand_lb[c];
+      tile_in = unit - a.unit_prefix[c];
+    }
+    float B = fminf(T, __int_as_float((int)ld_volatile(a.bound)));
+    if (lbv > B) break;  // candidates are in ascending LB order
+    if (tile_in == 0) ++n_leaves;
+    const uint64_t row = (((lstart >> 5) + tile_in) << 5) + lane;
+    bool alive = row >= lstart && row < lstart + lsize && row < a.nrows;
+    if (alive) ++n_rows;
+    if (a.use_lbsax && alive) {
+      const uint4 w = reinterpret_cast<const uint4*>(a.sax)[row];
+      const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+      float d[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) d[j] = hg_lb_sax_lane(spaa[j], (ws[j >> 2] >> ((j & 3) * 8)) & 255, sbp);
+      float s8[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) s8[j] = __fadd_rn(d[j], d[j + 8]);
+      const float lbs = __fmul_rn(hg_hsum8(s8[0], s8[1], s8[2], s8[3], s8[4], s8[5], s8[6], s8[7]),
+                                  (float)(a.L / HG_PAA_SEGMENTS));
+      // LB_SAX is a lower bound of the exact distance; the margin covers the
+      // float rounding of both sides so no true neighbour is skipped.
+      if (lbs > __fadd_rn(__fmul_rn(B, 1.0009765625f), 1e-6f)) {
+        alive = false;
+        ++n_pruned;
+      }
+    }
+    float dist = 0.0f;
+    int ch = 0;
+    const float* base = a.rows + tile_off(row, 0, nch);
+    while (__any_sync(HG_FULL, alive) && ch < nch) {
+      float4 x0 = make_float4(0.f, 0.f, 0.f, 0.f), x1 = x0, y0 = x0, y1 = x0;
+      const bool two = ch + 1 < nch;
+      if (alive) {
+        const float4* p = reinterpret_cast<const float4*>(base + ((uint64_t)ch << 8));
+        x0 = __ldcs(p);
+        x1 = __ldcs(p + 1);
+        if (two) {
+          y0 = __ldcs(p + 64);
+          y1 = __ldcs(p + 65);
+        }
+      }
+      if (alive) {
+        const float4 q0 = *reinterpret_cast<const float4*>(q + ch * 8);
+        const float4 q1 = *reinterpret_cast<const float4*>(q + ch * 8 + 4);
+        const float qa[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+        const float xa[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+        dist = __fadd_rn(dist, hg_chunk_d2(qa, xa));
+        ++n_chunks;
+        if (dist > B) alive = false;
+      }
+      if (alive && two) {
+        const float4 q0 = *reinterpret_cast<const float4*>(q + ch * 8 + 8);
+        const float4 q1 = *reinterpret_cast<const float4*>(q + ch * 8 + 12);
+        const float qa[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+        const float ya[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+        dist = __fadd_rn(dist, hg_chunk_d2(qa, ya));
+        ++n_chunks;
+        if (dist > B) alive = false;
+      }
+      ch += 2;
+      if ((ch & 15) == 0) B = fminf(T, __int_as_float((int)ld_volatile(a.bound)));
+    }
+    // rows still alive completed every chunk: dist is the full distance.
+    // The list holds at most k entries between tiles (it is compacted as
+    // soon as it reaches k), so up to 32 new entries always fit.
+    const bool take = alive && dist <= B && dist <= T;
+    const uint32_t m = __ballot_sync(HG_FULL, take);
+    if (m) {
+      if (take) {
+        const int r = __popc(m & ((1u << lane) - 1));
+        const uint32_t id = (uint32_t)a.ids[row];
+        list[cnt + r] = ((unsigned long long)__float_as_uint(dist) << 32) | id;
+      }
+      cnt += __popc(m);
+      __syncwarp();
+      if (cnt >= a.k) {
+        cnt = warp_compact(list, cnt, a.k);
+        if (cnt == a.k) {
+          const float nt = __uint_as_float((uint32_t)(list[a.k - 1] >> 32));
+          if (nt < T) {
+            T = nt;
+            if (lane == 0) atomicMin(a.bound, __float_as_uint(T));
+          }
+        }
+      }
+    }
+  }
+  cnt = warp_compact(list, cnt, a.k);
+  if (cnt == a.k && lane == 0) atomicMin(a.bound, (uint32_t)(list[a.k - 1] >> 32));
+  unsigned long long* out = a.parts + (uint64_t)gw * kWarpListCap;
+  for (int i = lane; i < cnt; i += 32) out[i] = list[i];
+  if (lane == 0) {
+    a.part_count[gw] = cnt;
+    atomicAdd(&a.stats[0], n_rows);
+    atomicAdd(&a.stats[3], n_leaves);
+  }
+  // per-lane counters
+  atomicAdd(&a.stats[1], n_chunks);
+  atomicAdd(&a.stats[2], n_pruned);
+}
+
+// Merges the per-warp lists (and the current top-k, passed as part -1) into
+// the k smallest distinct distances, lowest id per distance.  Only entries
+// <= the final bound can belong to the answer.
+constexpr int kMergeThreads = 1024;
+__global__ void __launch_bounds__(kMergeThreads) k_merge(const unsigned long long* __restrict__ parts,
+                                                         const int* __restrict__ part_count, int nparts, int k,
+                                                         unsigned long long* topk, int* topk_count,
+                                                         uint32_t* bound, int* err) {
+  extern __shared__ unsigned long long buf[];  // kMergeCap
+  __shared__ unsigned long long best[kMaxK];
+  __shared__ uint32_t tmp[kMergeThreads / 32 + 1];
+  __shared__ uint32_t total;
+  __shared__ int nbest;
+  const int t = threadIdx.x;
+  const uint32_t B = ld_volatile(bound);
+  // previous top-k
+  if (t == 0) nbest = *topk_count;
+  __syncthreads();
+  for (int i = t; i < kMaxK; i += kMergeThreads) best[i] = (i < nbest) ? topk[i] : ~0ull;
+  __syncthreads();
+  // count entries <= B per part (lists are sorted ascending)
+  const int per = (nparts + kMergeThreads - 1) / kMergeThreads;
+  const int p0 = min(nparts, t * per), p1 = min(nparts, p0 + per);
+  uint32_t mine = 0;
+  for (int p = p0; p < p1; ++p) {
+    const unsigned long long* l = parts + (uint64_t)p * kWarpListCap;
+    int lo = 0, hi = part_count[p];
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if ((uint32_t)(l[mid] >> 32) <= B) lo = mid + 1;
+      else hi = mid;
+    }
+    mine += lo;
+  }
+  const uint32_t start = block_exclusive_scan<kMergeThreads>(mine, tmp, &total);
+  const uint32_t M = total;
+  const int room = kMergeCap - k;
+  for (uint32_t r0 = 0; r0 < M || r0 == 0; r0 += room) {
+    // this round takes global positions [r0, r0 + room) after the current best
+    const uint32_t rem = M > r0 ? M - r0 : 0u;
+    const uint32_t m = rem < (uint32_t)room ? rem : (uint32_t)room;
+    int nsort = 32;
+    while (nsort < k + (int)m) nsort <<= 1;
+    for (int i = t; i < nsort; i += kMergeThreads) buf[i] = (i < k) ? best[i] : ~0ull;
+    __syncthreads();
+    uint32_t g = start;
+    for (int p = p0; p < p1; ++p) {
+      const unsigned long long* l = parts + (uint64_t)p * kWarpListCap;
+      const int cntp = part_count[p];
+      for (int j = 0; j < cntp; ++j) {
+        const unsigned long long v = l[j];
+        if ((uint32_t)(v >> 32) > B) break;
+        if (g >= r0 && g < r0 + room) buf[k + (g - r0)] = v;
+        ++g;
+      }
+    }
+    __syncthreads();
+    // bitonic sort of nsort keys
+    for (int size = 2; size <= nsort; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int i = t; i < nsort / 2; i += kMergeThreads) {
+          const int pos = 2 * i - (i & (stride - 1));
+          const int partner = pos + stride;
+          const bool asc = (pos & size) == 0;
+          const unsigned long long x = buf[pos], y = buf[partner];
+          if ((x > y) == asc) {
+            buf[pos] = y;
+            buf[partner] = x;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // dedup by distance, keep k (thread 0; at most kMergeCap steps, exits at k)
+    if (t == 0) {
+      int out = 0;
+      uint32_t prev = 0;
+      for (int i = 0; i < nsort && out < k; ++i) {
+        const unsigned long long v = buf[i];
+        if (v == ~0ull) break;
+        const uint32_t d = (uint32_t)(v >> 32);
+        if (out > 0 && d == prev) continue;
+        best[out++] = v;
+        prev = d;
+      }
+      for (int i = out; i < kMaxK; ++i) best[i] = ~0ull;
+      nbest = out;
+    }
+    __syncthreads();
+    if (M == 0) break;
+  }
+  for (int i = t; i < k; i += kMergeThreads) topk[i] = best[i];
+  if (t == 0) {
+    *topk_count = nbest;
+    if (nbest == k) atomicMin(bound, (uint32_t)(best[k - 1] >> 32));
+    (void)err;
+  }
+}
+
+__global__ void k_emit(const unsigned long long* topk, const int* topk_count, int k, float* dist_out,
+                       int64_t* id_out) {
+  const int i = threadIdx.x + blockIdx.x * blockDim.x;
+  if (i >= k) return;
+  const int n = *topk_count;
+  if (i < n) {
+    const unsigned long long v = topk[i];
+    if (dist_out) dist_out[i] = __uint_as_float((uint32_t)(v >> 32));
+    if (id_out) id_out[i] = (int64_t)(uint32_t)v;
+  } else {
+    if (dist_out) dist_out[i] = __int_as_float(0x7f800000);
+    if (id_out) id_out[i] = -1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// data generation
+// ---------------------------------------------------------------------------
+
+__global__ void k_generate_walks(uint64_t seed, uint64_t first, uint64_t n, int L, float* out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  // each thread writes its own row; the L2 merges the partial sectors
+  random_walk(seed, first + i, L, out + i * (uint64_t)L);
+}
+
+__global__ void k_generate_queries(uint64_t seed, const float* data, uint64_t n, int L, int nq,
+                                   const double* sigma2, float* out, uint64_t* base_ids) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nq) return;
+  const uint64_t b = pick_row(seed, (uint64_t)j, n);
+  if (base_ids) base_ids[j] = b;
+  noisy_query(seed, (uint64_t)j, data + b * (uint64_t)L, L, sigma2[j], out + (uint64_t)j * L);
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+static inline unsigned blocks_for(uint64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+int scan_grid_blocks(int device) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  return sms * 4;
+}
+
+cudaError_t launch_route_rows(const float* X, int L, const uint32_t* rows, uint64_t first, uint32_t count,
+                              Tree t, int* leaf_out, cudaStream_t s) {
+  if (!count) return cudaSuccess;
+  k_route_rows<<<blocks_for(count, 128), 128, 0, s>>>(X, L, rows, first, count, t, leaf_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sketch_members(const float* X, int L, const uint32_t* members, uint32_t count,
+                                  const short* seg_from, const short* seg_to, int nsegs, int* keys_out,
+                                  cudaStream_t s) {
+  if (!count || !nsegs) return cudaSuccess;
+  unsigned b = blocks_for(count, 256);
+  if (b > 148 * 8) b = 148 * 8;
+  k_sketch_members<<<b, 256, sizeof(int) * 4 * nsegs, s>>>(X, L, members, count, seg_from, seg_to, nsegs,
+                                                           keys_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_route_flags(const float* X, int L, const uint32_t* members, uint32_t count, short from,
+                               short to, int idx, float value, uint8_t* flags, cudaStream_t s) {
+  if (!count) return cudaSuccess;
+  k_route_flags<<<blocks_for(count, 256), 256, 0, s>>>(X, L, members, count, from, to, idx, value, flags);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_tiles(const float* X, int L, const uint32_t* perm, uint64_t n, float* tiles,
+                                cudaStream_t s) {
+  const uint64_t ntiles = (n + 31) / 32;
+  const uint64_t threads = ntiles * 32 * (L / 8);
+  if (!threads) return cudaSuccess;
+  k_gather_tiles<<<blocks_for(threads, 256), 256, 0, s>>>(X, L, perm, n, tiles);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tiles_from_rowmajor(const float* rm, int L, uint64_t first, uint64_t count, float* tiles,
+                                       cudaStream_t s) {
+  const uint64_t threads = (count + 31) / 32 * 32 * (L / 8);
+  if (!threads) return cudaSuccess;
+  k_tiles_from_rowmajor<<<blocks_for(threads, 256), 256, 0, s>>>(rm, L, first, count, tiles);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rowmajor_from_tiles(const float* tiles, int L, uint64_t first, uint64_t count, float* rm,
+                                       cudaStream_t s) {
+  const uint64_t threads = count * (L / 8);
+  if (!threads) return cudaSuccess;
+  k_rowmajor_from_tiles<<<blocks_for(threads, 256), 256, 0, s>>>(tiles, L, first, count, rm);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sax_rows(const float* tiles, int L, uint64_t n, const float* bp, uint8_t* sax,
+                            cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  k_sax_rows<<<blocks_for(n, 128), 128, 0, s>>>(tiles, L, n, bp, sax);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_query_prep(const float* q, int L, Tree t, const uint64_t* leaf_start,
+                              const uint32_t* leaf_size, int* approx_leaf, float* paa, int* cand,
+                              float* cand_lb, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
+                              int* topk_count, cudaStream_t s) {
+  k_query_prep<<<1, 32, 0, s>>>(q, L, t, leaf_start, leaf_size, approx_leaf, paa, cand, cand_lb, cand_count,
+                                unit_prefix, bound, topk_count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_route_queries(const float* Q, int nq, int L, Tree t, int* leaf_out, cudaStream_t s) {
+  if (!nq) return cudaSuccess;
+  k_route_queries<<<blocks_for((uint64_t)nq * 32, 128), 128, 0, s>>>(Q, nq, L, t, leaf_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_leaf_lb(const float* q, int L, int nleaves, const int* seg_off, const short* points,
+                           const float* sk, float* lb_out, cudaStream_t s) {
+  if (!nleaves) return cudaSuccess;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_leaf_lb, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
+    attr = true;
+  }
+  k_leaf_lb<<<blocks_for((uint64_t)nleaves * 32, 256), 256, sizeof(float) * L, s>>>(q, L, nleaves, seg_off,
+                                                                                  points, sk, lb_out);
+  return cudaGetLastError();
+}
+
+static size_t select_smem() { return sizeof(uint32_t) * 4 * kMaxLeavesSort + sizeof(uint16_t) * 16 * kSortThreads; }
+
+cudaError_t launch_select_sort(const float* lb, int nleaves, const uint32_t* bound, const int* approx_leaf,
+                               const uint64_t* leaf_start, const uint32_t* leaf_size, int* cand,
+                               float* cand_lb, int* cand_count, uint32_t* unit_prefix, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_select_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)select_smem());
+    attr = true;
+  }
+  k_select_sort<<<1, kSortThreads, select_smem(), s>>>(lb, nleaves, bound, approx_leaf, leaf_start, leaf_size,
+                                                       cand, cand_lb, cand_count, unit_prefix);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
+                              int* topk_count, cudaStream_t s) {
+  k_pscan_prep<<<1, 32, 0, s>>>(nrows, cand_count, unit_prefix, bound, topk_count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scan(const ScanArgs& a, int blocks, cudaStream_t s) {
+  k_scan<<<blocks, kScanThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_merge(const unsigned long long* parts, const int* part_count, int nparts, int k,
+                         unsigned long long* topk, int* topk_count, uint32_t* bound, int* err,
+                         cudaStream_t s) {
+  static bool attr = false;
+  const int smem = sizeof(unsigned long long) * kMergeCap;
+  if (!attr) {
+    cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr = true;
+  }
+  k_merge<<<1, kMergeThreads, smem, s>>>(parts, part_count, nparts, k, topk, topk_count, bound, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_emit(const unsigned long long* topk, const int* topk_count, int k, float* dist_out,
+                        int64_t* id_out, cudaStream_t s) {
+  k_emit<<<blocks_for(k, 128), 128, 0, s>>>(topk, topk_count, k, dist_out, id_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_generate_walks(uint64_t seed, uint64_t first, uint64_t n, int L, float* out,
+                                  cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  k_generate_walks<<<blocks_for(n, 128), 128, 0, s>>>(seed, first, n, L, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_generate_queries(uint64_t seed, const float* data, uint64_t n, int L, int nq,
+                                    const double* sigma2, float* out, uint64_t* base_ids, cudaStream_t s) {
+  if (!nq) return cudaSuccess;
+  k_generate_queries<<<blocks_for(nq, 64), 64, 0, s>>>(seed, data, n, L, nq, sigma2, out, base_ids);
+  return cudaGetLastError();
+}
+
+}  // namespace hg

@@ -1,0 +1,101 @@
+// hg_kernels.h -- launchers of the sm_100a kernels (host side declarations).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hg {
+
+// scan block geometry: 8 warps, one 32-row tile per warp iteration
+constexpr int kScanWarps = 8;
+constexpr int kScanThreads = kScanWarps * 32;
+constexpr int kWarpListCap = 256;  // per-warp candidate buffer (k <= kWarpListCap - 32)
+constexpr int kMaxK = kWarpListCap - 32;
+constexpr int kMaxLeavesSort = 8192;  // single-CTA radix sort capacity
+constexpr int kMergeCap = 8192;       // single-CTA bitonic merge capacity
+
+// A routing node of the EAPCA tree: an internal node's split policy
+// (hercules_node_split.h:21-34) and its children; a child < 0 is the leaf ~child.
+struct DNode {
+  int left, right;
+  float value;
+  short from, to;
+  int idx;
+  int pad;
+};
+
+struct Tree {
+  const DNode* nodes;
+  int root;  // >= 0 internal node, < 0 the leaf ~root
+};
+
+struct ScanArgs {
+  const float* rows;  // chunk-interleaved tiles
+  const int64_t* ids;
+  const uint8_t* sax;
+  const float* bp;
+  int L;
+  uint64_t nrows;
+  const uint64_t* leaf_start;
+  const uint32_t* leaf_size;
+  const int* cand;
+  const float* cand_lb;
+  const int* cand_count;
+  const uint32_t* unit_prefix;  // exclusive prefix of tiles per candidate, [cand_count] = total
+  int pscan;                    // 1: every tile of the whole matrix, no leaves
+  const float* q;
+  const float* paa;
+  int use_lbsax;
+  int k;
+  uint32_t* bound;  // float bits of the running k-th bound (atomicMin)
+  unsigned long long* parts;  // per-warp sorted lists (kWarpListCap stride)
+  int* part_count;
+  unsigned long long* stats;  // [0] rows visited [1] chunks loaded [2] lbsax pruned [3] leaves scanned
+};
+
+int scan_grid_blocks(int device);
+
+// build
+cudaError_t launch_route_rows(const float* X, int L, const uint32_t* rows, uint64_t first, uint32_t count,
+                              Tree t, int* leaf_out, cudaStream_t s);
+cudaError_t launch_sketch_members(const float* X, int L, const uint32_t* members, uint32_t count,
+                                  const short* seg_from, const short* seg_to, int nsegs, int* keys_out,
+                                  cudaStream_t s);
+cudaError_t launch_route_flags(const float* X, int L, const uint32_t* members, uint32_t count, short from,
+                               short to, int idx, float value, uint8_t* flags, cudaStream_t s);
+cudaError_t launch_gather_tiles(const float* X, int L, const uint32_t* perm, uint64_t n, float* tiles,
+                                cudaStream_t s);
+cudaError_t launch_tiles_from_rowmajor(const float* rm, int L, uint64_t first, uint64_t count, float* tiles,
+                                       cudaStream_t s);
+cudaError_t launch_rowmajor_from_tiles(const float* tiles, int L, uint64_t first, uint64_t count, float* rm,
+                                       cudaStream_t s);
+cudaError_t launch_sax_rows(const float* tiles, int L, uint64_t n, const float* bp, uint8_t* sax,
+                            cudaStream_t s);
+
+// queries
+cudaError_t launch_query_prep(const float* q, int L, Tree t, const uint64_t* leaf_start,
+                              const uint32_t* leaf_size, int* approx_leaf, float* paa, int* cand,
+                              float* cand_lb, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
+                              int* topk_count, cudaStream_t s);
+cudaError_t launch_route_queries(const float* Q, int nq, int L, Tree t, int* leaf_out, cudaStream_t s);
+cudaError_t launch_leaf_lb(const float* q, int L, int nleaves, const int* seg_off, const short* points,
+                           const float* sk, float* lb_out, cudaStream_t s);
+cudaError_t launch_select_sort(const float* lb, int nleaves, const uint32_t* bound, const int* approx_leaf,
+                               const uint64_t* leaf_start, const uint32_t* leaf_size, int* cand,
+                               float* cand_lb, int* cand_count, uint32_t* unit_prefix, cudaStream_t s);
+cudaError_t launch_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
+                              int* topk_count, cudaStream_t s);
+cudaError_t launch_scan(const ScanArgs& a, int blocks, cudaStream_t s);
+cudaError_t launch_merge(const unsigned long long* parts, const int* part_count, int nparts, int k,
+                         unsigned long long* topk, int* topk_count, uint32_t* bound, int* err,
+                         cudaStream_t s);
+cudaError_t launch_emit(const unsigned long long* topk, const int* topk_count, int k, float* dist_out,
+                        int64_t* id_out, cudaStream_t s);
+
+// data
+cudaError_t launch_generate_walks(uint64_t seed, uint64_t first, uint64_t n, int L, float* out,
+                                  cudaStream_t s);
+cudaError_t launch_generate_queries(uint64_t seed, const float* data, uint64_t n, int L, int nq,
+                                    const double* sigma2, float* out, uint64_t* base_ids, cudaStream_t s);
+
+}  // namespace hg

@@ -1,0 +1,190 @@
+/*
+ * hercules_gpu.h -- C ABI of the B200-native Hercules exact k-NN path.
+ *
+ * libhercules_gpu.so replaces the exact k-NN query path of the Hercules C
+ * library (karimaechihabi/hercules, code/hercules) with sm_100a kernels and
+ * keeps its index format and semantics.  Each entry point names the
+ * reference interface it replaces.  Plain C types and pointers only; every
+ * call returns an hg_status and never exits the process; every device wait
+ * is bounded.  A handle owns one CUDA stream and is not re-entrant: calls on
+ * one handle must not overlap (the reference's query entry is not
+ * re-entrant either, hercules_query_engine.c mutates index->stats).
+ *
+ * Conventions
+ *   - series are float32 rows of length L (L a multiple of 16);
+ *   - distances are squared Euclidean distances in float32, computed in the
+ *     reference's summation order (ts_euclidean_distance_SIMD, ts.c:83-109);
+ *   - a result list holds the k smallest DISTINCT distances; for each the
+ *     row with the lowest dataset id among rows at exactly that distance;
+ *     missing entries (fewer than k rows) have distance +inf and id -1.
+ */
+#ifndef HERCULES_GPU_H
+#define HERCULES_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HG_API __attribute__((visibility("default")))
+#else
+#define HG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int hg_status;
+#define HG_OK 0
+#define HG_ERR_ARG (-1)      /* invalid argument */
+#define HG_ERR_IO (-2)       /* file missing, short read or write */
+#define HG_ERR_FORMAT (-3)   /* root.idx not in the reference's format */
+#define HG_ERR_CUDA (-4)     /* CUDA runtime error (no device, launch failure) */
+#define HG_ERR_NOMEM (-5)    /* host or device allocation failed */
+#define HG_ERR_TIMEOUT (-6)  /* a bounded device wait gave up */
+#define HG_ERR_LIMIT (-7)    /* a size beyond a documented limit */
+
+typedef struct hg_index hg_index;
+
+/* Index-wide facts (hercules_index_settings, hercules_index.h). */
+typedef struct {
+  uint64_t num_series;    /* dataset size */
+  uint32_t ts_length;     /* timeseries_size */
+  uint32_t leaf_size;     /* max_leaf_size */
+  uint32_t num_leaves;    /* leaf_nodes_count */
+  uint32_t num_nodes;     /* total nodes */
+  uint32_t max_segments;  /* most EAPCA segments in any leaf */
+  uint32_t has_ids;       /* 1 when row -> dataset id is known */
+  uint64_t device_bytes;  /* HBM held by the index */
+} hg_index_info;
+
+/* Per-call query counters (the Query_* TSV fields of print_query_stats,
+ * hercules_query_engine.c:3558-3918, that this path defines). */
+typedef struct {
+  uint64_t queries;
+  uint64_t leaves_scanned;    /* Query_total_loaded_nodes_count, summed */
+  uint64_t rows_visited;      /* rows whose distance computation started */
+  uint64_t rows_lbsax_pruned; /* rows skipped by the per-row LB_SAX bound */
+  uint64_t chunks_loaded;     /* 32-byte chunks of raw data read by the scan */
+  uint64_t candidate_leaves;  /* leaves with LB_EAPCA <= k-th bound */
+  double device_ms;           /* device time of the call (CUDA events) */
+} hg_query_stats;
+
+/* Search mode. */
+#define HG_MODE_PLAIN 0    /* exact_de_knn_search per query */
+#define HG_MODE_PSCAN 1    /* parallel scan of every row (code/pscan) */
+
+typedef struct {
+  int mode;           /* HG_MODE_* */
+  int use_lb_sax;     /* 1: per-row LB_SAX filter before the distance */
+  int reserved[6];
+} hg_knn_opts;
+
+/* ---- status ----------------------------------------------------------- */
+
+/* Text for a status code. */
+HG_API const char *hg_status_string(hg_status s);
+
+/* Text of the last CUDA/runtime error seen on this thread. */
+HG_API const char *hg_last_error(void);
+
+/* ---- index construction ----------------------------------------------- */
+
+/* Builds the index from a raw float32 file of at least n series of length L.
+ * Replaces hercules_index_settings_init + hercules_index_init +
+ * hercules_root_node_init + hercules_index_build
+ * (hercules.c:355-420, hercules_index.c:32-153, 2354-2634) run with one
+ * insert worker: the EAPCA tree, leaf order and envelopes are those of the
+ * reference.  Routing, envelopes and iSAX words run on `device`. */
+HG_API hg_status hg_index_build_file(const char *dataset, uint64_t n, uint32_t L, uint32_t leaf_size,
+                              int device, hg_index **out);
+
+/* Same from memory.  data is n x L row-major float32; data_on_device = 1
+ * when it already lives on `device` (it is not freed and may be released
+ * after the call). */
+HG_API hg_status hg_index_build(const float *data, int data_on_device, uint64_t n, uint32_t L,
+                         uint32_t leaf_size, int device, hg_index **out);
+
+/* Writes root.idx, leaves_raw.idx and leaves_sims.idx into dir (which must
+ * end with '/') in the reference's format (hercules_index_write_sequential,
+ * hercules_index.c:1611-1692, 1967-2077), plus leaves_ids.idx (u64 dataset
+ * id per row, ignored by the reference).  buffer_mb is recorded in the
+ * header like --buffer-size. */
+HG_API hg_status hg_index_write(hg_index *ix, const char *dir, double buffer_mb);
+
+/* Loads an index written by the reference or by hg_index_write and makes
+ * it resident on `device` (hercules_index_read, hercules_index.c:1793-1905;
+ * leaves_raw.idx replaces the per-leaf fread of get_all_time_series_in_node).
+ * Without leaves_ids.idx the dataset id of a row is its leaves_raw.idx row. */
+HG_API hg_status hg_index_read(const char *dir, int device, hg_index **out);
+
+/* Frees host and device memory (hercules_index_destroy, hercules_index.c:1056). */
+HG_API void hg_index_destroy(hg_index *ix);
+
+HG_API hg_status hg_index_info_get(const hg_index *ix, hg_index_info *info);
+
+/* Leaf i (DFS order): first row (file_pos), size and EAPCA segment count. */
+HG_API hg_status hg_index_leaf(const hg_index *ix, uint32_t i, uint64_t *file_pos, uint32_t *size,
+                        uint32_t *num_segments);
+
+/* Copies leaf i's segment ends (short[num_segments]) and envelopes
+ * (float[4*num_segments]: mean max, mean min, stdev max, stdev min). */
+HG_API hg_status hg_index_leaf_envelope(const hg_index *ix, uint32_t i, short *points, float *envelope);
+
+/* Copies the dataset id of every leaf-ordered row (int64[num_series]). */
+HG_API hg_status hg_index_row_ids(const hg_index *ix, int64_t *ids);
+
+/* Copies rows [first, first+count) of the leaf-ordered data (row-major) and
+ * their iSAX words (uint8[count*16]); either output may be NULL. */
+HG_API hg_status hg_index_rows(const hg_index *ix, uint64_t first, uint64_t count, float *rows,
+                        uint8_t *sax);
+
+/* ---- queries ---------------------------------------------------------- */
+
+/* Exact k-NN for nq queries (row-major nq x L, HOST memory).  Replaces
+ * exact_de_knn_search (hercules_query_engine.c:2215-2448) as called per
+ * query by hercules_knn_query_binary_file (hercules_file_loaders.c:99-294).
+ * Outputs nq x k squared distances (ascending), dataset ids and the
+ * file_pos of each answer's leaf (Query_exact_node_file_pos).  Any output
+ * pointer may be NULL.  stats may be NULL. */
+HG_API hg_status hg_knn(hg_index *ix, const float *queries, uint32_t nq, uint32_t k,
+                 const hg_knn_opts *opts, float *dist_out, int64_t *id_out,
+                 uint64_t *leaf_pos_out, hg_query_stats *stats);
+
+/* Same with every buffer in device memory of the index's device, ordered
+ * on `stream` (a cudaStream_t, NULL = the handle's stream). */
+HG_API hg_status hg_knn_device(hg_index *ix, const float *d_queries, uint32_t nq, uint32_t k,
+                        const hg_knn_opts *opts, float *d_dist_out, int64_t *d_id_out,
+                        void *stream, hg_query_stats *stats);
+
+/* The approximate leaf of each query: the leaf the query routes to
+ * (approximate_knn_search's traversal, hercules_query_engine.c:176-222). */
+HG_API hg_status hg_route(hg_index *ix, const float *queries, uint32_t nq, int32_t *leaf_out);
+
+/* LB_EAPCA of one query against every leaf in DFS order
+ * (calculate_node_min_distance, hercules_node.c:879-924). */
+HG_API hg_status hg_leaf_lower_bounds(hg_index *ix, const float *query, float *lb_out);
+
+/* ---- data ------------------------------------------------------------- */
+
+/* Seeded z-normalised random walks: rows [first, first+n) of stream `seed`
+ * (tools/Cgenerator semantics, steps from Philox4x32-10 + Box-Muller).
+ * out_on_device = 1 writes device memory of `device`, else host memory
+ * (computed on the host CPU, same bits). */
+HG_API hg_status hg_generate_walks(uint64_t seed, uint64_t first, uint64_t n, uint32_t L, float *out,
+                            int out_on_device, int device);
+
+/* Noisy queries: query j = dataset row pick(j) plus N(0, sigma2[j]) noise,
+ * z-normalised.  data (n x L) and out (nq x L) are both host or both device
+ * memory.  base_ids (may be NULL) receives pick(j). */
+HG_API hg_status hg_generate_queries(uint64_t seed, const float *data, uint64_t n, uint32_t L,
+                              uint32_t nq, const double *sigma2, float *out, uint64_t *base_ids,
+                              int on_device, int device);
+
+/* The 255 iSAX breakpoints of cardinality 256 used by this library. */
+HG_API hg_status hg_sax_breakpoints(float *out255);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
