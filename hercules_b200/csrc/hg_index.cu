@@ -536,7 +536,9 @@ struct BuildCtx {
       CK(cudaStreamSynchronize(st));
       uint64_t next = c + w;
       for (uint32_t j = 0; j < w; ++j) {
-        const int nid = ~h_leaf_of[j];
+        const int nid = h_leaf_of[j];  // the kernel already decoded ~child
+        if (nid < 0 || (size_t)nid >= nodes.size() || !nodes[nid].is_leaf)
+          return set_error(HG_ERR_CUDA, "internal: routing returned a node that is not a leaf");
         Node& leaf = nodes[nid];
         leaf.members.push_back((uint32_t)(c + j));
         ++leaf.node_size;

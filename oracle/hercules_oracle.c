@@ -848,27 +848,37 @@ static int cmp_cand(const void *a, const void *b) {
   return x->n->file_pos < y->n->file_pos ? -1 : (x->n->file_pos > y->n->file_pos ? 1 : 0);
 }
 
+/* One leaf of the scan (hercules_query_engine.c:2391-2425).  The list keys
+ * are dataset ids (the tie rule compares them); aux carries the leaf-ordered
+ * row. */
 static void scan_leaf(const or_index *ix, const or_node *lf, const float *q, int k, int tie,
-                      float *dist, int64_t *row, uint64_t *fpos, int *cur, float *kth_var) {
+                      float *dist, int64_t *id, uint64_t *row, int *cur, float *kth_var) {
   for (unsigned m = 0; m < lf->node_size; ++m) {
     uint64_t r = lf->file_pos + m;
     float kth = dist[k - 1];
     *kth_var = kth;
-    if (tie) {
-      /* lowest-id rule: abandon only strictly above the bound */
-      float d = or_ed(q, ix->rows + r * ix->L, ix->L, kth);
-      if (d < kth) {
-        or_topk_insert(dist, row, fpos, cur, k, d, (int64_t)r, lf->file_pos, tie);
-      } else if (d == kth && *cur == k) {
-        /* a row whose partial sum reached exactly kth may still tie it */
-        float full = or_ed(q, ix->rows + r * ix->L, ix->L, FLT_MAX);
-        if (full == kth) or_topk_insert(dist, row, fpos, cur, k, full, (int64_t)r, lf->file_pos, tie);
-      }
-    } else {
-      float d = or_ed(q, ix->rows + r * ix->L, ix->L, kth);
-      if (d < kth) or_topk_insert(dist, row, fpos, cur, k, d, (int64_t)r, lf->file_pos, tie);
+    const float *x = ix->rows + r * ix->L;
+    float d = or_ed(q, x, ix->L, kth);
+    if (d < kth) {
+      or_topk_insert(dist, id, row, cur, k, d, ix->ids[r], r, tie);
+    } else if (tie && d == kth && *cur == k) {
+      /* lowest-id rule: a row whose partial sum reached exactly kth may
+       * still tie it */
+      float full = or_ed(q, x, ix->L, FLT_MAX);
+      if (full == kth) or_topk_insert(dist, id, row, cur, k, full, ix->ids[r], r, tie);
     }
   }
+}
+
+static uint64_t leaf_pos_of_row(const or_index *ix, uint64_t r) {
+  int lo = 0, hi = ix->num_leaves - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) / 2;
+    if (ix->leaves[mid]->file_pos <= r) lo = mid;
+    else hi = mid - 1;
+  }
+  while (lo > 0 && ix->leaves[lo]->node_size == 0) --lo;
+  return ix->leaves[lo]->file_pos;
 }
 
 /* hercules_query_engine.c:2215-2448 with epsilon = 0 and
@@ -877,12 +887,12 @@ int or_exact_knn(const or_index *ix, const float *q, int k, int tie_lowest, floa
                  int64_t *row_out, uint64_t *filepos_out, or_stats *st) {
   if (k <= 0 || !ix->root) return -1;
   float *dist = (float *)malloc(sizeof(float) * k);
-  int64_t *row = (int64_t *)malloc(sizeof(int64_t) * k);
-  uint64_t *fpos = (uint64_t *)malloc(sizeof(uint64_t) * k);
+  int64_t *id = (int64_t *)malloc(sizeof(int64_t) * k);
+  uint64_t *row = (uint64_t *)malloc(sizeof(uint64_t) * k);
   for (int i = 0; i < k; ++i) {
     dist[i] = FLT_MAX;
-    row[i] = -1;
-    fpos[i] = 0;
+    id[i] = -1;
+    row[i] = UINT64_MAX;
   }
   int cur = 0;
   or_stats s;
@@ -893,7 +903,7 @@ int or_exact_knn(const or_index *ix, const float *q, int k, int tie_lowest, floa
   or_node *n = ix->root;
   while (!n->is_leaf) n = route_left(n, q) ? n->left : n->right;
   const or_node *approx = n;
-  scan_leaf(ix, n, q, k, tie_lowest, dist, row, fpos, &cur, &kth_var);
+  scan_leaf(ix, n, q, k, tie_lowest, dist, id, row, &cur, &kth_var);
   s.loaded_leaves = 1;
   s.loaded_rows = n->node_size;
   s.approx_leaf = (uint32_t)n->leaf_index;
@@ -930,19 +940,19 @@ int or_exact_knn(const or_index *ix, const float *q, int k, int tie_lowest, floa
     if (cand[i].d <= kth_var) {
       s.loaded_leaves++;
       s.loaded_rows += cand[i].n->node_size;
-      scan_leaf(ix, cand[i].n, q, k, tie_lowest, dist, row, fpos, &cur, &kth_var);
+      scan_leaf(ix, cand[i].n, q, k, tie_lowest, dist, id, row, &cur, &kth_var);
     }
   }
   free(cand);
   for (int i = 0; i < k; ++i) {
     d_out[i] = dist[i];
-    if (row_out) row_out[i] = row[i];
-    if (filepos_out) filepos_out[i] = fpos[i];
+    if (row_out) row_out[i] = i < cur ? (int64_t)row[i] : -1;
+    if (filepos_out) filepos_out[i] = i < cur ? leaf_pos_of_row(ix, row[i]) : 0;
   }
   if (st) *st = s;
   free(dist);
+  free(id);
   free(row);
-  free(fpos);
   return cur;
 }
 
