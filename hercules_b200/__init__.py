@@ -44,14 +44,16 @@ class QueryStats(ctypes.Structure):
     _fields_ = [("queries", ctypes.c_uint64), ("leaves_scanned", ctypes.c_uint64),
                 ("rows_visited", ctypes.c_uint64), ("rows_lbsax_pruned", ctypes.c_uint64),
                 ("chunks_loaded", ctypes.c_uint64), ("candidate_leaves", ctypes.c_uint64),
-                ("device_ms", ctypes.c_double)]
+                ("device_ms", ctypes.c_double), ("rows_completed", ctypes.c_uint64),
+                ("scan_launches", ctypes.c_uint64), ("scan_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class KnnOpts(ctypes.Structure):
-    _fields_ = [("mode", ctypes.c_int), ("use_lb_sax", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+    _fields_ = [("mode", ctypes.c_int), ("use_lb_sax", ctypes.c_int), ("profile", ctypes.c_int),
+                ("reserved", ctypes.c_int * 5)]
 
 
 _lib = None
@@ -220,7 +222,8 @@ class HerculesIndex:
         return (rows, sax) if with_sax else rows
 
     # -- queries -------------------------------------------------------------
-    def knn(self, queries, k=1, mode=MODE_PLAIN, use_lb_sax=False, with_leaf_pos=False, stats=False):
+    def knn(self, queries, k=1, mode=MODE_PLAIN, use_lb_sax=False, with_leaf_pos=False, stats=False,
+            profile=False):
         """Exact k-NN (squared distances ascending, dataset ids)."""
         q = _f32(queries, self.L)
         nq = q.shape[0]
@@ -228,7 +231,7 @@ class HerculesIndex:
         ids = np.zeros((nq, k), dtype=np.int64)
         pos = np.zeros((nq, k), dtype=np.uint64) if with_leaf_pos else None
         st = QueryStats()
-        opts = KnnOpts(mode, 1 if use_lb_sax else 0)
+        opts = KnnOpts(mode, 1 if use_lb_sax else 0, 1 if profile else 0)
         _check(lib().hg_knn(self._h, _ptr(q), nq, k, ctypes.byref(opts), _ptr(d), _ptr(ids), _ptr(pos),
                             ctypes.byref(st)))
         out = [d, ids]
@@ -241,10 +244,11 @@ class HerculesIndex:
     def pscan(self, queries, k=1, stats=False):
         return self.knn(queries, k, mode=MODE_PSCAN, stats=stats)
 
-    def knn_device(self, q_ptr, nq, k, dist_ptr, id_ptr, stream=0, mode=MODE_PLAIN, use_lb_sax=False):
+    def knn_device(self, q_ptr, nq, k, dist_ptr, id_ptr, stream=0, mode=MODE_PLAIN, use_lb_sax=False,
+                   profile=False):
         """Device-resident variant; pointers are raw device addresses."""
         st = QueryStats()
-        opts = KnnOpts(mode, 1 if use_lb_sax else 0)
+        opts = KnnOpts(mode, 1 if use_lb_sax else 0, 1 if profile else 0)
         _check(lib().hg_knn_device(self._h, ctypes.c_void_p(q_ptr), nq, k, ctypes.byref(opts),
                                    ctypes.c_void_p(dist_ptr), ctypes.c_void_p(id_ptr), ctypes.c_void_p(stream),
                                    ctypes.byref(st)))

@@ -999,7 +999,7 @@ static hg_status ensure_scratch(hg_index* ix, int k) {
   CK(dalloc(&s.topk, hg::kMaxK));
   CK(dalloc(&s.topk_count, 1));
   CK(dalloc(&s.paa, 16));
-  CK(dalloc(&s.stats, 4));
+  CK(dalloc(&s.stats, 8));
   CK(dalloc(&s.err, 1));
   CK(dalloc(&s.q, 1));
   s.kmax = hg::kMaxK;
@@ -1010,8 +1010,23 @@ static hg::Tree index_tree(const hg_index* ix) { return hg::Tree{ix->d.nodes, ix
 
 // One query through the plain path: approximate leaf, LB_EAPCA of every
 // leaf, scan of the approximate leaf, candidates by LB, scan, merge.
+using ProfEvents = std::vector<std::pair<cudaEvent_t, cudaEvent_t>>;
+
+static hg_status scan_timed(const hg::ScanArgs& a, int blocks, cudaStream_t st, ProfEvents* prof) {
+  if (prof) {
+    std::pair<cudaEvent_t, cudaEvent_t> ev;
+    CK(cudaEventCreate(&ev.first));
+    CK(cudaEventCreate(&ev.second));
+    prof->push_back(ev);
+    CK(cudaEventRecord(ev.first, st));
+  }
+  CK(hg::launch_scan(a, blocks, st));
+  if (prof) CK(cudaEventRecord(prof->back().second, st));
+  return HG_OK;
+}
+
 static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opts& o, float* d_dist,
-                         int64_t* d_id, cudaStream_t st) {
+                         int64_t* d_id, cudaStream_t st, ProfEvents* prof) {
   hg::QueryScratch& s = ix->s;
   hg::DeviceIndex& d = ix->d;
   const int nl = (int)ix->leaves.size();
@@ -1040,7 +1055,7 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
     CK(hg::launch_pscan_prep(ix->n, s.cand_count, s.unit_prefix, s.bound, s.topk_count, st));
     a.pscan = 1;
     a.use_lbsax = 0;
-    CK(hg::launch_scan(a, blocks, st));
+    HCK(scan_timed(a, blocks, st, prof));
     CK(hg::launch_merge(s.parts, s.part_count, s.nparts, k, s.topk, s.topk_count, s.bound, s.err, st));
   } else {
     a.pscan = 0;
@@ -1048,11 +1063,11 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
     CK(hg::launch_query_prep(d_q, a.L, index_tree(ix), d.leaf_start, d.leaf_size, s.approx_leaf, s.paa, s.cand,
                              s.cand_lb, s.cand_count, s.unit_prefix, s.bound, s.topk_count, st));
     CK(hg::launch_leaf_lb(d_q, a.L, nl, d.leaf_seg_off, d.leaf_points, d.leaf_sk, s.lb, st));
-    CK(hg::launch_scan(a, blocks, st));
+    HCK(scan_timed(a, blocks, st, prof));
     CK(hg::launch_merge(s.parts, s.part_count, s.nparts, k, s.topk, s.topk_count, s.bound, s.err, st));
     CK(hg::launch_select_sort(s.lb, nl, s.bound, s.approx_leaf, d.leaf_start, d.leaf_size, s.cand, s.cand_lb,
                               s.cand_count, s.unit_prefix, st));
-    CK(hg::launch_scan(a, blocks, st));
+    HCK(scan_timed(a, blocks, st, prof));
     CK(hg::launch_merge(s.parts, s.part_count, s.nparts, k, s.topk, s.topk_count, s.bound, s.err, st));
   }
   CK(hg::launch_emit(s.topk, s.topk_count, k, d_dist, d_id, st));
@@ -1075,19 +1090,28 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  CK(cudaMemsetAsync(ix->s.stats, 0, sizeof(unsigned long long) * 4, st));
+  CK(cudaMemsetAsync(ix->s.stats, 0, sizeof(unsigned long long) * 8, st));
+  ProfEvents prof;
   CK(cudaEventRecord(e0, st));
   for (uint32_t i = 0; i < nq; ++i)
     HCK(knn_one(ix, d_queries + (uint64_t)i * ix->L, (int)k, o, d_dist ? d_dist + (uint64_t)i * k : nullptr,
-                d_id ? d_id + (uint64_t)i * k : nullptr, st));
+                d_id ? d_id + (uint64_t)i * k : nullptr, st, o.profile ? &prof : nullptr));
   CK(cudaEventRecord(e1, st));
-  unsigned long long hs[4];
+  unsigned long long hs[8];
   CK(cudaMemcpyAsync(hs, ix->s.stats, sizeof hs, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  double scan_ms = 0;
+  for (auto& ev : prof) {
+    float t = 0;
+    cudaEventElapsedTime(&t, ev.first, ev.second);
+    scan_ms += t;
+    cudaEventDestroy(ev.first);
+    cudaEventDestroy(ev.second);
+  }
   if (stats) {
     memset(stats, 0, sizeof *stats);
     stats->queries = nq;
@@ -1095,7 +1119,10 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
     stats->chunks_loaded = hs[1];
     stats->rows_lbsax_pruned = hs[2];
     stats->leaves_scanned = hs[3];
+    stats->rows_completed = hs[4];
     stats->device_ms = ms;
+    stats->scan_launches = prof.size();
+    stats->scan_ms = scan_ms;
   }
   return HG_OK;
 }

@@ -542,7 +542,7 @@ __global__ void __launch_bounds__(kScanThreads, 4) k_scan(ScanArgs a) {
   const float* q = a.q;
   int cnt = 0;
   float T = __int_as_float(0x7f800000);  // the warp's own k-th (when full)
-  unsigned long long n_rows = 0, n_chunks = 0, n_pruned = 0, n_leaves = 0;
+  unsigned long long n_rows = 0, n_chunks = 0, n_pruned = 0, n_leaves = 0, n_done = 0;
   int c = 0;
   for (uint32_t unit = gw; unit < total; unit += nwarps) {
     uint64_t lstart;
@@ -632,6 +632,7 @@ __global__ void __launch_bounds__(kScanThreads, 4) k_scan(ScanArgs a) {
     // rows still alive completed every chunk: dist is the full distance.
     // The list holds at most k entries between tiles (it is compacted as
     // soon as it reaches k), so up to 32 new entries always fit.
+    if (alive) ++n_done;
     const bool take = alive && dist <= B && dist <= T;
     const uint32_t m = __ballot_sync(HG_FULL, take);
     if (m) {
@@ -666,6 +667,7 @@ __global__ void __launch_bounds__(kScanThreads, 4) k_scan(ScanArgs a) {
   // per-lane counters
   atomicAdd(&a.stats[1], n_chunks);
   atomicAdd(&a.stats[2], n_pruned);
+  atomicAdd(&a.stats[4], n_done);
 }
 
 // Merges the per-warp lists (and the current top-k, passed as part -1) into

@@ -51,6 +51,7 @@ struct ScanArgs {
   unsigned long long* parts;  // per-warp sorted lists (kWarpListCap stride)
   int* part_count;
   unsigned long long* stats;  // [0] rows visited [1] chunks loaded [2] lbsax pruned [3] leaves scanned
+                              // [4] rows completed
 };
 
 int scan_grid_blocks(int device);

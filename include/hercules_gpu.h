@@ -68,6 +68,9 @@ typedef struct {
   uint64_t chunks_loaded;     /* 32-byte chunks of raw data read by the scan */
   uint64_t candidate_leaves;  /* leaves with LB_EAPCA <= k-th bound */
   double device_ms;           /* device time of the call (CUDA events) */
+  uint64_t rows_completed;    /* rows whose full distance was computed */
+  uint64_t scan_launches;     /* leaf-scan kernel launches (profile = 1) */
+  double scan_ms;             /* their summed device time (profile = 1) */
 } hg_query_stats;
 
 /* Search mode. */
@@ -77,7 +80,8 @@ typedef struct {
 typedef struct {
   int mode;           /* HG_MODE_* */
   int use_lb_sax;     /* 1: per-row LB_SAX filter before the distance */
-  int reserved[6];
+  int profile;        /* 1: time every leaf-scan launch with CUDA events */
+  int reserved[5];
 } hg_knn_opts;
 
 /* ---- status ----------------------------------------------------------- */
