@@ -285,28 +285,38 @@ def main():
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, device=torch.device("cuda", device))
     e2e_value = total_q / e2e_s
 
-    # roofline of the leaf-scan kernel (algorithmic bytes / measured time)
+    # roofline of the dominant kernel, the early-abandoning distance stream
+    # k_ed_stream: algorithmic bytes = 32 B per 8-float chunk it computed
+    # + 4 B list entry per row started + 8 B id per finished row, divided by
+    # its summed launch time (CUDA events around every launch)
     peak, peak_kind = measured_peaks()
-    alg_bytes = (32.0 * agg["chunks_loaded"] + 8.0 * agg["rows_completed"] +
-                 (16.0 * agg["rows_visited"] if args.lb_sax else 0.0))
+    launches = int(agg["scan_launches"])
+    alg_bytes = 32.0 * agg["chunks_loaded"] + 4.0 * agg["rows_visited"] + 8.0 * agg["rows_completed"]
     scan_s = agg["scan_ms"] / 1000.0
     achieved = alg_bytes / scan_s / 1e9 if scan_s > 0 else 0.0
-    launches = int(agg["scan_launches"])
     tr = ncu_traffic()
     traffic = None
-    if tr and tr.get("bytes_per_row_visited"):
-        traffic = tr["bytes_per_row_visited"] * agg["rows_visited"] / max(launches, 1)
-    roofline = {"bound": "hbm", "kernel": "k_scan (leaf scan)", "achieved": round(achieved, 1),
+    if tr and tr.get("dram_bytes_per_chunk"):
+        traffic = tr["dram_bytes_per_chunk"] * agg["chunks_loaded"] / max(launches, 1)
+    f_launches = int(agg["filter_launches"])
+    f_bytes = 16.0 * agg["rows_considered"] + 4.0 * (agg["rows_considered"] - agg["rows_lbsax_pruned"])
+    f_s = agg["filter_ms"] / 1000.0
+    roofline = {"bound": "hbm", "kernel": "k_ed_stream (leaf scan distances)", "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "peak_source": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": alg_bytes / max(launches, 1),
-                "avg_launch_ms": agg["scan_ms"] / max(launches, 1), "launches": launches}
+                "avg_launch_ms": agg["scan_ms"] / max(launches, 1), "launches": launches,
+                "filter": {"kernel": "k_lbsax_filter", "achieved": round(f_bytes / f_s / 1e9, 1) if f_s > 0 else None,
+                           "frac": round(f_bytes / f_s / 1e9 / peak, 4) if f_s > 0 else None,
+                           "avg_launch_ms": agg["filter_ms"] / max(f_launches, 1), "launches": f_launches}}
 
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu_baseline = cpu_baseline_leg(args, ix, cpu_q)
     ix.close()
-    per_query_launches = 8
+    # per query: prep, leaf LB, distances (approximate leaf), merge, sort,
+    # LB_SAX filter, distances (candidates), merge, emit
+    per_query_launches = 9
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warm,
         "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -322,11 +332,13 @@ def main():
         "roofline": roofline,
         "cpu_baseline": cpu_baseline,
         "clocks": ck,
-        "stats": {"rows_visited_per_query": agg["rows_visited"] / (nq_step * steps),
-                  "chunks_per_visited_row": agg["chunks_loaded"] / max(agg["rows_visited"], 1),
-                  "lbsax_pruned_frac": agg["rows_lbsax_pruned"] / max(agg["rows_visited"], 1),
+        "stats": {"candidate_rows_per_query": agg["rows_considered"] / (nq_step * steps),
+                  "lbsax_pruned_frac": agg["rows_lbsax_pruned"] / max(agg["rows_considered"], 1),
+                  "distance_rows_per_query": agg["rows_visited"] / (nq_step * steps),
+                  "chunks_per_distance_row": agg["chunks_loaded"] / max(agg["rows_visited"], 1),
                   "leaves_scanned_per_query": agg["leaves_scanned"] / (nq_step * steps),
-                  "scan_share_of_step": agg["scan_ms"] / ms if ms > 0 else None,
+                  "ed_share_of_step": agg["scan_ms"] / ms if ms > 0 else None,
+                  "filter_share_of_step": agg["filter_ms"] / ms if ms > 0 else None,
                   "index_build_s": round(build_s, 2), "setup_s": round(setup_s, 2)},
     }
     if rank == 0:

@@ -45,7 +45,9 @@ class QueryStats(ctypes.Structure):
                 ("rows_visited", ctypes.c_uint64), ("rows_lbsax_pruned", ctypes.c_uint64),
                 ("chunks_loaded", ctypes.c_uint64), ("candidate_leaves", ctypes.c_uint64),
                 ("device_ms", ctypes.c_double), ("rows_completed", ctypes.c_uint64),
-                ("scan_launches", ctypes.c_uint64), ("scan_ms", ctypes.c_double)]
+                ("scan_launches", ctypes.c_uint64), ("scan_ms", ctypes.c_double),
+                ("rows_considered", ctypes.c_uint64), ("filter_launches", ctypes.c_uint64),
+                ("filter_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -53,7 +55,7 @@ class QueryStats(ctypes.Structure):
 
 class KnnOpts(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("use_lb_sax", ctypes.c_int), ("profile", ctypes.c_int),
-                ("reserved", ctypes.c_int * 5)]
+                ("approx_blocks", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
 
 
 _lib = None

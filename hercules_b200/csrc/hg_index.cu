@@ -22,6 +22,10 @@
 
 using hg::Node;
 
+// Launch geometry of the leaf scan.
+constexpr int kEdBlocksPerSm = 3;      // k_ed_stream: 3 x 256 threads per SM
+constexpr int kFilterBlocksPerSm = 8;  // k_lbsax_filter
+
 // ---------------------------------------------------------------------------
 // errors
 // ---------------------------------------------------------------------------
@@ -613,11 +617,10 @@ static hg_status finalize_build(hg_index* ix, const float* X, cudaStream_t st) {
                                  d_seg + total_segs + koff[i], (int)lf.points.size(), d_keys + 4 * koff[i], st));
   }
   CK(cudaMemcpyAsync(keys.data(), d_keys, sizeof(int) * keys.size(), cudaMemcpyDeviceToHost, st));
-  // tiles, ids, iSAX words
+  // leaf-ordered rows, ids, iSAX words
   hg::DeviceIndex& d = ix->d;
-  ix->ntiles = (uint32_t)((ix->n + 31) / 32);
-  CK(dalloc(&d.rows, (size_t)ix->ntiles * 32 * ix->L));
-  CK(hg::launch_gather_tiles(X, ix->L, d_perm, ix->n, d.rows, st));
+  CK(dalloc(&d.rows, (size_t)ix->n * ix->L));
+  CK(hg::launch_gather_rows(X, ix->L, d_perm, ix->n, d.rows, st));
   ix->ids.assign(perm.begin(), perm.end());
   ix->has_ids = true;
   CK(dalloc(&d.ids, ix->n));
@@ -840,27 +843,23 @@ static hg_status write_impl(hg_index* ix, const char* dir, double buffer_mb) {
   w.put<int32_t>(1);
   w.put<int32_t>(1);
   write_node(ix, 0, w);
-  // leaf-ordered raw rows and iSAX words, in pieces
+  // leaf-ordered raw rows (the HBM image) and iSAX words, in pieces
   const uint64_t piece = std::max<uint64_t>(1, (64u << 20) / (sizeof(float) * ix->L));
-  float* d_rm = nullptr;
-  CK(dalloc(&d_rm, piece * ix->L));
   std::vector<float> h_rm(piece * ix->L);
   std::vector<uint8_t> h_sax(piece * 16);
   bool ok = w.ok;
   for (uint64_t r0 = 0; r0 < ix->n && ok; r0 += piece) {
     const uint64_t cnt = std::min(piece, ix->n - r0);
-    cudaError_t e = hg::launch_rowmajor_from_tiles(ix->d.rows, ix->L, r0, cnt, d_rm, ix->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h_rm.data(), d_rm, sizeof(float) * cnt * ix->L, cudaMemcpyDeviceToHost, ix->stream);
+    cudaError_t e = cudaMemcpyAsync(h_rm.data(), ix->d.rows + r0 * ix->L, sizeof(float) * cnt * ix->L,
+                                    cudaMemcpyDeviceToHost, ix->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_sax.data(), ix->d.sax + r0 * 16, cnt * 16, cudaMemcpyDeviceToHost, ix->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
     if (e != cudaSuccess) {
-      cudaFree(d_rm);
       close_all();
       return cuda_fail(e, "hg_index_write");
     }
     ok = fwrite(h_rm.data(), sizeof(float) * ix->L, cnt, raw) == cnt && fwrite(h_sax.data(), 16, cnt, sims) == cnt;
   }
-  cudaFree(d_rm);
   std::vector<uint64_t> ids64(ix->n);
   for (uint64_t i = 0; i < ix->n; ++i) ids64[i] = ix->has_ids ? (uint64_t)ix->ids[i] : i;
   ok = ok && fwrite(ids64.data(), 8, ix->n, idf) == ix->n;
@@ -909,29 +908,22 @@ static hg_status read_impl(const char* dir, int device, hg_index** out) {
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&ix->stream, cudaStreamNonBlocking));
   hg::DeviceIndex& d = ix->d;
-  ix->ntiles = (uint32_t)((ix->n + 31) / 32);
   FILE* raw = fopen(join(dir, "leaves_raw.idx").c_str(), "rb");
   if (!raw) return set_error(HG_ERR_IO, "hg_index_read: cannot open leaves_raw.idx");
-  const uint64_t piece = std::max<uint64_t>(32, ((64u << 20) / (sizeof(float) * ix->L)) / 32 * 32);
+  // leaves_raw.idx is the HBM image: copy it in pieces
+  const uint64_t piece = std::max<uint64_t>(1, (64u << 20) / (sizeof(float) * ix->L));
   std::vector<float> h_rm(piece * ix->L);
-  float* d_rm = nullptr;
-  cudaError_t e = dalloc(&d.rows, (size_t)ix->ntiles * 32 * ix->L);
-  if (e == cudaSuccess) e = cudaMemset(d.rows, 0, sizeof(float) * (size_t)ix->ntiles * 32 * ix->L);
-  if (e == cudaSuccess) e = dalloc(&d_rm, piece * ix->L);
+  cudaError_t e = dalloc(&d.rows, (size_t)ix->n * ix->L);
   for (uint64_t r0 = 0; r0 < ix->n && e == cudaSuccess; r0 += piece) {
     const uint64_t cnt = std::min(piece, ix->n - r0);
     if (fread(h_rm.data(), sizeof(float) * ix->L, cnt, raw) != cnt) {
       fclose(raw);
-      cudaFree(d_rm);
       free_device(ix.get());
       return set_error(HG_ERR_IO, "hg_index_read: leaves_raw.idx is shorter than the leaves");
     }
-    e = cudaMemcpyAsync(d_rm, h_rm.data(), sizeof(float) * cnt * ix->L, cudaMemcpyHostToDevice, ix->stream);
-    if (e == cudaSuccess) e = hg::launch_tiles_from_rowmajor(d_rm, ix->L, r0, cnt, d.rows, ix->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
+    e = cudaMemcpy(d.rows + r0 * ix->L, h_rm.data(), sizeof(float) * cnt * ix->L, cudaMemcpyHostToDevice);
   }
   fclose(raw);
-  if (d_rm) cudaFree(d_rm);
   if (e != cudaSuccess) {
     free_device(ix.get());
     return cuda_fail(e, "hg_index_read");
@@ -985,9 +977,12 @@ static hg_status ensure_scratch(hg_index* ix, int k) {
   dfree(s.paa);
   dfree(s.stats);
   dfree(s.err);
-  const int blocks = hg::scan_grid_blocks(ix->device);
-  s.nparts = blocks * hg::kScanWarps;
+  dfree(s.list);
+  dfree(s.counters);
+  s.nparts = hg::sm_count(ix->device) * kEdBlocksPerSm * hg::kEdWarps;
   CK(dalloc(&s.lb, nl));
+  CK(dalloc(&s.list, ix->n));
+  CK(dalloc(&s.counters, 8));
   CK(dalloc(&s.approx_leaf, 1));
   CK(dalloc(&s.cand, nl + 1));
   CK(dalloc(&s.cand_lb, nl + 1));
@@ -1012,63 +1007,120 @@ static hg::Tree index_tree(const hg_index* ix) { return hg::Tree{ix->d.nodes, ix
 // leaf, scan of the approximate leaf, candidates by LB, scan, merge.
 using ProfEvents = std::vector<std::pair<cudaEvent_t, cudaEvent_t>>;
 
-static hg_status scan_timed(const hg::ScanArgs& a, int blocks, cudaStream_t st, ProfEvents* prof) {
-  if (prof) {
-    std::pair<cudaEvent_t, cudaEvent_t> ev;
-    CK(cudaEventCreate(&ev.first));
-    CK(cudaEventCreate(&ev.second));
-    prof->push_back(ev);
-    CK(cudaEventRecord(ev.first, st));
-  }
-  CK(hg::launch_scan(a, blocks, st));
-  if (prof) CK(cudaEventRecord(prof->back().second, st));
+struct Prof {
+  ProfEvents ed, filter;
+};
+
+static hg_status timed_begin(ProfEvents* p, cudaStream_t st) {
+  if (!p) return HG_OK;
+  std::pair<cudaEvent_t, cudaEvent_t> ev;
+  CK(cudaEventCreate(&ev.first));
+  CK(cudaEventCreate(&ev.second));
+  p->push_back(ev);
+  CK(cudaEventRecord(ev.first, st));
   return HG_OK;
 }
 
+static hg_status timed_end(ProfEvents* p, cudaStream_t st) {
+  if (p) CK(cudaEventRecord(p->back().second, st));
+  return HG_OK;
+}
+
+static double drain(ProfEvents& p) {
+  double ms = 0;
+  for (auto& ev : p) {
+    float t = 0;
+    cudaEventElapsedTime(&t, ev.first, ev.second);
+    ms += t;
+    cudaEventDestroy(ev.first);
+    cudaEventDestroy(ev.second);
+  }
+  p.clear();
+  return ms;
+}
+
+// One query through the plain path:
+//   route + PAA (approximate_knn_search's traversal) -> LB_EAPCA of every
+//   leaf -> exact distances of the approximate leaf -> k-th bound ->
+//   candidate leaves sorted by LB -> LB_SAX filter -> exact distances of the
+//   survivors -> merge.
 static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opts& o, float* d_dist,
-                         int64_t* d_id, cudaStream_t st, ProfEvents* prof) {
+                         int64_t* d_id, cudaStream_t st, Prof* prof) {
   hg::QueryScratch& s = ix->s;
   hg::DeviceIndex& d = ix->d;
   const int nl = (int)ix->leaves.size();
-  const int blocks = hg::scan_grid_blocks(ix->device);
-  hg::ScanArgs a{};
-  a.rows = d.rows;
-  a.ids = d.ids;
-  a.sax = d.sax;
-  a.bp = d.bp;
-  a.L = (int)ix->L;
-  a.nrows = ix->n;
-  a.leaf_start = d.leaf_start;
-  a.leaf_size = d.leaf_size;
-  a.cand = s.cand;
-  a.cand_lb = s.cand_lb;
-  a.cand_count = s.cand_count;
-  a.unit_prefix = s.unit_prefix;
-  a.q = d_q;
-  a.paa = s.paa;
-  a.k = k;
-  a.bound = s.bound;
-  a.parts = s.parts;
-  a.part_count = s.part_count;
-  a.stats = s.stats;
+  const int sms = hg::sm_count(ix->device);
+  const int ed_blocks = sms * kEdBlocksPerSm;
+  hg::EdArgs e{};
+  e.rows = d.rows;
+  e.ids = d.ids;
+  e.L = (int)ix->L;
+  e.leaf_start = d.leaf_start;
+  e.leaf_size = d.leaf_size;
+  e.q = d_q;
+  e.k = k;
+  e.bound = s.bound;
+  e.parts = s.parts;
+  e.part_count = s.part_count;
+  e.stats = s.stats;
   if (o.mode == HG_MODE_PSCAN) {
-    CK(hg::launch_pscan_prep(ix->n, s.cand_count, s.unit_prefix, s.bound, s.topk_count, st));
-    a.pscan = 1;
-    a.use_lbsax = 0;
-    HCK(scan_timed(a, blocks, st, prof));
-    CK(hg::launch_merge(s.parts, s.part_count, s.nparts, k, s.topk, s.topk_count, s.bound, s.err, st));
+    CK(hg::launch_pscan_prep(ix->n, s.cand_count, s.unit_prefix, s.bound, s.topk_count, s.counters, st));
+    e.list = nullptr;
+    e.ident_leaf = nullptr;
+    e.ident_first = 0;
+    e.ident_count = ix->n;
+    e.head = s.counters + 0;
+    HCK(timed_begin(prof ? &prof->ed : nullptr, st));
+    CK(hg::launch_ed_stream(e, ed_blocks, st));
+    HCK(timed_end(prof ? &prof->ed : nullptr, st));
+    CK(hg::launch_merge(s.parts, s.part_count, ed_blocks * hg::kEdWarps, k, s.topk, s.topk_count, s.bound, s.err,
+                        st));
   } else {
-    a.pscan = 0;
-    a.use_lbsax = o.use_lb_sax ? 1 : 0;
-    CK(hg::launch_query_prep(d_q, a.L, index_tree(ix), d.leaf_start, d.leaf_size, s.approx_leaf, s.paa, s.cand,
-                             s.cand_lb, s.cand_count, s.unit_prefix, s.bound, s.topk_count, st));
-    CK(hg::launch_leaf_lb(d_q, a.L, nl, d.leaf_seg_off, d.leaf_points, d.leaf_sk, s.lb, st));
-    HCK(scan_timed(a, blocks, st, prof));
-    CK(hg::launch_merge(s.parts, s.part_count, s.nparts, k, s.topk, s.topk_count, s.bound, s.err, st));
+    CK(hg::launch_query_prep(d_q, e.L, index_tree(ix), d.leaf_start, d.leaf_size, s.approx_leaf, s.paa, s.cand,
+                             s.cand_lb, s.cand_count, s.unit_prefix, s.bound, s.topk_count, s.counters, st));
+    CK(hg::launch_leaf_lb(d_q, e.L, nl, d.leaf_seg_off, d.leaf_points, d.leaf_sk, s.lb, st));
+    // the approximate leaf, with an unbounded k-th distance at the start
+    const int a_blocks = std::max(1, std::min(ed_blocks, o.approx_blocks > 0 ? o.approx_blocks : sms));
+    e.list = nullptr;
+    e.ident_leaf = s.approx_leaf;
+    e.head = s.counters + 0;
+    HCK(timed_begin(prof ? &prof->ed : nullptr, st));
+    CK(hg::launch_ed_stream(e, a_blocks, st));
+    HCK(timed_end(prof ? &prof->ed : nullptr, st));
+    CK(hg::launch_merge(s.parts, s.part_count, a_blocks * hg::kEdWarps, k, s.topk, s.topk_count, s.bound, s.err,
+                        st));
     CK(hg::launch_select_sort(s.lb, nl, s.bound, s.approx_leaf, d.leaf_start, d.leaf_size, s.cand, s.cand_lb,
                               s.cand_count, s.unit_prefix, st));
-    HCK(scan_timed(a, blocks, st, prof));
-    CK(hg::launch_merge(s.parts, s.part_count, s.nparts, k, s.topk, s.topk_count, s.bound, s.err, st));
+    hg::FilterArgs f{};
+    f.sax = d.sax;
+    f.bp = d.bp;
+    f.L = e.L;
+    f.nrows = ix->n;
+    f.leaf_start = d.leaf_start;
+    f.leaf_size = d.leaf_size;
+    f.cand = s.cand;
+    f.cand_lb = s.cand_lb;
+    f.cand_count = s.cand_count;
+    f.unit_prefix = s.unit_prefix;
+    f.paa = s.paa;
+    f.use_lbsax = o.use_lb_sax ? 1 : 0;
+    f.bound = s.bound;
+    f.list = s.list;
+    f.list_count = s.counters + 2;
+    f.stats = s.stats;
+    HCK(timed_begin(prof ? &prof->filter : nullptr, st));
+    CK(hg::launch_lbsax_filter(f, sms * kFilterBlocksPerSm, st));
+    HCK(timed_end(prof ? &prof->filter : nullptr, st));
+    e.list = s.list;
+    e.list_count = s.counters + 2;
+    e.ident_leaf = nullptr;
+    e.head = s.counters + 1;
+    HCK(timed_begin(prof ? &prof->ed : nullptr, st));
+    CK(hg::launch_ed_stream(e, ed_blocks, st));
+    HCK(timed_end(prof ? &prof->ed : nullptr, st));
+    // the merge folds the approximate leaf's top-k (in topk) into the result
+    CK(hg::launch_merge(s.parts, s.part_count, ed_blocks * hg::kEdWarps, k, s.topk, s.topk_count, s.bound, s.err,
+                        st));
   }
   CK(hg::launch_emit(s.topk, s.topk_count, k, d_dist, d_id, st));
   return HG_OK;
@@ -1080,6 +1132,7 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
   if (!ix || (!d_queries && nq)) return set_error(HG_ERR_ARG, "hg_knn: null argument");
   if (k == 0) return set_error(HG_ERR_ARG, "hg_knn: k must be positive");
   if ((int)k > hg::kMaxK) return set_error(HG_ERR_LIMIT, "hg_knn: k above 224");
+  if (ix->L > 16384) return set_error(HG_ERR_LIMIT, "hg_knn: series longer than 16384");
   if (ix->leaves.size() > (size_t)hg::kMaxLeavesSort)
     return set_error(HG_ERR_LIMIT, "hg_knn: more than 8192 leaves");
   hg_knn_opts o{};
@@ -1091,7 +1144,7 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   CK(cudaMemsetAsync(ix->s.stats, 0, sizeof(unsigned long long) * 8, st));
-  ProfEvents prof;
+  Prof prof;
   CK(cudaEventRecord(e0, st));
   for (uint32_t i = 0; i < nq; ++i)
     HCK(knn_one(ix, d_queries + (uint64_t)i * ix->L, (int)k, o, d_dist ? d_dist + (uint64_t)i * k : nullptr,
@@ -1104,25 +1157,23 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  double scan_ms = 0;
-  for (auto& ev : prof) {
-    float t = 0;
-    cudaEventElapsedTime(&t, ev.first, ev.second);
-    scan_ms += t;
-    cudaEventDestroy(ev.first);
-    cudaEventDestroy(ev.second);
-  }
+  const size_t ed_launches = prof.ed.size(), filter_launches = prof.filter.size();
+  const double scan_ms = drain(prof.ed);
+  const double filter_ms = drain(prof.filter);
   if (stats) {
     memset(stats, 0, sizeof *stats);
     stats->queries = nq;
-    stats->rows_visited = hs[0];
+    stats->rows_considered = hs[0];
     stats->chunks_loaded = hs[1];
     stats->rows_lbsax_pruned = hs[2];
     stats->leaves_scanned = hs[3];
     stats->rows_completed = hs[4];
+    stats->rows_visited = hs[5];
     stats->device_ms = ms;
-    stats->scan_launches = prof.size();
+    stats->scan_launches = ed_launches;
     stats->scan_ms = scan_ms;
+    stats->filter_launches = filter_launches;
+    stats->filter_ms = filter_ms;
   }
   return HG_OK;
 }
@@ -1216,7 +1267,7 @@ hg_status hg_index_info_get(const hg_index* ix, hg_index_info* info) {
   info->num_nodes = (uint32_t)ix->nodes.size();
   info->max_segments = (uint32_t)ix->max_seg;
   info->has_ids = ix->has_ids ? 1 : 0;
-  info->device_bytes = (uint64_t)ix->ntiles * 32 * ix->L * 4 + ix->n * (8 + 16);
+  info->device_bytes = (uint64_t)ix->n * ix->L * 4 + ix->n * (8 + 16);
   return HG_OK;
 }
 
@@ -1247,15 +1298,7 @@ hg_status hg_index_rows(const hg_index* ix, uint64_t first, uint64_t count, floa
   if (!ix || first + count > ix->n) return set_error(HG_ERR_ARG, "hg_index_rows: range outside the index");
   if (count == 0) return HG_OK;
   CK(cudaSetDevice(ix->device));
-  if (rows) {
-    float* d_rm = nullptr;
-    CK(dalloc(&d_rm, count * ix->L));
-    cudaError_t e = hg::launch_rowmajor_from_tiles(ix->d.rows, ix->L, first, count, d_rm, ix->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(rows, d_rm, sizeof(float) * count * ix->L, cudaMemcpyDeviceToHost, ix->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
-    cudaFree(d_rm);
-    if (e != cudaSuccess) return cuda_fail(e, "hg_index_rows");
-  }
+  if (rows) CK(cudaMemcpy(rows, ix->d.rows + first * ix->L, sizeof(float) * count * ix->L, cudaMemcpyDeviceToHost));
   if (sax) CK(cudaMemcpy(sax, ix->d.sax + first * 16, count * 16, cudaMemcpyDeviceToHost));
   return HG_OK;
 }

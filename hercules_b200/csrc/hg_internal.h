@@ -69,7 +69,8 @@ struct QueryScratch {
   int* topk_count = nullptr;
   uint64_t* topk_row = nullptr;   // kmax leaf-ordered rows of the answers
   float* paa = nullptr;           // 16
-  unsigned long long* stats = nullptr;  // counters: rows visited, chunks loaded, rows lbsax-pruned, leaves scanned
+  unsigned long long* stats = nullptr;  // see EdArgs / FilterArgs
+  uint32_t* list = nullptr;       // LB_SAX survivors (rows), n entries
   int* err = nullptr;             // device error flag
 };
 
@@ -88,6 +89,5 @@ struct hg_index {
   hg::DeviceIndex d;
   hg::QueryScratch s;
   cudaStream_t stream = nullptr;
-  uint32_t ntiles = 0;
   int max_seg = 0;
 };

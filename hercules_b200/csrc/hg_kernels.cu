@@ -1,13 +1,10 @@
 // hg_kernels.cu -- sm_100a kernels of the Hercules exact k-NN path.
 //
-// Data layout in HBM: the leaf-ordered rows (leaves_raw.idx order) are held
-// in 32-row tiles, chunk-interleaved: element (row r, column j) lives at
-//   ((r/32) * (L/8) + j/8) * 256 + (r%32) * 8 + j%8
-// so one 8-float chunk (32 bytes, one DRAM sector) of 32 consecutive rows
-// is a contiguous 1 KiB block.  A warp scanning 32 rows chunk by chunk reads
-// fully coalesced 1 KiB blocks, and a row that abandons stops requesting its
-// sectors.  Distances follow the reference's summation order exactly
-// (hg_arith.cuh).
+// Data layout in HBM: the leaf-ordered rows, row-major -- the image of
+// leaves_raw.idx.  A row of L floats is L/8 chunks of 32 bytes; the distance
+// kernel reads a row four chunks (one 128-byte line) at a time and stops at
+// the line where the row abandons.  Distances follow the reference's
+// summation order exactly (hg_arith.cuh).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -18,10 +15,6 @@
 namespace hg {
 
 #define HG_FULL 0xffffffffu
-
-__device__ __forceinline__ uint64_t tile_off(uint64_t row, int chunk, int nchunks) {
-  return ((((row >> 5) * (uint64_t)nchunks + (uint64_t)chunk) << 5) + (row & 31)) << 3;
-}
 
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
   return *(const volatile uint32_t*)p;
@@ -195,88 +188,32 @@ __global__ void k_route_flags(const float* __restrict__ X, int L, const uint32_t
   flags[i] = ((idx ? s : m) < value) ? 1 : 0;
 }
 
-// tiles[row] = X[perm[row]]; one thread per (row, chunk), rows fastest so
-// that a warp writes one contiguous 1 KiB tile block.
-__global__ void k_gather_tiles(const float* __restrict__ X, int L, const uint32_t* __restrict__ perm, uint64_t n,
-                               float* __restrict__ tiles) {
-  const int nch = L >> 3;
+// rows[r] = X[perm[r]], one thread per 16 bytes (a row is L/4 of them).
+__global__ void k_gather_rows(const float* __restrict__ X, int L, const uint32_t* __restrict__ perm, uint64_t n,
+                              float* __restrict__ rows) {
+  const int v4 = L >> 2;
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t tile = t / (32ull * nch);
-  const int within = (int)(t % (32ull * nch));
-  const int chunk = within >> 5, lane = within & 31;
-  const uint64_t row = tile * 32 + lane;
-  if (tile * 32 >= n) return;
-  float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
-  if (row < n) {
-    const float4* src = reinterpret_cast<const float4*>(X + (uint64_t)perm[row] * L + chunk * 8);
-    a = src[0];
-    b = src[1];
-  }
-  float4* dst = reinterpret_cast<float4*>(tiles + tile_off(row, chunk, nch));
-  dst[0] = a;
-  dst[1] = b;
-}
-
-__global__ void k_tiles_from_rowmajor(const float* __restrict__ rm, int L, uint64_t first, uint64_t count,
-                                      float* __restrict__ tiles) {
-  // rm holds rows [first, first+count); first is a multiple of 32
-  const int nch = L >> 3;
-  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t tl = t / (32ull * nch);
-  const int within = (int)(t % (32ull * nch));
-  const int chunk = within >> 5, lane = within & 31;
-  const uint64_t local = tl * 32 + lane;
-  if (tl * 32 >= count) return;
-  float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
-  if (local < count) {
-    const float4* src = reinterpret_cast<const float4*>(rm + local * L + chunk * 8);
-    a = src[0];
-    b = src[1];
-  }
-  float4* dst = reinterpret_cast<float4*>(tiles + tile_off(first + local, chunk, nch));
-  dst[0] = a;
-  dst[1] = b;
-}
-
-__global__ void k_rowmajor_from_tiles(const float* __restrict__ tiles, int L, uint64_t first, uint64_t count,
-                                      float* __restrict__ rm) {
-  const int nch = L >> 3;
-  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t local = t / nch;
-  const int chunk = (int)(t % nch);
-  if (local >= count) return;
-  const float4* src = reinterpret_cast<const float4*>(tiles + tile_off(first + local, chunk, nch));
-  float4* dst = reinterpret_cast<float4*>(rm + local * L + chunk * 8);
-  dst[0] = src[0];
-  dst[1] = src[1];
+  const uint64_t r = t / v4;
+  if (r >= n) return;
+  const int j = (int)(t % v4);
+  reinterpret_cast<float4*>(rows + r * L)[j] = reinterpret_cast<const float4*>(X + (uint64_t)perm[r] * L)[j];
 }
 
 // iSAX word of every leaf-ordered row (sax_from_ts, sax.c:86-135).
-__global__ void k_sax_rows(const float* __restrict__ tiles, int L, uint64_t n, const float* __restrict__ bp,
+__global__ void k_sax_rows(const float* __restrict__ rows, int L, uint64_t n, const float* __restrict__ bp,
                            uint8_t* __restrict__ sax) {
   __shared__ float sbp[256];
   for (int i = threadIdx.x; i < 255; i += blockDim.x) sbp[i] = bp[i];
   __syncthreads();
   const uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= n) return;
-  const int nch = L >> 3;
   const int per = L / HG_PAA_SEGMENTS;
+  const float* x = rows + row * L;
   uint8_t w[16];
-  float acc = 0.0f;
-  int seg = 0, in_seg = 0;
-  for (int c = 0; c < nch; ++c) {
-    const float4* p = reinterpret_cast<const float4*>(tiles + tile_off(row, c, nch));
-    const float4 a = p[0], b = p[1];
-    const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      acc = __fadd_rn(acc, v[j]);
-      if (++in_seg == per) {
-        w[seg++] = (uint8_t)hg_sax_symbol(__fdiv_rn(acc, (float)per), sbp);
-        acc = 0.0f;
-        in_seg = 0;
-      }
-    }
+  for (int s = 0; s < HG_PAA_SEGMENTS; ++s) {
+    float acc = 0.0f;
+    for (int i = 0; i < per; ++i) acc = __fadd_rn(acc, x[s * per + i]);
+    w[s] = (uint8_t)hg_sax_symbol(__fdiv_rn(acc, (float)per), sbp);
   }
   uint4 out;
   out.x = w[0] | (w[1] << 8) | (w[2] << 16) | ((uint32_t)w[3] << 24);
@@ -296,8 +233,9 @@ __global__ void k_sax_rows(const float* __restrict__ tiles, int L, uint64_t n, c
 __global__ void k_query_prep(const float* __restrict__ q, int L, Tree t, const uint64_t* __restrict__ leaf_start,
                              const uint32_t* __restrict__ leaf_size, int* approx_leaf, float* paa, int* cand,
                              float* cand_lb, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
-                             int* topk_count) {
+                             int* topk_count, uint32_t* counters) {
   const int lane = threadIdx.x & 31;
+  if (lane < 4) counters[lane] = 0;
   const int leaf = warp_route(q, t);
   if (lane < HG_PAA_SEGMENTS) {
     const int per = L / HG_PAA_SEGMENTS;
@@ -449,7 +387,8 @@ __global__ void __launch_bounds__(kSortThreads) k_select_sort(const float* __res
 }
 
 __global__ void k_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
-                             int* topk_count) {
+                             int* topk_count, uint32_t* counters) {
+  if (threadIdx.x < 4) counters[threadIdx.x] = 0;
   if (threadIdx.x == 0) {
     *cand_count = 1;
     unit_prefix[0] = 0;
@@ -515,67 +454,81 @@ __device__ int warp_compact(unsigned long long* list, int cnt, int k) {
   return out;
 }
 
-// The leaf scan: every warp takes 32-row tiles of the candidate leaves in
-// LB order (grid-stride), computes each row's reference-order squared
-// distance chunk by chunk and abandons a row as soon as its partial sum
-// exceeds the running k-th bound.  Finished rows within the bound enter the
-// warp's list; whenever the list holds k distances its k-th lowers the
-// global bound (atomicMin on the float bits).
-__global__ void __launch_bounds__(kScanThreads, 4) k_scan(ScanArgs a) {
-  __shared__ unsigned long long lists[kScanWarps][kWarpListCap];
+// Appends (key, id) candidates of the lanes in `take` to the warp's list and
+// compacts it once it holds k entries; returns the warp's k-th distance T
+// (+inf until k distinct distances are held) and lowers the global bound.
+__device__ __forceinline__ void warp_list_add(unsigned long long* list, int& cnt, float& T, int k, uint32_t* bound,
+                                              bool take, float dist, uint32_t id) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t m = __ballot_sync(HG_FULL, take);
+  if (!m) return;
+  if (take) {
+    const int r = __popc(m & ((1u << lane) - 1));
+    list[cnt + r] = ((unsigned long long)__float_as_uint(dist) << 32) | id;
+  }
+  cnt += __popc(m);
+  __syncwarp();
+  if (cnt >= k) {
+    cnt = warp_compact(list, cnt, k);
+    if (cnt == k) {
+      const float nt = __uint_as_float((uint32_t)(list[k - 1] >> 32));
+      if (nt < T) {
+        T = nt;
+        if (lane == 0) atomicMin(bound, __float_as_uint(T));
+      }
+    }
+  }
+}
+
+// Candidate index of `unit` among the LB-ordered candidate leaves: the
+// largest c with unit_prefix[c] <= unit, searched from the previous c.
+__device__ __forceinline__ int unit_candidate(const uint32_t* unit_prefix, int ncand, int c, uint32_t unit) {
+  int lo = c, hi = ncand - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (unit_prefix[mid] <= unit) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Stage 1 of the leaf scan: walk the candidate leaves in LB_EAPCA order in
+// 32-row units, stop at the first leaf whose LB exceeds the bound, compute
+// each row's LB_SAX from its 16-byte iSAX word (minidist_paa_to_isax_raw_SIMD,
+// sax.c:310-479) and append the rows that can still hold a neighbour to a
+// compact list.
+__global__ void __launch_bounds__(256) k_lbsax_filter(FilterArgs a) {
   __shared__ float sbp[256];
   __shared__ float spaa[16];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  unsigned long long* list = lists[wib];
-  for (int i = lane; i < kWarpListCap; i += 32) list[i] = ~0ull;
   if (a.use_lbsax) {
     for (int i = threadIdx.x; i < 255; i += blockDim.x) sbp[i] = a.bp[i];
     if (threadIdx.x < 16) spaa[threadIdx.x] = a.paa[threadIdx.x];
   }
   __syncthreads();
-  const int nch = a.L >> 3;
+  const int lane = threadIdx.x & 31;
   const int ncand = *a.cand_count;
   const uint32_t total = a.unit_prefix[ncand];
-  const uint32_t nwarps = gridDim.x * kScanWarps;
-  const uint32_t gw = blockIdx.x * kScanWarps + wib;
-  // this lane's query chunk is re-read from L1 each iteration
-  const float* q = a.q;
-  int cnt = 0;
-  float T = __int_as_float(0x7f800000);  // the warp's own k-th (when full)
-  unsigned long long n_rows = 0, n_chunks = 0, n_pruned = 0, n_leaves = 0, n_done = 0;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const float B = __int_as_float((int)ld_volatile(a.bound));
+  // LB_SAX is a lower bound of the exact distance; the margin covers the
+  // float rounding of both sides so that no true neighbour is dropped.
+  const float Bs = __fadd_rn(__fmul_rn(B, 1.0009765625f), 1e-6f);
+  const float ratio = (float)(a.L / HG_PAA_SEGMENTS);
+  unsigned long long n_rows = 0, n_pruned = 0, n_leaves = 0;
   int c = 0;
   for (uint32_t unit = gw; unit < total; unit += nwarps) {
-    uint64_t lstart;
-    uint32_t lsize;
-    float lbv;
-    uint32_t tile_in;
-    if (a.pscan) {
-      lstart = 0;
-      lsize = (uint32_t)(a.nrows < 0xffffffffull ? a.nrows : 0xffffffffull);
-      lbv = 0.0f;
-      tile_in = unit;
-    } else {
-      // candidate index: largest c with unit_prefix[c] <= unit (c only grows)
-      int lo = c, hi = ncand - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (a.unit_prefix[mid] <= unit) lo = mid;
-        else hi = mid - 1;
-      }
-      c = lo;
-      const int leaf = a.cand[c];
-      lstart = a.leaf_start[leaf];
-      lsize = a.leaf_size[leaf];
-      lbv = a.cand_lb[c];
-      tile_in = unit - a.unit_prefix[c];
-    }
-    float B = fminf(T, __int_as_float((int)ld_volatile(a.bound)));
-    if (lbv > B) break;  // candidates are in ascending LB order
+    c = unit_candidate(a.unit_prefix, ncand, c, unit);
+    if (a.cand_lb[c] > B) break;  // candidates are in ascending LB order
+    const int leaf = a.cand[c];
+    const uint64_t lstart = a.leaf_start[leaf];
+    const uint32_t lsize = a.leaf_size[leaf];
+    const uint32_t tile_in = unit - a.unit_prefix[c];
     if (tile_in == 0) ++n_leaves;
     const uint64_t row = (((lstart >> 5) + tile_in) << 5) + lane;
-    bool alive = row >= lstart && row < lstart + lsize && row < a.nrows;
-    if (alive) ++n_rows;
-    if (a.use_lbsax && alive) {
+    bool pass = row >= lstart && row < lstart + lsize && row < a.nrows;
+    if (pass) ++n_rows;
+    if (pass && a.use_lbsax) {
       const uint4 w = reinterpret_cast<const uint4*>(a.sax)[row];
       const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
       float d[16];
@@ -584,90 +537,154 @@ __global__ void __launch_bounds__(kScanThreads, 4) k_scan(ScanArgs a) {
       float s8[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) s8[j] = __fadd_rn(d[j], d[j + 8]);
-      const float lbs = __fmul_rn(hg_hsum8(s8[0], s8[1], s8[2], s8[3], s8[4], s8[5], s8[6], s8[7]),
-                                  (float)(a.L / HG_PAA_SEGMENTS));
-      // LB_SAX is a lower bound of the exact distance; the margin covers the
-      // float rounding of both sides so no true neighbour is skipped.
-      if (lbs > __fadd_rn(__fmul_rn(B, 1.0009765625f), 1e-6f)) {
-        alive = false;
+      const float lbs = __fmul_rn(hg_hsum8(s8[0], s8[1], s8[2], s8[3], s8[4], s8[5], s8[6], s8[7]), ratio);
+      if (lbs > Bs) {
+        pass = false;
         ++n_pruned;
       }
     }
-    float dist = 0.0f;
-    int ch = 0;
-    const float* base = a.rows + tile_off(row, 0, nch);
-    while (__any_sync(HG_FULL, alive) && ch < nch) {
-      float4 x0 = make_float4(0.f, 0.f, 0.f, 0.f), x1 = x0, y0 = x0, y1 = x0;
-      const bool two = ch + 1 < nch;
-      if (alive) {
-        const float4* p = reinterpret_cast<const float4*>(base + ((uint64_t)ch << 8));
-        x0 = __ldcs(p);
-        x1 = __ldcs(p + 1);
-        if (two) {
-          y0 = __ldcs(p + 64);
-          y1 = __ldcs(p + 65);
-        }
-      }
-      if (alive) {
-        const float4 q0 = *reinterpret_cast<const float4*>(q + ch * 8);
-        const float4 q1 = *reinterpret_cast<const float4*>(q + ch * 8 + 4);
-        const float qa[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-        const float xa[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-        dist = __fadd_rn(dist, hg_chunk_d2(qa, xa));
-        ++n_chunks;
-        if (dist > B) alive = false;
-      }
-      if (alive && two) {
-        const float4 q0 = *reinterpret_cast<const float4*>(q + ch * 8 + 8);
-        const float4 q1 = *reinterpret_cast<const float4*>(q + ch * 8 + 12);
-        const float qa[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-        const float ya[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
-        dist = __fadd_rn(dist, hg_chunk_d2(qa, ya));
-        ++n_chunks;
-        if (dist > B) alive = false;
-      }
-      ch += 2;
-      if ((ch & 15) == 0) B = fminf(T, __int_as_float((int)ld_volatile(a.bound)));
-    }
-    // rows still alive completed every chunk: dist is the full distance.
-    // The list holds at most k entries between tiles (it is compacted as
-    // soon as it reaches k), so up to 32 new entries always fit.
-    if (alive) ++n_done;
-    const bool take = alive && dist <= B && dist <= T;
-    const uint32_t m = __ballot_sync(HG_FULL, take);
+    const uint32_t m = __ballot_sync(HG_FULL, pass);
     if (m) {
-      if (take) {
-        const int r = __popc(m & ((1u << lane) - 1));
-        const uint32_t id = (uint32_t)a.ids[row];
-        list[cnt + r] = ((unsigned long long)__float_as_uint(dist) << 32) | id;
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(a.list_count, (uint32_t)__popc(m));
+      base = __shfl_sync(HG_FULL, base, 0);
+      if (pass) a.list[base + __popc(m & ((1u << lane) - 1))] = (uint32_t)row;
+    }
+  }
+  // warp totals
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    n_rows += __shfl_xor_sync(HG_FULL, n_rows, o);
+    n_pruned += __shfl_xor_sync(HG_FULL, n_pruned, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&a.stats[0], n_rows);
+    atomicAdd(&a.stats[2], n_pruned);
+    atomicAdd(&a.stats[3], n_leaves);
+  }
+}
+
+// Stage 2 of the leaf scan: the early-abandoning squared distance
+// (ts_euclidean_distance_SIMD, ts.c:83-109) over a row list.  Every lane owns
+// one row at a time and advances it one 128-byte line (four 8-float chunks)
+// per step, testing the running sum against the k-th bound after each chunk
+// (a strict test: a row whose distance equals the bound is finished, so ties
+// keep the lowest id).  A lane whose row abandoned or finished takes the next
+// row from the warp's batch of 32 list entries, and the warp fetches batches
+// from a global counter, so lanes stay busy until the list is exhausted.
+constexpr int kEdThreads = 256;
+__global__ void __launch_bounds__(kEdThreads, 3) k_ed_stream(EdArgs a) {
+  __shared__ unsigned long long lists[kEdThreads / 32][kWarpListCap];
+  extern __shared__ float4 qs4[];  // L/4 float4 of the query
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  unsigned long long* list = lists[wib];
+  for (int i = lane; i < kWarpListCap; i += 32) list[i] = ~0ull;
+  for (int i = threadIdx.x; i < (a.L >> 2); i += blockDim.x) qs4[i] = reinterpret_cast<const float4*>(a.q)[i];
+  __syncthreads();
+  const int nch = a.L >> 3;
+  uint64_t first = a.ident_first;
+  uint32_t total;
+  if (a.list) {
+    total = *a.list_count;
+  } else if (a.ident_leaf) {
+    const int leaf = *a.ident_leaf;
+    first = a.leaf_start[leaf];
+    total = a.leaf_size[leaf];
+  } else {
+    total = (uint32_t)a.ident_count;
+  }
+  int cnt = 0;
+  float T = __int_as_float(0x7f800000);
+  float B = __int_as_float((int)ld_volatile(a.bound));
+  uint32_t bbase = 0, bused = 0, bleft = 0;
+  bool more = true;
+  bool valid = false;
+  uint32_t row = 0;
+  int ch = 0;
+  float dist = 0.0f;
+  unsigned long long n_chunks = 0, n_done = 0, n_rows = 0;
+  const uint32_t lt = (1u << lane) - 1;
+  for (int iter = 1;; ++iter) {
+    // refill the lanes without a row from the warp's batch
+    uint32_t need = __ballot_sync(HG_FULL, !valid);
+    while (need && more) {
+      if (bleft == 0) {
+        uint32_t b = 0;
+        if (lane == 0) b = atomicAdd(a.head, 32u);
+        b = __shfl_sync(HG_FULL, b, 0);
+        if (b >= total) {
+          more = false;
+          break;
+        }
+        bbase = b;
+        bused = 0;
+        bleft = min(32u, total - b);
       }
-      cnt += __popc(m);
-      __syncwarp();
-      if (cnt >= a.k) {
-        cnt = warp_compact(list, cnt, a.k);
-        if (cnt == a.k) {
-          const float nt = __uint_as_float((uint32_t)(list[a.k - 1] >> 32));
-          if (nt < T) {
-            T = nt;
-            if (lane == 0) atomicMin(a.bound, __float_as_uint(T));
-          }
+      const int take = min(__popc(need), (int)bleft);
+      const int r = __popc(need & lt);
+      if (!valid && r < take) {
+        const uint32_t idx = bbase + bused + r;
+        row = a.list ? a.list[idx] : (uint32_t)(first + idx);
+        valid = true;
+        dist = 0.0f;
+        ch = 0;
+        ++n_rows;
+      }
+      bused += take;
+      bleft -= take;
+      need = __ballot_sync(HG_FULL, !valid);
+    }
+    if (!__any_sync(HG_FULL, valid)) break;
+    bool finished = false;
+    if (valid) {
+      const float4* x = reinterpret_cast<const float4*>(a.rows + (uint64_t)row * a.L) + (ch << 1);
+      const int nc = min(4, nch - ch);
+      float4 v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = (j < 2 * nc) ? __ldcs(x + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        if (cc < nc && valid) {
+          const float4 q0 = qs4[(ch + cc) * 2], q1 = qs4[(ch + cc) * 2 + 1];
+          const float qa[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+          const float xa[8] = {v[2 * cc].x, v[2 * cc].y, v[2 * cc].z, v[2 * cc].w,
+                               v[2 * cc + 1].x, v[2 * cc + 1].y, v[2 * cc + 1].z, v[2 * cc + 1].w};
+          dist = __fadd_rn(dist, hg_chunk_d2(qa, xa));
+          ++n_chunks;
+          if (dist > B) valid = false;  // abandoned
+        }
+      }
+      if (valid) {
+        ch += nc;
+        if (ch >= nch) {
+          finished = true;
+          valid = false;
         }
       }
     }
+    if (finished) ++n_done;
+    const bool take = finished && dist <= B && dist <= T;
+    warp_list_add(list, cnt, T, a.k, a.bound, take, dist, take ? (uint32_t)a.ids[row] : 0u);
+    B = fminf(B, T);
+    if ((iter & 7) == 0) B = fminf(B, __int_as_float((int)ld_volatile(a.bound)));
   }
   cnt = warp_compact(list, cnt, a.k);
   if (cnt == a.k && lane == 0) atomicMin(a.bound, (uint32_t)(list[a.k - 1] >> 32));
+  const uint32_t gw = blockIdx.x * (kEdThreads / 32) + wib;
   unsigned long long* out = a.parts + (uint64_t)gw * kWarpListCap;
   for (int i = lane; i < cnt; i += 32) out[i] = list[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    n_chunks += __shfl_xor_sync(HG_FULL, n_chunks, o);
+    n_done += __shfl_xor_sync(HG_FULL, n_done, o);
+    n_rows += __shfl_xor_sync(HG_FULL, n_rows, o);
+  }
   if (lane == 0) {
     a.part_count[gw] = cnt;
-    atomicAdd(&a.stats[0], n_rows);
-    atomicAdd(&a.stats[3], n_leaves);
+    atomicAdd(&a.stats[1], n_chunks);
+    atomicAdd(&a.stats[4], n_done);
+    atomicAdd(&a.stats[5], n_rows);
   }
-  // per-lane counters
-  atomicAdd(&a.stats[1], n_chunks);
-  atomicAdd(&a.stats[2], n_pruned);
-  atomicAdd(&a.stats[4], n_done);
 }
 
 // Merges the per-warp lists (and the current top-k, passed as part -1) into
@@ -810,10 +827,10 @@ __global__ void k_generate_queries(uint64_t seed, const float* data, uint64_t n,
 
 static inline unsigned blocks_for(uint64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-int scan_grid_blocks(int device) {
+int sm_count(int device) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  return sms * 4;
+  return sms;
 }
 
 cudaError_t launch_route_rows(const float* X, int L, const uint32_t* rows, uint64_t first, uint32_t count,
@@ -841,44 +858,27 @@ cudaError_t launch_route_flags(const float* X, int L, const uint32_t* members, u
   return cudaGetLastError();
 }
 
-cudaError_t launch_gather_tiles(const float* X, int L, const uint32_t* perm, uint64_t n, float* tiles,
-                                cudaStream_t s) {
-  const uint64_t ntiles = (n + 31) / 32;
-  const uint64_t threads = ntiles * 32 * (L / 8);
+cudaError_t launch_gather_rows(const float* X, int L, const uint32_t* perm, uint64_t n, float* rows,
+                               cudaStream_t s) {
+  const uint64_t threads = n * (L / 4);
   if (!threads) return cudaSuccess;
-  k_gather_tiles<<<blocks_for(threads, 256), 256, 0, s>>>(X, L, perm, n, tiles);
+  k_gather_rows<<<blocks_for(threads, 256), 256, 0, s>>>(X, L, perm, n, rows);
   return cudaGetLastError();
 }
 
-cudaError_t launch_tiles_from_rowmajor(const float* rm, int L, uint64_t first, uint64_t count, float* tiles,
-                                       cudaStream_t s) {
-  const uint64_t threads = (count + 31) / 32 * 32 * (L / 8);
-  if (!threads) return cudaSuccess;
-  k_tiles_from_rowmajor<<<blocks_for(threads, 256), 256, 0, s>>>(rm, L, first, count, tiles);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_rowmajor_from_tiles(const float* tiles, int L, uint64_t first, uint64_t count, float* rm,
-                                       cudaStream_t s) {
-  const uint64_t threads = count * (L / 8);
-  if (!threads) return cudaSuccess;
-  k_rowmajor_from_tiles<<<blocks_for(threads, 256), 256, 0, s>>>(tiles, L, first, count, rm);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_sax_rows(const float* tiles, int L, uint64_t n, const float* bp, uint8_t* sax,
+cudaError_t launch_sax_rows(const float* rows, int L, uint64_t n, const float* bp, uint8_t* sax,
                             cudaStream_t s) {
   if (!n) return cudaSuccess;
-  k_sax_rows<<<blocks_for(n, 128), 128, 0, s>>>(tiles, L, n, bp, sax);
+  k_sax_rows<<<blocks_for(n, 128), 128, 0, s>>>(rows, L, n, bp, sax);
   return cudaGetLastError();
 }
 
 cudaError_t launch_query_prep(const float* q, int L, Tree t, const uint64_t* leaf_start,
                               const uint32_t* leaf_size, int* approx_leaf, float* paa, int* cand,
                               float* cand_lb, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
-                              int* topk_count, cudaStream_t s) {
+                              int* topk_count, uint32_t* counters, cudaStream_t s) {
   k_query_prep<<<1, 32, 0, s>>>(q, L, t, leaf_start, leaf_size, approx_leaf, paa, cand, cand_lb, cand_count,
-                                unit_prefix, bound, topk_count);
+                                unit_prefix, bound, topk_count, counters);
   return cudaGetLastError();
 }
 
@@ -917,13 +917,23 @@ cudaError_t launch_select_sort(const float* lb, int nleaves, const uint32_t* bou
 }
 
 cudaError_t launch_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
-                              int* topk_count, cudaStream_t s) {
-  k_pscan_prep<<<1, 32, 0, s>>>(nrows, cand_count, unit_prefix, bound, topk_count);
+                              int* topk_count, uint32_t* counters, cudaStream_t s) {
+  k_pscan_prep<<<1, 32, 0, s>>>(nrows, cand_count, unit_prefix, bound, topk_count, counters);
   return cudaGetLastError();
 }
 
-cudaError_t launch_scan(const ScanArgs& a, int blocks, cudaStream_t s) {
-  k_scan<<<blocks, kScanThreads, 0, s>>>(a);
+cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s) {
+  k_lbsax_filter<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_ed_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
+    attr = true;
+  }
+  k_ed_stream<<<blocks, kEdThreads, sizeof(float) * a.L, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -6,9 +6,7 @@
 
 namespace hg {
 
-// scan block geometry: 8 warps, one 32-row tile per warp iteration
-constexpr int kScanWarps = 8;
-constexpr int kScanThreads = kScanWarps * 32;
+constexpr int kEdWarps = 8;  // warps per block of the distance kernel
 constexpr int kWarpListCap = 256;  // per-warp candidate buffer (k <= kWarpListCap - 32)
 constexpr int kMaxK = kWarpListCap - 32;
 constexpr int kMaxLeavesSort = 8192;  // single-CTA radix sort capacity
@@ -29,9 +27,8 @@ struct Tree {
   int root;  // >= 0 internal node, < 0 the leaf ~root
 };
 
-struct ScanArgs {
-  const float* rows;  // chunk-interleaved tiles
-  const int64_t* ids;
+// Stage 1 of the leaf scan: candidate leaves -> LB_SAX survivors.
+struct FilterArgs {
   const uint8_t* sax;
   const float* bp;
   int L;
@@ -41,20 +38,38 @@ struct ScanArgs {
   const int* cand;
   const float* cand_lb;
   const int* cand_count;
-  const uint32_t* unit_prefix;  // exclusive prefix of tiles per candidate, [cand_count] = total
-  int pscan;                    // 1: every tile of the whole matrix, no leaves
-  const float* q;
+  const uint32_t* unit_prefix;  // exclusive prefix of 32-row units per candidate
   const float* paa;
   int use_lbsax;
-  int k;
-  uint32_t* bound;  // float bits of the running k-th bound (atomicMin)
-  unsigned long long* parts;  // per-warp sorted lists (kWarpListCap stride)
-  int* part_count;
-  unsigned long long* stats;  // [0] rows visited [1] chunks loaded [2] lbsax pruned [3] leaves scanned
-                              // [4] rows completed
+  const uint32_t* bound;
+  uint32_t* list;        // surviving rows
+  uint32_t* list_count;  // must be 0 before the launch
+  unsigned long long* stats;  // [0] rows considered [2] rows pruned by LB_SAX [3] leaves visited
 };
 
-int scan_grid_blocks(int device);
+// Stage 2: early-abandoning distances over a row list (or a row range).
+struct EdArgs {
+  const float* rows;  // leaf-ordered, row-major
+  const int64_t* ids;
+  int L;
+  const uint32_t* list;        // rows; NULL: the range below
+  const uint32_t* list_count;
+  const int* ident_leaf;       // range = this leaf's rows (device pointer), else
+  uint64_t ident_first;        //   [ident_first, ident_first + ident_count)
+  uint64_t ident_count;
+  const uint64_t* leaf_start;
+  const uint32_t* leaf_size;
+  uint32_t* head;              // batch counter, must be 0 before the launch
+  const float* q;
+  int k;
+  uint32_t* bound;             // float bits of the running k-th bound (atomicMin)
+  unsigned long long* parts;   // per-warp sorted lists (kWarpListCap stride)
+  int* part_count;
+  unsigned long long* stats;   // [1] chunks computed [4] rows completed [5] rows started
+};
+
+int sm_count(int device);
+
 
 // build
 cudaError_t launch_route_rows(const float* X, int L, const uint32_t* rows, uint64_t first, uint32_t count,
@@ -64,20 +79,16 @@ cudaError_t launch_sketch_members(const float* X, int L, const uint32_t* members
                                   cudaStream_t s);
 cudaError_t launch_route_flags(const float* X, int L, const uint32_t* members, uint32_t count, short from,
                                short to, int idx, float value, uint8_t* flags, cudaStream_t s);
-cudaError_t launch_gather_tiles(const float* X, int L, const uint32_t* perm, uint64_t n, float* tiles,
-                                cudaStream_t s);
-cudaError_t launch_tiles_from_rowmajor(const float* rm, int L, uint64_t first, uint64_t count, float* tiles,
-                                       cudaStream_t s);
-cudaError_t launch_rowmajor_from_tiles(const float* tiles, int L, uint64_t first, uint64_t count, float* rm,
-                                       cudaStream_t s);
-cudaError_t launch_sax_rows(const float* tiles, int L, uint64_t n, const float* bp, uint8_t* sax,
+cudaError_t launch_gather_rows(const float* X, int L, const uint32_t* perm, uint64_t n, float* rows,
+                               cudaStream_t s);
+cudaError_t launch_sax_rows(const float* rows, int L, uint64_t n, const float* bp, uint8_t* sax,
                             cudaStream_t s);
 
 // queries
 cudaError_t launch_query_prep(const float* q, int L, Tree t, const uint64_t* leaf_start,
                               const uint32_t* leaf_size, int* approx_leaf, float* paa, int* cand,
                               float* cand_lb, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
-                              int* topk_count, cudaStream_t s);
+                              int* topk_count, uint32_t* counters, cudaStream_t s);
 cudaError_t launch_route_queries(const float* Q, int nq, int L, Tree t, int* leaf_out, cudaStream_t s);
 cudaError_t launch_leaf_lb(const float* q, int L, int nleaves, const int* seg_off, const short* points,
                            const float* sk, float* lb_out, cudaStream_t s);
@@ -85,8 +96,9 @@ cudaError_t launch_select_sort(const float* lb, int nleaves, const uint32_t* bou
                                const uint64_t* leaf_start, const uint32_t* leaf_size, int* cand,
                                float* cand_lb, int* cand_count, uint32_t* unit_prefix, cudaStream_t s);
 cudaError_t launch_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
-                              int* topk_count, cudaStream_t s);
-cudaError_t launch_scan(const ScanArgs& a, int blocks, cudaStream_t s);
+                              int* topk_count, uint32_t* counters, cudaStream_t s);
+cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s);
+cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s);
 cudaError_t launch_merge(const unsigned long long* parts, const int* part_count, int nparts, int k,
                          unsigned long long* topk, int* topk_count, uint32_t* bound, int* err,
                          cudaStream_t s);

@@ -64,13 +64,16 @@ typedef struct {
   uint64_t queries;
   uint64_t leaves_scanned;    /* Query_total_loaded_nodes_count, summed */
   uint64_t rows_visited;      /* rows whose distance computation started */
-  uint64_t rows_lbsax_pruned; /* rows skipped by the per-row LB_SAX bound */
+  uint64_t rows_lbsax_pruned; /* rows of candidate leaves skipped by LB_SAX */
   uint64_t chunks_loaded;     /* 32-byte chunks of raw data read by the scan */
   uint64_t candidate_leaves;  /* leaves with LB_EAPCA <= k-th bound */
   double device_ms;           /* device time of the call (CUDA events) */
   uint64_t rows_completed;    /* rows whose full distance was computed */
-  uint64_t scan_launches;     /* leaf-scan kernel launches (profile = 1) */
+  uint64_t scan_launches;     /* distance-kernel launches (profile = 1) */
   double scan_ms;             /* their summed device time (profile = 1) */
+  uint64_t rows_considered;   /* rows of candidate leaves seen by the LB_SAX filter */
+  uint64_t filter_launches;   /* LB_SAX filter launches (profile = 1) */
+  double filter_ms;           /* their summed device time (profile = 1) */
 } hg_query_stats;
 
 /* Search mode. */
@@ -81,7 +84,8 @@ typedef struct {
   int mode;           /* HG_MODE_* */
   int use_lb_sax;     /* 1: per-row LB_SAX filter before the distance */
   int profile;        /* 1: time every leaf-scan launch with CUDA events */
-  int reserved[5];
+  int approx_blocks;  /* blocks of the approximate-leaf scan (0 = one per SM) */
+  int reserved[4];
 } hg_knn_opts;
 
 /* ---- status ----------------------------------------------------------- */
