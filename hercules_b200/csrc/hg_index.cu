@@ -1003,8 +1003,6 @@ static hg_status ensure_scratch(hg_index* ix, int k) {
 
 static hg::Tree index_tree(const hg_index* ix) { return hg::Tree{ix->d.nodes, ix->d.root}; }
 
-// One query through the plain path: approximate leaf, LB_EAPCA of every
-// leaf, scan of the approximate leaf, candidates by LB, scan, merge.
 using ProfEvents = std::vector<std::pair<cudaEvent_t, cudaEvent_t>>;
 
 struct Prof {
@@ -1038,6 +1036,11 @@ static double drain(ProfEvents& p) {
   p.clear();
   return ms;
 }
+
+// One query through the plain path: approximate leaf, LB_EAPCA of every
+// leaf, scan of the approximate leaf, candidates by LB, scan, merge.
+
+
 
 // One query through the plain path:
 //   route + PAA (approximate_knn_search's traversal) -> LB_EAPCA of every

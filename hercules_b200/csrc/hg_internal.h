@@ -69,7 +69,7 @@ struct QueryScratch {
   int* topk_count = nullptr;
   uint64_t* topk_row = nullptr;   // kmax leaf-ordered rows of the answers
   float* paa = nullptr;           // 16
-  unsigned long long* stats = nullptr;  // see EdArgs / FilterArgs
+  unsigned long long* stats = nullptr;  // see ScanArgs
   uint32_t* list = nullptr;       // LB_SAX survivors (rows), n entries
   int* err = nullptr;             // device error flag
 };

@@ -304,7 +304,8 @@ __global__ void __launch_bounds__(kSortThreads) k_select_sort(const float* __res
   const int t = threadIdx.x;
   const float B = __int_as_float((int)ld_volatile(bound));
   const int approx = *approx_leaf;
-  // 1. select (order preserving compaction)
+  // 1. select the non-empty leaves within the bound, the approximate leaf
+  //    excepted (it was scanned first), order preserving
   const int per = (nleaves + kSortThreads - 1) / kSortThreads;
   const int b0 = min(nleaves, t * per), b1 = min(nleaves, b0 + per);
   uint32_t mine = 0;
@@ -317,7 +318,7 @@ __global__ void __launch_bounds__(kSortThreads) k_select_sort(const float* __res
   for (int i = b0; i < b1; ++i) {
     const float l = lb[i];
     if (leaf_size[i] > 0 && i != approx && !(l > B)) {
-      keys0[pos] = (l == l) ? __float_as_uint(l) : 0u;  // NaN bound: never pruned, scanned first
+      keys0[pos] = (l == l) ? __float_as_uint(l) : 0u;  // a NaN bound never prunes
       vals0[pos] = (uint32_t)i;
       ++pos;
     }
@@ -492,70 +493,144 @@ __device__ __forceinline__ int unit_candidate(const uint32_t* unit_prefix, int n
   return lo;
 }
 
-// Stage 1 of the leaf scan: walk the candidate leaves in LB_EAPCA order in
-// 32-row units, stop at the first leaf whose LB exceeds the bound, compute
-// each row's LB_SAX from its 16-byte iSAX word (minidist_paa_to_isax_raw_SIMD,
-// sax.c:310-479) and append the rows that can still hold a neighbour to a
-// compact list.
-__global__ void __launch_bounds__(256) k_lbsax_filter(FilterArgs a) {
-  __shared__ float sbp[256];
-  __shared__ float spaa[16];
+// ---------------------------------------------------------------------------
+// The leaf scan (exact_de_knn_search's refine loop, hercules_query_engine.c:
+// 2391-2425, with the per-row LB_SAX test of the reference's SIMS path,
+// :2183-2211) runs as two kernels: a streaming LB_SAX filter that turns the
+// candidate leaves into a compact list of surviving rows, and a distance
+// stream over that list.
+// ---------------------------------------------------------------------------
+
+// Stage 1.  Work: the candidate leaves in ascending LB_EAPCA order, cut into
+// 32-row units (32-aligned rows; a unit's rows outside its leaf are skipped).
+// Block b owns a contiguous range of units and its 8 warps take 4 units each
+// per iteration (1024 rows, 16 KiB of iSAX words in flight per block); the
+// block stops at the first leaf whose LB exceeds the bound.  Each row's
+// LB_SAX comes from its 16-byte iSAX word (minidist_paa_to_isax_raw_SIMD,
+// sax.c:310-479); survivors are appended with one atomicAdd per block
+// iteration.
+constexpr int kFilterThreads = 256;
+constexpr int kFilterUnits = 4;
+__global__ void __launch_bounds__(kFilterThreads) k_lbsax_filter(FilterArgs a) {
+  constexpr int W = kFilterThreads / 32;
+  // per-query table of the per-segment LB_SAX terms: dtab[j][s] is the
+  // squared gap between the query's PAA value j and symbol s's region
+  __shared__ float dtab[HG_PAA_SEGMENTS][HG_SAX_CARD];
+  __shared__ uint32_t wcount[W];
+  __shared__ uint32_t wbase[W];
+  __shared__ int s_stop;
   if (a.use_lbsax) {
-    for (int i = threadIdx.x; i < 255; i += blockDim.x) sbp[i] = a.bp[i];
-    if (threadIdx.x < 16) spaa[threadIdx.x] = a.paa[threadIdx.x];
+    for (int i = threadIdx.x; i < HG_PAA_SEGMENTS * HG_SAX_CARD; i += blockDim.x)
+      dtab[i >> 8][i & 255] = hg_lb_sax_lane(a.paa[i >> 8], i & 255, a.bp);
   }
+  if (threadIdx.x == 0) s_stop = 0;
   __syncthreads();
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1;
   const int ncand = *a.cand_count;
   const uint32_t total = a.unit_prefix[ncand];
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t per_block = (total + gridDim.x - 1) / gridDim.x;
+  const uint32_t u0 = blockIdx.x * per_block;
+  const uint32_t u1 = min(total, u0 + per_block);
+  if (u0 >= u1) return;
   const float B = __int_as_float((int)ld_volatile(a.bound));
   // LB_SAX is a lower bound of the exact distance; the margin covers the
   // float rounding of both sides so that no true neighbour is dropped.
   const float Bs = __fadd_rn(__fmul_rn(B, 1.0009765625f), 1e-6f);
   const float ratio = (float)(a.L / HG_PAA_SEGMENTS);
+  int c = unit_candidate(a.unit_prefix, ncand, 0, u0);
+  int cur = -1;
+  uint64_t lstart = 0, lend = 0;
+  float clb = 0.0f;
   unsigned long long n_rows = 0, n_pruned = 0, n_leaves = 0;
-  int c = 0;
-  for (uint32_t unit = gw; unit < total; unit += nwarps) {
-    c = unit_candidate(a.unit_prefix, ncand, c, unit);
-    if (a.cand_lb[c] > B) break;  // candidates are in ascending LB order
-    const int leaf = a.cand[c];
-    const uint64_t lstart = a.leaf_start[leaf];
-    const uint32_t lsize = a.leaf_size[leaf];
-    const uint32_t tile_in = unit - a.unit_prefix[c];
-    if (tile_in == 0) ++n_leaves;
-    const uint64_t row = (((lstart >> 5) + tile_in) << 5) + lane;
-    bool pass = row >= lstart && row < lstart + lsize && row < a.nrows;
-    if (pass) ++n_rows;
-    if (pass && a.use_lbsax) {
-      const uint4 w = reinterpret_cast<const uint4*>(a.sax)[row];
-      const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
-      float d[16];
+  for (uint32_t base = u0; base < u1; base += W * kFilterUnits) {
+    uint32_t m[kFilterUnits];
+    uint64_t rr[kFilterUnits];
+    bool ok[kFilterUnits];
+    uint4 w[kFilterUnits];
+    bool stop = false;
 #pragma unroll
-      for (int j = 0; j < 16; ++j) d[j] = hg_lb_sax_lane(spaa[j], (ws[j >> 2] >> ((j & 3) * 8)) & 255, sbp);
-      float s8[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) s8[j] = __fadd_rn(d[j], d[j + 8]);
-      const float lbs = __fmul_rn(hg_hsum8(s8[0], s8[1], s8[2], s8[3], s8[4], s8[5], s8[6], s8[7]), ratio);
-      if (lbs > Bs) {
-        pass = false;
-        ++n_pruned;
+    for (int j = 0; j < kFilterUnits; ++j) {
+      const uint32_t unit = base + wib * kFilterUnits + j;
+      ok[j] = false;
+      rr[j] = 0;
+      if (unit < u1 && !stop) {
+        while (c + 1 < ncand && a.unit_prefix[c + 1] <= unit) ++c;
+        if (c != cur) {
+          cur = c;
+          const int leaf = a.cand[c];
+          lstart = a.leaf_start[leaf];
+          lend = lstart + a.leaf_size[leaf];
+          clb = a.cand_lb[c];
+        }
+        if (clb > B) {
+          stop = true;  // every later unit belongs to a leaf with a larger LB
+        } else {
+          const uint32_t tile_in = unit - a.unit_prefix[c];
+          if (tile_in == 0 && lane == 0) ++n_leaves;
+          rr[j] = (((lstart >> 5) + tile_in) << 5) + lane;
+          ok[j] = rr[j] >= lstart && rr[j] < lend;
+        }
       }
+      if (a.use_lbsax && ok[j]) w[j] = reinterpret_cast<const uint4*>(a.sax)[rr[j]];
     }
-    const uint32_t m = __ballot_sync(HG_FULL, pass);
-    if (m) {
-      uint32_t base = 0;
-      if (lane == 0) base = atomicAdd(a.list_count, (uint32_t)__popc(m));
-      base = __shfl_sync(HG_FULL, base, 0);
-      if (pass) a.list[base + __popc(m & ((1u << lane) - 1))] = (uint32_t)row;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int j = 0; j < kFilterUnits; ++j) {
+      bool pass = ok[j];
+      if (pass) ++n_rows;
+      if (pass && a.use_lbsax) {
+        const uint32_t ws[4] = {w[j].x, w[j].y, w[j].z, w[j].w};
+        float d[16];
+#pragma unroll
+        for (int t = 0; t < 16; ++t) d[t] = dtab[t][(ws[t >> 2] >> ((t & 3) * 8)) & 255];
+        float s8[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) s8[t] = __fadd_rn(d[t], d[t + 8]);
+        const float lbs = __fmul_rn(hg_hsum8(s8[0], s8[1], s8[2], s8[3], s8[4], s8[5], s8[6], s8[7]), ratio);
+        if (lbs > Bs) {
+          pass = false;
+          ++n_pruned;
+        }
+      }
+      m[j] = __ballot_sync(HG_FULL, pass);
+      cnt += __popc(m[j]);
     }
+    if (lane == 0) {
+      wcount[wib] = cnt;
+      if (stop) s_stop = 1;
+    }
+    __syncthreads();
+    if (wib == 0) {
+      const uint32_t v = lane < W ? wcount[lane] : 0u;
+      uint32_t x = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(HG_FULL, x, o);
+        if (lane >= o) x += y;
+      }
+      uint32_t blk = 0;
+      const uint32_t tot = __shfl_sync(HG_FULL, x, W - 1);
+      if (lane == 0 && tot) blk = atomicAdd(a.list_count, tot);
+      blk = __shfl_sync(HG_FULL, blk, 0);
+      if (lane < W) wbase[lane] = blk + x - v;
+    }
+    __syncthreads();
+    uint32_t pos = wbase[wib];
+#pragma unroll
+    for (int j = 0; j < kFilterUnits; ++j) {
+      if ((m[j] >> lane) & 1u) a.list[pos + __popc(m[j] & lt)] = (uint32_t)rr[j];
+      pos += __popc(m[j]);
+    }
+    const int st = s_stop;
+    __syncthreads();  // s_stop and wcount are reused by the next iteration
+    if (st) break;
   }
-  // warp totals
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     n_rows += __shfl_xor_sync(HG_FULL, n_rows, o);
     n_pruned += __shfl_xor_sync(HG_FULL, n_pruned, o);
+    n_leaves += __shfl_xor_sync(HG_FULL, n_leaves, o);
   }
   if (lane == 0) {
     atomicAdd(&a.stats[0], n_rows);
@@ -564,18 +639,22 @@ __global__ void __launch_bounds__(256) k_lbsax_filter(FilterArgs a) {
   }
 }
 
-// Stage 2 of the leaf scan: the early-abandoning squared distance
-// (ts_euclidean_distance_SIMD, ts.c:83-109) over a row list.  Every lane owns
-// one row at a time and advances it one 128-byte line (four 8-float chunks)
-// per step, testing the running sum against the k-th bound after each chunk
-// (a strict test: a row whose distance equals the bound is finished, so ties
-// keep the lowest id).  A lane whose row abandoned or finished takes the next
-// row from the warp's batch of 32 list entries, and the warp fetches batches
-// from a global counter, so lanes stay busy until the list is exhausted.
+// Stage 2: the early-abandoning squared distance (ts_euclidean_distance_SIMD,
+// ts.c:83-109) over a row list, or over a row range when there is no list.
+// Every lane owns one row at a time and advances it one 128-byte line (four
+// 8-float chunks) per step, testing the running sum against the k-th bound
+// after each chunk (a strict test: a row whose distance equals the bound is
+// finished, so ties keep the lowest id).  A lane whose row abandoned or
+// finished takes the next row of its warp's batch.  Warp w of W owns the
+// 32-entry batches w, w + W, w + 2W, ... of the list; the entries of the
+// next batch are loaded while the current one is consumed.  Finished rows
+// within the bound enter the warp's top-k list, which lowers the global
+// bound (atomicMin) once it holds k distances.
 constexpr int kEdThreads = 256;
 __global__ void __launch_bounds__(kEdThreads, 3) k_ed_stream(EdArgs a) {
-  __shared__ unsigned long long lists[kEdThreads / 32][kWarpListCap];
-  extern __shared__ float4 qs4[];  // L/4 float4 of the query
+  constexpr int W = kEdThreads / 32;
+  __shared__ unsigned long long lists[W][kWarpListCap];
+  extern __shared__ float4 qs4[];  // the query, L/4 float4
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   unsigned long long* list = lists[wib];
   for (int i = lane; i < kWarpListCap; i += 32) list[i] = ~0ull;
@@ -593,48 +672,59 @@ __global__ void __launch_bounds__(kEdThreads, 3) k_ed_stream(EdArgs a) {
   } else {
     total = (uint32_t)a.ident_count;
   }
+  const uint32_t nwarps = gridDim.x * W;
+  const uint32_t gw = blockIdx.x * W + wib;
+  const uint32_t lt = (1u << lane) - 1;
+  // batch b of this warp covers entries [(gw + b * nwarps) * 32, +32)
+  auto entry = [&](uint32_t batch) -> uint32_t {
+    const uint64_t idx = (uint64_t)batch * 32 + lane;
+    if (idx >= total) return 0xffffffffu;
+    return a.list ? a.list[idx] : (uint32_t)(first + idx);
+  };
+  uint32_t batch = gw;
+  uint32_t cur = entry(batch);  // lane j holds entry j of the current batch
+  uint32_t cur_n = batch * 32ull < total ? min(32u, total - batch * 32) : 0u;
+  uint32_t cur_used = 0;
+  batch += nwarps;
+  uint32_t nxt = entry(batch);
+  uint32_t nxt_n = (uint64_t)batch * 32 < total ? min(32u, total - batch * 32) : 0u;
+
   int cnt = 0;
   float T = __int_as_float(0x7f800000);
   float B = __int_as_float((int)ld_volatile(a.bound));
-  uint32_t bbase = 0, bused = 0, bleft = 0;
-  bool more = true;
   bool valid = false;
   uint32_t row = 0;
   int ch = 0;
   float dist = 0.0f;
   unsigned long long n_chunks = 0, n_done = 0, n_rows = 0;
-  const uint32_t lt = (1u << lane) - 1;
   for (int iter = 1;; ++iter) {
-    // refill the lanes without a row from the warp's batch
+    // refill the lanes without a row
     uint32_t need = __ballot_sync(HG_FULL, !valid);
-    while (need && more) {
-      if (bleft == 0) {
-        uint32_t b = 0;
-        if (lane == 0) b = atomicAdd(a.head, 32u);
-        b = __shfl_sync(HG_FULL, b, 0);
-        if (b >= total) {
-          more = false;
-          break;
-        }
-        bbase = b;
-        bused = 0;
-        bleft = min(32u, total - b);
+    while (need) {
+      if (cur_used == cur_n) {
+        if (nxt_n == 0) break;
+        cur = nxt;
+        cur_n = nxt_n;
+        cur_used = 0;
+        batch += nwarps;
+        nxt = entry(batch);  // loaded while the current batch is consumed
+        nxt_n = (uint64_t)batch * 32 < total ? min(32u, total - batch * 32) : 0u;
       }
-      const int take = min(__popc(need), (int)bleft);
+      const int take = min(__popc(need), (int)(cur_n - cur_used));
       const int r = __popc(need & lt);
+      const uint32_t got = __shfl_sync(HG_FULL, cur, (cur_used + (r < take ? r : 0)) & 31);
       if (!valid && r < take) {
-        const uint32_t idx = bbase + bused + r;
-        row = a.list ? a.list[idx] : (uint32_t)(first + idx);
+        row = got;
         valid = true;
         dist = 0.0f;
         ch = 0;
         ++n_rows;
       }
-      bused += take;
-      bleft -= take;
+      cur_used += take;
       need = __ballot_sync(HG_FULL, !valid);
     }
     if (!__any_sync(HG_FULL, valid)) break;
+    const uint32_t bnext = ((iter & 7) == 0) ? ld_volatile(a.bound) : 0x7f800000u;
     bool finished = false;
     if (valid) {
       const float4* x = reinterpret_cast<const float4*>(a.rows + (uint64_t)row * a.L) + (ch << 1);
@@ -665,12 +755,10 @@ __global__ void __launch_bounds__(kEdThreads, 3) k_ed_stream(EdArgs a) {
     if (finished) ++n_done;
     const bool take = finished && dist <= B && dist <= T;
     warp_list_add(list, cnt, T, a.k, a.bound, take, dist, take ? (uint32_t)a.ids[row] : 0u);
-    B = fminf(B, T);
-    if ((iter & 7) == 0) B = fminf(B, __int_as_float((int)ld_volatile(a.bound)));
+    B = fminf(fminf(B, T), __int_as_float((int)bnext));
   }
   cnt = warp_compact(list, cnt, a.k);
   if (cnt == a.k && lane == 0) atomicMin(a.bound, (uint32_t)(list[a.k - 1] >> 32));
-  const uint32_t gw = blockIdx.x * (kEdThreads / 32) + wib;
   unsigned long long* out = a.parts + (uint64_t)gw * kWarpListCap;
   for (int i = lane; i < cnt; i += 32) out[i] = list[i];
 #pragma unroll
@@ -923,7 +1011,7 @@ cudaError_t launch_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_pr
 }
 
 cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s) {
-  k_lbsax_filter<<<blocks, 256, 0, s>>>(a);
+  k_lbsax_filter<<<blocks, kFilterThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 
