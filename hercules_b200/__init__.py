@@ -89,6 +89,7 @@ _SIGS = [
     ("hg_generate_queries", ctypes.c_int, [ctypes.c_uint64, _P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
                                            _P, _P, _P, ctypes.c_int, ctypes.c_int]),
     ("hg_sax_breakpoints", ctypes.c_int, [_P]),
+    ("hg_pscan_noalloc", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint32, _P, ctypes.c_uint32, _P, _P, _P]),
 ]
 
 EXPORTED = [s[0] for s in _SIGS]
@@ -304,3 +305,10 @@ def sax_breakpoints():
     out = np.zeros(255, dtype=np.float32)
     _check(lib().hg_sax_breakpoints(_ptr(out)))
     return out
+
+
+def pscan_noalloc(rows_ptr, n, L, query_ptr, k, dist_ptr, id_ptr, stream=0):
+    """Allocation-free exact k-NN scan of a caller-owned device matrix
+    (hg_pscan_noalloc); all pointers are device addresses."""
+    _check(lib().hg_pscan_noalloc(ctypes.c_void_p(rows_ptr), n, L, ctypes.c_void_p(query_ptr), k,
+                                  ctypes.c_void_p(dist_ptr), ctypes.c_void_p(id_ptr), ctypes.c_void_p(stream)))

@@ -37,6 +37,8 @@ static hg_status set_error(hg_status s, const char* what) {
   return s;
 }
 
+void hg_record_error(const char* msg) { set_error(HG_OK, msg); }
+
 static hg_status cuda_fail(cudaError_t e, const char* where) {
   char buf[512];
   snprintf(buf, sizeof buf, "%s: %s", where, cudaGetErrorString(e));

@@ -650,7 +650,9 @@ __global__ void __launch_bounds__(kFilterThreads) k_lbsax_filter(FilterArgs a) {
 // next batch are loaded while the current one is consumed.  Finished rows
 // within the bound enter the warp's top-k list, which lowers the global
 // bound (atomicMin) once it holds k distances.
+// kRowIds: the id of a row is its row index (a matrix without an id map).
 constexpr int kEdThreads = 256;
+template <bool kRowIds>
 __global__ void __launch_bounds__(kEdThreads, 3) k_ed_stream(EdArgs a) {
   constexpr int W = kEdThreads / 32;
   __shared__ unsigned long long lists[W][kWarpListCap];
@@ -754,7 +756,8 @@ __global__ void __launch_bounds__(kEdThreads, 3) k_ed_stream(EdArgs a) {
     }
     if (finished) ++n_done;
     const bool take = finished && dist <= B && dist <= T;
-    warp_list_add(list, cnt, T, a.k, a.bound, take, dist, take ? (uint32_t)a.ids[row] : 0u);
+    warp_list_add(list, cnt, T, a.k, a.bound, take, dist,
+                  take ? (kRowIds ? row : (uint32_t)a.ids[row]) : 0u);
     B = fminf(fminf(B, T), __int_as_float((int)bnext));
   }
   cnt = warp_compact(list, cnt, a.k);
@@ -1018,10 +1021,20 @@ cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s)
 cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_ed_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
+    cudaFuncSetAttribute(k_ed_stream<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
     attr = true;
   }
-  k_ed_stream<<<blocks, kEdThreads, sizeof(float) * a.L, s>>>(a);
+  k_ed_stream<false><<<blocks, kEdThreads, sizeof(float) * a.L, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ed_stream_row_ids(const EdArgs& a, int blocks, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_ed_stream<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
+    attr = true;
+  }
+  k_ed_stream<true><<<blocks, kEdThreads, sizeof(float) * a.L, s>>>(a);
   return cudaGetLastError();
 }
 
