@@ -23,7 +23,7 @@
 using hg::Node;
 
 // Launch geometry of the leaf scan.
-constexpr int kEdBlocksPerSm = 3;      // k_ed_stream: 3 x 256 threads per SM
+constexpr int kEdBlocksPerSm = 4;      // k_ed_stream: 4 x 256 threads per SM
 constexpr int kFilterBlocksPerSm = 8;  // k_lbsax_filter
 
 // ---------------------------------------------------------------------------

@@ -641,26 +641,40 @@ __global__ void __launch_bounds__(kFilterThreads) k_lbsax_filter(FilterArgs a) {
 
 // Stage 2: the early-abandoning squared distance (ts_euclidean_distance_SIMD,
 // ts.c:83-109) over a row list, or over a row range when there is no list.
-// Every lane owns one row at a time and advances it one 128-byte line (four
-// 8-float chunks) per step, testing the running sum against the k-th bound
-// after each chunk (a strict test: a row whose distance equals the bound is
-// finished, so ties keep the lowest id).  A lane whose row abandoned or
-// finished takes the next row of its warp's batch.  Warp w of W owns the
-// 32-entry batches w, w + W, w + 2W, ... of the list; the entries of the
-// next batch are loaded while the current one is consumed.  Finished rows
-// within the bound enter the warp's top-k list, which lowers the global
-// bound (atomicMin) once it holds k distances.
-// kRowIds: the id of a row is its row index (a matrix without an id map).
+//
+// A warp works on 8 rows at a time, 4 lanes per row ("slot").  Per step the
+// 4 lanes of a slot load one 128-byte line of their row (chunk ch + j in
+// lane j), each computes its 8-float chunk sum, and the slot adds the 4 chunk
+// sums to the running distance in chunk order (shuffles), testing the bound
+// after each (a strict test: a row whose distance equals the bound finishes,
+// so ties keep the lowest id).  A slot whose row abandoned or finished takes
+// the next row of its warp's batch: warp w of W owns the 32-entry batches w,
+// w + W, w + 2W, ... of the list, and the next batch's entries are loaded
+// while the current one is consumed.  Finished rows within the bound enter
+// the warp's top-k list, which lowers the global bound (atomicMin) once it
+// holds k distances.  The query lives in shared memory in blocks of 32
+// chunks (40 float4 pairs each): chunk r of a block sits at pair r + r / 4,
+// so the slots of a warp, which sit at different 4-chunk positions, read
+// different banks.
 constexpr int kEdThreads = 256;
+__device__ __forceinline__ int q4_index(int chunk, int half) {
+  const int r = chunk & 31;
+  return ((chunk >> 5) * 40 + r + (r >> 2)) * 2 + half;
+}
+// bytes of that layout for a series of L floats
+__host__ __device__ inline size_t q4_bytes(int L) { return (size_t)((L / 8 + 31) / 32) * 40 * 2 * 16; }
+// kRowIds: the id of a row is its row index (a matrix without an id map).
 template <bool kRowIds>
-__global__ void __launch_bounds__(kEdThreads, 3) k_ed_stream(EdArgs a) {
+__global__ void __launch_bounds__(kEdThreads, 4) k_ed_stream(EdArgs a) {
   constexpr int W = kEdThreads / 32;
   __shared__ unsigned long long lists[W][kWarpListCap];
-  extern __shared__ float4 qs4[];  // the query, L/4 float4
+  extern __shared__ float4 qs4[];  // the query, q4_bytes(L) bytes
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int slot_lead = lane & ~3, j = lane & 3;
   unsigned long long* list = lists[wib];
   for (int i = lane; i < kWarpListCap; i += 32) list[i] = ~0ull;
-  for (int i = threadIdx.x; i < (a.L >> 2); i += blockDim.x) qs4[i] = reinterpret_cast<const float4*>(a.q)[i];
+  for (int i = threadIdx.x; i < (a.L >> 2); i += blockDim.x)
+    qs4[q4_index(i >> 1, i & 1)] = reinterpret_cast<const float4*>(a.q)[i];
   __syncthreads();
   const int nch = a.L >> 3;
   uint64_t first = a.ident_first;
@@ -677,31 +691,36 @@ __global__ void __launch_bounds__(kEdThreads, 3) k_ed_stream(EdArgs a) {
   const uint32_t nwarps = gridDim.x * W;
   const uint32_t gw = blockIdx.x * W + wib;
   const uint32_t lt = (1u << lane) - 1;
+  const uint32_t leaders = 0x11111111u;
   // batch b of this warp covers entries [(gw + b * nwarps) * 32, +32)
   auto entry = [&](uint32_t batch) -> uint32_t {
     const uint64_t idx = (uint64_t)batch * 32 + lane;
     if (idx >= total) return 0xffffffffu;
     return a.list ? a.list[idx] : (uint32_t)(first + idx);
   };
+  auto count_of = [&](uint32_t batch) -> uint32_t {
+    const uint64_t b0 = (uint64_t)batch * 32;
+    return b0 < total ? (uint32_t)(total - b0 < 32 ? total - b0 : 32) : 0u;
+  };
   uint32_t batch = gw;
-  uint32_t cur = entry(batch);  // lane j holds entry j of the current batch
-  uint32_t cur_n = batch * 32ull < total ? min(32u, total - batch * 32) : 0u;
+  uint32_t cur = entry(batch);  // lane i holds entry i of the current batch
+  uint32_t cur_n = count_of(batch);
   uint32_t cur_used = 0;
   batch += nwarps;
   uint32_t nxt = entry(batch);
-  uint32_t nxt_n = (uint64_t)batch * 32 < total ? min(32u, total - batch * 32) : 0u;
+  uint32_t nxt_n = count_of(batch);
 
   int cnt = 0;
   float T = __int_as_float(0x7f800000);
   float B = __int_as_float((int)ld_volatile(a.bound));
-  bool valid = false;
+  bool valid = false;  // slot-uniform
   uint32_t row = 0;
   int ch = 0;
   float dist = 0.0f;
   unsigned long long n_chunks = 0, n_done = 0, n_rows = 0;
   for (int iter = 1;; ++iter) {
-    // refill the lanes without a row
-    uint32_t need = __ballot_sync(HG_FULL, !valid);
+    // refill the slots without a row
+    uint32_t need = __ballot_sync(HG_FULL, !valid) & leaders;
     while (need) {
       if (cur_used == cur_n) {
         if (nxt_n == 0) break;
@@ -710,52 +729,54 @@ __global__ void __launch_bounds__(kEdThreads, 3) k_ed_stream(EdArgs a) {
         cur_used = 0;
         batch += nwarps;
         nxt = entry(batch);  // loaded while the current batch is consumed
-        nxt_n = (uint64_t)batch * 32 < total ? min(32u, total - batch * 32) : 0u;
+        nxt_n = count_of(batch);
       }
       const int take = min(__popc(need), (int)(cur_n - cur_used));
-      const int r = __popc(need & lt);
-      const uint32_t got = __shfl_sync(HG_FULL, cur, (cur_used + (r < take ? r : 0)) & 31);
-      if (!valid && r < take) {
+      const int r = __popc(need & ((1u << slot_lead) - 1));  // rank among the free slots
+      const bool mine = ((need >> slot_lead) & 1u) && r < take;
+      const uint32_t got = __shfl_sync(HG_FULL, cur, (cur_used + (mine ? r : 0)) & 31);
+      if (mine) {
         row = got;
         valid = true;
         dist = 0.0f;
         ch = 0;
-        ++n_rows;
+        if (j == 0) ++n_rows;
       }
       cur_used += take;
-      need = __ballot_sync(HG_FULL, !valid);
+      need = __ballot_sync(HG_FULL, !valid) & leaders;
     }
     if (!__any_sync(HG_FULL, valid)) break;
     const uint32_t bnext = ((iter & 7) == 0) ? ld_volatile(a.bound) : 0x7f800000u;
+    // one line of every owned row: lane j computes chunk ch + j
+    const int c = ch + j;
+    float d = 0.0f;
+    if (valid && c < nch) {
+      const float4* x = reinterpret_cast<const float4*>(a.rows + (uint64_t)row * a.L) + (c << 1);
+      const float4 x0 = __ldcs(x), x1 = __ldcs(x + 1);
+      const float4 q0 = qs4[q4_index(c, 0)], q1 = qs4[q4_index(c, 1)];
+      const float qa[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+      const float xa[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+      d = hg_chunk_d2(qa, xa);
+    }
     bool finished = false;
-    if (valid) {
-      const float4* x = reinterpret_cast<const float4*>(a.rows + (uint64_t)row * a.L) + (ch << 1);
-      const int nc = min(4, nch - ch);
-      float4 v[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) v[j] = (j < 2 * nc) ? __ldcs(x + j) : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-      for (int cc = 0; cc < 4; ++cc) {
-        if (cc < nc && valid) {
-          const float4 q0 = qs4[(ch + cc) * 2], q1 = qs4[(ch + cc) * 2 + 1];
-          const float qa[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-          const float xa[8] = {v[2 * cc].x, v[2 * cc].y, v[2 * cc].z, v[2 * cc].w,
-                               v[2 * cc + 1].x, v[2 * cc + 1].y, v[2 * cc + 1].z, v[2 * cc + 1].w};
-          dist = __fadd_rn(dist, hg_chunk_d2(qa, xa));
-          ++n_chunks;
-          if (dist > B) valid = false;  // abandoned
-        }
-      }
-      if (valid) {
-        ch += nc;
-        if (ch >= nch) {
-          finished = true;
-          valid = false;
-        }
+    for (int t = 0; t < 4; ++t) {
+      const float dt = __shfl_sync(HG_FULL, d, slot_lead + t);
+      if (valid && ch + t < nch) {
+        dist = __fadd_rn(dist, dt);
+        if (j == 0) ++n_chunks;
+        if (dist > B) valid = false;  // abandoned
       }
     }
-    if (finished) ++n_done;
-    const bool take = finished && dist <= B && dist <= T;
+    if (valid) {
+      ch += 4;
+      if (ch >= nch) {
+        finished = true;
+        valid = false;
+      }
+    }
+    if (finished && j == 0) ++n_done;
+    const bool take = finished && j == 0 && dist <= B && dist <= T;
     warp_list_add(list, cnt, T, a.k, a.bound, take, dist,
                   take ? (kRowIds ? row : (uint32_t)a.ids[row]) : 0u);
     B = fminf(fminf(B, T), __int_as_float((int)bnext));
@@ -1021,20 +1042,20 @@ cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s)
 cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_ed_stream<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
+    cudaFuncSetAttribute(k_ed_stream<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q4_bytes(16384));
     attr = true;
   }
-  k_ed_stream<false><<<blocks, kEdThreads, sizeof(float) * a.L, s>>>(a);
+  k_ed_stream<false><<<blocks, kEdThreads, q4_bytes(a.L), s>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ed_stream_row_ids(const EdArgs& a, int blocks, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_ed_stream<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
+    cudaFuncSetAttribute(k_ed_stream<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q4_bytes(16384));
     attr = true;
   }
-  k_ed_stream<true><<<blocks, kEdThreads, sizeof(float) * a.L, s>>>(a);
+  k_ed_stream<true><<<blocks, kEdThreads, q4_bytes(a.L), s>>>(a);
   return cudaGetLastError();
 }
 
