@@ -149,9 +149,9 @@ def measured_peaks():
 
 
 def ncu_traffic():
-    """Per-launch DRAM traffic of the leaf-scan kernel from the committed ncu
-    summary (profiles/k_scan_traffic.json), scaled to bytes per visited row."""
-    p = os.path.join(ROOT, "profiles", "k_scan_traffic.json")
+    """DRAM traffic per algorithmic byte of the distance kernel, from the
+    committed ncu summary (profiles/k_ed_stream_traffic.json)."""
+    p = os.path.join(ROOT, "profiles", "k_ed_stream_traffic.json")
     if not os.path.exists(p):
         return None
     try:
@@ -296,8 +296,10 @@ def main():
     achieved = alg_bytes / scan_s / 1e9 if scan_s > 0 else 0.0
     tr = ncu_traffic()
     traffic = None
-    if tr and tr.get("dram_bytes_per_chunk"):
-        traffic = tr["dram_bytes_per_chunk"] * agg["chunks_loaded"] / max(launches, 1)
+    if tr and tr.get("dram_bytes_per_algorithmic_byte"):
+        # ncu traffic of a small capture, scaled to a 25M launch by its
+        # algorithmic bytes (traffic grows in proportion)
+        traffic = tr["dram_bytes_per_algorithmic_byte"] * alg_bytes / max(launches, 1)
     f_launches = int(agg["filter_launches"])
     f_bytes = 16.0 * agg["rows_considered"] + 4.0 * (agg["rows_considered"] - agg["rows_lbsax_pruned"])
     f_s = agg["filter_ms"] / 1000.0

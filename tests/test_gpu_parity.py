@@ -196,3 +196,36 @@ def test_other_lengths(hg, oracle_mod, gpu_available, L, n, leaf):
         od, orow, _, _ = oi.knn(q, 10)
         assert np.array_equal(bits(d[j]), bits(od))
         assert np.array_equal(ids[j], ids_map[orow])
+
+
+def test_cli_is_a_drop_in_for_the_reference_cli(hg, tmp_path, gpu_available):
+    """bin/hercules with the reference's flags (build, then query) prints
+    the same Query_exact_distance / Query_exact_node_file_pos lines as the
+    reference CLI (golden)."""
+    import subprocess
+    from hercules_b200 import build as B
+    g = golden("n20000_L64_leaf500")
+    X = hg.generate_walks(g["data_seed"], g["n"], g["L"])
+    Q = hg.generate_queries(g["query_seed"], X, np.array(g["sigma2"]))
+    data, qf = str(tmp_path / "data.bin"), str(tmp_path / "q.bin")
+    X.tofile(data)
+    Q.tofile(qf)
+    idx = str(tmp_path / "idx") + "/"
+    cli = B.build_cli()
+    r = subprocess.run([cli, "--mode", "0", "--serial", "1", "--sims", "--num-threads", "2", "--num-write-threads",
+                        "1", "--initial-db-size", "120000", "--buffer-size", "500", "--leaf-size", str(g["leaf"]),
+                        "--timeseries-size", str(g["L"]), "--dataset-size", str(g["n"]), "--dataset", data,
+                        "--index-path", idx], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([cli, "--mode", "1", "--serial", "1", "--num-threads", "1", "--k", str(g["k"]), "--queries",
+                        qf, "--queries-size", str(g["nq"]), "--index-path", idx], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = {}
+    for line in r.stdout.splitlines():
+        p = line.split("\t")
+        if len(p) == 5 and p[0] in ("Query_exact_distance", "Query_exact_node_file_pos"):
+            got[(p[0], int(p[3]), int(p[4]))] = p[1]
+    for j in range(g["nq"]):
+        for r_ in range(g["k"]):
+            assert got[("Query_exact_distance", j + 1, r_ + 1)] == g["answers"]["exact_distance"][j][r_]
+            assert got[("Query_exact_node_file_pos", j + 1, r_ + 1)] == g["answers"]["exact_node_file_pos"][j][r_]
