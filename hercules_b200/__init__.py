@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(_HERE, "libhercules_gpu.so")
 
 MODE_PLAIN = 0
 MODE_PSCAN = 1
+MODE_BATCH = 2
 
 _STATUS = {0: "ok", -1: "invalid argument", -2: "i/o error", -3: "index format error", -4: "CUDA error",
            -5: "out of memory", -6: "device wait timed out", -7: "size limit exceeded"}
@@ -47,7 +48,10 @@ class QueryStats(ctypes.Structure):
                 ("device_ms", ctypes.c_double), ("rows_completed", ctypes.c_uint64),
                 ("scan_launches", ctypes.c_uint64), ("scan_ms", ctypes.c_double),
                 ("rows_considered", ctypes.c_uint64), ("filter_launches", ctypes.c_uint64),
-                ("filter_ms", ctypes.c_double)]
+                ("filter_ms", ctypes.c_double), ("bf16_pairs", ctypes.c_uint64),
+                ("survivors", ctypes.c_uint64), ("fallback_queries", ctypes.c_uint64),
+                ("bound_ms", ctypes.c_double), ("gemm_ms", ctypes.c_double), ("rerank_ms", ctypes.c_double),
+                ("fallback_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -55,7 +59,7 @@ class QueryStats(ctypes.Structure):
 
 class KnnOpts(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("use_lb_sax", ctypes.c_int), ("profile", ctypes.c_int),
-                ("approx_blocks", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+                ("approx_blocks", ctypes.c_int), ("bucket_cap", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
 
 
 _lib = None
@@ -82,6 +86,10 @@ _SIGS = [
                               ctypes.POINTER(QueryStats)]),
     ("hg_knn_device", ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(KnnOpts), _P, _P,
                                      _P, ctypes.POINTER(QueryStats)]),
+    ("hg_knn_batch", ctypes.c_int, [_P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, ctypes.POINTER(KnnOpts), _P, _P,
+                                    ctypes.POINTER(QueryStats)]),
+    ("hg_knn_batch_device", ctypes.c_int, [_P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, ctypes.POINTER(KnnOpts),
+                                           _P, _P, _P, ctypes.POINTER(QueryStats)]),
     ("hg_route", ctypes.c_int, [_P, _P, ctypes.c_uint32, _P]),
     ("hg_leaf_lower_bounds", ctypes.c_int, [_P, _P, _P]),
     ("hg_generate_walks", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, _P,
@@ -255,6 +263,35 @@ class HerculesIndex:
         _check(lib().hg_knn_device(self._h, ctypes.c_void_p(q_ptr), nq, k, ctypes.byref(opts),
                                    ctypes.c_void_p(dist_ptr), ctypes.c_void_p(id_ptr), ctypes.c_void_p(stream),
                                    ctypes.byref(st)))
+        return st.as_dict()
+
+    def knn_batch(self, queries, k, stats=False, bucket_cap=0):
+        """Batched exact k-NN (BF16 tensor-core filter + exact re-rank); k is
+        an int or one k per query.  Outputs are nq x max(k); entries past a
+        query's k are +inf / -1."""
+        q = _f32(queries, self.L)
+        nq = q.shape[0]
+        ks = np.broadcast_to(np.asarray(k, dtype=np.uint32), (nq,)).copy()
+        kmax = int(ks.max()) if nq else int(np.max(k))
+        d = np.zeros((nq, kmax), dtype=np.float32)
+        ids = np.zeros((nq, kmax), dtype=np.int64)
+        st = QueryStats()
+        opts = KnnOpts(MODE_BATCH, 1, 0, 0, bucket_cap)
+        _check(lib().hg_knn_batch(self._h, _ptr(q), nq, _ptr(ks), kmax, ctypes.byref(opts), _ptr(d), _ptr(ids),
+                                  ctypes.byref(st)))
+        return (d, ids, st.as_dict()) if stats else (d, ids)
+
+    def knn_batch_device(self, q_ptr, nq, ks, kmax, dist_ptr, id_ptr, stream=0, bucket_cap=0):
+        """Device-resident batched variant; ks is a host array (or None)."""
+        st = QueryStats()
+        opts = KnnOpts(MODE_BATCH, 1, 0, 0, bucket_cap)
+        kp = None
+        if ks is not None:
+            ks = np.ascontiguousarray(ks, dtype=np.uint32)
+            kp = _ptr(ks)
+        _check(lib().hg_knn_batch_device(self._h, ctypes.c_void_p(q_ptr), nq, kp, kmax, ctypes.byref(opts),
+                                         ctypes.c_void_p(dist_ptr), ctypes.c_void_p(id_ptr),
+                                         ctypes.c_void_p(stream), ctypes.byref(st)))
         return st.as_dict()
 
     def route(self, queries):

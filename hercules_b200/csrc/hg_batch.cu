@@ -1,0 +1,534 @@
+// hg_batch.cu -- batched exact k-NN: a BF16 tensor-core filter with a
+// certified error bound, then an exact FP32 re-rank in the reference's
+// summation order (ts_euclidean_distance_SIMD, ts.c:83-109).
+//
+// For thousands of queries at once the dot products q.x of every (query,
+// row) pair are cheap on the tensor cores.  With BF16 operands (unit
+// roundoff u = 2^-8) and FP32 accumulation,
+//     d~(q, x) = |q|^2 + |x|^2 - 2 (q~ . x~)
+// differs from the reference's FP32 squared distance by at most
+//     err(q, tile) = c_dot |q| max_tile |x| + c_sq (|q|^2 + max_tile |x|^2 + B) + 1e-5
+//     c_dot = 2 (2u + u^2 + L 2^-20)        BF16 rounding of q and x, FP32 accumulation
+//     c_sq  = (L/8 + 16) 2^-22              rounded-up FP64 norms, the reference's own
+//                                           FP32 summation, the FP32 epilogue
+// with |x|^2 and |q|^2 computed in FP64 and rounded up.  The pipeline:
+//   1. route every query to its approximate leaf (approximate_knn_search's
+//      traversal, hercules_query_engine.c:176-222);
+//   2. bound: the tensor cores give the minimum d~ of every group of 8..128
+//      rows of the approximate leaf; the k smallest groups' rows are ranked
+//      exactly and their k-th distinct distance is B_q, an exact upper bound
+//      of the query's k-th neighbour distance;
+//   3. filter: every row against every query; (q, x) is kept when
+//      d~ - err <= B_q, which holds for every row whose exact distance is <= B_q;
+//   4. re-rank the kept rows exactly (early abandon at the running k-th
+//      distance), merged with step 2's rows: k distinct distances, lowest id
+//      per distance (queue_bounded_sorted_insert, hercules_query_engine.c:4034);
+//   5. verify per query: B_q finite, k distances found, no bucket overflow;
+//      a query that fails goes through the plain path.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hg_arith.cuh"
+#include "hg_batch.h"
+#include "hg_device.cuh"
+
+namespace hg {
+
+constexpr int kBM = kBatchTileRows, kBN = 128, kBK = 64, kStages = 3, kGemmThreads = 256;
+
+// ---------------------------------------------------------------------------
+// preparation
+// ---------------------------------------------------------------------------
+
+// One warp per row: BF16 copy (round to nearest) and |x|^2 in FP64 rounded up.
+__global__ void k_rows_to_bf16(const float* __restrict__ rows, uint64_t n, int L, __nv_bfloat16* __restrict__ out,
+                               float* __restrict__ n2, float* __restrict__ norm) {
+  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= n) return;
+  const float4* x = reinterpret_cast<const float4*>(rows + w * L);
+  __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(out + w * L);
+  double acc = 0.0;
+  for (int i = lane; i < (L >> 2); i += 32) {
+    const float4 v = x[i];
+    acc += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
+    o[2 * i] = __floats2bfloat162_rn(v.x, v.y);
+    o[2 * i + 1] = __floats2bfloat162_rn(v.z, v.w);
+  }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(HG_FULL, acc, s);
+  if (lane == 0) {
+    n2[w] = __double2float_ru(acc * (1.0 + 1e-12));
+    if (norm) norm[w] = __double2float_ru(sqrt(acc) * (1.0 + 1e-12));
+  }
+}
+
+// Per 128-row tile of the leaf-ordered rows: max |x|^2 and max |x|.
+__global__ void k_tile_norms(const float* __restrict__ n2, uint64_t n, float* __restrict__ tile_n2,
+                             float* __restrict__ tile_norm) {
+  const uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint64_t r0 = t * kBM;
+  if (r0 >= n) return;
+  float m = 0.0f;
+  for (uint64_t r = r0 + lane; r < r0 + kBM && r < n; r += 32) m = fmaxf(m, n2[r]);
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) m = fmaxf(m, __shfl_xor_sync(HG_FULL, m, s));
+  if (lane == 0) {
+    tile_n2[t] = m;
+    tile_norm[t] = __fsqrt_ru(m);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the BF16 GEMM with fused epilogues (mma.sync m16n8k16, FP32 accumulation)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t ordered_key(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// 16-byte asynchronous copy; src-size 0 zero-fills the destination.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+  const int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void ldmatrix_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"(addr));
+}
+
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// A stage holds 128 rows x 64 BF16 (128 B per row) of each operand; the
+// 16-byte chunk c of row r sits at chunk c ^ (r & 7), so the eight row
+// addresses of one ldmatrix phase fall in eight different bank groups.
+__device__ __forceinline__ uint32_t swz(int r, int c) { return (uint32_t)((r * 8 + (c ^ (r & 7))) * 16); }
+
+// Work item -> tiles and queries.  Mode 0 (bound): item = tiles [tile_lo,
+// tile_hi) of one approximate leaf for one group of queries routed there.
+// Mode 1 (filter): item w = (row chunk w / QT, query tile w % QT), so the QT
+// items of one row chunk run side by side and read it from HBM once.
+__global__ void __launch_bounds__(kGemmThreads, 2) k_bf16_filter(BatchGemm a) {
+  extern __shared__ __align__(128) unsigned char gsm[];
+  unsigned char* sA = gsm;                            // kStages x 16 KB of rows
+  unsigned char* sB = gsm + kStages * kBM * kBK * 2;  // kStages x 16 KB of queries
+  __shared__ uint32_t s_item;
+  __shared__ uint32_t s_qidx[kBN];
+  __shared__ float s_qn2[kBN], s_qn[kBN], s_qb[kBN];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps, 64 rows x 32 queries each
+  const int g = lane >> 2, tig = lane & 3;
+  const int ksteps = (a.L + kBK - 1) / kBK;
+  const uint32_t QT = (uint32_t)((a.nq + kBN - 1) / kBN);
+  const uint64_t ntiles = (a.nrows + kBM - 1) / kBM;
+  const uint32_t nchunks = (uint32_t)((ntiles + a.tiles_per_item - 1) / a.tiles_per_item);
+  const uint32_t total_items = a.mode == 0 ? a.nitems : nchunks * QT;
+  const float inf = __int_as_float(0x7f800000);
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(a.work_head, 1u);
+    __syncthreads();
+    const uint32_t w = s_item;
+    if (w >= total_items) break;
+    uint64_t rb, re;
+    uint32_t qoff, qcnt, t_lo, t_hi, sub = 1;
+    if (a.mode == 0) {
+      const BatchItem it = a.items[w];
+      rb = it.row_begin;
+      re = it.row_end;
+      qoff = it.q_off;
+      qcnt = it.q_cnt;
+      t_lo = it.tile_lo;
+      t_hi = it.tile_hi;
+      sub = it.sub;
+    } else {
+      const uint32_t chunk = w / QT, qt = w % QT;
+      rb = 0;
+      re = a.nrows;
+      qoff = qt * kBN;
+      qcnt = (uint32_t)min(a.nq - (int)qoff, kBN);
+      t_lo = chunk * a.tiles_per_item;
+      const uint64_t th = (uint64_t)t_lo + a.tiles_per_item;
+      t_hi = (uint32_t)(th < ntiles ? th : ntiles);
+    }
+    if (tid < kBN) {
+      const uint32_t q = tid < (int)qcnt ? a.qperm[qoff + tid] : 0xffffffffu;
+      s_qidx[tid] = q;
+      const bool ok = q != 0xffffffffu;
+      s_qn2[tid] = ok ? a.qn2[q] : 0.0f;
+      s_qn[tid] = ok ? a.qnorm[q] : 0.0f;
+      // the filter skips queries without a finite bound (they take the plain path)
+      const float b = (ok && a.mode == 1) ? a.bound[q] : 0.0f;
+      s_qb[tid] = (ok && b < inf) ? b : -1.0f;
+    }
+    __syncthreads();
+    const uint32_t nstage_total = (t_hi - t_lo) * (uint32_t)ksteps;
+    auto issue = [&](uint32_t s) {
+      if (s < nstage_total) {
+        const uint64_t row0 = rb + (uint64_t)(t_lo + s / ksteps) * kBM;
+        const uint64_t nvalid = row0 < re ? (re - row0 < (uint64_t)kBM ? re - row0 : (uint64_t)kBM) : 0;
+        const int kb = (int)(s % ksteps) * kBK;
+        const int buf = (int)(s % kStages);
+        unsigned char* A = sA + buf * kBM * kBK * 2;
+        unsigned char* Bm = sB + buf * kBN * kBK * 2;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int idx = tid + i * kGemmThreads;  // 0..1023: 128 rows x 8 chunks
+          const int r = idx >> 3, c = idx & 7;
+          const bool kv = kb + c * 8 < a.L;
+          const bool va = kv && (uint64_t)r < nvalid;
+          const __nv_bfloat16* srcA = static_cast<const __nv_bfloat16*>(a.xbf) + (va ? (row0 + r) * (uint64_t)a.L + kb + c * 8 : 0);
+          cp_async16(smem_u32(A + swz(r, c)), srcA, va);
+          const uint32_t q = s_qidx[r];
+          const bool vb = kv && q != 0xffffffffu;
+          const __nv_bfloat16* srcB = static_cast<const __nv_bfloat16*>(a.qbf) + (vb ? (uint64_t)q * a.L + kb + c * 8 : 0);
+          cp_async16(smem_u32(Bm + swz(r, c)), srcB, vb);
+        }
+      }
+      cp_async_commit();
+    };
+    for (int s = 0; s < kStages - 1; ++s) issue((uint32_t)s);
+    float acc[4][4][4];
+    for (uint32_t s = 0; s < nstage_total; ++s) {
+      const int kk = (int)(s % ksteps);
+      if (kk == 0) {
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[mi][ni][e] = 0.0f;
+      }
+      cp_async_wait<kStages - 2>();
+      __syncthreads();
+      issue(s + kStages - 1);
+      const int buf = (int)(s % kStages);
+      const unsigned char* A = sA + buf * kBM * kBK * 2;
+      const unsigned char* Bm = sB + buf * kBN * kBK * 2;
+#pragma unroll
+      for (int k16 = 0; k16 < kBK / 16; ++k16) {
+        uint32_t af[4][4];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi) {
+          const int r = wm * 64 + mi * 16 + (lane & 15);
+          const int c = k16 * 2 + (lane >> 4);
+          ldmatrix_x4(smem_u32(A + swz(r, c)), af[mi][0], af[mi][1], af[mi][2], af[mi][3]);
+        }
+        uint32_t bfr[4][2];
+#pragma unroll
+        for (int nj = 0; nj < 2; ++nj) {
+          const int r = wn * 32 + nj * 16 + (lane & 7) + ((lane >> 4) << 3);
+          const int c = k16 * 2 + ((lane >> 3) & 1);
+          ldmatrix_x4(smem_u32(Bm + swz(r, c)), bfr[nj * 2][0], bfr[nj * 2][1], bfr[nj * 2 + 1][0],
+                      bfr[nj * 2 + 1][1]);
+        }
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) mma_bf16(acc[mi][ni], af[mi], bfr[ni][0], bfr[ni][1]);
+      }
+      if (kk != ksteps - 1) continue;
+      // ---- epilogue of one 128 x 128 tile
+      const uint32_t tl = t_lo + s / ksteps;
+      const uint64_t row0 = rb + (uint64_t)tl * kBM;
+      const uint64_t nvalid = row0 < re ? (re - row0 < (uint64_t)kBM ? re - row0 : (uint64_t)kBM) : 0;
+      if (a.mode == 1) {
+        const uint64_t gt = row0 / kBM;
+        const float tn = a.tile_norm[gt], tn2 = a.tile_n2[gt];
+        float thr[8];
+#pragma unroll
+        for (int ci = 0; ci < 8; ++ci) {
+          const int col = wn * 32 + (ci >> 1) * 8 + tig * 2 + (ci & 1);
+          const float b = s_qb[col], qn2 = s_qn2[col];
+          const float err = a.c_dot * s_qn[col] * tn + a.c_sq * (qn2 + tn2 + b) + 1e-5f;
+          // keep when |x|^2 + (|q|^2 - B - err) - 2 acc <= 0
+          thr[ci] = b >= 0.0f ? qn2 - b - err : inf;
+        }
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int r = wm * 64 + mi * 16 + g + h * 8;
+            if ((uint64_t)r >= nvalid) continue;
+            const uint64_t row = row0 + r;
+            const float xn = a.xn2[row];
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                const float v = xn + thr[ni * 2 + e] - 2.0f * acc[mi][ni][h * 2 + e];
+                if (v <= 0.0f) {
+                  const uint32_t q = s_qidx[wn * 32 + ni * 8 + tig * 2 + e];
+                  const uint32_t pos = atomicAdd(&a.bucket_cnt[q], 1u);
+                  if (pos < a.bucket_cap) a.bucket[(uint64_t)q * a.bucket_cap + pos] = (uint32_t)row;
+                }
+              }
+          }
+      } else {
+        // per query column: min d~ (and its row) over the thread's 8 rows,
+        // reduced over the groups that share a slot
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int col = wn * 32 + ni * 8 + tig * 2 + e;
+            const uint32_t q = s_qidx[col];
+            const float qn2 = s_qn2[col];
+            unsigned long long best = ~0ull;
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const int r = wm * 64 + mi * 16 + g + h * 8;
+                if ((uint64_t)r < nvalid) {
+                  const uint64_t row = row0 + r;
+                  const float d = a.xn2[row] + qn2 - 2.0f * acc[mi][ni][h * 2 + e];
+                  const unsigned long long key = ((unsigned long long)ordered_key(d) << 32) | (uint32_t)row;
+                  best = key < best ? key : best;
+                }
+              }
+            // the 8 rows of one thread and column form group wm * 8 + g of
+            // the tile; `span` consecutive groups share one slot
+            const int span = 16 / (int)sub;
+            const int gshift = span >= 8 ? 3 : (span == 4 ? 2 : (span == 2 ? 1 : 0));
+            for (int l = 0; l < gshift; ++l) {
+              const unsigned long long o = __shfl_xor_sync(HG_FULL, best, 4 << l);
+              best = o < best ? o : best;
+            }
+            const uint32_t slot = tl * sub + (uint32_t)((wm * 8 + g) / span);
+            if ((g & ((1 << gshift) - 1)) == 0 && q != 0xffffffffu && best != ~0ull && slot < a.bm_cap)
+              atomicMin(&a.bm[(uint64_t)q * a.bm_cap + slot], best);
+          }
+      }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// bound, re-rank, verification
+// ---------------------------------------------------------------------------
+
+// Step 2: one block per query.  The slots' minima are distinct rows; the k
+// smallest are ranked exactly (hg_ed, reference order) and the k-th distinct
+// distance among them bounds the query's k-th neighbour distance.
+constexpr int kSelThreads = 256;
+__global__ void __launch_bounds__(kSelThreads) k_bound_select(BatchRank a) {
+  extern __shared__ unsigned long long ssel[];
+  unsigned long long* buf = ssel;                    // bm_pow2 keys
+  __shared__ unsigned long long list[kWarpListCap];  // exact (distance, id) keys
+  const int tid = threadIdx.x;
+  const int q = blockIdx.x;
+  const int k = (int)a.kq[q];
+  const uint32_t ns = min(a.slots_of_query[q], a.bm_cap);
+  int n = 32;
+  while (n < (int)ns) n <<= 1;
+  for (int i = tid; i < n; i += kSelThreads) buf[i] = i < (int)ns ? a.bm[(uint64_t)q * a.bm_cap + i] : ~0ull;
+  __syncthreads();
+  for (int size = 2; size <= n; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = tid; i < (n >> 1); i += kSelThreads) {
+        const int pos = 2 * i - (i & (stride - 1));
+        const int partner = pos + stride;
+        const bool asc = (pos & size) == 0;
+        const unsigned long long x = buf[pos], y = buf[partner];
+        if ((x > y) == asc) {
+          buf[pos] = y;
+          buf[partner] = x;
+        }
+      }
+      __syncthreads();
+    }
+  const float* qv = a.Q + (uint64_t)q * a.L;
+  for (int i = tid; i < kWarpListCap; i += kSelThreads) {
+    unsigned long long v = ~0ull;
+    if (i < k && i < n && buf[i] != ~0ull) {
+      const uint32_t row = (uint32_t)buf[i];
+      const float d = hg_ed(qv, a.rows + (uint64_t)row * a.L, a.L, __int_as_float(0x7f800000));
+      v = ((unsigned long long)__float_as_uint(d) << 32) | (uint32_t)a.ids[row];
+    }
+    list[i] = v;
+  }
+  __syncthreads();
+  if (tid < 32) {
+    // the valid keys are a prefix (rows of the sorted prefix), the rest ~0
+    int take = 0;
+    for (int i = tid; i < kWarpListCap; i += 32) take += list[i] != ~0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) take += __shfl_xor_sync(HG_FULL, take, o);
+    const int cnt = warp_compact(list, take, k);
+    if (tid == 0) {
+      a.bound[q] = cnt == k ? __uint_as_float((uint32_t)(list[k - 1] >> 32)) : __int_as_float(0x7f800000);
+      a.init_cnt[q] = cnt;
+    }
+    for (int i = tid; i < cnt; i += 32) a.init[(uint64_t)q * kMaxK + i] = list[i];
+  }
+}
+
+// Steps 4-5: one warp per query re-ranks its bucket with 4-lane slots (lane
+// j of a slot computes chunk ch + j; the slot adds the four in order), from
+// step 2's list and bound.
+constexpr int kRankWarps = 8;
+__global__ void __launch_bounds__(kRankWarps * 32) k_rerank(BatchRank a) {
+  __shared__ unsigned long long lists[kRankWarps][kWarpListCap];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int q = blockIdx.x * kRankWarps + wib;
+  if (q >= a.nq) return;
+  const int slot_lead = lane & ~3, j = lane & 3;
+  unsigned long long* list = lists[wib];
+  const int k = (int)a.kq[q];
+  const float Bq = a.bound[q];
+  const int c0 = a.init_cnt[q];
+  for (int i = lane; i < kWarpListCap; i += 32) list[i] = i < c0 ? a.init[(uint64_t)q * kMaxK + i] : ~0ull;
+  __syncwarp();
+  int cnt = c0;
+  const float inf = __int_as_float(0x7f800000);
+  float T = cnt == k ? __uint_as_float((uint32_t)(list[k - 1] >> 32)) : inf;
+  float B = T;
+  const uint32_t nb = a.bucket_cnt[q];
+  const bool usable = Bq < inf && nb <= a.bucket_cap;
+  const uint32_t total = usable ? nb : 0u;
+  const uint32_t* bk = a.bucket + (uint64_t)q * a.bucket_cap;
+  const float* qv = a.Q + (uint64_t)q * a.L;
+  const int nch = a.L >> 3;
+  uint32_t next = 0;
+  bool valid = false;
+  uint32_t row = 0;
+  int ch = 0;
+  float dist = 0.0f;
+  unsigned long long n_rows = 0, n_chunks = 0;
+  const uint32_t leaders = 0x11111111u;
+  for (;;) {
+    const uint32_t need = __ballot_sync(HG_FULL, !valid) & leaders;
+    if (need && next < total) {
+      const int r = __popc(need & ((1u << slot_lead) - 1));
+      const uint32_t avail = min(total - next, 8u);
+      if (((need >> slot_lead) & 1u) && (uint32_t)r < avail) {
+        row = bk[next + r];
+        valid = true;
+        dist = 0.0f;
+        ch = 0;
+        if (j == 0) ++n_rows;
+      }
+      next += min((uint32_t)__popc(need), avail);
+    }
+    if (!__any_sync(HG_FULL, valid)) break;
+    const int c = ch + j;
+    float d = 0.0f;
+    if (valid && c < nch) d = hg_chunk_d2(qv + c * 8, a.rows + (uint64_t)row * a.L + c * 8);
+    bool finished = false;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const float dt = __shfl_sync(HG_FULL, d, slot_lead + t);
+      if (valid && ch + t < nch) {
+        dist = __fadd_rn(dist, dt);
+        if (j == 0) ++n_chunks;
+        if (dist > B) valid = false;  // partial sums only grow: this row cannot enter
+      }
+    }
+    if (valid) {
+      ch += 4;
+      if (ch >= nch) {
+        finished = true;
+        valid = false;
+      }
+    }
+    const bool take = finished && j == 0;
+    warp_list_add(list, cnt, T, k, nullptr, take, dist, take ? (uint32_t)a.ids[row] : 0u);
+    B = fminf(B, T);
+  }
+  cnt = warp_compact(list, cnt, k);
+  const bool ok = usable && cnt == k && __uint_as_float((uint32_t)(list[k - 1] >> 32)) <= Bq;
+  for (int i = lane; i < a.kmax; i += 32) {
+    const bool have = i < cnt;
+    a.dist_out[(uint64_t)q * a.kmax + i] = have ? __uint_as_float((uint32_t)(list[i] >> 32)) : inf;
+    a.id_out[(uint64_t)q * a.kmax + i] = have ? (int64_t)(uint32_t)list[i] : -1;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    n_rows += __shfl_xor_sync(HG_FULL, n_rows, o);
+    n_chunks += __shfl_xor_sync(HG_FULL, n_chunks, o);
+  }
+  if (lane == 0) {
+    a.ok_out[q] = ok ? 1 : 0;
+    atomicAdd(&a.stats[0], n_rows);
+    atomicAdd(&a.stats[1], n_chunks);
+    atomicAdd(&a.stats[2], (unsigned long long)nb);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+static inline unsigned nblk(uint64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+cudaError_t launch_rows_to_bf16(const float* rows, uint64_t n, int L, void* out, float* n2, float* norm,
+                                cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  k_rows_to_bf16<<<nblk(n * 32, 256), 256, 0, s>>>(rows, n, L, static_cast<__nv_bfloat16*>(out), n2, norm);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tile_norms(const float* n2, uint64_t n, float* tile_n2, float* tile_norm, cudaStream_t s) {
+  const uint64_t nt = (n + kBM - 1) / kBM;
+  if (!nt) return cudaSuccess;
+  k_tile_norms<<<nblk(nt * 32, 256), 256, 0, s>>>(n2, n, tile_n2, tile_norm);
+  return cudaGetLastError();
+}
+
+size_t bf16_filter_smem() { return (size_t)kStages * (kBM + kBN) * kBK * 2; }
+
+cudaError_t launch_bf16_filter(const BatchGemm& g, int blocks, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_bf16_filter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bf16_filter_smem());
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_bf16_filter<<<blocks, kGemmThreads, bf16_filter_smem(), s>>>(g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bound_select(const BatchRank& r, cudaStream_t s) {
+  if (!r.nq) return cudaSuccess;
+  int n = 32;
+  while (n < (int)r.bm_cap) n <<= 1;
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e = cudaFuncSetAttribute(k_bound_select, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)(sizeof(unsigned long long) * kBatchMaxSlots));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_bound_select<<<r.nq, kSelThreads, sizeof(unsigned long long) * n, s>>>(r);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rerank(const BatchRank& r, cudaStream_t s) {
+  if (!r.nq) return cudaSuccess;
+  k_rerank<<<nblk(r.nq, kRankWarps), kRankWarps * 32, 0, s>>>(r);
+  return cudaGetLastError();
+}
+
+}  // namespace hg

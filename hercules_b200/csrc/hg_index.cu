@@ -301,7 +301,32 @@ static void free_device(hg_index* ix) {
   dfree(s.paa);
   dfree(s.stats);
   dfree(s.err);
+  dfree(s.list);
   s.kmax = 0;
+  hg::BatchData& bd = ix->bd;
+  dfree(bd.xbf);
+  dfree(bd.xn2);
+  dfree(bd.tile_n2);
+  dfree(bd.tile_norm);
+  hg::BatchScratch& b = ix->bs;
+  dfree(b.qbf);
+  dfree(b.qn2);
+  dfree(b.qnorm);
+  dfree(b.qperm);
+  dfree(b.approx);
+  dfree(b.kq);
+  dfree(b.slots);
+  dfree(b.items);
+  dfree(b.bm);
+  dfree(b.bound);
+  dfree(b.init);
+  dfree(b.init_cnt);
+  dfree(b.bucket);
+  dfree(b.bucket_cnt);
+  dfree(b.ok);
+  dfree(b.stats);
+  dfree(b.heads);
+  b = hg::BatchScratch{};
 }
 
 // Routing tree in the final encoding: internal nodes renumbered densely,
@@ -1131,6 +1156,10 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
   return HG_OK;
 }
 
+static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, const uint32_t* ks, uint32_t kmax,
+                                const hg_knn_opts& o, float* d_dist, int64_t* d_id, cudaStream_t st,
+                                hg_query_stats* stats);
+
 static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t nq, uint32_t k,
                                  const hg_knn_opts* opts, float* d_dist, int64_t* d_id, cudaStream_t st,
                                  hg_query_stats* stats) {
@@ -1142,6 +1171,7 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
     return set_error(HG_ERR_LIMIT, "hg_knn: more than 8192 leaves");
   hg_knn_opts o{};
   if (opts) o = *opts;
+  if (o.mode == HG_MODE_BATCH) return knn_batch_impl(ix, d_queries, nq, nullptr, k, o, d_dist, d_id, st, stats);
   CK(cudaSetDevice(ix->device));
   HCK(ensure_scratch(ix, (int)k));
   if (!st) st = ix->stream;
@@ -1179,6 +1209,298 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
     stats->scan_ms = scan_ms;
     stats->filter_launches = filter_launches;
     stats->filter_ms = filter_ms;
+  }
+  return HG_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// batched queries: BF16 tensor-core filter + exact re-rank (hg_batch.cu)
+// ---------------------------------------------------------------------------
+
+constexpr int kGemmBlocksPerSm = 2;       // k_bf16_filter: 2 x 256 threads, 98 KB smem each
+constexpr uint32_t kBoundTilesPerItem = 8;
+constexpr uint32_t kFilterTilesPerItem = 32;  // 4096 rows per item: a row chunk stays in L2
+constexpr uint32_t kDefaultBucket = 16384;
+
+static hg_status ensure_batch_data(hg_index* ix, cudaStream_t st) {
+  hg::BatchData& b = ix->bd;
+  if (b.xbf) return HG_OK;
+  const uint64_t nt = (ix->n + hg::kBatchTileRows - 1) / hg::kBatchTileRows;
+  uint16_t* x = nullptr;
+  CK(dalloc(&x, ix->n * ix->L));
+  b.xbf = x;
+  CK(dalloc(&b.xn2, ix->n));
+  CK(dalloc(&b.tile_n2, nt));
+  CK(dalloc(&b.tile_norm, nt));
+  CK(hg::launch_rows_to_bf16(ix->d.rows, ix->n, (int)ix->L, b.xbf, b.xn2, nullptr, st));
+  CK(hg::launch_tile_norms(b.xn2, ix->n, b.tile_n2, b.tile_norm, st));
+  return HG_OK;
+}
+
+static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket_cap, uint32_t bm_cap,
+                                      uint32_t nitems) {
+  hg::BatchScratch& b = ix->bs;
+  if (nq > b.nq_cap) {
+    dfree(b.qbf);
+    dfree(b.qn2);
+    dfree(b.qnorm);
+    dfree(b.qperm);
+    dfree(b.approx);
+    dfree(b.kq);
+    dfree(b.slots);
+    dfree(b.bound);
+    dfree(b.init);
+    dfree(b.init_cnt);
+    dfree(b.bucket_cnt);
+    dfree(b.ok);
+    uint16_t* q = nullptr;
+    CK(dalloc(&q, (size_t)nq * ix->L));
+    b.qbf = q;
+    CK(dalloc(&b.qn2, nq));
+    CK(dalloc(&b.qnorm, nq));
+    CK(dalloc(&b.qperm, nq));
+    CK(dalloc(&b.approx, nq));
+    CK(dalloc(&b.kq, nq));
+    CK(dalloc(&b.slots, nq));
+    CK(dalloc(&b.bound, nq));
+    CK(dalloc(&b.init, (size_t)nq * hg::kMaxK));
+    CK(dalloc(&b.init_cnt, nq));
+    CK(dalloc(&b.bucket_cnt, nq));
+    CK(dalloc(&b.ok, nq));
+    b.nq_cap = nq;
+    b.bucket_cap = 0;
+    b.bm_cap = 0;
+  }
+  if (!b.stats) {
+    CK(dalloc(&b.stats, 8));
+    CK(dalloc(&b.heads, 4));
+  }
+  if ((uint64_t)b.nq_cap * bucket_cap > (uint64_t)b.nq_cap * b.bucket_cap || !b.bucket) {
+    dfree(b.bucket);
+    CK(dalloc(&b.bucket, (size_t)b.nq_cap * bucket_cap));
+    b.bucket_cap = bucket_cap;
+  }
+  if (bm_cap > b.bm_cap || !b.bm) {
+    dfree(b.bm);
+    CK(dalloc(&b.bm, (size_t)b.nq_cap * bm_cap));
+    b.bm_cap = bm_cap;
+  }
+  if (nitems > b.items_cap || !b.items) {
+    dfree(b.items);
+    CK(dalloc(&b.items, std::max<uint32_t>(nitems, 1)));
+    b.items_cap = std::max<uint32_t>(nitems, 1);
+  }
+  return HG_OK;
+}
+
+// Error-bound coefficients of the BF16 filter for series length L (see
+// hg_batch.cu): c_dot = 2 (2u + u^2 + L 2^-20) with u = 2^-8, and
+// c_sq = (L/8 + 16) 2^-22, both rounded up to float.
+static void filter_coefficients(uint32_t L, float* c_dot, float* c_sq) {
+  const double u = 1.0 / 256.0;
+  const double cd = 2.0 * (2.0 * u + u * u + L * std::ldexp(1.0, -20));
+  const double cs = (L / 8.0 + 16.0) * std::ldexp(1.0, -22);
+  *c_dot = std::nextafter((float)cd, INFINITY);
+  *c_sq = std::nextafter((float)cs, INFINITY);
+}
+
+static hg_status record(cudaEvent_t e, cudaStream_t st) {
+  CK(cudaEventRecord(e, st));
+  return HG_OK;
+}
+
+// Batched exact k-NN over device queries; ks is a host array (or null).
+static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, const uint32_t* ks, uint32_t kmax,
+                                const hg_knn_opts& o, float* d_dist, int64_t* d_id, cudaStream_t st,
+                                hg_query_stats* stats) {
+  if (!ix || (!d_Q && nq)) return set_error(HG_ERR_ARG, "hg_knn_batch: null argument");
+  if (kmax == 0) return set_error(HG_ERR_ARG, "hg_knn_batch: k must be positive");
+  if ((int)kmax > hg::kMaxK) return set_error(HG_ERR_LIMIT, "hg_knn_batch: k above 224");
+  if (ix->L > 16384) return set_error(HG_ERR_LIMIT, "hg_knn_batch: series longer than 16384");
+  if (ix->leaves.size() > (size_t)hg::kMaxLeavesSort)
+    return set_error(HG_ERR_LIMIT, "hg_knn_batch: more than 8192 leaves");
+  if (nq > (1u << 24)) return set_error(HG_ERR_LIMIT, "hg_knn_batch: more than 2^24 queries");
+  std::vector<uint32_t> kq(nq, kmax);
+  if (ks)
+    for (uint32_t i = 0; i < nq; ++i) {
+      if (ks[i] == 0 || ks[i] > kmax) return set_error(HG_ERR_ARG, "hg_knn_batch: ks[i] outside 1..kmax");
+      kq[i] = ks[i];
+    }
+  if (stats) memset(stats, 0, sizeof *stats);
+  if (nq == 0) return HG_OK;
+  CK(cudaSetDevice(ix->device));
+  if (!st) st = ix->stream;
+  HCK(ensure_scratch(ix, (int)kmax));
+  HCK(ensure_batch_data(ix, st));
+  const uint32_t L = ix->L;
+  const int sms = hg::sm_count(ix->device);
+  const uint32_t bucket_cap = o.bucket_cap > 0 ? (uint32_t)o.bucket_cap : kDefaultBucket;
+  hg::BatchScratch& b = ix->bs;
+  HCK(ensure_batch_scratch(ix, std::max(nq, b.nq_cap), bucket_cap, 1, 1));
+
+  cudaEvent_t ev[6];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() {
+      for (int i = 0; i < 6; ++i) cudaEventDestroy(e[i]);
+    }
+  } guard{ev};
+  HCK(record(ev[0], st));
+  // 1. approximate leaves
+  CK(hg::launch_route_queries(d_Q, (int)nq, (int)L, index_tree(ix), b.approx, st));
+  std::vector<int> approx(nq);
+  CK(cudaMemcpyAsync(approx.data(), b.approx, sizeof(int) * nq, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+
+  // queries grouped by approximate leaf; slots per tile for the bound pass
+  const uint32_t T = hg::kBatchTileRows;
+  std::vector<uint32_t> perm(nq);
+  for (uint32_t i = 0; i < nq; ++i) perm[i] = i;
+  std::stable_sort(perm.begin(), perm.end(), [&](uint32_t a, uint32_t c) { return approx[a] < approx[c]; });
+  auto leaf_rows = [&](int li, uint64_t* start, uint64_t* size) {
+    const Node& nd = ix->nodes[ix->leaves[li]];
+    *start = nd.file_pos;
+    *size = nd.node_size;
+  };
+  // bound slots per tile, per leaf: enough slots for 2k + 32 candidate rows
+  // where the leaf has them, at most kBatchMaxSlots per query
+  const uint64_t want = 2ull * kmax + 32;
+  auto sub_of = [&](uint32_t tiles) {
+    uint32_t sub = 1;
+    while (sub < 16 && (uint64_t)std::max<uint32_t>(tiles, 1) * sub < want) sub <<= 1;
+    return sub;
+  };
+  uint32_t bm_cap = 1;
+  for (uint32_t i = 0; i < nq; ++i) {
+    uint64_t st0, sz;
+    leaf_rows(approx[i], &st0, &sz);
+    const uint32_t tiles = (uint32_t)((sz + T - 1) / T);
+    bm_cap = std::max<uint32_t>(bm_cap, (uint32_t)std::min<uint64_t>(hg::kBatchMaxSlots, (uint64_t)tiles * sub_of(tiles)));
+  }
+  std::vector<hg::BatchItem> items;
+  std::vector<uint32_t> slots(nq);
+  for (uint32_t i = 0; i < nq;) {
+    uint32_t j = i;
+    while (j < nq && approx[perm[j]] == approx[perm[i]] && j - i < 128) ++j;
+    uint64_t st0, sz;
+    leaf_rows(approx[perm[i]], &st0, &sz);
+    const uint32_t tiles = (uint32_t)((sz + T - 1) / T);
+    const uint32_t sub = sub_of(tiles);
+    const uint32_t use_tiles = std::min<uint32_t>(tiles, bm_cap / sub);
+    for (uint32_t t = 0; t < use_tiles; t += kBoundTilesPerItem)
+      items.push_back(
+          hg::BatchItem{st0, st0 + sz, i, j - i, t, std::min(use_tiles, t + kBoundTilesPerItem), sub, 0});
+    for (uint32_t x = i; x < j; ++x) slots[perm[x]] = use_tiles * sub;
+    i = j;
+  }
+  HCK(ensure_batch_scratch(ix, b.nq_cap, bucket_cap, bm_cap, (uint32_t)items.size()));
+  CK(cudaMemcpyAsync(b.qperm, perm.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(b.kq, kq.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(b.slots, slots.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
+  if (!items.empty())
+    CK(cudaMemcpyAsync(b.items, items.data(), sizeof(hg::BatchItem) * items.size(), cudaMemcpyHostToDevice, st));
+  CK(hg::launch_rows_to_bf16(d_Q, nq, (int)L, b.qbf, b.qn2, b.qnorm, st));
+
+  // 2. bound pass
+  hg::BatchGemm g{};
+  g.xbf = ix->bd.xbf;
+  g.qbf = b.qbf;
+  g.L = (int)L;
+  g.nrows = ix->n;
+  g.xn2 = ix->bd.xn2;
+  g.tile_n2 = ix->bd.tile_n2;
+  g.tile_norm = ix->bd.tile_norm;
+  g.qn2 = b.qn2;
+  g.qnorm = b.qnorm;
+  g.qperm = b.qperm;
+  g.nq = (int)nq;
+  g.mode = 0;
+  g.items = b.items;
+  g.nitems = (uint32_t)items.size();
+  g.bm = b.bm;
+  g.bm_cap = bm_cap;
+  g.tiles_per_item = kFilterTilesPerItem;
+  filter_coefficients(L, &g.c_dot, &g.c_sq);
+  g.bound = b.bound;
+  g.bucket = b.bucket;
+  g.bucket_cnt = b.bucket_cnt;
+  g.bucket_cap = bucket_cap;
+  g.work_head = b.heads;
+  CK(cudaMemsetAsync(b.bm, 0xff, sizeof(unsigned long long) * nq * bm_cap, st));
+  CK(cudaMemsetAsync(b.heads, 0, sizeof(uint32_t) * 4, st));
+  CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
+  CK(cudaMemsetAsync(b.stats, 0, sizeof(unsigned long long) * 8, st));
+  const int gemm_blocks = sms * kGemmBlocksPerSm;
+  CK(hg::launch_bf16_filter(g, gemm_blocks, st));
+  hg::BatchRank r{};
+  r.rows = ix->d.rows;
+  r.ids = ix->d.ids;
+  r.Q = d_Q;
+  r.L = (int)L;
+  r.nq = (int)nq;
+  r.kq = b.kq;
+  r.kmax = (int)kmax;
+  r.bm = b.bm;
+  r.bm_cap = bm_cap;
+  r.slots_of_query = b.slots;
+  r.bound = b.bound;
+  r.init = b.init;
+  r.init_cnt = b.init_cnt;
+  r.bucket = b.bucket;
+  r.bucket_cnt = b.bucket_cnt;
+  r.bucket_cap = bucket_cap;
+  r.dist_out = d_dist;
+  r.id_out = d_id;
+  r.ok_out = b.ok;
+  r.stats = b.stats;
+  CK(hg::launch_bound_select(r, st));
+  HCK(record(ev[1], st));
+  // 3. certified filter over every row
+  g.mode = 1;
+  g.work_head = b.heads + 1;
+  CK(hg::launch_bf16_filter(g, gemm_blocks, st));
+  HCK(record(ev[2], st));
+  // 4-5. exact re-rank and verification
+  CK(hg::launch_rerank(r, st));
+  HCK(record(ev[3], st));
+  std::vector<int> ok(nq);
+  unsigned long long hs[8];
+  CK(cudaMemcpyAsync(ok.data(), b.ok, sizeof(int) * nq, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(hs, b.stats, sizeof hs, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  // queries that did not verify: the plain path
+  hg_knn_opts po{};
+  po.mode = HG_MODE_PLAIN;
+  po.use_lb_sax = 1;
+  uint64_t fallbacks = 0;
+  for (uint32_t q = 0; q < nq; ++q) {
+    if (ok[q]) continue;
+    ++fallbacks;
+    HCK(knn_one(ix, d_Q + (uint64_t)q * L, (int)kq[q], po, d_dist + (uint64_t)q * kmax, d_id + (uint64_t)q * kmax,
+                st, nullptr));
+  }
+  HCK(record(ev[4], st));
+  CK(cudaStreamSynchronize(st));
+  if (stats) {
+    float t01 = 0, t12 = 0, t23 = 0, t34 = 0, t04 = 0;
+    cudaEventElapsedTime(&t01, ev[0], ev[1]);
+    cudaEventElapsedTime(&t12, ev[1], ev[2]);
+    cudaEventElapsedTime(&t23, ev[2], ev[3]);
+    cudaEventElapsedTime(&t34, ev[3], ev[4]);
+    cudaEventElapsedTime(&t04, ev[0], ev[4]);
+    stats->queries = nq;
+    stats->rows_visited = hs[0];
+    stats->chunks_loaded = hs[1];
+    stats->survivors = hs[2];
+    stats->bf16_pairs = (uint64_t)nq * ix->n;
+    stats->fallback_queries = fallbacks;
+    stats->bound_ms = t01;
+    stats->gemm_ms = t12;
+    stats->rerank_ms = t23;
+    stats->fallback_ms = t34;
+    stats->device_ms = t04;
   }
   return HG_OK;
 }
@@ -1364,6 +1686,49 @@ hg_status hg_knn(hg_index* ix, const float* queries, uint32_t nq, uint32_t k, co
     }
   }
   return HG_OK;
+}
+
+hg_status hg_knn_batch_device(hg_index* ix, const float* d_queries, uint32_t nq, const uint32_t* ks, uint32_t kmax,
+                              const hg_knn_opts* opts, float* d_dist_out, int64_t* d_id_out, void* stream,
+                              hg_query_stats* stats) {
+  if (!d_dist_out || !d_id_out) return set_error(HG_ERR_ARG, "hg_knn_batch_device: null output");
+  hg_knn_opts o{};
+  if (opts) o = *opts;
+  return knn_batch_impl(ix, d_queries, nq, ks, kmax, o, d_dist_out, d_id_out, (cudaStream_t)stream, stats);
+}
+
+hg_status hg_knn_batch(hg_index* ix, const float* queries, uint32_t nq, const uint32_t* ks, uint32_t kmax,
+                       const hg_knn_opts* opts, float* dist_out, int64_t* id_out, hg_query_stats* stats) {
+  if (!ix || (!queries && nq)) return set_error(HG_ERR_ARG, "hg_knn_batch: null argument");
+  if (nq == 0 || kmax == 0) {
+    hg_knn_opts o{};
+    return knn_batch_impl(ix, nullptr, 0, ks, kmax, o, nullptr, nullptr, nullptr, stats);
+  }
+  CK(cudaSetDevice(ix->device));
+  float* d_q = nullptr;
+  float* d_dist = nullptr;
+  int64_t* d_id = nullptr;
+  const size_t nout = (size_t)nq * kmax;
+  cudaError_t e = dalloc(&d_q, (size_t)nq * ix->L);
+  if (e == cudaSuccess) e = dalloc(&d_dist, nout);
+  if (e == cudaSuccess) e = dalloc(&d_id, nout);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_q, queries, sizeof(float) * nq * ix->L, cudaMemcpyHostToDevice, ix->stream);
+  hg_status s = e == cudaSuccess ? HG_OK : cuda_fail(e, "hg_knn_batch");
+  hg_knn_opts o{};
+  if (opts) o = *opts;
+  if (s == HG_OK) s = knn_batch_impl(ix, d_q, nq, ks, kmax, o, d_dist, d_id, ix->stream, stats);
+  if (s == HG_OK) {
+    if (id_out) e = cudaMemcpyAsync(id_out, d_id, sizeof(int64_t) * nout, cudaMemcpyDeviceToHost, ix->stream);
+    if (e == cudaSuccess && dist_out)
+      e = cudaMemcpyAsync(dist_out, d_dist, sizeof(float) * nout, cudaMemcpyDeviceToHost, ix->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
+    if (e != cudaSuccess) s = cuda_fail(e, "hg_knn_batch");
+  }
+  if (d_q) cudaFree(d_q);
+  if (d_dist) cudaFree(d_dist);
+  if (d_id) cudaFree(d_id);
+  return s;
 }
 
 hg_status hg_route(hg_index* ix, const float* queries, uint32_t nq, int32_t* leaf_out) {

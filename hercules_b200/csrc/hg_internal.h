@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/hercules_gpu.h"
+#include "hg_batch.h"
 #include "hg_kernels.h"
 
 namespace hg {
@@ -34,7 +35,7 @@ struct Node {
 
 // Device buffers sized by an index (one GPU per handle).
 struct DeviceIndex {
-  float* rows = nullptr;      // leaf-ordered rows, 32-row chunk-interleaved tiles
+  float* rows = nullptr;      // leaf-ordered rows, row-major (the leaves_raw.idx image)
   float* rows_rm = nullptr;   // optional row-major copy (write/export), may be null
   int64_t* ids = nullptr;     // dataset id of each leaf-ordered row
   uint8_t* sax = nullptr;     // iSAX word (16 symbols) of each leaf-ordered row
@@ -74,6 +75,37 @@ struct QueryScratch {
   int* err = nullptr;             // device error flag
 };
 
+// Batched path: BF16 copy of the rows and their norms, built on the first
+// batched call and kept with the index.
+struct BatchData {
+  void* xbf = nullptr;         // n x L BF16, row-major, leaf order
+  float* xn2 = nullptr;        // |x|^2 per row (FP64, rounded up)
+  float* tile_n2 = nullptr;    // per 128-row tile: max |x|^2
+  float* tile_norm = nullptr;  //                   max |x|
+};
+
+// Batched path scratch, grown to the largest batch seen.
+struct BatchScratch {
+  uint32_t nq_cap = 0, bucket_cap = 0, bm_cap = 0, items_cap = 0;
+  void* qbf = nullptr;
+  float* qn2 = nullptr;
+  float* qnorm = nullptr;
+  uint32_t* qperm = nullptr;
+  int* approx = nullptr;
+  uint32_t* kq = nullptr;
+  uint32_t* slots = nullptr;
+  BatchItem* items = nullptr;
+  unsigned long long* bm = nullptr;
+  float* bound = nullptr;
+  unsigned long long* init = nullptr;
+  int* init_cnt = nullptr;
+  uint32_t* bucket = nullptr;
+  uint32_t* bucket_cnt = nullptr;
+  int* ok = nullptr;
+  unsigned long long* stats = nullptr;
+  uint32_t* heads = nullptr;
+};
+
 }  // namespace hg
 
 struct hg_index {
@@ -88,6 +120,8 @@ struct hg_index {
   bool has_ids = false;         // false for an index built by the reference
   hg::DeviceIndex d;
   hg::QueryScratch s;
+  hg::BatchData bd;
+  hg::BatchScratch bs;
   cudaStream_t stream = nullptr;
   int max_seg = 0;
 };

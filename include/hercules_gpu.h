@@ -74,18 +74,30 @@ typedef struct {
   uint64_t rows_considered;   /* rows of candidate leaves seen by the LB_SAX filter */
   uint64_t filter_launches;   /* LB_SAX filter launches (profile = 1) */
   double filter_ms;           /* their summed device time (profile = 1) */
+  /* batched path (HG_MODE_BATCH, hg_knn_batch) */
+  uint64_t bf16_pairs;        /* (query, row) pairs through the BF16 filter */
+  uint64_t survivors;         /* pairs kept by the certified filter */
+  uint64_t fallback_queries;  /* queries answered by the plain path instead */
+  double bound_ms;            /* device time: BF16 pass over the approximate leaves + bound */
+  double gemm_ms;             /* device time: BF16 filter over every row */
+  double rerank_ms;           /* device time: exact re-rank of the survivors */
+  double fallback_ms;         /* device time: plain path for the fallback queries */
 } hg_query_stats;
 
 /* Search mode. */
 #define HG_MODE_PLAIN 0    /* exact_de_knn_search per query */
 #define HG_MODE_PSCAN 1    /* parallel scan of every row (code/pscan) */
+#define HG_MODE_BATCH 2    /* all queries at once: BF16 tensor-core filter with a
+                              certified error bound + exact FP32 re-rank */
 
 typedef struct {
   int mode;           /* HG_MODE_* */
   int use_lb_sax;     /* 1: per-row LB_SAX filter before the distance */
   int profile;        /* 1: time every leaf-scan launch with CUDA events */
   int approx_blocks;  /* blocks of the approximate-leaf scan (0 = one per SM) */
-  int reserved[4];
+  int bucket_cap;     /* HG_MODE_BATCH: filter survivors kept per query before the
+                         query falls back to the plain path (0 = 16384) */
+  int reserved[3];
 } hg_knn_opts;
 
 /* ---- status ----------------------------------------------------------- */
@@ -164,6 +176,28 @@ HG_API hg_status hg_knn(hg_index *ix, const float *queries, uint32_t nq, uint32_
 HG_API hg_status hg_knn_device(hg_index *ix, const float *d_queries, uint32_t nq, uint32_t k,
                         const hg_knn_opts *opts, float *d_dist_out, int64_t *d_id_out,
                         void *stream, hg_query_stats *stats);
+
+/* Batched exact k-NN: every query of the call at once, with per-query k.
+ * Same answers as hg_knn (bit-identical distances and ids).  The reference
+ * answers queries one at a time (hercules_knn_query_binary_file loops over
+ * exact_de_knn_search, hercules_file_loaders.c:99-294); this entry point
+ * replaces that loop.  A BF16 tensor-core pass computes |q|^2 + |x|^2 - 2 q.x
+ * for every (query, row) pair against FP64 norms, keeps the pairs within a
+ * certified rounding-error bound of an exact k-th-distance bound taken from
+ * the query's approximate leaf, and re-ranks them in FP32 in the reference's
+ * order; a query whose survivors overflow opts->bucket_cap goes through the
+ * plain path.  ks: k of each query (HOST array, NULL = every query uses
+ * kmax), each 1..kmax; outputs are nq x kmax (entries past a query's k are
+ * +inf / -1).  HOST buffers; opts->mode is ignored. */
+HG_API hg_status hg_knn_batch(hg_index *ix, const float *queries, uint32_t nq, const uint32_t *ks,
+                              uint32_t kmax, const hg_knn_opts *opts, float *dist_out, int64_t *id_out,
+                              hg_query_stats *stats);
+
+/* Same with queries and outputs in device memory, ordered on `stream`
+ * (NULL = the handle's stream); ks stays a host array. */
+HG_API hg_status hg_knn_batch_device(hg_index *ix, const float *d_queries, uint32_t nq, const uint32_t *ks,
+                                     uint32_t kmax, const hg_knn_opts *opts, float *d_dist_out,
+                                     int64_t *d_id_out, void *stream, hg_query_stats *stats);
 
 /* The approximate leaf of each query: the leaf the query routes to
  * (approximate_knn_search's traversal, hercules_query_engine.c:176-222). */
