@@ -50,6 +50,7 @@ class QueryStats(ctypes.Structure):
                 ("rows_considered", ctypes.c_uint64), ("filter_launches", ctypes.c_uint64),
                 ("filter_ms", ctypes.c_double), ("bf16_pairs", ctypes.c_uint64),
                 ("survivors", ctypes.c_uint64), ("fallback_queries", ctypes.c_uint64),
+                ("retried_queries", ctypes.c_uint64),
                 ("bound_ms", ctypes.c_double), ("gemm_ms", ctypes.c_double), ("rerank_ms", ctypes.c_double),
                 ("fallback_ms", ctypes.c_double)]
 

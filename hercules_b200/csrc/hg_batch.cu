@@ -3,14 +3,16 @@
 // summation order (ts_euclidean_distance_SIMD, ts.c:83-109).
 //
 // For thousands of queries at once the dot products q.x of every (query,
-// row) pair are cheap on the tensor cores.  With BF16 operands (unit
-// roundoff u = 2^-8) and FP32 accumulation,
-//     d~(q, x) = |q|^2 + |x|^2 - 2 (q~ . x~)
-// differs from the reference's FP32 squared distance by at most
-//     err(q, tile) = c_dot |q| max_tile |x| + c_sq (|q|^2 + max_tile |x|^2 + B) + 1e-5
-//     c_dot = 2 (2u + u^2 + L 2^-20)        BF16 rounding of q and x, FP32 accumulation
-//     c_sq  = (L/8 + 16) 2^-22              rounded-up FP64 norms, the reference's own
-//                                           FP32 summation, the FP32 epilogue
+// row) pair are cheap on the tensor cores.  With q~, x~ the BF16 roundings of
+// q and x, r_q = q - q~, r_x = x - x~ and FP32 accumulation,
+//     d~(q, x) = |q|^2 + |x|^2 - 2 acc(q~ . x~)
+// and q.x - q~.x~ = q~.r_x + r_q.x~ + r_q.r_x, so by Cauchy-Schwarz
+//     |d~ - D| <= 2 (|q~| |r_x| + |r_q| |x~| + |r_q| |r_x|) + 2 L 2^-20 |q~| |x~|
+// (the last term covers the tensor cores' FP32 accumulation), and D differs
+// from the reference's FP32 sum by (L/8 + 4) 2^-24 D at most.  Per 128-row
+// tile the row terms are replaced by their maxima:
+//     err(q, tile) = 2 (1 + 2^-20) (|q~| R + r |X~| + r R + L 2^-20 |q~| X~)
+//                    + c_sq (|q|^2 + max |x|^2 + B) + 1e-5,   c_sq = (L/8 + 16) 2^-22
 // with |x|^2 and |q|^2 computed in FP64 and rounded up.  The pipeline:
 //   1. route every query to its approximate leaf (approximate_knn_search's
 //      traversal, hercules_query_engine.c:176-222);
@@ -41,44 +43,67 @@ constexpr int kBM = kBatchTileRows, kBN = 128, kBK = 64, kStages = 3, kGemmThrea
 // preparation
 // ---------------------------------------------------------------------------
 
-// One warp per row: BF16 copy (round to nearest) and |x|^2 in FP64 rounded up.
+// One warp per row: BF16 copy (round to nearest) and, in FP64 rounded up,
+// meta = {|x|^2, |x~|, |x - x~|, 0} (x~ the BF16 row).
 __global__ void k_rows_to_bf16(const float* __restrict__ rows, uint64_t n, int L, __nv_bfloat16* __restrict__ out,
-                               float* __restrict__ n2, float* __restrict__ norm) {
+                               float4* __restrict__ meta) {
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= n) return;
   const float4* x = reinterpret_cast<const float4*>(rows + w * L);
   __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(out + w * L);
-  double acc = 0.0;
+  double a2 = 0.0, t2 = 0.0, r2 = 0.0;
+  auto acc = [&](float v, float t) {
+    const double dv = v, dt = t, dr = dv - dt;  // exact: both are floats
+    a2 += dv * dv;
+    t2 += dt * dt;
+    r2 += dr * dr;
+  };
   for (int i = lane; i < (L >> 2); i += 32) {
     const float4 v = x[i];
-    acc += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
-    o[2 * i] = __floats2bfloat162_rn(v.x, v.y);
-    o[2 * i + 1] = __floats2bfloat162_rn(v.z, v.w);
+    const __nv_bfloat162 b0 = __floats2bfloat162_rn(v.x, v.y), b1 = __floats2bfloat162_rn(v.z, v.w);
+    o[2 * i] = b0;
+    o[2 * i + 1] = b1;
+    const float2 f0 = __bfloat1622float2(b0), f1 = __bfloat1622float2(b1);
+    acc(v.x, f0.x);
+    acc(v.y, f0.y);
+    acc(v.z, f1.x);
+    acc(v.w, f1.y);
   }
 #pragma unroll
-  for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(HG_FULL, acc, s);
+  for (int s = 16; s > 0; s >>= 1) {
+    a2 += __shfl_xor_sync(HG_FULL, a2, s);
+    t2 += __shfl_xor_sync(HG_FULL, t2, s);
+    r2 += __shfl_xor_sync(HG_FULL, r2, s);
+  }
   if (lane == 0) {
-    n2[w] = __double2float_ru(acc * (1.0 + 1e-12));
-    if (norm) norm[w] = __double2float_ru(sqrt(acc) * (1.0 + 1e-12));
+    // FP64 sums of L non-negative terms: relative error below L 2^-53
+    const double up = 1.0 + 1e-12;
+    meta[w] = make_float4(__double2float_ru(a2 * up), __double2float_ru(sqrt(t2) * up),
+                          __double2float_ru(sqrt(r2) * up), 0.0f);
   }
 }
 
-// Per 128-row tile of the leaf-ordered rows: max |x|^2 and max |x|.
-__global__ void k_tile_norms(const float* __restrict__ n2, uint64_t n, float* __restrict__ tile_n2,
-                             float* __restrict__ tile_norm) {
+// Per 128-row tile of the leaf-ordered rows: the maximum of each meta field.
+__global__ void k_tile_norms(const float4* __restrict__ meta, uint64_t n, float4* __restrict__ tile_meta) {
   const uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const uint64_t r0 = t * kBM;
   if (r0 >= n) return;
-  float m = 0.0f;
-  for (uint64_t r = r0 + lane; r < r0 + kBM && r < n; r += 32) m = fmaxf(m, n2[r]);
-#pragma unroll
-  for (int s = 16; s > 0; s >>= 1) m = fmaxf(m, __shfl_xor_sync(HG_FULL, m, s));
-  if (lane == 0) {
-    tile_n2[t] = m;
-    tile_norm[t] = __fsqrt_ru(m);
+  float4 m = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  for (uint64_t r = r0 + lane; r < r0 + kBM && r < n; r += 32) {
+    const float4 v = meta[r];
+    m.x = fmaxf(m.x, v.x);
+    m.y = fmaxf(m.y, v.y);
+    m.z = fmaxf(m.z, v.z);
   }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    m.x = fmaxf(m.x, __shfl_xor_sync(HG_FULL, m.x, s));
+    m.y = fmaxf(m.y, __shfl_xor_sync(HG_FULL, m.y, s));
+    m.z = fmaxf(m.z, __shfl_xor_sync(HG_FULL, m.z, s));
+  }
+  if (lane == 0) tile_meta[t] = m;
 }
 
 // ---------------------------------------------------------------------------
@@ -132,7 +157,7 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_bf16_filter(BatchGemm a) {
   unsigned char* sB = gsm + kStages * kBM * kBK * 2;  // kStages x 16 KB of queries
   __shared__ uint32_t s_item;
   __shared__ uint32_t s_qidx[kBN];
-  __shared__ float s_qn2[kBN], s_qn[kBN], s_qb[kBN];
+  __shared__ float s_qn2[kBN], s_qt[kBN], s_qr[kBN], s_qb[kBN];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps, 64 rows x 32 queries each
   const int g = lane >> 2, tig = lane & 3;
@@ -173,8 +198,10 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_bf16_filter(BatchGemm a) {
       const uint32_t q = tid < (int)qcnt ? a.qperm[qoff + tid] : 0xffffffffu;
       s_qidx[tid] = q;
       const bool ok = q != 0xffffffffu;
-      s_qn2[tid] = ok ? a.qn2[q] : 0.0f;
-      s_qn[tid] = ok ? a.qnorm[q] : 0.0f;
+      const float4 qm = ok ? a.qmeta[q] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      s_qn2[tid] = qm.x;
+      s_qt[tid] = qm.y;
+      s_qr[tid] = qm.z;
       // the filter skips queries without a finite bound (they take the plain path)
       const float b = (ok && a.mode == 1) ? a.bound[q] : 0.0f;
       s_qb[tid] = (ok && b < inf) ? b : -1.0f;
@@ -252,13 +279,14 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_bf16_filter(BatchGemm a) {
       const uint64_t nvalid = row0 < re ? (re - row0 < (uint64_t)kBM ? re - row0 : (uint64_t)kBM) : 0;
       if (a.mode == 1) {
         const uint64_t gt = row0 / kBM;
-        const float tn = a.tile_norm[gt], tn2 = a.tile_n2[gt];
+        const float4 tm = a.tile_meta[gt];  // max |x|^2, max |x~|, max |x - x~|
         float thr[8];
 #pragma unroll
         for (int ci = 0; ci < 8; ++ci) {
           const int col = wn * 32 + (ci >> 1) * 8 + tig * 2 + (ci & 1);
-          const float b = s_qb[col], qn2 = s_qn2[col];
-          const float err = a.c_dot * s_qn[col] * tn + a.c_sq * (qn2 + tn2 + b) + 1e-5f;
+          const float b = s_qb[col], qn2 = s_qn2[col], qt = s_qt[col], qr = s_qr[col];
+          const float err = 2.000002f * (qt * tm.z + qr * tm.y + qr * tm.z + a.c_acc * qt * tm.y) +
+                            a.c_sq * (qn2 + tm.x + b) + 1e-5f;
           // keep when |x|^2 + (|q|^2 - B - err) - 2 acc <= 0
           thr[ci] = b >= 0.0f ? qn2 - b - err : inf;
         }
@@ -269,7 +297,7 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_bf16_filter(BatchGemm a) {
             const int r = wm * 64 + mi * 16 + g + h * 8;
             if ((uint64_t)r >= nvalid) continue;
             const uint64_t row = row0 + r;
-            const float xn = a.xn2[row];
+            const float xn = a.xmeta[row].x;
 #pragma unroll
             for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
@@ -300,7 +328,7 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_bf16_filter(BatchGemm a) {
                 const int r = wm * 64 + mi * 16 + g + h * 8;
                 if ((uint64_t)r < nvalid) {
                   const uint64_t row = row0 + r;
-                  const float d = a.xn2[row] + qn2 - 2.0f * acc[mi][ni][h * 2 + e];
+                  const float d = a.xmeta[row].x + qn2 - 2.0f * acc[mi][ni][h * 2 + e];
                   const unsigned long long key = ((unsigned long long)ordered_key(d) << 32) | (uint32_t)row;
                   best = key < best ? key : best;
                 }
@@ -384,94 +412,214 @@ __global__ void __launch_bounds__(kSelThreads) k_bound_select(BatchRank a) {
   }
 }
 
-// Steps 4-5: one warp per query re-ranks its bucket with 4-lane slots (lane
-// j of a slot computes chunk ch + j; the slot adds the four in order), from
-// step 2's list and bound.
+// Steps 4-5 run in three kernels over the queries qlist[0 .. nlist) (all
+// queries when qlist is null).  Plan: each query's surviving rows (the first
+// bucket_cap of them when its bucket overflowed) are cut into at most
+// kBatchMaxSeg segments of at least kBatchSegMin rows; segments are numbered
+// over the list (exclusive prefix seg_prefix, by list position).
+__global__ void __launch_bounds__(1024) k_rerank_plan(BatchRank a) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t carry;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  const float inf = __int_as_float(0x7f800000);
+  for (int base = 0; base < a.nlist; base += 1024) {
+    const int i = base + tid;
+    uint32_t nseg = 0, seg = 0;
+    if (i < a.nlist) {
+      const int q = a.qlist ? (int)a.qlist[i] : i;
+      const uint32_t n = a.bound[q] < inf ? min(a.bucket_cnt[q], a.bucket_cap) : 0u;
+      seg = max((uint32_t)kBatchSegMin, (n + kBatchMaxSeg - 1) / kBatchMaxSeg);
+      nseg = (n + seg - 1) / seg;
+      a.seg_rows[i] = seg;
+      a.qbound[q] = __float_as_uint(a.bound[q]);
+    }
+    // block-wide exclusive scan of nseg
+    uint32_t v = nseg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(HG_FULL, v, o);
+      if (lane >= o) v += t;
+    }
+    if (lane == 31) warp_sums[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t w = warp_sums[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(HG_FULL, w, o);
+        if (lane >= o) w += t;
+      }
+      warp_sums[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t excl = carry + (wid ? warp_sums[wid - 1] : 0u) + v - nseg;
+    if (i < a.nlist) a.seg_prefix[i] = excl;
+    __syncthreads();
+    if (tid == 1023) carry = excl + nseg;
+    __syncthreads();
+  }
+  if (tid == 0) {
+    a.seg_prefix[a.nlist] = carry;
+    a.heads[0] = 0;  // work counter of k_rerank_part
+  }
+}
+
+// Segment re-rank: persistent warps take segments from a counter.  A warp
+// starts from step 2's list, shares the query's running k-th distance through
+// qbound (float bits, atomicMin) and writes its compacted list as one part.
+// Within the warp, 4-lane slots: lane j of a slot computes chunk ch + j and
+// the slot adds the four in order (ts_euclidean_distance_SIMD's order).
 constexpr int kRankWarps = 8;
-__global__ void __launch_bounds__(kRankWarps * 32) k_rerank(BatchRank a) {
+__global__ void __launch_bounds__(kRankWarps * 32) k_rerank_part(BatchRank a) {
   __shared__ unsigned long long lists[kRankWarps][kWarpListCap];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int q = blockIdx.x * kRankWarps + wib;
-  if (q >= a.nq) return;
   const int slot_lead = lane & ~3, j = lane & 3;
   unsigned long long* list = lists[wib];
-  const int k = (int)a.kq[q];
-  const float Bq = a.bound[q];
-  const int c0 = a.init_cnt[q];
-  for (int i = lane; i < kWarpListCap; i += 32) list[i] = i < c0 ? a.init[(uint64_t)q * kMaxK + i] : ~0ull;
-  __syncwarp();
-  int cnt = c0;
   const float inf = __int_as_float(0x7f800000);
-  float T = cnt == k ? __uint_as_float((uint32_t)(list[k - 1] >> 32)) : inf;
-  float B = T;
-  const uint32_t nb = a.bucket_cnt[q];
-  const bool usable = Bq < inf && nb <= a.bucket_cap;
-  const uint32_t total = usable ? nb : 0u;
-  const uint32_t* bk = a.bucket + (uint64_t)q * a.bucket_cap;
-  const float* qv = a.Q + (uint64_t)q * a.L;
+  const uint32_t total_items = a.seg_prefix[a.nlist];
   const int nch = a.L >> 3;
-  uint32_t next = 0;
-  bool valid = false;
-  uint32_t row = 0;
-  int ch = 0;
-  float dist = 0.0f;
-  unsigned long long n_rows = 0, n_chunks = 0;
   const uint32_t leaders = 0x11111111u;
+  unsigned long long n_rows = 0, n_chunks = 0;
   for (;;) {
-    const uint32_t need = __ballot_sync(HG_FULL, !valid) & leaders;
-    if (need && next < total) {
-      const int r = __popc(need & ((1u << slot_lead) - 1));
-      const uint32_t avail = min(total - next, 8u);
-      if (((need >> slot_lead) & 1u) && (uint32_t)r < avail) {
-        row = bk[next + r];
-        valid = true;
-        dist = 0.0f;
-        ch = 0;
-        if (j == 0) ++n_rows;
-      }
-      next += min((uint32_t)__popc(need), avail);
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&a.heads[0], 1u);
+    item = __shfl_sync(HG_FULL, item, 0);
+    if (item >= total_items) break;
+    // list position of the item: the last i with seg_prefix[i] <= item
+    int lo = 0, hi = a.nlist - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.seg_prefix[mid] <= item) lo = mid;
+      else hi = mid - 1;
     }
-    if (!__any_sync(HG_FULL, valid)) break;
-    const int c = ch + j;
-    float d = 0.0f;
-    if (valid && c < nch) d = hg_chunk_d2(qv + c * 8, a.rows + (uint64_t)row * a.L + c * 8);
-    bool finished = false;
+    const int q = a.qlist ? (int)a.qlist[lo] : lo;
+    const uint32_t seg = item - a.seg_prefix[lo];
+    const uint32_t per = a.seg_rows[lo];
+    const uint32_t first = seg * per;
+    const uint32_t last = min(a.bucket_cnt[q], first + per);
+    const int k = (int)a.kq[q];
+    const int c0 = a.init_cnt[q];
+    for (int i = lane; i < kWarpListCap; i += 32) list[i] = i < c0 ? a.init[(uint64_t)q * kMaxK + i] : ~0ull;
+    __syncwarp();
+    int cnt = c0;
+    float T = cnt == k ? __uint_as_float((uint32_t)(list[k - 1] >> 32)) : inf;
+    float B = fminf(T, __uint_as_float(ld_volatile(&a.qbound[q])));
+    const uint32_t* bk = a.bucket + (uint64_t)q * a.bucket_cap;
+    const float* qv = a.Q + (uint64_t)q * a.L;
+    uint32_t next = first;
+    bool valid = false;
+    uint32_t row = 0;
+    int ch = 0;
+    float dist = 0.0f;
+    for (;;) {
+      const uint32_t need = __ballot_sync(HG_FULL, !valid) & leaders;
+      if (need && next < last) {
+        const int r = __popc(need & ((1u << slot_lead) - 1));
+        const uint32_t avail = min(last - next, 8u);
+        if (((need >> slot_lead) & 1u) && (uint32_t)r < avail) {
+          row = bk[next + r];
+          valid = true;
+          dist = 0.0f;
+          ch = 0;
+          if (j == 0) ++n_rows;
+        }
+        next += min((uint32_t)__popc(need), avail);
+        // the other warps of this query may have lowered its k-th distance
+        B = fminf(B, __uint_as_float(ld_volatile(&a.qbound[q])));
+      }
+      if (!__any_sync(HG_FULL, valid)) break;
+      const int c = ch + j;
+      float d = 0.0f;
+      if (valid && c < nch) d = hg_chunk_d2(qv + c * 8, a.rows + (uint64_t)row * a.L + c * 8);
+      bool finished = false;
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const float dt = __shfl_sync(HG_FULL, d, slot_lead + t);
-      if (valid && ch + t < nch) {
-        dist = __fadd_rn(dist, dt);
-        if (j == 0) ++n_chunks;
-        if (dist > B) valid = false;  // partial sums only grow: this row cannot enter
+      for (int t = 0; t < 4; ++t) {
+        const float dt = __shfl_sync(HG_FULL, d, slot_lead + t);
+        if (valid && ch + t < nch) {
+          dist = __fadd_rn(dist, dt);
+          if (j == 0) ++n_chunks;
+          if (dist > B) valid = false;  // partial sums only grow: this row cannot enter
+        }
       }
-    }
-    if (valid) {
-      ch += 4;
-      if (ch >= nch) {
-        finished = true;
-        valid = false;
+      if (valid) {
+        ch += 4;
+        if (ch >= nch) {
+          finished = true;
+          valid = false;
+        }
       }
+      const bool take = finished && j == 0;
+      warp_list_add(list, cnt, T, k, &a.qbound[q], take, dist, take ? (uint32_t)a.ids[row] : 0u);
+      B = fminf(B, T);
     }
-    const bool take = finished && j == 0;
-    warp_list_add(list, cnt, T, k, nullptr, take, dist, take ? (uint32_t)a.ids[row] : 0u);
-    B = fminf(B, T);
-  }
-  cnt = warp_compact(list, cnt, k);
-  const bool ok = usable && cnt == k && __uint_as_float((uint32_t)(list[k - 1] >> 32)) <= Bq;
-  for (int i = lane; i < a.kmax; i += 32) {
-    const bool have = i < cnt;
-    a.dist_out[(uint64_t)q * a.kmax + i] = have ? __uint_as_float((uint32_t)(list[i] >> 32)) : inf;
-    a.id_out[(uint64_t)q * a.kmax + i] = have ? (int64_t)(uint32_t)list[i] : -1;
+    cnt = warp_compact(list, cnt, k);
+    unsigned long long* part = a.parts + (uint64_t)item * a.kmax;
+    for (int i = lane; i < cnt; i += 32) part[i] = list[i];
+    if (lane == 0) a.part_cnt[item] = cnt;
+    __syncwarp();
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     n_rows += __shfl_xor_sync(HG_FULL, n_rows, o);
     n_chunks += __shfl_xor_sync(HG_FULL, n_chunks, o);
   }
-  if (lane == 0) {
-    a.ok_out[q] = ok ? 1 : 0;
+  if (lane == 0 && n_rows) {
     atomicAdd(&a.stats[0], n_rows);
     atomicAdd(&a.stats[1], n_chunks);
+  }
+}
+
+// Merge: one warp per query folds its starting list and its parts into the
+// answer (k distinct distances, lowest id per distance) and verifies it:
+//   ok 1: the filter kept every row within B_q and the k-th distance is <= B_q;
+//   ok 0: the bucket overflowed but its first rows gave k distances below
+//         B_q: B_q is lowered to the k-th, the list kept, the query retried;
+//   ok -1: neither: the plain path answers it.
+__global__ void __launch_bounds__(kRankWarps * 32) k_rerank_merge(BatchRank a) {
+  __shared__ unsigned long long lists[kRankWarps][kWarpListCap];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int pos = blockIdx.x * kRankWarps + wib;
+  if (pos >= a.nlist) return;
+  const int q = a.qlist ? (int)a.qlist[pos] : pos;
+  unsigned long long* list = lists[wib];
+  const int k = (int)a.kq[q];
+  const float inf = __int_as_float(0x7f800000);
+  const int c0 = a.init_cnt[q];
+  for (int i = lane; i < kWarpListCap; i += 32) list[i] = i < c0 ? a.init[(uint64_t)q * kMaxK + i] : ~0ull;
+  __syncwarp();
+  int cnt = c0;
+  float T = cnt == k ? __uint_as_float((uint32_t)(list[k - 1] >> 32)) : inf;
+  const uint32_t p0 = a.seg_prefix[pos], p1 = a.seg_prefix[pos + 1];
+  for (uint32_t p = p0; p < p1; ++p) {
+    const int pc = a.part_cnt[p];
+    const unsigned long long* part = a.parts + (uint64_t)p * a.kmax;
+    for (int base = 0; base < pc; base += 32) {
+      const bool take = base + lane < pc;
+      const unsigned long long v = take ? part[base + lane] : 0ull;
+      warp_list_add(list, cnt, T, k, nullptr, take, __uint_as_float((uint32_t)(v >> 32)), (uint32_t)v);
+    }
+  }
+  cnt = warp_compact(list, cnt, k);
+  const float Bq = a.bound[q];
+  const uint32_t nb = a.bucket_cnt[q];
+  const float dk = cnt == k ? __uint_as_float((uint32_t)(list[k - 1] >> 32)) : inf;
+  const int ok = (Bq < inf && nb <= a.bucket_cap && dk <= Bq) ? 1 : ((Bq < inf && dk < Bq) ? 0 : -1);
+  for (int i = lane; i < a.kmax; i += 32) {
+    const bool have = i < cnt;
+    a.dist_out[(uint64_t)q * a.kmax + i] = have ? __uint_as_float((uint32_t)(list[i] >> 32)) : inf;
+    a.id_out[(uint64_t)q * a.kmax + i] = have ? (int64_t)(uint32_t)list[i] : -1;
+  }
+  if (ok == 0) {
+    for (int i = lane; i < cnt; i += 32) a.init[(uint64_t)q * kMaxK + i] = list[i];
+    if (lane == 0) {
+      a.init_cnt[q] = cnt;
+      a.bound[q] = dk;
+    }
+  }
+  if (lane == 0) {
+    a.ok_out[q] = ok;
     atomicAdd(&a.stats[2], (unsigned long long)nb);
   }
 }
@@ -482,17 +630,16 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank(BatchRank a) {
 
 static inline unsigned nblk(uint64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-cudaError_t launch_rows_to_bf16(const float* rows, uint64_t n, int L, void* out, float* n2, float* norm,
-                                cudaStream_t s) {
+cudaError_t launch_rows_to_bf16(const float* rows, uint64_t n, int L, void* out, float4* meta, cudaStream_t s) {
   if (!n) return cudaSuccess;
-  k_rows_to_bf16<<<nblk(n * 32, 256), 256, 0, s>>>(rows, n, L, static_cast<__nv_bfloat16*>(out), n2, norm);
+  k_rows_to_bf16<<<nblk(n * 32, 256), 256, 0, s>>>(rows, n, L, static_cast<__nv_bfloat16*>(out), meta);
   return cudaGetLastError();
 }
 
-cudaError_t launch_tile_norms(const float* n2, uint64_t n, float* tile_n2, float* tile_norm, cudaStream_t s) {
+cudaError_t launch_tile_norms(const float4* meta, uint64_t n, float4* tile_meta, cudaStream_t s) {
   const uint64_t nt = (n + kBM - 1) / kBM;
   if (!nt) return cudaSuccess;
-  k_tile_norms<<<nblk(nt * 32, 256), 256, 0, s>>>(n2, n, tile_n2, tile_norm);
+  k_tile_norms<<<nblk(nt * 32, 256), 256, 0, s>>>(meta, n, tile_meta);
   return cudaGetLastError();
 }
 
@@ -525,9 +672,15 @@ cudaError_t launch_bound_select(const BatchRank& r, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_rerank(const BatchRank& r, cudaStream_t s) {
-  if (!r.nq) return cudaSuccess;
-  k_rerank<<<nblk(r.nq, kRankWarps), kRankWarps * 32, 0, s>>>(r);
+cudaError_t launch_rerank(const BatchRank& r, int part_blocks, cudaStream_t s) {
+  if (!r.nlist) return cudaSuccess;
+  k_rerank_plan<<<1, 1024, 0, s>>>(r);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_rerank_part<<<part_blocks, kRankWarps * 32, 0, s>>>(r);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_rerank_merge<<<nblk(r.nlist, kRankWarps), kRankWarps * 32, 0, s>>>(r);
   return cudaGetLastError();
 }
 

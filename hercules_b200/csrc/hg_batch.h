@@ -10,6 +10,8 @@ namespace hg {
 
 constexpr int kBatchTileRows = 128;   // rows per tensor-core tile (and per tile norm)
 constexpr int kBatchMaxSlots = 4096;  // bound slots per query (sorted in one block)
+constexpr int kBatchMaxSeg = 16;      // re-rank segments per query
+constexpr int kBatchSegMin = 256;     // rows per re-rank segment, at least
 
 // One work item of the bound pass: tiles [tile_lo, tile_hi) of the rows
 // [row_begin, row_end) (one approximate leaf) against queries
@@ -27,11 +29,9 @@ struct BatchGemm {
   const void* qbf;  // BF16 queries
   int L;
   uint64_t nrows;
-  const float* xn2;        // |x|^2 rounded up
-  const float* tile_n2;    // per 128-row tile: max |x|^2
-  const float* tile_norm;  //                   max |x|
-  const float* qn2;        // |q|^2 rounded up
-  const float* qnorm;      // |q| rounded up
+  const float4* xmeta;      // per row: |x|^2, |x~|, |x - x~|, 0 (FP64, rounded up)
+  const float4* tile_meta;  // per 128-row tile: the maxima of xmeta
+  const float4* qmeta;      // per query: |q|^2, |q~|, |q - q~|, 0
   const uint32_t* qperm;   // queries in tile order
   int nq;
   int mode;  // 0: bound pass over the items; 1: filter over every row
@@ -42,7 +42,7 @@ struct BatchGemm {
   uint32_t bm_cap;
   // mode 1
   uint32_t tiles_per_item;
-  float c_dot, c_sq;       // error-bound coefficients
+  float c_acc, c_sq;       // error-bound coefficients: L 2^-20 and (L/8 + 16) 2^-22
   const float* bound;      // B_q
   uint32_t* bucket;        // [q][bucket_cap] surviving rows
   uint32_t* bucket_cnt;    // 0 before the launch
@@ -69,16 +69,24 @@ struct BatchRank {
   uint32_t bucket_cap;
   float* dist_out;  // [q][kmax]
   int64_t* id_out;
-  int* ok_out;                // 1: verified; 0: take the plain path
+  int* ok_out;                // 1 verified, 0 retry with the lowered bound, -1 plain path
   unsigned long long* stats;  // [0] rows re-ranked [1] chunks [2] filter survivors
+  // re-rank of the queries qlist[0 .. nlist) (qlist null: 0 .. nlist)
+  const uint32_t* qlist;
+  int nlist;
+  uint32_t* seg_rows;         // [list position] rows per segment
+  uint32_t* seg_prefix;       // [nlist + 1] exclusive prefix of segments
+  uint32_t* qbound;           // [q] running k-th distance (float bits)
+  unsigned long long* parts;  // [segment][kmax] compacted lists
+  int* part_cnt;              // [segment]
+  uint32_t* heads;            // [0] segment counter
 };
 
-cudaError_t launch_rows_to_bf16(const float* rows, uint64_t n, int L, void* out, float* n2, float* norm,
-                                cudaStream_t s);
-cudaError_t launch_tile_norms(const float* n2, uint64_t n, float* tile_n2, float* tile_norm, cudaStream_t s);
+cudaError_t launch_rows_to_bf16(const float* rows, uint64_t n, int L, void* out, float4* meta, cudaStream_t s);
+cudaError_t launch_tile_norms(const float4* meta, uint64_t n, float4* tile_meta, cudaStream_t s);
 size_t bf16_filter_smem();
 cudaError_t launch_bf16_filter(const BatchGemm& g, int blocks, cudaStream_t s);
 cudaError_t launch_bound_select(const BatchRank& r, cudaStream_t s);
-cudaError_t launch_rerank(const BatchRank& r, cudaStream_t s);
+cudaError_t launch_rerank(const BatchRank& r, int part_blocks, cudaStream_t s);
 
 }  // namespace hg

@@ -305,13 +305,11 @@ static void free_device(hg_index* ix) {
   s.kmax = 0;
   hg::BatchData& bd = ix->bd;
   dfree(bd.xbf);
-  dfree(bd.xn2);
-  dfree(bd.tile_n2);
-  dfree(bd.tile_norm);
+  dfree(bd.xmeta);
+  dfree(bd.tile_meta);
   hg::BatchScratch& b = ix->bs;
   dfree(b.qbf);
-  dfree(b.qn2);
-  dfree(b.qnorm);
+  dfree(b.qmeta);
   dfree(b.qperm);
   dfree(b.approx);
   dfree(b.kq);
@@ -326,6 +324,12 @@ static void free_device(hg_index* ix) {
   dfree(b.ok);
   dfree(b.stats);
   dfree(b.heads);
+  dfree(b.qlist);
+  dfree(b.seg_rows);
+  dfree(b.seg_prefix);
+  dfree(b.qbound);
+  dfree(b.parts);
+  dfree(b.part_cnt);
   b = hg::BatchScratch{};
 }
 
@@ -1221,7 +1225,9 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
 constexpr int kGemmBlocksPerSm = 2;       // k_bf16_filter: 2 x 256 threads, 98 KB smem each
 constexpr uint32_t kBoundTilesPerItem = 8;
 constexpr uint32_t kFilterTilesPerItem = 32;  // 4096 rows per item: a row chunk stays in L2
-constexpr uint32_t kDefaultBucket = 16384;
+constexpr uint32_t kDefaultBucket = 65536;
+constexpr int kBatchRetries = 3;  // filter rounds after the first for overflowed buckets
+constexpr int kRerankBlocksPerSm = 8;      // k_rerank_part: 8 x 8 warps per SM
 
 static hg_status ensure_batch_data(hg_index* ix, cudaStream_t st) {
   hg::BatchData& b = ix->bd;
@@ -1230,21 +1236,25 @@ static hg_status ensure_batch_data(hg_index* ix, cudaStream_t st) {
   uint16_t* x = nullptr;
   CK(dalloc(&x, ix->n * ix->L));
   b.xbf = x;
-  CK(dalloc(&b.xn2, ix->n));
-  CK(dalloc(&b.tile_n2, nt));
-  CK(dalloc(&b.tile_norm, nt));
-  CK(hg::launch_rows_to_bf16(ix->d.rows, ix->n, (int)ix->L, b.xbf, b.xn2, nullptr, st));
-  CK(hg::launch_tile_norms(b.xn2, ix->n, b.tile_n2, b.tile_norm, st));
+  CK(dalloc(&b.xmeta, ix->n));
+  CK(dalloc(&b.tile_meta, nt));
+  CK(hg::launch_rows_to_bf16(ix->d.rows, ix->n, (int)ix->L, b.xbf, b.xmeta, st));
+  CK(hg::launch_tile_norms(b.xmeta, ix->n, b.tile_meta, st));
   return HG_OK;
 }
 
 static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket_cap, uint32_t bm_cap,
-                                      uint32_t nitems) {
+                                      uint32_t nitems, uint32_t kmax) {
   hg::BatchScratch& b = ix->bs;
   if (nq > b.nq_cap) {
+    dfree(b.qlist);
+    dfree(b.seg_rows);
+    dfree(b.seg_prefix);
+    dfree(b.qbound);
+    dfree(b.parts);
+    dfree(b.part_cnt);
     dfree(b.qbf);
-    dfree(b.qn2);
-    dfree(b.qnorm);
+    dfree(b.qmeta);
     dfree(b.qperm);
     dfree(b.approx);
     dfree(b.kq);
@@ -1257,8 +1267,7 @@ static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket
     uint16_t* q = nullptr;
     CK(dalloc(&q, (size_t)nq * ix->L));
     b.qbf = q;
-    CK(dalloc(&b.qn2, nq));
-    CK(dalloc(&b.qnorm, nq));
+    CK(dalloc(&b.qmeta, nq));
     CK(dalloc(&b.qperm, nq));
     CK(dalloc(&b.approx, nq));
     CK(dalloc(&b.kq, nq));
@@ -1268,9 +1277,20 @@ static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket
     CK(dalloc(&b.init_cnt, nq));
     CK(dalloc(&b.bucket_cnt, nq));
     CK(dalloc(&b.ok, nq));
+    CK(dalloc(&b.qlist, nq));
+    CK(dalloc(&b.seg_rows, nq));
+    CK(dalloc(&b.seg_prefix, (size_t)nq + 1));
+    CK(dalloc(&b.qbound, nq));
+    CK(dalloc(&b.part_cnt, (size_t)nq * hg::kBatchMaxSeg));
     b.nq_cap = nq;
     b.bucket_cap = 0;
     b.bm_cap = 0;
+    b.parts_kmax = 0;
+  }
+  if (kmax > b.parts_kmax || !b.parts) {
+    dfree(b.parts);
+    CK(dalloc(&b.parts, (size_t)b.nq_cap * hg::kBatchMaxSeg * kmax));
+    b.parts_kmax = kmax;
   }
   if (!b.stats) {
     CK(dalloc(&b.stats, 8));
@@ -1295,14 +1315,11 @@ static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket
 }
 
 // Error-bound coefficients of the BF16 filter for series length L (see
-// hg_batch.cu): c_dot = 2 (2u + u^2 + L 2^-20) with u = 2^-8, and
+// hg_batch.cu): c_acc = L 2^-20 (FP32 accumulation on the tensor cores) and
 // c_sq = (L/8 + 16) 2^-22, both rounded up to float.
-static void filter_coefficients(uint32_t L, float* c_dot, float* c_sq) {
-  const double u = 1.0 / 256.0;
-  const double cd = 2.0 * (2.0 * u + u * u + L * std::ldexp(1.0, -20));
-  const double cs = (L / 8.0 + 16.0) * std::ldexp(1.0, -22);
-  *c_dot = std::nextafter((float)cd, INFINITY);
-  *c_sq = std::nextafter((float)cs, INFINITY);
+static void filter_coefficients(uint32_t L, float* c_acc, float* c_sq) {
+  *c_acc = std::nextafter((float)(L * std::ldexp(1.0, -20)), INFINITY);
+  *c_sq = std::nextafter((float)((L / 8.0 + 16.0) * std::ldexp(1.0, -22)), INFINITY);
 }
 
 static hg_status record(cudaEvent_t e, cudaStream_t st) {
@@ -1337,7 +1354,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   const int sms = hg::sm_count(ix->device);
   const uint32_t bucket_cap = o.bucket_cap > 0 ? (uint32_t)o.bucket_cap : kDefaultBucket;
   hg::BatchScratch& b = ix->bs;
-  HCK(ensure_batch_scratch(ix, std::max(nq, b.nq_cap), bucket_cap, 1, 1));
+  HCK(ensure_batch_scratch(ix, std::max(nq, b.nq_cap), bucket_cap, 1, 1, kmax));
 
   cudaEvent_t ev[6];
   for (auto& e : ev) CK(cudaEventCreate(&e));
@@ -1395,13 +1412,13 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     for (uint32_t x = i; x < j; ++x) slots[perm[x]] = use_tiles * sub;
     i = j;
   }
-  HCK(ensure_batch_scratch(ix, b.nq_cap, bucket_cap, bm_cap, (uint32_t)items.size()));
+  HCK(ensure_batch_scratch(ix, b.nq_cap, bucket_cap, bm_cap, (uint32_t)items.size(), kmax));
   CK(cudaMemcpyAsync(b.qperm, perm.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(b.kq, kq.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(b.slots, slots.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
   if (!items.empty())
     CK(cudaMemcpyAsync(b.items, items.data(), sizeof(hg::BatchItem) * items.size(), cudaMemcpyHostToDevice, st));
-  CK(hg::launch_rows_to_bf16(d_Q, nq, (int)L, b.qbf, b.qn2, b.qnorm, st));
+  CK(hg::launch_rows_to_bf16(d_Q, nq, (int)L, b.qbf, b.qmeta, st));
 
   // 2. bound pass
   hg::BatchGemm g{};
@@ -1409,11 +1426,9 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   g.qbf = b.qbf;
   g.L = (int)L;
   g.nrows = ix->n;
-  g.xn2 = ix->bd.xn2;
-  g.tile_n2 = ix->bd.tile_n2;
-  g.tile_norm = ix->bd.tile_norm;
-  g.qn2 = b.qn2;
-  g.qnorm = b.qnorm;
+  g.xmeta = ix->bd.xmeta;
+  g.tile_meta = ix->bd.tile_meta;
+  g.qmeta = b.qmeta;
   g.qperm = b.qperm;
   g.nq = (int)nq;
   g.mode = 0;
@@ -1422,7 +1437,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   g.bm = b.bm;
   g.bm_cap = bm_cap;
   g.tiles_per_item = kFilterTilesPerItem;
-  filter_coefficients(L, &g.c_dot, &g.c_sq);
+  filter_coefficients(L, &g.c_acc, &g.c_sq);
   g.bound = b.bound;
   g.bucket = b.bucket;
   g.bucket_cnt = b.bucket_cnt;
@@ -1455,52 +1470,92 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   r.id_out = d_id;
   r.ok_out = b.ok;
   r.stats = b.stats;
+  r.seg_rows = b.seg_rows;
+  r.seg_prefix = b.seg_prefix;
+  r.qbound = b.qbound;
+  r.parts = b.parts;
+  r.part_cnt = b.part_cnt;
+  r.heads = b.heads + 2;
+  r.qlist = nullptr;
+  r.nlist = (int)nq;
   CK(hg::launch_bound_select(r, st));
   HCK(record(ev[1], st));
-  // 3. certified filter over every row
-  g.mode = 1;
-  g.work_head = b.heads + 1;
-  CK(hg::launch_bf16_filter(g, gemm_blocks, st));
-  HCK(record(ev[2], st));
-  // 4-5. exact re-rank and verification
-  CK(hg::launch_rerank(r, st));
-  HCK(record(ev[3], st));
+  // 3-5. certified filter, exact re-rank, verification; a query whose bucket
+  // overflowed is retried with the bound its first survivors gave
+  const int gemm_rounds_max = 1 + kBatchRetries;
   std::vector<int> ok(nq);
+  std::vector<uint32_t> retry;
+  double gemm_ms = 0, rerank_ms = 0;
+  uint64_t pairs = 0, retried = 0;
+  for (int round = 0; round < gemm_rounds_max; ++round) {
+    const uint32_t cnt = round == 0 ? nq : (uint32_t)retry.size();
+    if (round > 0) {
+      CK(cudaMemcpyAsync(b.qlist, retry.data(), sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice, st));
+      g.qperm = b.qlist;
+      r.qlist = b.qlist;
+      retried += cnt;
+    }
+    g.nq = (int)cnt;
+    r.nlist = (int)cnt;
+    g.mode = 1;
+    g.work_head = b.heads + 1;
+    CK(cudaMemsetAsync(b.heads + 1, 0, sizeof(uint32_t), st));
+    CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
+    HCK(record(ev[2], st));
+    CK(hg::launch_bf16_filter(g, gemm_blocks, st));
+    HCK(record(ev[3], st));
+    CK(hg::launch_rerank(r, sms * kRerankBlocksPerSm, st));
+    HCK(record(ev[4], st));
+    CK(cudaMemcpyAsync(ok.data(), b.ok, sizeof(int) * nq, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float tg = 0, tr = 0;
+    cudaEventElapsedTime(&tg, ev[2], ev[3]);
+    cudaEventElapsedTime(&tr, ev[3], ev[4]);
+    gemm_ms += tg;
+    rerank_ms += tr;
+    pairs += (uint64_t)cnt * ix->n;
+    std::vector<uint32_t> next;
+    const uint32_t* lst = round == 0 ? nullptr : retry.data();
+    for (uint32_t i = 0; i < cnt; ++i) {
+      const uint32_t q = lst ? lst[i] : i;
+      if (ok[q] == 0) next.push_back(q);
+    }
+    retry.swap(next);
+    if (retry.empty()) break;
+  }
   unsigned long long hs[8];
-  CK(cudaMemcpyAsync(ok.data(), b.ok, sizeof(int) * nq, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(hs, b.stats, sizeof hs, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
   // queries that did not verify: the plain path
+  HCK(record(ev[2], st));
   hg_knn_opts po{};
   po.mode = HG_MODE_PLAIN;
   po.use_lb_sax = 1;
   uint64_t fallbacks = 0;
   for (uint32_t q = 0; q < nq; ++q) {
-    if (ok[q]) continue;
+    if (ok[q] == 1) continue;
     ++fallbacks;
     HCK(knn_one(ix, d_Q + (uint64_t)q * L, (int)kq[q], po, d_dist + (uint64_t)q * kmax, d_id + (uint64_t)q * kmax,
                 st, nullptr));
   }
-  HCK(record(ev[4], st));
+  HCK(record(ev[3], st));
   CK(cudaStreamSynchronize(st));
   if (stats) {
-    float t01 = 0, t12 = 0, t23 = 0, t34 = 0, t04 = 0;
+    float t01 = 0, tf = 0, t03 = 0;
     cudaEventElapsedTime(&t01, ev[0], ev[1]);
-    cudaEventElapsedTime(&t12, ev[1], ev[2]);
-    cudaEventElapsedTime(&t23, ev[2], ev[3]);
-    cudaEventElapsedTime(&t34, ev[3], ev[4]);
-    cudaEventElapsedTime(&t04, ev[0], ev[4]);
+    cudaEventElapsedTime(&tf, ev[2], ev[3]);
+    cudaEventElapsedTime(&t03, ev[0], ev[3]);
     stats->queries = nq;
     stats->rows_visited = hs[0];
     stats->chunks_loaded = hs[1];
     stats->survivors = hs[2];
-    stats->bf16_pairs = (uint64_t)nq * ix->n;
+    stats->bf16_pairs = pairs;
     stats->fallback_queries = fallbacks;
+    stats->retried_queries = retried;
     stats->bound_ms = t01;
-    stats->gemm_ms = t12;
-    stats->rerank_ms = t23;
-    stats->fallback_ms = t34;
-    stats->device_ms = t04;
+    stats->gemm_ms = gemm_ms;
+    stats->rerank_ms = rerank_ms;
+    stats->fallback_ms = tf;
+    stats->device_ms = t03;
   }
   return HG_OK;
 }

@@ -78,18 +78,16 @@ struct QueryScratch {
 // Batched path: BF16 copy of the rows and their norms, built on the first
 // batched call and kept with the index.
 struct BatchData {
-  void* xbf = nullptr;         // n x L BF16, row-major, leaf order
-  float* xn2 = nullptr;        // |x|^2 per row (FP64, rounded up)
-  float* tile_n2 = nullptr;    // per 128-row tile: max |x|^2
-  float* tile_norm = nullptr;  //                   max |x|
+  void* xbf = nullptr;          // n x L BF16, row-major, leaf order
+  float4* xmeta = nullptr;      // per row: |x|^2, |x~|, |x - x~| (FP64, rounded up)
+  float4* tile_meta = nullptr;  // per 128-row tile: maxima of xmeta
 };
 
 // Batched path scratch, grown to the largest batch seen.
 struct BatchScratch {
   uint32_t nq_cap = 0, bucket_cap = 0, bm_cap = 0, items_cap = 0;
   void* qbf = nullptr;
-  float* qn2 = nullptr;
-  float* qnorm = nullptr;
+  float4* qmeta = nullptr;
   uint32_t* qperm = nullptr;
   int* approx = nullptr;
   uint32_t* kq = nullptr;
@@ -104,6 +102,13 @@ struct BatchScratch {
   int* ok = nullptr;
   unsigned long long* stats = nullptr;
   uint32_t* heads = nullptr;
+  uint32_t parts_kmax = 0;
+  uint32_t* qlist = nullptr;  // queries of a retry round
+  uint32_t* seg_rows = nullptr;
+  uint32_t* seg_prefix = nullptr;
+  uint32_t* qbound = nullptr;
+  unsigned long long* parts = nullptr;
+  int* part_cnt = nullptr;
 };
 
 }  // namespace hg

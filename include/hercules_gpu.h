@@ -78,6 +78,7 @@ typedef struct {
   uint64_t bf16_pairs;        /* (query, row) pairs through the BF16 filter */
   uint64_t survivors;         /* pairs kept by the certified filter */
   uint64_t fallback_queries;  /* queries answered by the plain path instead */
+  uint64_t retried_queries;   /* filter passes repeated with a tighter bound (bucket overflow) */
   double bound_ms;            /* device time: BF16 pass over the approximate leaves + bound */
   double gemm_ms;             /* device time: BF16 filter over every row */
   double rerank_ms;           /* device time: exact re-rank of the survivors */
@@ -96,7 +97,7 @@ typedef struct {
   int profile;        /* 1: time every leaf-scan launch with CUDA events */
   int approx_blocks;  /* blocks of the approximate-leaf scan (0 = one per SM) */
   int bucket_cap;     /* HG_MODE_BATCH: filter survivors kept per query before the
-                         query falls back to the plain path (0 = 16384) */
+                         query falls back to the plain path (0 = 65536) */
   int reserved[3];
 } hg_knn_opts;
 

@@ -73,6 +73,16 @@ def test_batch_fallback_when_buckets_overflow(mid):
     same_as_plain(ix, Q[:12], np.full(12, 10), d, ids)
 
 
+def test_batch_retry_with_tighter_bound(mid):
+    """Small buckets overflow; the first survivors lower the bound and the
+    filter runs again for those queries only; answers stay identical."""
+    X, Q, ix = mid
+    ks = np.array([10, 100] * 20, np.uint32)
+    d, ids, st = ix.knn_batch(Q[-40:], ks, stats=True, bucket_cap=150)
+    assert st["retried_queries"] > 0, st
+    same_as_plain(ix, Q[-40:], ks, d, ids)
+
+
 def test_batch_via_hg_knn_mode(mid, hg):
     X, Q, ix = mid
     d, ids = ix.knn(Q[:40], 10, mode=hg.MODE_BATCH)
