@@ -91,6 +91,7 @@ _SIGS = [
                                     ctypes.POINTER(QueryStats)]),
     ("hg_knn_batch_device", ctypes.c_int, [_P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, ctypes.POINTER(KnnOpts),
                                            _P, _P, _P, ctypes.POINTER(QueryStats)]),
+    ("hg_bf16_dots", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint32, _P, ctypes.c_uint32, _P, _P]),
     ("hg_route", ctypes.c_int, [_P, _P, ctypes.c_uint32, _P]),
     ("hg_leaf_lower_bounds", ctypes.c_int, [_P, _P, _P]),
     ("hg_generate_walks", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, _P,
@@ -306,6 +307,12 @@ class HerculesIndex:
         out = np.zeros(self.info.num_leaves, dtype=np.float32)
         _check(lib().hg_leaf_lower_bounds(self._h, _ptr(q), _ptr(out)))
         return out
+
+
+def bf16_dots_device(rows_ptr, n, L, q_ptr, nq, out_ptr, stream=0):
+    """Tensor-core products q~.x~ of the batched filter (diagnostics)."""
+    _check(lib().hg_bf16_dots(ctypes.c_void_p(rows_ptr), n, L, ctypes.c_void_p(q_ptr), nq, ctypes.c_void_p(out_ptr),
+                              ctypes.c_void_p(stream)))
 
 
 # -- data --------------------------------------------------------------------

@@ -20,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhercules_gpu.so")
 CLI = os.path.join(HERE, "bin", "hercules")
 
-SOURCES = ["hg_kernels.cu", "hg_index.cu", "hg_noalloc.cu", "hg_batch.cu"]
+SOURCES = ["hg_kernels.cu", "hg_index.cu", "hg_noalloc.cu", "hg_batch.cu", "hg_umma.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

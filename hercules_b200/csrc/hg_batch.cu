@@ -43,14 +43,16 @@ constexpr int kBM = kBatchTileRows, kBN = 128, kBK = 64, kStages = 3, kGemmThrea
 // preparation
 // ---------------------------------------------------------------------------
 
-// One warp per row: BF16 copy (round to nearest) and, in FP64 rounded up,
-// meta = {|x|^2, |x~|, |x - x~|, 0} (x~ the BF16 row).
-__global__ void k_rows_to_bf16(const float* __restrict__ rows, uint64_t n, int L, __nv_bfloat16* __restrict__ out,
-                               float4* __restrict__ meta) {
+// One warp per output row w: the BF16 copy of source row src = idx ? idx[w] : w
+// (round to nearest) and, in FP64 rounded up, meta[src] = {|x|^2, |x~|,
+// |x - x~|, 0} (x~ the BF16 row).
+__global__ void k_rows_to_bf16(const float* __restrict__ rows, const uint32_t* __restrict__ idx, uint64_t n, int L,
+                               __nv_bfloat16* __restrict__ out, float4* __restrict__ meta) {
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= n) return;
-  const float4* x = reinterpret_cast<const float4*>(rows + w * L);
+  const uint64_t src = idx ? idx[w] : w;
+  const float4* x = reinterpret_cast<const float4*>(rows + src * L);
   __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(out + w * L);
   double a2 = 0.0, t2 = 0.0, r2 = 0.0;
   auto acc = [&](float v, float t) {
@@ -79,7 +81,7 @@ __global__ void k_rows_to_bf16(const float* __restrict__ rows, uint64_t n, int L
   if (lane == 0) {
     // FP64 sums of L non-negative terms: relative error below L 2^-53
     const double up = 1.0 + 1e-12;
-    meta[w] = make_float4(__double2float_ru(a2 * up), __double2float_ru(sqrt(t2) * up),
+    meta[src] = make_float4(__double2float_ru(a2 * up), __double2float_ru(sqrt(t2) * up),
                           __double2float_ru(sqrt(r2) * up), 0.0f);
   }
 }
@@ -630,9 +632,10 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_merge(BatchRank a) {
 
 static inline unsigned nblk(uint64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-cudaError_t launch_rows_to_bf16(const float* rows, uint64_t n, int L, void* out, float4* meta, cudaStream_t s) {
+cudaError_t launch_rows_to_bf16(const float* rows, const uint32_t* idx, uint64_t n, int L, void* out, float4* meta,
+                                cudaStream_t s) {
   if (!n) return cudaSuccess;
-  k_rows_to_bf16<<<nblk(n * 32, 256), 256, 0, s>>>(rows, n, L, static_cast<__nv_bfloat16*>(out), meta);
+  k_rows_to_bf16<<<nblk(n * 32, 256), 256, 0, s>>>(rows, idx, n, L, static_cast<__nv_bfloat16*>(out), meta);
   return cudaGetLastError();
 }
 

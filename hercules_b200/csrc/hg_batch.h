@@ -1,6 +1,7 @@
 // hg_batch.h -- launchers and argument blocks of the batched BF16 filter path.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -9,6 +10,7 @@
 namespace hg {
 
 constexpr int kBatchTileRows = 128;   // rows per tensor-core tile (and per tile norm)
+constexpr int kBatchQueryTile = 256;  // queries per tensor-core tile
 constexpr int kBatchMaxSlots = 4096;  // bound slots per query (sorted in one block)
 constexpr int kBatchMaxSeg = 16;      // re-rank segments per query
 constexpr int kBatchSegMin = 256;     // rows per re-rank segment, at least
@@ -48,6 +50,10 @@ struct BatchGemm {
   uint32_t* bucket_cnt;    // 0 before the launch
   uint32_t bucket_cap;
   uint32_t* work_head;     // 0 before the launch
+  int* err;                // raised (1) when a bounded wait gave up
+  // mode 2 (diagnostics): raw dot products q~.x~, [query position][dots_ld]
+  float* dots;
+  uint64_t dots_ld;
 };
 
 struct BatchRank {
@@ -82,11 +88,15 @@ struct BatchRank {
   uint32_t* heads;            // [0] segment counter
 };
 
-cudaError_t launch_rows_to_bf16(const float* rows, uint64_t n, int L, void* out, float4* meta, cudaStream_t s);
+cudaError_t launch_rows_to_bf16(const float* rows, const uint32_t* idx, uint64_t n, int L, void* out, float4* meta,
+                                cudaStream_t s);
 cudaError_t launch_tile_norms(const float4* meta, uint64_t n, float4* tile_meta, cudaStream_t s);
 size_t bf16_filter_smem();
 cudaError_t launch_bf16_filter(const BatchGemm& g, int blocks, cudaStream_t s);
 cudaError_t launch_bound_select(const BatchRank& r, cudaStream_t s);
+size_t umma_filter_smem();
+cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q_map, const BatchGemm& g, int blocks,
+                               cudaStream_t s);
 cudaError_t launch_rerank(const BatchRank& r, int part_blocks, cudaStream_t s);
 
 }  // namespace hg

@@ -1,6 +1,8 @@
 // hg_index.cu -- host side of the B200 Hercules index: tree construction with
 // GPU-side routing and envelopes, the reference's on-disk format, and the
 // query orchestration behind the C ABI of include/hercules_gpu.h.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <float.h>
 #include <limits.h>
@@ -1222,12 +1224,36 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
 // batched queries: BF16 tensor-core filter + exact re-rank (hg_batch.cu)
 // ---------------------------------------------------------------------------
 
-constexpr int kGemmBlocksPerSm = 2;       // k_bf16_filter: 2 x 256 threads, 98 KB smem each
 constexpr uint32_t kBoundTilesPerItem = 8;
 constexpr uint32_t kFilterTilesPerItem = 32;  // 4096 rows per item: a row chunk stays in L2
 constexpr uint32_t kDefaultBucket = 65536;
 constexpr int kBatchRetries = 3;  // filter rounds after the first for overflowed buckets
 constexpr int kRerankBlocksPerSm = 8;      // k_rerank_part: 8 x 8 warps per SM
+
+// TMA descriptor of a row-major n x L BF16 matrix, boxes of 64 columns
+// (128 bytes, the swizzle span) x box_rows rows, 128-byte swizzle, zero fill
+// outside the matrix.  The encoder comes from the driver through the runtime.
+static hg_status encode_bf16_map(CUtensorMap* map, const void* base, uint64_t n, uint32_t L, uint32_t box_rows) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (!fn || q != cudaDriverEntryPointSuccess) return set_error(HG_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  if (n == 0 || n >= (1ull << 31) || (L * 2) % 16 != 0)
+    return set_error(HG_ERR_LIMIT, "BF16 tensor map: n must be below 2^31 and L a multiple of 8");
+  const cuuint64_t dims[2] = {L, n};
+  const cuuint64_t strides[1] = {(cuuint64_t)L * 2};
+  const cuuint32_t box[2] = {64, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(HG_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  return HG_OK;
+}
 
 static hg_status ensure_batch_data(hg_index* ix, cudaStream_t st) {
   hg::BatchData& b = ix->bd;
@@ -1238,8 +1264,9 @@ static hg_status ensure_batch_data(hg_index* ix, cudaStream_t st) {
   b.xbf = x;
   CK(dalloc(&b.xmeta, ix->n));
   CK(dalloc(&b.tile_meta, nt));
-  CK(hg::launch_rows_to_bf16(ix->d.rows, ix->n, (int)ix->L, b.xbf, b.xmeta, st));
+  CK(hg::launch_rows_to_bf16(ix->d.rows, nullptr, ix->n, (int)ix->L, b.xbf, b.xmeta, st));
   CK(hg::launch_tile_norms(b.xmeta, ix->n, b.tile_meta, st));
+  HCK(encode_bf16_map(&b.rows_map, b.xbf, ix->n, ix->L, 128));
   return HG_OK;
 }
 
@@ -1400,7 +1427,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   std::vector<uint32_t> slots(nq);
   for (uint32_t i = 0; i < nq;) {
     uint32_t j = i;
-    while (j < nq && approx[perm[j]] == approx[perm[i]] && j - i < 128) ++j;
+    while (j < nq && approx[perm[j]] == approx[perm[i]] && j - i < (uint32_t)hg::kBatchQueryTile) ++j;
     uint64_t st0, sz;
     leaf_rows(approx[perm[i]], &st0, &sz);
     const uint32_t tiles = (uint32_t)((sz + T - 1) / T);
@@ -1418,7 +1445,10 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   CK(cudaMemcpyAsync(b.slots, slots.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
   if (!items.empty())
     CK(cudaMemcpyAsync(b.items, items.data(), sizeof(hg::BatchItem) * items.size(), cudaMemcpyHostToDevice, st));
-  CK(hg::launch_rows_to_bf16(d_Q, nq, (int)L, b.qbf, b.qmeta, st));
+  // BF16 queries in processing order (tile columns), norms by query
+  CK(hg::launch_rows_to_bf16(d_Q, b.qperm, nq, (int)L, b.qbf, b.qmeta, st));
+  CUtensorMap qmap;
+  HCK(encode_bf16_map(&qmap, b.qbf, nq, L, hg::kBatchQueryTile));
 
   // 2. bound pass
   hg::BatchGemm g{};
@@ -1443,12 +1473,12 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   g.bucket_cnt = b.bucket_cnt;
   g.bucket_cap = bucket_cap;
   g.work_head = b.heads;
+  g.err = reinterpret_cast<int*>(b.heads + 3);
   CK(cudaMemsetAsync(b.bm, 0xff, sizeof(unsigned long long) * nq * bm_cap, st));
   CK(cudaMemsetAsync(b.heads, 0, sizeof(uint32_t) * 4, st));
   CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
   CK(cudaMemsetAsync(b.stats, 0, sizeof(unsigned long long) * 8, st));
-  const int gemm_blocks = sms * kGemmBlocksPerSm;
-  CK(hg::launch_bf16_filter(g, gemm_blocks, st));
+  CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
   hg::BatchRank r{};
   r.rows = ix->d.rows;
   r.ids = ix->d.ids;
@@ -1491,6 +1521,8 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     const uint32_t cnt = round == 0 ? nq : (uint32_t)retry.size();
     if (round > 0) {
       CK(cudaMemcpyAsync(b.qlist, retry.data(), sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice, st));
+      CK(hg::launch_rows_to_bf16(d_Q, b.qlist, cnt, (int)L, b.qbf, b.qmeta, st));
+      HCK(encode_bf16_map(&qmap, b.qbf, cnt, L, hg::kBatchQueryTile));
       g.qperm = b.qlist;
       r.qlist = b.qlist;
       retried += cnt;
@@ -1502,7 +1534,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     CK(cudaMemsetAsync(b.heads + 1, 0, sizeof(uint32_t), st));
     CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
     HCK(record(ev[2], st));
-    CK(hg::launch_bf16_filter(g, gemm_blocks, st));
+    CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
     HCK(record(ev[3], st));
     CK(hg::launch_rerank(r, sms * kRerankBlocksPerSm, st));
     HCK(record(ev[4], st));
@@ -1524,7 +1556,11 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     if (retry.empty()) break;
   }
   unsigned long long hs[8];
+  uint32_t dev_err = 0;
   CK(cudaMemcpyAsync(hs, b.stats, sizeof hs, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&dev_err, b.heads + 3, sizeof dev_err, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (dev_err) return set_error(HG_ERR_TIMEOUT, "hg_knn_batch: a tensor-core filter wait timed out");
   // queries that did not verify: the plain path
   HCK(record(ev[2], st));
   hg_knn_opts po{};
@@ -1784,6 +1820,79 @@ hg_status hg_knn_batch(hg_index* ix, const float* queries, uint32_t nq, const ui
   if (d_dist) cudaFree(d_dist);
   if (d_id) cudaFree(d_id);
   return s;
+}
+
+hg_status hg_bf16_dots(const float* d_rows, uint64_t n, uint32_t L, const float* d_queries, uint32_t nq,
+                       float* d_dots, void* stream) {
+  if (!d_rows || !d_queries || !d_dots) return set_error(HG_ERR_ARG, "hg_bf16_dots: null argument");
+  if (n == 0 || nq == 0) return HG_OK;
+  if (L == 0 || L % 16 != 0 || L > 16384) return set_error(HG_ERR_ARG, "hg_bf16_dots: L must be a multiple of 16");
+  if (n >= (1ull << 31) || nq >= (1u << 24)) return set_error(HG_ERR_LIMIT, "hg_bf16_dots: too many rows");
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  uint16_t* xbf = nullptr;
+  uint16_t* qbf = nullptr;
+  float4* xmeta = nullptr;
+  float4* qmeta = nullptr;
+  float4* tmeta = nullptr;
+  uint32_t* perm = nullptr;
+  int* err = nullptr;
+  auto release = [&]() {
+    dfree(xbf);
+    dfree(qbf);
+    dfree(xmeta);
+    dfree(qmeta);
+    dfree(tmeta);
+    dfree(perm);
+    dfree(err);
+  };
+  std::vector<uint32_t> ident(nq);
+  for (uint32_t i = 0; i < nq; ++i) ident[i] = i;
+  cudaError_t e = dalloc(&xbf, n * L);
+  if (e == cudaSuccess) e = dalloc(&qbf, (size_t)nq * L);
+  if (e == cudaSuccess) e = dalloc(&xmeta, n);
+  if (e == cudaSuccess) e = dalloc(&qmeta, nq);
+  if (e == cudaSuccess) e = dalloc(&tmeta, (n + 127) / 128);
+  if (e == cudaSuccess) e = dalloc(&perm, nq);
+  if (e == cudaSuccess) e = dalloc(&err, 1);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(perm, ident.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = hg::launch_rows_to_bf16(d_rows, nullptr, n, (int)L, xbf, xmeta, st);
+  if (e == cudaSuccess) e = hg::launch_rows_to_bf16(d_queries, nullptr, nq, (int)L, qbf, qmeta, st);
+  if (e == cudaSuccess) e = hg::launch_tile_norms(xmeta, n, tmeta, st);
+  if (e != cudaSuccess) {
+    release();
+    return cuda_fail(e, "hg_bf16_dots");
+  }
+  CUtensorMap xmap, qmap;
+  hg_status hs = encode_bf16_map(&xmap, xbf, n, L, 128);
+  if (hs == HG_OK) hs = encode_bf16_map(&qmap, qbf, nq, L, hg::kBatchQueryTile);
+  if (hs != HG_OK) {
+    release();
+    return hs;
+  }
+  hg::BatchGemm g{};
+  g.L = (int)L;
+  g.nrows = n;
+  g.xmeta = xmeta;
+  g.tile_meta = tmeta;
+  g.qmeta = qmeta;
+  g.qperm = perm;
+  g.nq = (int)nq;
+  g.mode = 2;
+  g.tiles_per_item = 8;
+  g.err = err;
+  g.dots = d_dots;
+  g.dots_ld = n;
+  e = hg::launch_umma_filter(xmap, qmap, g, hg::sm_count(dev), st);
+  int herr = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof herr, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  release();
+  if (e != cudaSuccess) return cuda_fail(e, "hg_bf16_dots");
+  if (herr) return set_error(HG_ERR_TIMEOUT, "hg_bf16_dots: a tensor-core wait timed out");
+  return HG_OK;
 }
 
 hg_status hg_route(hg_index* ix, const float* queries, uint32_t nq, int32_t* leaf_out) {

@@ -81,6 +81,7 @@ struct BatchData {
   void* xbf = nullptr;          // n x L BF16, row-major, leaf order
   float4* xmeta = nullptr;      // per row: |x|^2, |x~|, |x - x~| (FP64, rounded up)
   float4* tile_meta = nullptr;  // per 128-row tile: maxima of xmeta
+  CUtensorMap rows_map;         // TMA descriptor of xbf (64 x 128 boxes, 128-byte swizzle)
 };
 
 // Batched path scratch, grown to the largest batch seen.

@@ -1,0 +1,463 @@
+// hg_umma.cu -- the batched filter's q.x products on the 5th-generation tensor
+// cores: tcgen05.mma (BF16 x BF16 -> FP32 in tensor memory), operands staged
+// by TMA with the 128-byte swizzle, fused epilogues read back with tcgen05.ld.
+//
+// One persistent CTA per SM, 12 warps:
+//   warp 0      TMA producer (one elected lane): row tiles (A, 128 rows x 64 K
+//               per stage) and the query tile (B, 256 queries x L, resident
+//               in shared memory for L <= 256, else streamed with A);
+//   warp 1      MMA issuer (one lane): per 128-row tile, L/16 MMAs of
+//               M=128, N=256, K=16 into one of two TMEM accumulators;
+//   warp 2      allocates / frees the 512 TMEM columns;
+//   warps 4-11  epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (the
+//               tile's rows) and columns 128 ((w - 4) / 4) .. +127 (queries).
+// Work items are (128-row tiles, query tile) pairs in a static round robin:
+// mode 1 walks row chunks x query tiles (a chunk's query tiles run side by
+// side so the chunk is read from HBM once); mode 0 walks the host's items
+// (approximate leaves x the queries routed there); mode 2 writes the raw dot
+// products (diagnostics).  Every mbarrier wait gives up after kWaitNs of
+// global time: the CTA then raises *err, drains its copies and MMAs, frees
+// TMEM and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hg_batch.h"
+#include "hg_device.cuh"
+
+namespace hg {
+namespace {
+
+constexpr int kUM = 128;       // rows per tile (MMA M)
+constexpr int kUN = 256;       // queries per tile (MMA N)
+constexpr int kUK = 64;        // K elements per stage: one 128-byte swizzle row
+constexpr int kAStages = 4;
+constexpr int kThreads = 384;  // 12 warps
+constexpr int kEpiThreads = 256;
+constexpr uint32_t kABytes = kUM * kUK * 2;  // 16 KB per A stage
+constexpr uint32_t kQBytes = kUN * kUK * 2;  // 32 KB per query K block
+constexpr int kResidentKB = 4;               // L <= 256: the query tile stays resident
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s per wait
+constexpr int kErrTimeout = 1;
+
+// shared memory map (offsets from a 1024-byte aligned base)
+constexpr uint32_t kSmQ = 0;                                   // 4 x 32 KB
+constexpr uint32_t kSmA = kSmQ + kResidentKB * kQBytes;        // 4 x 16 KB
+constexpr uint32_t kSmBar = kSmA + kAStages * kABytes;         // mbarriers
+constexpr uint32_t kNumBars = 2 * kAStages + 2 + 4 + 1;        // full/empty, q full/empty, tmem full/empty x2, done
+constexpr uint32_t kSmTmem = kSmBar + kNumBars * 8;            // TMEM base address
+constexpr uint32_t kSmAbort = kSmTmem + 4;
+constexpr uint32_t kSmThr = (kSmAbort + 4 + 15) & ~15u;        // float [2][256]
+constexpr uint32_t kSmQidx = kSmThr + 2 * kUN * 4;             // uint32 [256]
+constexpr uint32_t kSmQn2 = kSmQidx + kUN * 4;                 // float [256]
+constexpr uint32_t kSmGo = kSmQn2 + kUN * 4;                   // int [2]
+constexpr uint32_t kSmBytes = kSmGo + 8;
+constexpr size_t kDynSmem = kSmBytes + 1024;                   // + alignment slack
+
+// --- PTX wrappers -------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t s2u(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Bounded wait for the phase of `parity`; false when this CTA aborted or
+// the wait ran past kWaitNs (then the CTA aborts and *err is raised).
+__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err) {
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try(bar, parity)) return true;
+    if ((i & 63) == 0) {
+      if (*abort_flag) return false;
+      if (global_ns() - t0 > kWaitNs) {
+        *abort_flag = 1;
+        atomicExch(err, kErrTimeout);
+        return false;
+      }
+    }
+  }
+}
+
+// Wait for a phase that is known to complete on its own (copies and MMAs
+// already issued), bounded, ignoring the abort flag.
+__device__ __noinline__ void drain_wait(uint32_t bar, uint32_t parity) {
+  const uint64_t t0 = global_ns();
+  while (!mbar_try(bar, parity) && global_ns() - t0 < kWaitNs) {
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+// D[tmem] (+)= A[smem] x B[smem]^T, both K-major
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void named_sync(uint32_t id, uint32_t n) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major operand in the 128-byte
+// swizzle layout: rows of 128 bytes, 8-row groups 1024 bytes apart
+// (stride byte offset 64 x 16 B), leading byte offset unused (1),
+// descriptor version 1, layout type 2 (128-byte swizzle).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)64 << 32) | ((uint64_t)1 << 46) |
+         ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor: FP32 accumulator, BF16 A and B, both K-major,
+// N = 256 (bits 17-22: N / 8), M = 128 (bits 24-28: M / 16).
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kUN >> 3) << 17) |
+                            ((uint32_t)(kUM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t ordered_key(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+struct Item {
+  uint64_t rb, re;  // rows of the item
+  uint32_t qoff, qcnt;
+  uint32_t t_lo, t_hi;
+  uint32_t sub;
+};
+
+__device__ __forceinline__ Item item_of(const BatchGemm& a, uint32_t w, uint32_t QT, uint64_t ntiles) {
+  Item it;
+  if (a.mode == 0) {
+    const BatchItem b = a.items[w];
+    it.rb = b.row_begin;
+    it.re = b.row_end;
+    it.qoff = b.q_off;
+    it.qcnt = b.q_cnt;
+    it.t_lo = b.tile_lo;
+    it.t_hi = b.tile_hi;
+    it.sub = b.sub;
+  } else {
+    const uint32_t chunk = w / QT, qt = w % QT;
+    it.rb = 0;
+    it.re = a.nrows;
+    it.qoff = qt * kUN;
+    it.qcnt = (uint32_t)min(a.nq - (int)it.qoff, kUN);
+    it.t_lo = chunk * a.tiles_per_item;
+    const uint64_t th = (uint64_t)it.t_lo + a.tiles_per_item;
+    it.t_hi = (uint32_t)(th < ntiles ? th : ntiles);
+    it.sub = 1;
+  }
+  return it;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_umma_filter(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmQ, BatchGemm a) {
+  extern __shared__ unsigned char umma_raw[];
+  unsigned char* sm = umma_raw + ((1024 - (s2u(umma_raw) & 1023)) & 1023);
+  const uint32_t base = s2u(sm);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t bar0 = base + kSmBar;
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (kAStages + s); };
+  const uint32_t qfull_bar = bar0 + 8u * (2 * kAStages);
+  const uint32_t qempty_bar = qfull_bar + 8;
+  auto tfull_bar = [&](int b) { return qempty_bar + 8u + 8u * b; };
+  auto tempty_bar = [&](int b) { return qempty_bar + 24u + 8u * b; };
+  const uint32_t done_bar = qempty_bar + 40u;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + kSmAbort);
+  float* s_thr = reinterpret_cast<float*>(sm + kSmThr);
+  uint32_t* s_qidx = reinterpret_cast<uint32_t*>(sm + kSmQidx);
+  float* s_qn2 = reinterpret_cast<float*>(sm + kSmQn2);
+  volatile int* s_go = reinterpret_cast<volatile int*>(sm + kSmGo);
+
+  const int nkb = (a.L + kUK - 1) / kUK;
+  const bool resident = nkb <= kResidentKB;
+  const uint32_t QT = (uint32_t)((a.nq + kUN - 1) / kUN);
+  const uint64_t ntiles = (a.nrows + kUM - 1) / kUM;
+  const uint32_t nchunks = (uint32_t)((ntiles + a.tiles_per_item - 1) / a.tiles_per_item);
+  const uint32_t total = a.mode == 0 ? a.nitems : nchunks * QT;
+
+  if (tid == 0) {
+    for (int s = 0; s < kAStages; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(qfull_bar, 1);
+    mbar_init(qempty_bar, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(tfull_bar(b), 1);
+      mbar_init(tempty_bar(b), kEpiThreads / 32);
+    }
+    mbar_init(done_bar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(base + kSmTmem)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kSmTmem);
+
+  if (warp == 0) {
+    // ---------------- TMA producer
+    if (lane == 0) {
+      uint32_t g = 0, it_n = 0;
+      bool ok = true;
+      for (uint32_t w = blockIdx.x; ok && w < total; w += gridDim.x, ++it_n) {
+        const Item it = item_of(a, w, QT, ntiles);
+        if (resident) {
+          ok = mbar_wait(qempty_bar, (it_n & 1) ^ 1, abort_flag, a.err);
+          if (!ok) break;
+          mbar_expect_tx(qfull_bar, (uint32_t)nkb * kQBytes);
+          for (int kb = 0; kb < nkb; ++kb)
+            tma_load_2d(base + kSmQ + kb * kQBytes, &tmQ, kb * kUK, (int)it.qoff, qfull_bar);
+        }
+        for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t) {
+          const int row0 = (int)(it.rb + (uint64_t)t * kUM);
+          for (int kb = 0; kb < nkb; ++kb, ++g) {
+            const int s = (int)(g % kAStages);
+            ok = mbar_wait(empty_bar(s), ((g / kAStages) & 1) ^ 1, abort_flag, a.err);
+            if (!ok) break;
+            mbar_expect_tx(full_bar(s), resident ? kABytes : kABytes + kQBytes);
+            tma_load_2d(base + kSmA + s * kABytes, &tmA, kb * kUK, row0, full_bar(s));
+            if (!resident) tma_load_2d(base + kSmQ + s * kQBytes, &tmQ, kb * kUK, (int)it.qoff, full_bar(s));
+          }
+        }
+      }
+      if (!ok) {
+        // drain the copies still in flight before the CTA leaves
+        const uint32_t first = g > (uint32_t)kAStages ? g - kAStages : 0;
+        for (uint32_t gg = first; gg < g; ++gg) drain_wait(full_bar((int)(gg % kAStages)), (gg / kAStages) & 1);
+        if (resident && it_n > 0) drain_wait(qfull_bar, (it_n - 1) & 1);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      uint32_t g = 0, tcount = 0, it_n = 0;
+      bool ok = true;
+      for (uint32_t w = blockIdx.x; ok && w < total; w += gridDim.x, ++it_n) {
+        const Item it = item_of(a, w, QT, ntiles);
+        if (resident) {
+          ok = mbar_wait(qfull_bar, it_n & 1, abort_flag, a.err);
+          if (!ok) break;
+          tc_fence_after();
+        }
+        for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t, ++tcount) {
+          const int b = (int)(tcount & 1);
+          ok = mbar_wait(tempty_bar(b), ((tcount >> 1) & 1) ^ 1, abort_flag, a.err);
+          if (!ok) break;
+          tc_fence_after();
+          const uint32_t d = tmem + (uint32_t)b * kUN;
+          for (int kb = 0; kb < nkb; ++kb, ++g) {
+            const int s = (int)(g % kAStages);
+            ok = mbar_wait(full_bar(s), (g / kAStages) & 1, abort_flag, a.err);
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t sa = base + kSmA + s * kABytes;
+            const uint32_t sq = base + kSmQ + (resident ? kb : s) * kQBytes;
+#pragma unroll
+            for (int k16 = 0; k16 < kUK / 16; ++k16)
+              tc_mma(d, sw128_desc(sa + k16 * 32), sw128_desc(sq + k16 * 32), kIdesc, (kb | k16) != 0);
+            tc_commit(empty_bar(s));
+          }
+          if (ok) tc_commit(tfull_bar(b));
+        }
+        if (ok && resident) tc_commit(qempty_bar);
+      }
+      // every MMA issued has completed before TMEM is freed
+      tc_commit(done_bar);
+      drain_wait(done_bar, 0);
+    }
+  } else if (warp >= 4) {
+    // ---------------- epilogue
+    const int etid = tid - 128;
+    const int quarter = warp & 3;
+    const int half = (warp - 4) >> 2;
+    const float inf = __int_as_float(0x7f800000);
+    uint32_t tcount = 0;
+    bool ok = true;
+    for (uint32_t w = blockIdx.x; ok && w < total; w += gridDim.x) {
+      const Item it = item_of(a, w, QT, ntiles);
+      named_sync(1, kEpiThreads);
+      // column etid of the query tile
+      uint32_t q = 0xffffffffu;
+      float4 qm = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      float qb = -1.0f;
+      if ((uint32_t)etid < it.qcnt) {
+        q = a.qperm[it.qoff + etid];
+        qm = a.qmeta[q];
+        if (a.mode == 1) {
+          const float b = a.bound[q];
+          qb = b < inf ? b : -1.0f;
+        }
+      }
+      s_qidx[etid] = q;
+      s_qn2[etid] = qm.x;
+      named_sync(1, kEpiThreads);
+      const int c_lo = half * 128;
+      const int c_hi = min(c_lo + 128, (int)it.qcnt);
+      for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t, ++tcount) {
+        const int b = (int)(tcount & 1);
+        const uint64_t row0 = it.rb + (uint64_t)t * kUM;
+        const uint64_t row = row0 + quarter * 32 + lane;
+        const bool row_ok = row < it.re && row < a.nrows;
+        float* thr = s_thr + b * kUN;
+        float h_row = inf;
+        if (a.mode == 1) {
+          // per-tile threshold of column etid: keep (row, q) when
+          // acc >= |x|^2 / 2 + (|q|^2 - B - err) / 2
+          const float4 tm = a.tile_meta[row0 / kUM];
+          float tv = inf;
+          if (qb >= 0.0f) {
+            const float err = 2.000002f * (qm.y * tm.z + qm.z * tm.y + qm.z * tm.z + a.c_acc * qm.y * tm.y) +
+                              a.c_sq * (qm.x + tm.x + qb) + 1e-5f;
+            tv = 0.5f * (qm.x - qb - err);
+          }
+          thr[etid] = tv;
+          if (row_ok) h_row = 0.5f * a.xmeta[row].x;
+        }
+        // one thread waits for the accumulator; the group learns the outcome
+        // at the barrier, so every epilogue thread takes the same branch
+        if (etid == 0) s_go[b] = mbar_wait(tfull_bar(b), (tcount >> 1) & 1, abort_flag, a.err) ? 1 : 0;
+        named_sync(1, kEpiThreads);
+        ok = s_go[b] != 0;
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)b * kUN;
+        for (int c0 = c_lo; c0 < c_hi; c0 += 32) {
+          uint32_t r[32];
+          tc_ld32(tbase + (uint32_t)c0, r);
+          tc_wait_ld();
+          if (a.mode == 1) {
+            uint32_t mask = 0;
+#pragma unroll
+            for (int j = 0; j < 32; j += 4) {
+              const float4 t4 = *reinterpret_cast<const float4*>(thr + c0 + j);
+              mask |= (__uint_as_float(r[j]) >= h_row + t4.x) ? (1u << j) : 0u;
+              mask |= (__uint_as_float(r[j + 1]) >= h_row + t4.y) ? (2u << j) : 0u;
+              mask |= (__uint_as_float(r[j + 2]) >= h_row + t4.z) ? (4u << j) : 0u;
+              mask |= (__uint_as_float(r[j + 3]) >= h_row + t4.w) ? (8u << j) : 0u;
+            }
+            while (mask) {
+              const int j = __ffs(mask) - 1;
+              mask &= mask - 1;
+              const uint32_t qq = s_qidx[c0 + j];
+              const uint32_t pos = atomicAdd(&a.bucket_cnt[qq], 1u);
+              if (pos < a.bucket_cap) a.bucket[(uint64_t)qq * a.bucket_cap + pos] = (uint32_t)row;
+            }
+          } else if (a.mode == 0) {
+            const float xn2 = row_ok ? a.xmeta[row].x : 0.0f;
+            const int span = kUM / (int)it.sub;  // rows per slot: 8 .. 128
+            const int grp = span < 32 ? span : 32;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              if (c0 + j >= c_hi) break;  // uniform over the warp
+              unsigned long long key = ~0ull;
+              if (row_ok) {
+                const float dd = xn2 + s_qn2[c0 + j] - 2.0f * __uint_as_float(r[j]);
+                key = ((unsigned long long)ordered_key(dd) << 32) | (uint32_t)row;
+              }
+              for (int o = 1; o < grp; o <<= 1) {
+                const unsigned long long v = __shfl_xor_sync(HG_FULL, key, o);
+                key = v < key ? v : key;
+              }
+              const uint32_t slot = t * it.sub + (uint32_t)((quarter * 32 + lane) / span);
+              if ((lane & (grp - 1)) == 0 && key != ~0ull && slot < a.bm_cap)
+                atomicMin(&a.bm[(uint64_t)s_qidx[c0 + j] * a.bm_cap + slot], key);
+            }
+          } else if (row_ok) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (c0 + j < c_hi) a.dots[(uint64_t)(it.qoff + c0 + j) * a.dots_ld + row] = __uint_as_float(r[j]);
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(tempty_bar(b));
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+  }
+}
+
+size_t umma_filter_smem() { return kDynSmem; }
+
+cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q_map, const BatchGemm& g, int blocks,
+                               cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_umma_filter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDynSmem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const uint64_t ntiles = (g.nrows + kUM - 1) / kUM;
+  const uint32_t QT = (uint32_t)((g.nq + kUN - 1) / kUN);
+  const uint64_t total =
+      g.mode == 0 ? g.nitems : ((ntiles + g.tiles_per_item - 1) / g.tiles_per_item) * (uint64_t)QT;
+  if (total == 0) return cudaSuccess;
+  const int grid = (int)(total < (uint64_t)blocks ? total : (uint64_t)blocks);
+  k_umma_filter<<<grid, kThreads, kDynSmem, s>>>(rows_map, q_map, g);
+  return cudaGetLastError();
+}
+
+}  // namespace hg

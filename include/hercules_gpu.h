@@ -200,6 +200,15 @@ HG_API hg_status hg_knn_batch_device(hg_index *ix, const float *d_queries, uint3
                                      uint32_t kmax, const hg_knn_opts *opts, float *d_dist_out,
                                      int64_t *d_id_out, void *stream, hg_query_stats *stats);
 
+/* Diagnostics (no counterpart in the reference): the batched filter's
+ * tensor-core products q~.x~ -- BF16 roundings of every query and row,
+ * multiplied on the tensor cores with FP32 accumulation -- of nq device
+ * queries against n device rows (both row-major float32, L a multiple of 16),
+ * written to d_dots as nq x n float32 (row-major by query), ordered on
+ * `stream`.  Allocates its own temporaries. */
+HG_API hg_status hg_bf16_dots(const float *d_rows, uint64_t n, uint32_t L, const float *d_queries, uint32_t nq,
+                              float *d_dots, void *stream);
+
 /* The approximate leaf of each query: the leaf the query routes to
  * (approximate_knn_search's traversal, hercules_query_engine.c:176-222). */
 HG_API hg_status hg_route(hg_index *ix, const float *queries, uint32_t nq, int32_t *leaf_out);
