@@ -1,17 +1,24 @@
 #!/usr/bin/env python
 """bench.py -- exact k-NN queries/s on one B200 at 25M x 256 (Hercules path).
 
-Workload (default): 25,000,000 z-normalised random walks of length 256
-(25.6 GB float32, resident in HBM; seeded synthetic data, dataset seed 1184),
-leaf size 100,000, exact k-NN with k = 10 for noisy queries (a random dataset
-series plus N(0, sigma^2) noise, sigma^2 cycling 0.01 / 0.1 / 1.0, query seed
-14784).  A step is one batch of --queries-per-step queries through the plain
-per-query path (hg_knn_device); `value` is queries per second over the timed
-steps with the collection already in HBM; `e2e` is the same through hg_knn
-with the queries in pinned host memory and results copied back every step.
+Collection: 25,000,000 z-normalised random walks of length 256 (25.6 GB
+float32 resident in HBM; seeded synthetic data, dataset seed 1184), leaf
+size 100,000, built into the Hercules EAPCA index on the GPU.
 
-The data (25.6 GB) is far larger than L2 (126 MB); every query streams from
-HBM, so no L2 flush is needed between steps.
+Headline workload (a step): one batch of 4,096 queries answered exactly by
+the batched path (hg_knn_batch_device): equal thirds of noisy queries (a
+random dataset series plus N(0, sigma^2) noise, sigma^2 = 0.01 / 0.1 / 1.0,
+z-normalised) plus 10% fresh random walks, k cycling 1 / 10 / 100.  `value`
+is queries per second over the timed steps (CUDA events on the stream, the
+collection and the step's queries already in HBM); `e2e` is the same through
+hg_knn_batch with the queries in pinned host memory and the answers copied
+back every step.  The plain per-query path (hg_knn_device, k = 10) is timed
+beside it on the same collection (`plain`), with the leaf-scan kernel's
+HBM roofline (`leaf_scan`).
+
+The BF16 copy of the collection (12.8 GB) and the raw rows (25.6 GB) are far
+larger than L2 (126 MB); every step streams them from HBM, so no L2 flush is
+needed between steps.
 
 --impl reference runs the reference Hercules query path (oracle/_ref/hercules,
 compiled from the reference's own sources) on the host cores over the same
@@ -34,24 +41,27 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "exact k-NN queries/s @25Mx256"
+METRIC = "exact k-NN queries/s @25Mx256, batched-BF16 vs plain GPU; leaf-scan HBM GB/s"
 UNIT = "queries/s"
 DATA_SEED = 1184
 QUERY_SEED = 14784
+FRESH_SEED = 99991
+K_CYCLE = (1, 10, 100)
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--n", type=int, default=25_000_000)
     p.add_argument("--L", type=int, default=256)
     p.add_argument("--leaf", type=int, default=100_000)
-    p.add_argument("--k", type=int, default=10)
-    p.add_argument("--queries-per-step", type=int, default=64)
-    p.add_argument("--lb-sax", type=int, default=1)
+    p.add_argument("--batch", type=int, default=4096, help="queries per batched step")
+    p.add_argument("--fresh-frac", type=float, default=0.1)
+    p.add_argument("--plain-queries", type=int, default=128, help="queries through the plain path")
+    p.add_argument("--plain-k", type=int, default=10)
     p.add_argument("--cpu-sample-queries", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--ref-queries-per-step", type=int, default=2)
@@ -140,18 +150,20 @@ def max_over_ranks(x, world, device=None):
     return float(t.item())
 
 
-def measured_peaks():
+def measured_peaks_all():
+    """Roofline denominators: the driver-measured copy bandwidth and bf16
+    GEMM throughput of this pool's B200s, else the earlier pool figures."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return {"hbm": float(d["hbm_gbs"]), "bf16": float(d["bf16_tflops"]),
+                "bf16_sustained": float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "source": "measured"}
+    return {"hbm": 6650.0, "bf16": 1590.0, "bf16_sustained": 1400.0, "source": "fallback"}
 
 
-def ncu_traffic():
-    """DRAM traffic per algorithmic byte of the distance kernel, from the
-    committed ncu summary (profiles/k_ed_stream_traffic.json)."""
-    p = os.path.join(ROOT, "profiles", "k_ed_stream_traffic.json")
+def profile_json(name):
+    """A committed ncu summary figure (profiles/<name>), or None."""
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     try:
@@ -176,7 +188,24 @@ def make_queries(args, torch, H, X, nq, device, offset):
     return Q
 
 
-def cpu_reference_run(args, index_dir, queries_host, threads, extra=()):
+def make_batches(args, torch, H, X, nbatches, device, offset):
+    """nbatches batches of args.batch queries: noisy queries (sigma^2 in
+    equal thirds) followed by fresh random walks (args.fresh_frac)."""
+    nb = args.batch
+    nf = int(round(nb * args.fresh_frac))
+    Q = torch.empty((nbatches, nb, args.L), dtype=torch.float32, device=device)
+    for i in range(nbatches):
+        H.generate_queries_device(QUERY_SEED + offset + i, X.data_ptr(), args.n, args.L, sigma2_for(nb - nf),
+                                  Q[i].data_ptr(), device=device)
+        if nf:
+            H.generate_walks_device(FRESH_SEED + offset, nf, args.L, Q[i, nb - nf:].data_ptr(),
+                                    first=(offset + i) * nf, device=device)
+    torch.cuda.synchronize()
+    ks = np.array(K_CYCLE, np.uint32)[np.arange(nb) % len(K_CYCLE)]
+    return Q, ks
+
+
+def cpu_reference_run(args, index_dir, queries_host, threads, extra=(), k=10):
     """Runs the reference CLI over the written index; per-query seconds from
     its own Query_total_time_secs lines."""
     from oracle import oracle as O
@@ -184,7 +213,7 @@ def cpu_reference_run(args, index_dir, queries_host, threads, extra=()):
     qfile = os.path.join(index_dir, "bench_queries.bin")
     np.ascontiguousarray(queries_host, np.float32).tofile(qfile)
     nq = queries_host.shape[0]
-    cmd = [binary, "--mode", "1", "--serial", "1", "--num-threads", str(threads), "--k", str(args.k),
+    cmd = [binary, "--mode", "1", "--serial", "1", "--num-threads", str(threads), "--k", str(k),
            "--queries", qfile, "--queries-size", str(nq), "--index-path", index_dir, *extra]
     t0 = time.perf_counter()
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800, cwd=index_dir)
@@ -226,30 +255,33 @@ def main():
     B.build()
     torch.cuda.set_device(local)
     device = local
-    nq_step = args.queries_per_step
-    steps, warm = args.steps, args.warmup
+    steps, warm, nb = args.steps, args.warmup, args.batch
     t_setup = time.perf_counter()
     X = build_collection(args, torch, H, device)
-    Q = make_queries(args, torch, H, X, (steps + warm) * nq_step, device, offset=rank * 7919)
-    Qe = make_queries(args, torch, H, X, (steps + warm) * nq_step, device, offset=rank * 7919 + 1)
+    off = rank * 7919
+    Qb, ks = make_batches(args, torch, H, X, steps + warm, device, offset=off)
+    Qe, _ = make_batches(args, torch, H, X, steps + warm, device, offset=off + 5000)
+    Qp = make_queries(args, torch, H, X, args.plain_queries, device, offset=off + 9000)
     t0 = time.perf_counter()
     ix = H.HerculesIndex.build_device(X.data_ptr(), args.n, args.L, args.leaf, device=device)
     build_s = time.perf_counter() - t0
-    cpu_q = Q[:args.cpu_sample_queries].cpu().numpy() if (rank == 0 and world == 1) else None
+    cpu_q = Qb[0, :args.cpu_sample_queries].cpu().numpy() if (rank == 0 and world == 1) else None
     del X
     torch.cuda.empty_cache()
-    setup_s = time.perf_counter() - t_setup
-    k = args.k
-    D = torch.empty((nq_step, k), dtype=torch.float32, device=device)
-    I = torch.empty((nq_step, k), dtype=torch.int64, device=device)
+    kmax = int(ks.max())
+    D = torch.empty((nb, kmax), dtype=torch.float32, device=device)
+    I = torch.empty((nb, kmax), dtype=torch.int64, device=device)
     stream = torch.cuda.current_stream().cuda_stream
 
-    def step(i, profile):
-        return ix.knn_device(Q[i * nq_step:(i + 1) * nq_step].data_ptr(), nq_step, k, D.data_ptr(), I.data_ptr(),
-                             stream=stream, use_lb_sax=bool(args.lb_sax), profile=profile)
+    def batch_step(i):
+        return ix.knn_batch_device(Qb[i].data_ptr(), nb, ks, kmax, D.data_ptr(), I.data_ptr(), stream=stream)
 
-    for i in range(warm):
-        step(i, False)
+    t1 = time.perf_counter()
+    batch_step(0)  # the first call also builds the BF16 copy of the collection
+    torch.cuda.synchronize()
+    prep_s = time.perf_counter() - t1
+    for i in range(1, warm):
+        batch_step(i)
     torch.cuda.synchronize()
     barrier(world)
     clocks = ClockSampler(device)
@@ -259,90 +291,115 @@ def main():
     e0.record()
     agg = {}
     for i in range(warm, warm + steps):
-        st = step(i, True)
+        st = batch_step(i)
         for kk, v in st.items():
             agg[kk] = agg.get(kk, 0) + v
     e1.record()
     torch.cuda.synchronize()
     ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    ms = max_over_ranks(ms, world, device=torch.device("cuda", device))
-    total_q = nq_step * steps * world
+    ms = max_over_ranks(e0.elapsed_time(e1), world, device=torch.device("cuda", device))
+    total_q = nb * steps * world
     value = total_q / (ms / 1000.0)
 
-    # end to end: host queries (pinned) in, host results out, every step
-    Qh = torch.empty((nq_step * (steps + warm), args.L), dtype=torch.float32, pin_memory=True)
+    # end to end through the host API: pinned host queries in, answers out
+    Qh = torch.empty(tuple(Qe.shape), dtype=torch.float32, pin_memory=True)
     Qh.copy_(Qe.cpu())
     Qhn = Qh.numpy()
     for i in range(warm):
-        ix.knn(Qhn[i * nq_step:(i + 1) * nq_step], k, use_lb_sax=bool(args.lb_sax))
+        ix.knn_batch(Qhn[i], ks)
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for i in range(warm, warm + steps):
-        ix.knn(Qhn[i * nq_step:(i + 1) * nq_step], k, use_lb_sax=bool(args.lb_sax))
+        ix.knn_batch(Qhn[i], ks)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, device=torch.device("cuda", device))
     e2e_value = total_q / e2e_s
 
-    # roofline of the dominant kernel, the distance stream k_ed_stream:
-    # algorithmic bytes = 32 B per 8-float chunk whose distance it computed
-    # + 4 B list entry per row started + 8 B id per finished row, divided by
-    # its summed launch time (CUDA events around every launch)
-    peak, peak_kind = measured_peaks()
-    launches = int(agg["scan_launches"])
-    alg_bytes = 32.0 * agg["chunks_loaded"] + 4.0 * agg["rows_visited"] + 8.0 * agg["rows_completed"]
-    scan_s = agg["scan_ms"] / 1000.0
-    achieved = alg_bytes / scan_s / 1e9 if scan_s > 0 else 0.0
-    tr = ncu_traffic()
-    traffic = None
-    if tr and tr.get("dram_bytes_per_algorithmic_byte"):
-        # ncu traffic of a small capture, scaled to a 25M launch by its
-        # algorithmic bytes (traffic grows in proportion)
-        traffic = tr["dram_bytes_per_algorithmic_byte"] * alg_bytes / max(launches, 1)
-    f_launches = int(agg["filter_launches"])
-    f_bytes = 16.0 * agg["rows_considered"] + 4.0 * (agg["rows_considered"] - agg["rows_lbsax_pruned"])
-    f_s = agg["filter_ms"] / 1000.0
-    roofline = {"bound": "hbm", "kernel": "k_ed_stream", "achieved": round(achieved, 1),
-                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "peak_source": peak_kind, "traffic": traffic,
-                "algorithmic_bytes_per_launch": alg_bytes / max(launches, 1),
-                "avg_launch_ms": agg["scan_ms"] / max(launches, 1), "launches": launches,
-                "second_kernel": {"kernel": "k_lbsax_filter",
-                                  "achieved": round(f_bytes / f_s / 1e9, 1) if f_s > 0 else None,
-                                  "frac": round(f_bytes / f_s / 1e9 / peak, 4) if f_s > 0 else None,
-                                  "avg_launch_ms": agg["filter_ms"] / max(f_launches, 1), "launches": f_launches}}
+    # the plain per-query path on the same collection, every scan launch timed
+    pk = args.plain_k
+    Dp = torch.empty((args.plain_queries, pk), dtype=torch.float32, device=device)
+    Ip = torch.empty((args.plain_queries, pk), dtype=torch.int64, device=device)
+    ix.knn_device(Qp.data_ptr(), min(8, args.plain_queries), pk, Dp.data_ptr(), Ip.data_ptr(), stream=stream,
+                  use_lb_sax=True)
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    pst = ix.knn_device(Qp.data_ptr(), args.plain_queries, pk, Dp.data_ptr(), Ip.data_ptr(), stream=stream,
+                        use_lb_sax=True, profile=True)
+    p1.record()
+    torch.cuda.synchronize()
+    plain_ms = p0.elapsed_time(p1)
+    plain_qps = args.plain_queries / (plain_ms / 1000.0)
 
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu_baseline = cpu_baseline_leg(args, ix, cpu_q)
+        cpu_baseline = cpu_baseline_leg(args, ix, cpu_q, ks[:args.cpu_sample_queries])
     ix.close()
-    # per query: prep, leaf LB, distances (approximate leaf), merge, sort,
-    # LB_SAX filter, distances (candidates), merge, emit
-    per_query_launches = 9
+
+    # roofline of the dominant kernel, the tensor-core filter k_umma_filter:
+    # algorithmic FLOPs = 2 L per (query, row) pair it evaluated, over its
+    # summed launch time (CUDA events around every launch)
+    peaks = measured_peaks_all()
+    gemm_s = agg["gemm_ms"] / 1000.0
+    flops = 2.0 * args.L * agg["bf16_pairs"]
+    achieved_tf = flops / gemm_s / 1e12 if gemm_s > 0 else 0.0
+    filt_launches = steps  # one full filter pass per step, plus retry rounds on a few queries
+    tr = profile_json("k_umma_filter_traffic.json")
+    traffic = None
+    if tr and tr.get("dram_bytes_per_row_pass"):
+        traffic = tr["dram_bytes_per_row_pass"] * args.n
+    roofline = {"bound": "tensor", "kernel": "k_umma_filter", "achieved": round(achieved_tf, 1),
+                "peak": peaks["bf16_sustained"], "unit": "TFLOP/s",
+                "frac": round(achieved_tf / peaks["bf16_sustained"], 4),
+                "peak_source": peaks["source"] + " sustained bf16 (the filter runs inside seconds-long steps)",
+                "traffic": traffic, "algorithmic_flops_per_step": flops / steps,
+                "avg_ms_per_step": agg["gemm_ms"] / steps, "pairs_per_step": agg["bf16_pairs"] / steps}
+    # leaf scan of the plain path: k_ed_stream's algorithmic bytes = 32 B per
+    # 8-float chunk computed + 4 B list entry per row started + 8 B id per
+    # finished row, over its summed launch time
+    launches = int(pst["scan_launches"])
+    alg_bytes = 32.0 * pst["chunks_loaded"] + 4.0 * pst["rows_visited"] + 8.0 * pst["rows_completed"]
+    scan_s = pst["scan_ms"] / 1000.0
+    ed_gbs = alg_bytes / scan_s / 1e9 if scan_s > 0 else 0.0
+    tre = profile_json("k_ed_stream_traffic.json")
+    ed_traffic = None
+    if tre and tre.get("dram_bytes_per_algorithmic_byte"):
+        ed_traffic = tre["dram_bytes_per_algorithmic_byte"] * alg_bytes / max(launches, 1)
+    leaf_scan = {"bound": "hbm", "kernel": "k_ed_stream", "achieved": round(ed_gbs, 1), "peak": peaks["hbm"],
+                 "unit": "GB/s", "frac": round(ed_gbs / peaks["hbm"], 4), "peak_source": peaks["source"],
+                 "traffic": ed_traffic, "algorithmic_bytes_per_launch": alg_bytes / max(launches, 1),
+                 "avg_launch_ms": pst["scan_ms"] / max(launches, 1), "launches": launches}
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warm,
         "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded z-normalised random walks; noisy queries)",
-        "config": {"workload": "plain per-query exact k-NN, %d x %d float32, leaf %d, k=%d, %d queries/step, "
-                               "sigma2 0.01/0.1/1.0" % (args.n, args.L, args.leaf, k, nq_step),
-                   "n": args.n, "L": args.L, "leaf_size": args.leaf, "k": k, "queries_per_step": nq_step,
-                   "lb_sax": bool(args.lb_sax), "l2": "inputs (25.6 GB) larger than L2; no flush needed",
+        "dtype": "bf16 filter (fp32 accumulate) + f32 exact re-rank",
+        "data": "synthetic (seeded z-normalised random walks; noisy and fresh queries)",
+        "config": {"workload": "batched exact k-NN, %d x %d float32, leaf %d, %d queries/step, k cycling 1/10/100, "
+                               "sigma2 thirds 0.01/0.1/1.0 + %d%% fresh walks"
+                               % (args.n, args.L, args.leaf, nb, int(round(100 * args.fresh_frac))),
+                   "n": args.n, "L": args.L, "leaf_size": args.leaf, "queries_per_step": nb, "k": list(K_CYCLE),
+                   "l2": "inputs (25.6 GB f32 + 12.8 GB bf16) larger than L2; no flush needed",
                    "parallelism": "replica per GPU" if world > 1 else "single GPU"},
-        "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": nq_step * args.L * 4,
-                "d2h_bytes_per_step": nq_step * k * (4 + 8)},
-        "gpu_launches": per_query_launches * nq_step * steps,
+        "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": nb * args.L * 4,
+                "d2h_bytes_per_step": nb * kmax * (4 + 8)},
+        "gpu_launches": int(agg["kernel_launches"]),
         "roofline": roofline,
+        "leaf_scan": leaf_scan,
+        "plain": {"value": round(plain_qps, 2), "unit": UNIT, "queries": args.plain_queries, "k": pk,
+                  "path": "hg_knn_device (one query at a time, LB_SAX on)",
+                  "batched_over_plain": round(value / plain_qps, 2) if plain_qps > 0 else None},
         "cpu_baseline": cpu_baseline,
         "clocks": ck,
-        "stats": {"candidate_rows_per_query": agg["rows_considered"] / (nq_step * steps),
-                  "lbsax_pruned_frac": agg["rows_lbsax_pruned"] / max(agg["rows_considered"], 1),
-                  "distance_rows_per_query": agg["rows_visited"] / (nq_step * steps),
-                  "chunks_per_distance_row": agg["chunks_loaded"] / max(agg["rows_visited"], 1),
-                  "leaves_scanned_per_query": agg["leaves_scanned"] / (nq_step * steps),
-                  "ed_share_of_step": agg["scan_ms"] / ms if ms > 0 else None,
-                  "filter_share_of_step": agg["filter_ms"] / ms if ms > 0 else None,
-                  "index_build_s": round(build_s, 2), "setup_s": round(setup_s, 2)},
+        "stats": {"survivors_per_query": agg["survivors"] / (nb * steps),
+                  "survivor_fraction": agg["survivors"] / max(agg["bf16_pairs"], 1),
+                  "rerank_rows_per_query": agg["rows_visited"] / (nb * steps),
+                  "retried_queries_per_step": agg["retried_queries"] / steps,
+                  "fallback_queries_per_step": agg["fallback_queries"] / steps,
+                  "bound_ms_per_step": agg["bound_ms"] / steps, "filter_ms_per_step": agg["gemm_ms"] / steps,
+                  "rerank_ms_per_step": agg["rerank_ms"] / steps, "fallback_ms_per_step": agg["fallback_ms"] / steps,
+                  "first_call_prep_s": round(prep_s, 2), "index_build_s": round(build_s, 2),
+                  "setup_s": round(time.perf_counter() - t_setup, 2)},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -351,9 +408,10 @@ def main():
         dist.destroy_process_group()
 
 
-def cpu_baseline_leg(args, ix, cpu_q):
+def cpu_baseline_leg(args, ix, cpu_q, cpu_k):
     """The reference's serial exact search (oracle/_ref/hercules, built from
-    the reference sources) on a few of the same queries over the same index."""
+    the reference sources) on a few of the timed queries, each with its own
+    k, over the same index."""
     from oracle import oracle as O
     d = None
     try:
@@ -364,13 +422,17 @@ def cpu_baseline_leg(args, ix, cpu_q):
         if d is None:
             return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                     "sample": "unavailable: no host space for the index files"}
-        per_q, wall = cpu_reference_run(args, d, cpu_q, threads=1)
-        secs = sum(per_q.values())
-        return {"value": round(len(per_q) / secs, 4) if secs > 0 else None, "unit": UNIT, "cores": 1,
+        secs, nq, wall = 0.0, 0, 0.0
+        for q, k in zip(cpu_q, cpu_k):
+            per_q, w = cpu_reference_run(args, d, q[None, :], threads=1, k=int(k))
+            secs += sum(per_q.values())
+            nq += len(per_q)
+            wall += w
+        return {"value": round(nq / secs, 4) if secs > 0 else None, "unit": UNIT, "cores": 1,
                 "kind": "reference",
-                "sample": "%d of the timed queries, reference exact_de_knn_search (--num-threads 1) over the "
-                          "same %dx%d index; per-query time from its Query_total_time_secs; wall %.1f s"
-                          % (len(per_q), args.n, args.L, wall)}
+                "sample": "%d of the timed queries (k = %s), reference exact_de_knn_search (--num-threads 1) over "
+                          "the same %dx%d index; per-query time from its Query_total_time_secs; wall %.1f s"
+                          % (nq, ",".join(str(int(k)) for k in cpu_k), args.n, args.L, wall)}
     except Exception as e:  # the baseline is reported, never fatal
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": "failed: %s" % e}
     finally:
@@ -380,7 +442,8 @@ def cpu_baseline_leg(args, ix, cpu_q):
 
 def run_reference(args, rank, world, local):
     """--impl reference: the reference's multi-threaded query path on the
-    host cores over the same index files."""
+    host cores over the same index files, on queries of the batched
+    workload (each with its own k)."""
     if rank != 0:
         return
     from oracle import oracle as O
@@ -395,7 +458,7 @@ def run_reference(args, rank, world, local):
     torch.cuda.set_device(local)
     nps = args.ref_queries_per_step
     X = build_collection(args, torch, H, local)
-    Q = make_queries(args, torch, H, X, (args.steps + args.warmup) * nps, local, offset=0)
+    Qb, ks = make_batches(args, torch, H, X, 1, local, offset=0)
     ix = H.HerculesIndex.build_device(X.data_ptr(), args.n, args.L, args.leaf, device=local)
     del X
     torch.cuda.empty_cache()
@@ -411,23 +474,32 @@ def run_reference(args, rank, world, local):
         # branch: its threaded refine worker never advances and hangs
         # (hercules_query_engine.c:1987-2026)
         extra = ("--sims", "--eapca-threshold", "0.25", "--sax-threshold", "1.1")
-        per_q, wall = cpu_reference_run(args, d, Q.cpu().numpy(), threads=threads, extra=extra)
-        qs = sorted(per_q)
-        timed = qs[args.warmup * nps:]
-        secs = sum(per_q[q] for q in timed)
+        total = (args.steps + args.warmup) * nps
+        # spread the sample over the batch so the noise levels, fresh walks
+        # and k values appear in the batch's proportions
+        pick = np.linspace(0, args.batch - 1, total).astype(np.int64)
+        Qh = Qb[0].cpu().numpy()
+        times, wall = [], 0.0
+        for j in pick:
+            per_q, w = cpu_reference_run(args, d, Qh[j][None, :], threads=threads, extra=extra, k=int(ks[j]))
+            times.append(sum(per_q.values()))
+            wall += w
+        timed = times[args.warmup * nps:]
+        secs = sum(timed)
         value = len(timed) / secs if secs > 0 else None
         line = {"impl": "reference", "metric": METRIC, "value": round(value, 4) if value else None, "unit": UNIT,
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1000.0 * secs / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded z-normalised random walks)",
-                "config": {"workload": "plain per-query exact k-NN, %d x %d float32, leaf %d, k=%d"
-                                       % (args.n, args.L, args.leaf, args.k), "queries_per_step": nps},
+                "config": {"workload": "batched exact k-NN workload, %d x %d float32, leaf %d, k cycling 1/10/100, "
+                                       "queries answered one at a time by the reference" % (args.n, args.L, args.leaf),
+                           "queries_per_step": nps},
                 "cpu_baseline": {"value": round(value, 4) if value else None, "unit": UNIT, "cores": threads,
                                  "kind": "reference",
-                                 "sample": "%d queries per step; reference --num-threads %d --sims "
-                                           "--eapca-threshold 0.25 --sax-threshold 1.1 over the index files "
-                                           "(built on the GPU, byte-identical to the reference's); wall %.1f s"
-                                           % (nps, threads, wall)},
+                                 "sample": "%d queries per step spread over a batch of the workload; reference "
+                                           "--num-threads %d --sims --eapca-threshold 0.25 --sax-threshold 1.1 "
+                                           "over the index files (built on the GPU, byte-identical to the "
+                                           "reference's); wall %.1f s" % (nps, threads, wall)},
                 "e2e": {"value": round(value, 4) if value else None, "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)

@@ -52,7 +52,7 @@ class QueryStats(ctypes.Structure):
                 ("survivors", ctypes.c_uint64), ("fallback_queries", ctypes.c_uint64),
                 ("retried_queries", ctypes.c_uint64),
                 ("bound_ms", ctypes.c_double), ("gemm_ms", ctypes.c_double), ("rerank_ms", ctypes.c_double),
-                ("fallback_ms", ctypes.c_double)]
+                ("fallback_ms", ctypes.c_double), ("kernel_launches", ctypes.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

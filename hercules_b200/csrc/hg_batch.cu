@@ -37,7 +37,7 @@
 
 namespace hg {
 
-constexpr int kBM = kBatchTileRows, kBN = 128, kBK = 64, kStages = 3, kGemmThreads = 256;
+constexpr int kBM = kBatchTileRows;
 
 // ---------------------------------------------------------------------------
 // preparation
@@ -109,258 +109,13 @@ __global__ void k_tile_norms(const float4* __restrict__ meta, uint64_t n, float4
 }
 
 // ---------------------------------------------------------------------------
-// the BF16 GEMM with fused epilogues (mma.sync m16n8k16, FP32 accumulation)
-// ---------------------------------------------------------------------------
-
-__device__ __forceinline__ uint32_t ordered_key(float f) {
-  const uint32_t b = __float_as_uint(f);
-  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// 16-byte asynchronous copy; src-size 0 zero-fills the destination.
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
-  const int sz = valid ? 16 : 0;
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(sz));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-__device__ __forceinline__ void ldmatrix_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-               : "r"(addr));
-}
-
-__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-// A stage holds 128 rows x 64 BF16 (128 B per row) of each operand; the
-// 16-byte chunk c of row r sits at chunk c ^ (r & 7), so the eight row
-// addresses of one ldmatrix phase fall in eight different bank groups.
-__device__ __forceinline__ uint32_t swz(int r, int c) { return (uint32_t)((r * 8 + (c ^ (r & 7))) * 16); }
-
-// Work item -> tiles and queries.  Mode 0 (bound): item = tiles [tile_lo,
-// tile_hi) of one approximate leaf for one group of queries routed there.
-// Mode 1 (filter): item w = (row chunk w / QT, query tile w % QT), so the QT
-// items of one row chunk run side by side and read it from HBM once.
-__global__ void __launch_bounds__(kGemmThreads, 2) k_bf16_filter(BatchGemm a) {
-  extern __shared__ __align__(128) unsigned char gsm[];
-  unsigned char* sA = gsm;                            // kStages x 16 KB of rows
-  unsigned char* sB = gsm + kStages * kBM * kBK * 2;  // kStages x 16 KB of queries
-  __shared__ uint32_t s_item;
-  __shared__ uint32_t s_qidx[kBN];
-  __shared__ float s_qn2[kBN], s_qt[kBN], s_qr[kBN], s_qb[kBN];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps, 64 rows x 32 queries each
-  const int g = lane >> 2, tig = lane & 3;
-  const int ksteps = (a.L + kBK - 1) / kBK;
-  const uint32_t QT = (uint32_t)((a.nq + kBN - 1) / kBN);
-  const uint64_t ntiles = (a.nrows + kBM - 1) / kBM;
-  const uint32_t nchunks = (uint32_t)((ntiles + a.tiles_per_item - 1) / a.tiles_per_item);
-  const uint32_t total_items = a.mode == 0 ? a.nitems : nchunks * QT;
-  const float inf = __int_as_float(0x7f800000);
-
-  for (;;) {
-    if (tid == 0) s_item = atomicAdd(a.work_head, 1u);
-    __syncthreads();
-    const uint32_t w = s_item;
-    if (w >= total_items) break;
-    uint64_t rb, re;
-    uint32_t qoff, qcnt, t_lo, t_hi, sub = 1;
-    if (a.mode == 0) {
-      const BatchItem it = a.items[w];
-      rb = it.row_begin;
-      re = it.row_end;
-      qoff = it.q_off;
-      qcnt = it.q_cnt;
-      t_lo = it.tile_lo;
-      t_hi = it.tile_hi;
-      sub = it.sub;
-    } else {
-      const uint32_t chunk = w / QT, qt = w % QT;
-      rb = 0;
-      re = a.nrows;
-      qoff = qt * kBN;
-      qcnt = (uint32_t)min(a.nq - (int)qoff, kBN);
-      t_lo = chunk * a.tiles_per_item;
-      const uint64_t th = (uint64_t)t_lo + a.tiles_per_item;
-      t_hi = (uint32_t)(th < ntiles ? th : ntiles);
-    }
-    if (tid < kBN) {
-      const uint32_t q = tid < (int)qcnt ? a.qperm[qoff + tid] : 0xffffffffu;
-      s_qidx[tid] = q;
-      const bool ok = q != 0xffffffffu;
-      const float4 qm = ok ? a.qmeta[q] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      s_qn2[tid] = qm.x;
-      s_qt[tid] = qm.y;
-      s_qr[tid] = qm.z;
-      // the filter skips queries without a finite bound (they take the plain path)
-      const float b = (ok && a.mode == 1) ? a.bound[q] : 0.0f;
-      s_qb[tid] = (ok && b < inf) ? b : -1.0f;
-    }
-    __syncthreads();
-    const uint32_t nstage_total = (t_hi - t_lo) * (uint32_t)ksteps;
-    auto issue = [&](uint32_t s) {
-      if (s < nstage_total) {
-        const uint64_t row0 = rb + (uint64_t)(t_lo + s / ksteps) * kBM;
-        const uint64_t nvalid = row0 < re ? (re - row0 < (uint64_t)kBM ? re - row0 : (uint64_t)kBM) : 0;
-        const int kb = (int)(s % ksteps) * kBK;
-        const int buf = (int)(s % kStages);
-        unsigned char* A = sA + buf * kBM * kBK * 2;
-        unsigned char* Bm = sB + buf * kBN * kBK * 2;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int idx = tid + i * kGemmThreads;  // 0..1023: 128 rows x 8 chunks
-          const int r = idx >> 3, c = idx & 7;
-          const bool kv = kb + c * 8 < a.L;
-          const bool va = kv && (uint64_t)r < nvalid;
-          const __nv_bfloat16* srcA = static_cast<const __nv_bfloat16*>(a.xbf) + (va ? (row0 + r) * (uint64_t)a.L + kb + c * 8 : 0);
-          cp_async16(smem_u32(A + swz(r, c)), srcA, va);
-          const uint32_t q = s_qidx[r];
-          const bool vb = kv && q != 0xffffffffu;
-          const __nv_bfloat16* srcB = static_cast<const __nv_bfloat16*>(a.qbf) + (vb ? (uint64_t)q * a.L + kb + c * 8 : 0);
-          cp_async16(smem_u32(Bm + swz(r, c)), srcB, vb);
-        }
-      }
-      cp_async_commit();
-    };
-    for (int s = 0; s < kStages - 1; ++s) issue((uint32_t)s);
-    float acc[4][4][4];
-    for (uint32_t s = 0; s < nstage_total; ++s) {
-      const int kk = (int)(s % ksteps);
-      if (kk == 0) {
-#pragma unroll
-        for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-          for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) acc[mi][ni][e] = 0.0f;
-      }
-      cp_async_wait<kStages - 2>();
-      __syncthreads();
-      issue(s + kStages - 1);
-      const int buf = (int)(s % kStages);
-      const unsigned char* A = sA + buf * kBM * kBK * 2;
-      const unsigned char* Bm = sB + buf * kBN * kBK * 2;
-#pragma unroll
-      for (int k16 = 0; k16 < kBK / 16; ++k16) {
-        uint32_t af[4][4];
-#pragma unroll
-        for (int mi = 0; mi < 4; ++mi) {
-          const int r = wm * 64 + mi * 16 + (lane & 15);
-          const int c = k16 * 2 + (lane >> 4);
-          ldmatrix_x4(smem_u32(A + swz(r, c)), af[mi][0], af[mi][1], af[mi][2], af[mi][3]);
-        }
-        uint32_t bfr[4][2];
-#pragma unroll
-        for (int nj = 0; nj < 2; ++nj) {
-          const int r = wn * 32 + nj * 16 + (lane & 7) + ((lane >> 4) << 3);
-          const int c = k16 * 2 + ((lane >> 3) & 1);
-          ldmatrix_x4(smem_u32(Bm + swz(r, c)), bfr[nj * 2][0], bfr[nj * 2][1], bfr[nj * 2 + 1][0],
-                      bfr[nj * 2 + 1][1]);
-        }
-#pragma unroll
-        for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-          for (int ni = 0; ni < 4; ++ni) mma_bf16(acc[mi][ni], af[mi], bfr[ni][0], bfr[ni][1]);
-      }
-      if (kk != ksteps - 1) continue;
-      // ---- epilogue of one 128 x 128 tile
-      const uint32_t tl = t_lo + s / ksteps;
-      const uint64_t row0 = rb + (uint64_t)tl * kBM;
-      const uint64_t nvalid = row0 < re ? (re - row0 < (uint64_t)kBM ? re - row0 : (uint64_t)kBM) : 0;
-      if (a.mode == 1) {
-        const uint64_t gt = row0 / kBM;
-        const float4 tm = a.tile_meta[gt];  // max |x|^2, max |x~|, max |x - x~|
-        float thr[8];
-#pragma unroll
-        for (int ci = 0; ci < 8; ++ci) {
-          const int col = wn * 32 + (ci >> 1) * 8 + tig * 2 + (ci & 1);
-          const float b = s_qb[col], qn2 = s_qn2[col], qt = s_qt[col], qr = s_qr[col];
-          const float err = 2.000002f * (qt * tm.z + qr * tm.y + qr * tm.z + a.c_acc * qt * tm.y) +
-                            a.c_sq * (qn2 + tm.x + b) + 1e-5f;
-          // keep when |x|^2 + (|q|^2 - B - err) - 2 acc <= 0
-          thr[ci] = b >= 0.0f ? qn2 - b - err : inf;
-        }
-#pragma unroll
-        for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int r = wm * 64 + mi * 16 + g + h * 8;
-            if ((uint64_t)r >= nvalid) continue;
-            const uint64_t row = row0 + r;
-            const float xn = a.xmeta[row].x;
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-              for (int e = 0; e < 2; ++e) {
-                const float v = xn + thr[ni * 2 + e] - 2.0f * acc[mi][ni][h * 2 + e];
-                if (v <= 0.0f) {
-                  const uint32_t q = s_qidx[wn * 32 + ni * 8 + tig * 2 + e];
-                  const uint32_t pos = atomicAdd(&a.bucket_cnt[q], 1u);
-                  if (pos < a.bucket_cap) a.bucket[(uint64_t)q * a.bucket_cap + pos] = (uint32_t)row;
-                }
-              }
-          }
-      } else {
-        // per query column: min d~ (and its row) over the thread's 8 rows,
-        // reduced over the groups that share a slot
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int col = wn * 32 + ni * 8 + tig * 2 + e;
-            const uint32_t q = s_qidx[col];
-            const float qn2 = s_qn2[col];
-            unsigned long long best = ~0ull;
-#pragma unroll
-            for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-              for (int h = 0; h < 2; ++h) {
-                const int r = wm * 64 + mi * 16 + g + h * 8;
-                if ((uint64_t)r < nvalid) {
-                  const uint64_t row = row0 + r;
-                  const float d = a.xmeta[row].x + qn2 - 2.0f * acc[mi][ni][h * 2 + e];
-                  const unsigned long long key = ((unsigned long long)ordered_key(d) << 32) | (uint32_t)row;
-                  best = key < best ? key : best;
-                }
-              }
-            // the 8 rows of one thread and column form group wm * 8 + g of
-            // the tile; `span` consecutive groups share one slot
-            const int span = 16 / (int)sub;
-            const int gshift = span >= 8 ? 3 : (span == 4 ? 2 : (span == 2 ? 1 : 0));
-            for (int l = 0; l < gshift; ++l) {
-              const unsigned long long o = __shfl_xor_sync(HG_FULL, best, 4 << l);
-              best = o < best ? o : best;
-            }
-            const uint32_t slot = tl * sub + (uint32_t)((wm * 8 + g) / span);
-            if ((g & ((1 << gshift) - 1)) == 0 && q != 0xffffffffu && best != ~0ull && slot < a.bm_cap)
-              atomicMin(&a.bm[(uint64_t)q * a.bm_cap + slot], best);
-          }
-      }
-    }
-    cp_async_wait<0>();
-    __syncthreads();
-  }
-}
-
-// ---------------------------------------------------------------------------
 // bound, re-rank, verification
 // ---------------------------------------------------------------------------
 
-// Step 2: one block per query.  The slots' minima are distinct rows; the k
-// smallest are ranked exactly (hg_ed, reference order) and the k-th distinct
-// distance among them bounds the query's k-th neighbour distance.
+// Step 2: one block per query.  The slots' minima are distinct rows; the
+// kMaxK smallest are ranked exactly (hg_ed, reference order) and the k-th
+// distinct distance among them bounds the query's k-th neighbour distance
+// (more rows than k: a tighter bound, and k distinct distances despite ties).
 constexpr int kSelThreads = 256;
 __global__ void __launch_bounds__(kSelThreads) k_bound_select(BatchRank a) {
   extern __shared__ unsigned long long ssel[];
@@ -391,7 +146,7 @@ __global__ void __launch_bounds__(kSelThreads) k_bound_select(BatchRank a) {
   const float* qv = a.Q + (uint64_t)q * a.L;
   for (int i = tid; i < kWarpListCap; i += kSelThreads) {
     unsigned long long v = ~0ull;
-    if (i < k && i < n && buf[i] != ~0ull) {
+    if (i < kMaxK && i < n && buf[i] != ~0ull) {
       const uint32_t row = (uint32_t)buf[i];
       const float d = hg_ed(qv, a.rows + (uint64_t)row * a.L, a.L, __int_as_float(0x7f800000));
       v = ((unsigned long long)__float_as_uint(d) << 32) | (uint32_t)a.ids[row];
@@ -643,20 +398,6 @@ cudaError_t launch_tile_norms(const float4* meta, uint64_t n, float4* tile_meta,
   const uint64_t nt = (n + kBM - 1) / kBM;
   if (!nt) return cudaSuccess;
   k_tile_norms<<<nblk(nt * 32, 256), 256, 0, s>>>(meta, n, tile_meta);
-  return cudaGetLastError();
-}
-
-size_t bf16_filter_smem() { return (size_t)kStages * (kBM + kBN) * kBK * 2; }
-
-cudaError_t launch_bf16_filter(const BatchGemm& g, int blocks, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    const cudaError_t e =
-        cudaFuncSetAttribute(k_bf16_filter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bf16_filter_smem());
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  k_bf16_filter<<<blocks, kGemmThreads, bf16_filter_smem(), s>>>(g);
   return cudaGetLastError();
 }
 

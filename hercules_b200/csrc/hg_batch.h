@@ -26,15 +26,15 @@ struct BatchItem {
   uint32_t pad;
 };
 
+// Arguments of the tensor-core filter (hg_umma.cu); the BF16 rows and the
+// BF16 queries (in tile order) reach it as TMA descriptors.
 struct BatchGemm {
-  const void* xbf;  // BF16 rows, row-major, leaf order
-  const void* qbf;  // BF16 queries
   int L;
   uint64_t nrows;
   const float4* xmeta;      // per row: |x|^2, |x~|, |x - x~|, 0 (FP64, rounded up)
   const float4* tile_meta;  // per 128-row tile: the maxima of xmeta
   const float4* qmeta;      // per query: |q|^2, |q~|, |q - q~|, 0
-  const uint32_t* qperm;   // queries in tile order
+  const uint32_t* qperm;   // query of each tile column (position in the BF16 query matrix)
   int nq;
   int mode;  // 0: bound pass over the items; 1: filter over every row
   // mode 0
@@ -49,7 +49,6 @@ struct BatchGemm {
   uint32_t* bucket;        // [q][bucket_cap] surviving rows
   uint32_t* bucket_cnt;    // 0 before the launch
   uint32_t bucket_cap;
-  uint32_t* work_head;     // 0 before the launch
   int* err;                // raised (1) when a bounded wait gave up
   // mode 2 (diagnostics): raw dot products q~.x~, [query position][dots_ld]
   float* dots;
@@ -91,8 +90,6 @@ struct BatchRank {
 cudaError_t launch_rows_to_bf16(const float* rows, const uint32_t* idx, uint64_t n, int L, void* out, float4* meta,
                                 cudaStream_t s);
 cudaError_t launch_tile_norms(const float4* meta, uint64_t n, float4* tile_meta, cudaStream_t s);
-size_t bf16_filter_smem();
-cudaError_t launch_bf16_filter(const BatchGemm& g, int blocks, cudaStream_t s);
 cudaError_t launch_bound_select(const BatchRank& r, cudaStream_t s);
 size_t umma_filter_smem();
 cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q_map, const BatchGemm& g, int blocks,

@@ -1215,6 +1215,7 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
     stats->scan_ms = scan_ms;
     stats->filter_launches = filter_launches;
     stats->filter_ms = filter_ms;
+    stats->kernel_launches = (uint64_t)nq * (o.mode == HG_MODE_PSCAN ? 4 : 9);
   }
   return HG_OK;
 }
@@ -1376,6 +1377,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   CK(cudaSetDevice(ix->device));
   if (!st) st = ix->stream;
   HCK(ensure_scratch(ix, (int)kmax));
+  const bool data_built = ix->bd.xbf == nullptr;
   HCK(ensure_batch_data(ix, st));
   const uint32_t L = ix->L;
   const int sms = hg::sm_count(ix->device);
@@ -1408,9 +1410,9 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     *start = nd.file_pos;
     *size = nd.node_size;
   };
-  // bound slots per tile, per leaf: enough slots for 2k + 32 candidate rows
+  // bound slots per tile, per leaf: enough slots for max(2k + 32, 256) candidate rows
   // where the leaf has them, at most kBatchMaxSlots per query
-  const uint64_t want = 2ull * kmax + 32;
+  const uint64_t want = std::max<uint64_t>(2ull * kmax + 32, 256);
   auto sub_of = [&](uint32_t tiles) {
     uint32_t sub = 1;
     while (sub < 16 && (uint64_t)std::max<uint32_t>(tiles, 1) * sub < want) sub <<= 1;
@@ -1452,8 +1454,6 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
 
   // 2. bound pass
   hg::BatchGemm g{};
-  g.xbf = ix->bd.xbf;
-  g.qbf = b.qbf;
   g.L = (int)L;
   g.nrows = ix->n;
   g.xmeta = ix->bd.xmeta;
@@ -1472,7 +1472,6 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   g.bucket = b.bucket;
   g.bucket_cnt = b.bucket_cnt;
   g.bucket_cap = bucket_cap;
-  g.work_head = b.heads;
   g.err = reinterpret_cast<int*>(b.heads + 3);
   CK(cudaMemsetAsync(b.bm, 0xff, sizeof(unsigned long long) * nq * bm_cap, st));
   CK(cudaMemsetAsync(b.heads, 0, sizeof(uint32_t) * 4, st));
@@ -1517,8 +1516,11 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   std::vector<uint32_t> retry;
   double gemm_ms = 0, rerank_ms = 0;
   uint64_t pairs = 0, retried = 0;
+  // route, query conversion, bound pass, bound selection
+  uint64_t launches = 4 + (data_built ? 2 : 0);
   for (int round = 0; round < gemm_rounds_max; ++round) {
     const uint32_t cnt = round == 0 ? nq : (uint32_t)retry.size();
+    launches += round == 0 ? 4 : 5;  // (gather,) filter, re-rank plan / segments / merge
     if (round > 0) {
       CK(cudaMemcpyAsync(b.qlist, retry.data(), sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice, st));
       CK(hg::launch_rows_to_bf16(d_Q, b.qlist, cnt, (int)L, b.qbf, b.qmeta, st));
@@ -1530,8 +1532,6 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     g.nq = (int)cnt;
     r.nlist = (int)cnt;
     g.mode = 1;
-    g.work_head = b.heads + 1;
-    CK(cudaMemsetAsync(b.heads + 1, 0, sizeof(uint32_t), st));
     CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
     HCK(record(ev[2], st));
     CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
@@ -1592,6 +1592,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     stats->rerank_ms = rerank_ms;
     stats->fallback_ms = tf;
     stats->device_ms = t03;
+    stats->kernel_launches = launches + 9 * fallbacks;
   }
   return HG_OK;
 }

@@ -83,6 +83,7 @@ typedef struct {
   double gemm_ms;             /* device time: BF16 filter over every row */
   double rerank_ms;           /* device time: exact re-rank of the survivors */
   double fallback_ms;         /* device time: plain path for the fallback queries */
+  uint64_t kernel_launches;   /* kernels this library launched for the call */
 } hg_query_stats;
 
 /* Search mode. */
