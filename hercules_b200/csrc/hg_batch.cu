@@ -223,21 +223,32 @@ __global__ void __launch_bounds__(1024) k_rerank_plan(BatchRank a) {
   }
 }
 
+// Squared distance of the 8-float chunk c of q and x (ts.c:83-109 order),
+// both read as two float4.
+__device__ __forceinline__ float chunk_d2_v4(const float* q, const float* x, int c) {
+  const float4 x0 = reinterpret_cast<const float4*>(x)[2 * c], x1 = reinterpret_cast<const float4*>(x)[2 * c + 1];
+  const float4 q0 = reinterpret_cast<const float4*>(q)[2 * c], q1 = reinterpret_cast<const float4*>(q)[2 * c + 1];
+  const float qq[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+  const float xx[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+  return hg_chunk_d2(qq, xx);
+}
+
 // Segment re-rank: persistent warps take segments from a counter.  A warp
 // starts from step 2's list, shares the query's running k-th distance through
 // qbound (float bits, atomicMin) and writes its compacted list as one part.
-// Within the warp, 4-lane slots: lane j of a slot computes chunk ch + j and
-// the slot adds the four in order (ts_euclidean_distance_SIMD's order).
+// Within the warp, 16 two-lane slots: lane j of a slot computes chunks
+// ch + 2j and ch + 2j + 1, and both lanes add the four in order
+// (ts_euclidean_distance_SIMD's order).
 constexpr int kRankWarps = 8;
 __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_part(BatchRank a) {
   __shared__ unsigned long long lists[kRankWarps][kWarpListCap];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int slot_lead = lane & ~3, j = lane & 3;
+  const int slot_lead = lane & ~1, j = lane & 1;
   unsigned long long* list = lists[wib];
   const float inf = __int_as_float(0x7f800000);
   const uint32_t total_items = a.seg_prefix[a.nlist];
   const int nch = a.L >> 3;
-  const uint32_t leaders = 0x11111111u;
+  const uint32_t leaders = 0x55555555u;
   unsigned long long n_rows = 0, n_chunks = 0;
   for (;;) {
     uint32_t item = 0;
@@ -274,7 +285,7 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_part(BatchRank a) {
       const uint32_t need = __ballot_sync(HG_FULL, !valid) & leaders;
       if (need && next < last) {
         const int r = __popc(need & ((1u << slot_lead) - 1));
-        const uint32_t avail = min(last - next, 8u);
+        const uint32_t avail = min(last - next, 16u);
         if (((need >> slot_lead) & 1u) && (uint32_t)r < avail) {
           row = bk[next + r];
           valid = true;
@@ -287,15 +298,19 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_part(BatchRank a) {
         B = fminf(B, __uint_as_float(ld_volatile(&a.qbound[q])));
       }
       if (!__any_sync(HG_FULL, valid)) break;
-      const int c = ch + j;
-      float d = 0.0f;
-      if (valid && c < nch) d = hg_chunk_d2(qv + c * 8, a.rows + (uint64_t)row * a.L + c * 8);
+      const float* xr = a.rows + (uint64_t)row * a.L;
+      const int ca = ch + 2 * j;
+      float d0 = 0.0f, d1 = 0.0f;
+      if (valid && ca < nch) d0 = chunk_d2_v4(qv, xr, ca);
+      if (valid && ca + 1 < nch) d1 = chunk_d2_v4(qv, xr, ca + 1);
+      const float p0 = __shfl_xor_sync(HG_FULL, d0, 1), p1 = __shfl_xor_sync(HG_FULL, d1, 1);
+      // the slot's four chunk values in order
+      const float dv[4] = {j ? p0 : d0, j ? p1 : d1, j ? d0 : p0, j ? d1 : p1};
       bool finished = false;
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
-        const float dt = __shfl_sync(HG_FULL, d, slot_lead + t);
         if (valid && ch + t < nch) {
-          dist = __fadd_rn(dist, dt);
+          dist = __fadd_rn(dist, dv[t]);
           if (j == 0) ++n_chunks;
           if (dist > B) valid = false;  // partial sums only grow: this row cannot enter
         }
@@ -348,14 +363,19 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_merge(BatchRank a) {
   __syncwarp();
   int cnt = c0;
   float T = cnt == k ? __uint_as_float((uint32_t)(list[k - 1] >> 32)) : inf;
+  // the segments shared the query's running k-th distance: no entry above
+  // its final value can be among the k, and every part is sorted
+  const float Tq = __uint_as_float(ld_volatile(&a.qbound[q]));
   const uint32_t p0 = a.seg_prefix[pos], p1 = a.seg_prefix[pos + 1];
   for (uint32_t p = p0; p < p1; ++p) {
     const int pc = a.part_cnt[p];
     const unsigned long long* part = a.parts + (uint64_t)p * a.kmax;
     for (int base = 0; base < pc; base += 32) {
-      const bool take = base + lane < pc;
-      const unsigned long long v = take ? part[base + lane] : 0ull;
-      warp_list_add(list, cnt, T, k, nullptr, take, __uint_as_float((uint32_t)(v >> 32)), (uint32_t)v);
+      const unsigned long long v = base + lane < pc ? part[base + lane] : ~0ull;
+      const float d = __uint_as_float((uint32_t)(v >> 32));
+      const bool take = base + lane < pc && d <= Tq && d <= T;
+      if (!__any_sync(HG_FULL, take)) break;  // sorted: nothing further qualifies
+      warp_list_add(list, cnt, T, k, nullptr, take, d, (uint32_t)v);
     }
   }
   cnt = warp_compact(list, cnt, k);

@@ -10,9 +10,10 @@
 namespace hg {
 
 constexpr int kBatchTileRows = 128;   // rows per tensor-core tile (and per tile norm)
-constexpr int kBatchQueryTile = 256;  // queries per tensor-core tile
+constexpr int kBatchQueryTile = 256;  // queries per tensor-core tile (filter pass)
+constexpr int kBatchBoundQueries = 64;  // queries per tile in the bound pass (MMA N = 64)
 constexpr int kBatchMaxSlots = 4096;  // bound slots per query (sorted in one block)
-constexpr int kBatchMaxSeg = 16;      // re-rank segments per query
+constexpr int kBatchMaxSeg = 64;      // re-rank segments per query
 constexpr int kBatchSegMin = 256;     // rows per re-rank segment, at least
 
 // One work item of the bound pass: tiles [tile_lo, tile_hi) of the rows
@@ -36,7 +37,8 @@ struct BatchGemm {
   const float4* qmeta;      // per query: |q|^2, |q~|, |q - q~|, 0
   const uint32_t* qperm;   // query of each tile column (position in the BF16 query matrix)
   int nq;
-  int mode;  // 0: bound pass over the items; 1: filter over every row
+  int mode;  // 0: bound pass over the items; 1: filter over every row; 2: raw products
+  int qtile; // modes 1 and 2: queries per tile (MMA N): 64, 128 or 256
   // mode 0
   const BatchItem* items;
   uint32_t nitems;

@@ -1366,6 +1366,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   if (ix->leaves.size() > (size_t)hg::kMaxLeavesSort)
     return set_error(HG_ERR_LIMIT, "hg_knn_batch: more than 8192 leaves");
   if (nq > (1u << 24)) return set_error(HG_ERR_LIMIT, "hg_knn_batch: more than 2^24 queries");
+  if (((uintptr_t)d_Q & 15) != 0) return set_error(HG_ERR_ARG, "hg_knn_batch: queries must be 16-byte aligned");
   std::vector<uint32_t> kq(nq, kmax);
   if (ks)
     for (uint32_t i = 0; i < nq; ++i) {
@@ -1429,7 +1430,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   std::vector<uint32_t> slots(nq);
   for (uint32_t i = 0; i < nq;) {
     uint32_t j = i;
-    while (j < nq && approx[perm[j]] == approx[perm[i]] && j - i < (uint32_t)hg::kBatchQueryTile) ++j;
+    while (j < nq && approx[perm[j]] == approx[perm[i]] && j - i < (uint32_t)hg::kBatchBoundQueries) ++j;
     uint64_t st0, sz;
     leaf_rows(approx[perm[i]], &st0, &sz);
     const uint32_t tiles = (uint32_t)((sz + T - 1) / T);
@@ -1462,6 +1463,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   g.qperm = b.qperm;
   g.nq = (int)nq;
   g.mode = 0;
+  g.qtile = hg::kBatchQueryTile;
   g.items = b.items;
   g.nitems = (uint32_t)items.size();
   g.bm = b.bm;
@@ -1532,6 +1534,8 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     g.nq = (int)cnt;
     r.nlist = (int)cnt;
     g.mode = 1;
+    // a narrow query tile when few queries take part (retry rounds)
+    g.qtile = cnt <= 64 ? 64 : (cnt <= 128 ? 128 : hg::kBatchQueryTile);
     CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
     HCK(record(ev[2], st));
     CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
@@ -1882,6 +1886,7 @@ hg_status hg_bf16_dots(const float* d_rows, uint64_t n, uint32_t L, const float*
   g.qperm = perm;
   g.nq = (int)nq;
   g.mode = 2;
+  g.qtile = nq <= 64 ? 64 : (nq <= 128 ? 128 : hg::kBatchQueryTile);
   g.tiles_per_item = 8;
   g.err = err;
   g.dots = d_dots;

@@ -32,7 +32,7 @@ namespace {
 constexpr int kUM = 128;       // rows per tile (MMA M)
 constexpr int kUN = 256;       // queries per tile (MMA N)
 constexpr int kUK = 64;        // K elements per stage: one 128-byte swizzle row
-constexpr int kAStages = 4;
+constexpr int kAStages = 5;      // A stages (4 when the query tile is streamed with A)
 constexpr int kThreads = 384;  // 12 warps
 constexpr int kEpiThreads = 256;
 constexpr uint32_t kABytes = kUM * kUK * 2;  // 16 KB per A stage
@@ -43,16 +43,16 @@ constexpr int kErrTimeout = 1;
 
 // shared memory map (offsets from a 1024-byte aligned base)
 constexpr uint32_t kSmQ = 0;                                   // 4 x 32 KB
-constexpr uint32_t kSmA = kSmQ + kResidentKB * kQBytes;        // 4 x 16 KB
+constexpr uint32_t kSmA = kSmQ + kResidentKB * kQBytes;        // kAStages x 16 KB
 constexpr uint32_t kSmBar = kSmA + kAStages * kABytes;         // mbarriers
 constexpr uint32_t kNumBars = 2 * kAStages + 2 + 4 + 1;        // full/empty, q full/empty, tmem full/empty x2, done
 constexpr uint32_t kSmTmem = kSmBar + kNumBars * 8;            // TMEM base address
 constexpr uint32_t kSmAbort = kSmTmem + 4;
-constexpr uint32_t kSmThr = (kSmAbort + 4 + 15) & ~15u;        // float [2][256]
-constexpr uint32_t kSmQidx = kSmThr + 2 * kUN * 4;             // uint32 [256]
+constexpr uint32_t kSmThr = (kSmAbort + 4 + 15) & ~15u;        // float [256]
+constexpr uint32_t kSmQidx = kSmThr + kUN * 4;                 // uint32 [256]
 constexpr uint32_t kSmQn2 = kSmQidx + kUN * 4;                 // float [256]
-constexpr uint32_t kSmGo = kSmQn2 + kUN * 4;                   // int [2]
-constexpr uint32_t kSmBytes = kSmGo + 8;
+constexpr uint32_t kSmOkw = kSmQn2 + kUN * 4;                  // int [8]: epilogue warps still running
+constexpr uint32_t kSmBytes = kSmOkw + 32;
 constexpr size_t kDynSmem = kSmBytes + 1024;                   // + alignment slack
 
 // --- PTX wrappers -------------------------------------------------------------
@@ -157,8 +157,11 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
 
 // Instruction descriptor: FP32 accumulator, BF16 A and B, both K-major,
 // N = 256 (bits 17-22: N / 8), M = 128 (bits 24-28: M / 16).
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kUN >> 3) << 17) |
-                            ((uint32_t)(kUM >> 4) << 24);
+__host__ __device__ constexpr uint32_t idesc_for(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kUM >> 4) << 24);
+}
+// the bound pass groups at most kBatchBoundQueries queries per approximate
+// leaf, so its MMAs are N = 64 wide
 
 __device__ __forceinline__ uint32_t ordered_key(float f) {
   const uint32_t b = __float_as_uint(f);
@@ -172,7 +175,7 @@ struct Item {
   uint32_t sub;
 };
 
-__device__ __forceinline__ Item item_of(const BatchGemm& a, uint32_t w, uint32_t QT, uint64_t ntiles) {
+__device__ __forceinline__ Item item_of(const BatchGemm& a, uint32_t w, uint32_t QT, uint64_t ntiles, int qtile) {
   Item it;
   if (a.mode == 0) {
     const BatchItem b = a.items[w];
@@ -187,8 +190,8 @@ __device__ __forceinline__ Item item_of(const BatchGemm& a, uint32_t w, uint32_t
     const uint32_t chunk = w / QT, qt = w % QT;
     it.rb = 0;
     it.re = a.nrows;
-    it.qoff = qt * kUN;
-    it.qcnt = (uint32_t)min(a.nq - (int)it.qoff, kUN);
+    it.qoff = qt * (uint32_t)qtile;
+    it.qcnt = (uint32_t)min(a.nq - (int)it.qoff, qtile);
     it.t_lo = chunk * a.tiles_per_item;
     const uint64_t th = (uint64_t)it.t_lo + a.tiles_per_item;
     it.t_hi = (uint32_t)(th < ntiles ? th : ntiles);
@@ -217,11 +220,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   float* s_thr = reinterpret_cast<float*>(sm + kSmThr);
   uint32_t* s_qidx = reinterpret_cast<uint32_t*>(sm + kSmQidx);
   float* s_qn2 = reinterpret_cast<float*>(sm + kSmQn2);
-  volatile int* s_go = reinterpret_cast<volatile int*>(sm + kSmGo);
+  volatile int* s_okw = reinterpret_cast<volatile int*>(sm + kSmOkw);
 
   const int nkb = (a.L + kUK - 1) / kUK;
   const bool resident = nkb <= kResidentKB;
-  const uint32_t QT = (uint32_t)((a.nq + kUN - 1) / kUN);
+  const uint32_t nst = resident ? kAStages : kResidentKB;  // streamed: one query slot per stage
+  // queries per tile (MMA N): 64 in the bound pass, else the launch's choice
+  const int qtile = a.mode == 0 ? kBatchBoundQueries : a.qtile;
+  const uint32_t QT = (uint32_t)((a.nq + qtile - 1) / qtile);
   const uint64_t ntiles = (a.nrows + kUM - 1) / kUM;
   const uint32_t nchunks = (uint32_t)((ntiles + a.tiles_per_item - 1) / a.tiles_per_item);
   const uint32_t total = a.mode == 0 ? a.nitems : nchunks * QT;
@@ -257,7 +263,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t g = 0, it_n = 0;
       bool ok = true;
       for (uint32_t w = blockIdx.x; ok && w < total; w += gridDim.x, ++it_n) {
-        const Item it = item_of(a, w, QT, ntiles);
+        const Item it = item_of(a, w, QT, ntiles, qtile);
         if (resident) {
           ok = mbar_wait(qempty_bar, (it_n & 1) ^ 1, abort_flag, a.err);
           if (!ok) break;
@@ -268,8 +274,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t) {
           const int row0 = (int)(it.rb + (uint64_t)t * kUM);
           for (int kb = 0; kb < nkb; ++kb, ++g) {
-            const int s = (int)(g % kAStages);
-            ok = mbar_wait(empty_bar(s), ((g / kAStages) & 1) ^ 1, abort_flag, a.err);
+            const int s = (int)(g % nst);
+            ok = mbar_wait(empty_bar(s), ((g / nst) & 1) ^ 1, abort_flag, a.err);
             if (!ok) break;
             mbar_expect_tx(full_bar(s), resident ? kABytes : kABytes + kQBytes);
             tma_load_2d(base + kSmA + s * kABytes, &tmA, kb * kUK, row0, full_bar(s));
@@ -279,8 +285,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       if (!ok) {
         // drain the copies still in flight before the CTA leaves
-        const uint32_t first = g > (uint32_t)kAStages ? g - kAStages : 0;
-        for (uint32_t gg = first; gg < g; ++gg) drain_wait(full_bar((int)(gg % kAStages)), (gg / kAStages) & 1);
+        const uint32_t first = g > nst ? g - nst : 0;
+        for (uint32_t gg = first; gg < g; ++gg) drain_wait(full_bar((int)(gg % nst)), (gg / nst) & 1);
         if (resident && it_n > 0) drain_wait(qfull_bar, (it_n - 1) & 1);
       }
     }
@@ -290,7 +296,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t g = 0, tcount = 0, it_n = 0;
       bool ok = true;
       for (uint32_t w = blockIdx.x; ok && w < total; w += gridDim.x, ++it_n) {
-        const Item it = item_of(a, w, QT, ntiles);
+        const Item it = item_of(a, w, QT, ntiles, qtile);
         if (resident) {
           ok = mbar_wait(qfull_bar, it_n & 1, abort_flag, a.err);
           if (!ok) break;
@@ -302,16 +308,17 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (!ok) break;
           tc_fence_after();
           const uint32_t d = tmem + (uint32_t)b * kUN;
+          const uint32_t idesc = idesc_for(qtile);
           for (int kb = 0; kb < nkb; ++kb, ++g) {
-            const int s = (int)(g % kAStages);
-            ok = mbar_wait(full_bar(s), (g / kAStages) & 1, abort_flag, a.err);
+            const int s = (int)(g % nst);
+            ok = mbar_wait(full_bar(s), (g / nst) & 1, abort_flag, a.err);
             if (!ok) break;
             tc_fence_after();
             const uint32_t sa = base + kSmA + s * kABytes;
             const uint32_t sq = base + kSmQ + (resident ? kb : s) * kQBytes;
 #pragma unroll
             for (int k16 = 0; k16 < kUK / 16; ++k16)
-              tc_mma(d, sw128_desc(sa + k16 * 32), sw128_desc(sq + k16 * 32), kIdesc, (kb | k16) != 0);
+              tc_mma(d, sw128_desc(sa + k16 * 32), sw128_desc(sq + k16 * 32), idesc, (kb | k16) != 0);
             tc_commit(empty_bar(s));
           }
           if (ok) tc_commit(tfull_bar(b));
@@ -325,14 +332,22 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp >= 4) {
     // ---------------- epilogue
     const int etid = tid - 128;
+    const int ew = warp - 4;
     const int quarter = warp & 3;
-    const int half = (warp - 4) >> 2;
+    const int half = ew >> 2;
     const float inf = __int_as_float(0x7f800000);
     uint32_t tcount = 0;
     bool ok = true;
-    for (uint32_t w = blockIdx.x; ok && w < total; w += gridDim.x) {
-      const Item it = item_of(a, w, QT, ntiles);
+    for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
+      const Item it = item_of(a, w, QT, ntiles, qtile);
+      // item boundary: every epilogue warp is done with the previous item
+      // and all of them learn whether any gave up
+      if (lane == 0) s_okw[ew] = ok ? 1 : 0;
       named_sync(1, kEpiThreads);
+      bool all_ok = true;
+#pragma unroll
+      for (int i = 0; i < kEpiThreads / 32; ++i) all_ok = all_ok && s_okw[i] != 0;
+      if (!all_ok) break;
       // column etid of the query tile
       uint32_t q = 0xffffffffu;
       float4 qm = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -347,82 +362,152 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       s_qidx[etid] = q;
       s_qn2[etid] = qm.x;
+      if (a.mode == 1) {
+        // norm maxima over the item's rows (its 128-row tiles), then the
+        // column's threshold: keep (row, q) when acc - t_q >= |x|^2 / 2 with
+        // t_q = (|q|^2 - B - err) / 2
+        float4 tm = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (uint32_t t = it.t_lo + lane; t < it.t_hi; t += 32) {
+          const float4 v = a.tile_meta[(it.rb + (uint64_t)t * kUM) / kUM];
+          tm.x = fmaxf(tm.x, v.x);
+          tm.y = fmaxf(tm.y, v.y);
+          tm.z = fmaxf(tm.z, v.z);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          tm.x = fmaxf(tm.x, __shfl_xor_sync(HG_FULL, tm.x, o));
+          tm.y = fmaxf(tm.y, __shfl_xor_sync(HG_FULL, tm.y, o));
+          tm.z = fmaxf(tm.z, __shfl_xor_sync(HG_FULL, tm.z, o));
+        }
+        float tv = inf;  // no bound (or no query): acc - inf = -inf never survives
+        if (qb >= 0.0f) {
+          const float err = 2.000002f * (qm.y * tm.z + qm.z * tm.y + qm.z * tm.z + a.c_acc * qm.y * tm.y) +
+                            a.c_sq * (qm.x + tm.x + qb) + 1e-5f;
+          tv = 0.5f * (qm.x - qb - err);
+        }
+        s_thr[etid] = tv;
+      }
       named_sync(1, kEpiThreads);
-      const int c_lo = half * 128;
-      const int c_hi = min(c_lo + 128, (int)it.qcnt);
+      // the two warp groups split the tile's columns
+      const int c_lo = half * (qtile / 2);
+      const int c_hi = min(c_lo + qtile / 2, (int)it.qcnt);
+      // the row's |x|^2, loaded one tile ahead
+      float xn_next = 0.0f;
+      auto prefetch = [&](uint32_t t) {
+        if (t >= it.t_hi) return;
+        const uint64_t rw = it.rb + (uint64_t)t * kUM + quarter * 32 + lane;
+        xn_next = (rw < it.re && rw < a.nrows) ? a.xmeta[rw].x : 0.0f;
+      };
+      prefetch(it.t_lo);
       for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t, ++tcount) {
         const int b = (int)(tcount & 1);
-        const uint64_t row0 = it.rb + (uint64_t)t * kUM;
-        const uint64_t row = row0 + quarter * 32 + lane;
+        const uint64_t row = it.rb + (uint64_t)t * kUM + quarter * 32 + lane;
         const bool row_ok = row < it.re && row < a.nrows;
-        float* thr = s_thr + b * kUN;
-        float h_row = inf;
-        if (a.mode == 1) {
-          // per-tile threshold of column etid: keep (row, q) when
-          // acc >= |x|^2 / 2 + (|q|^2 - B - err) / 2
-          const float4 tm = a.tile_meta[row0 / kUM];
-          float tv = inf;
-          if (qb >= 0.0f) {
-            const float err = 2.000002f * (qm.y * tm.z + qm.z * tm.y + qm.z * tm.z + a.c_acc * qm.y * tm.y) +
-                              a.c_sq * (qm.x + tm.x + qb) + 1e-5f;
-            tv = 0.5f * (qm.x - qb - err);
-          }
-          thr[etid] = tv;
-          if (row_ok) h_row = 0.5f * a.xmeta[row].x;
+        const float xn2 = xn_next;
+        prefetch(t + 1);
+        const float h_row = row_ok ? 0.5f * xn2 : inf;
+        // each warp waits for the accumulator itself (lane 0, result shared)
+        int go = 0;
+        if (lane == 0) go = mbar_wait(tfull_bar(b), (tcount >> 1) & 1, abort_flag, a.err) ? 1 : 0;
+        go = __shfl_sync(HG_FULL, go, 0);
+        if (!go) {
+          ok = false;
+          break;
         }
-        // one thread waits for the accumulator; the group learns the outcome
-        // at the barrier, so every epilogue thread takes the same branch
-        if (etid == 0) s_go[b] = mbar_wait(tfull_bar(b), (tcount >> 1) & 1, abort_flag, a.err) ? 1 : 0;
-        named_sync(1, kEpiThreads);
-        ok = s_go[b] != 0;
-        if (!ok) break;
         tc_fence_after();
         const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)b * kUN;
-        for (int c0 = c_lo; c0 < c_hi; c0 += 32) {
-          uint32_t r[32];
-          tc_ld32(tbase + (uint32_t)c0, r);
-          tc_wait_ld();
-          if (a.mode == 1) {
-            uint32_t mask = 0;
+        if (a.mode == 1) {
+          for (int c0 = c_lo; c0 < c_hi; c0 += 64) {
+            uint32_t r[2][32];
+            tc_ld32(tbase + (uint32_t)c0, r[0]);
+            tc_ld32(tbase + (uint32_t)(c0 + 32), r[1]);
+            tc_wait_ld();
 #pragma unroll
-            for (int j = 0; j < 32; j += 4) {
-              const float4 t4 = *reinterpret_cast<const float4*>(thr + c0 + j);
-              mask |= (__uint_as_float(r[j]) >= h_row + t4.x) ? (1u << j) : 0u;
-              mask |= (__uint_as_float(r[j + 1]) >= h_row + t4.y) ? (2u << j) : 0u;
-              mask |= (__uint_as_float(r[j + 2]) >= h_row + t4.z) ? (4u << j) : 0u;
-              mask |= (__uint_as_float(r[j + 3]) >= h_row + t4.w) ? (8u << j) : 0u;
-            }
-            while (mask) {
-              const int j = __ffs(mask) - 1;
-              mask &= mask - 1;
-              const uint32_t qq = s_qidx[c0 + j];
-              const uint32_t pos = atomicAdd(&a.bucket_cnt[qq], 1u);
-              if (pos < a.bucket_cap) a.bucket[(uint64_t)qq * a.bucket_cap + pos] = (uint32_t)row;
-            }
-          } else if (a.mode == 0) {
-            const float xn2 = row_ok ? a.xmeta[row].x : 0.0f;
-            const int span = kUM / (int)it.sub;  // rows per slot: 8 .. 128
-            const int grp = span < 32 ? span : 32;
+            for (int hh = 0; hh < 2; ++hh) {
+              const int cb = c0 + 32 * hh;
+              if (cb >= c_hi) break;  // uniform over the warp
+              // v_j = acc_j - t_j in place (packed FP32 adds), screen by the max
+              float* v = reinterpret_cast<float*>(r[hh]);
+              float m = -inf;
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              if (c0 + j >= c_hi) break;  // uniform over the warp
-              unsigned long long key = ~0ull;
-              if (row_ok) {
-                const float dd = xn2 + s_qn2[c0 + j] - 2.0f * __uint_as_float(r[j]);
-                key = ((unsigned long long)ordered_key(dd) << 32) | (uint32_t)row;
+              for (int j = 0; j < 32; j += 4) {
+                const float4 t4 = *reinterpret_cast<const float4*>(s_thr + cb + j);
+                const float2 d0 = __fadd2_rn(make_float2(v[j], v[j + 1]), make_float2(-t4.x, -t4.y));
+                const float2 d1 = __fadd2_rn(make_float2(v[j + 2], v[j + 3]), make_float2(-t4.z, -t4.w));
+                v[j] = d0.x;
+                v[j + 1] = d0.y;
+                v[j + 2] = d1.x;
+                v[j + 3] = d1.y;
+                m = fmaxf(m, fmaxf(fmaxf(d0.x, d0.y), fmaxf(d1.x, d1.y)));
               }
-              for (int o = 1; o < grp; o <<= 1) {
-                const unsigned long long v = __shfl_xor_sync(HG_FULL, key, o);
-                key = v < key ? v : key;
-              }
-              const uint32_t slot = t * it.sub + (uint32_t)((quarter * 32 + lane) / span);
-              if ((lane & (grp - 1)) == 0 && key != ~0ull && slot < a.bm_cap)
-                atomicMin(&a.bm[(uint64_t)s_qidx[c0 + j] * a.bm_cap + slot], key);
-            }
-          } else if (row_ok) {
+              if (m >= h_row) {
+                uint32_t mask = 0;
 #pragma unroll
-            for (int j = 0; j < 32; ++j)
-              if (c0 + j < c_hi) a.dots[(uint64_t)(it.qoff + c0 + j) * a.dots_ld + row] = __uint_as_float(r[j]);
+                for (int j = 0; j < 32; ++j) mask |= (v[j] >= h_row) ? (1u << j) : 0u;
+                while (mask) {
+                  const int j = __ffs(mask) - 1;
+                  mask &= mask - 1;
+                  const uint32_t qq = s_qidx[cb + j];
+                  const uint32_t pos = atomicAdd(&a.bucket_cnt[qq], 1u);
+                  if (pos < a.bucket_cap) a.bucket[(uint64_t)qq * a.bucket_cap + pos] = (uint32_t)row;
+                }
+              }
+            }
+          }
+        } else {
+          for (int c0 = c_lo; c0 < c_hi; c0 += 32) {
+            uint32_t r[32];
+            tc_ld32(tbase + (uint32_t)c0, r);
+            tc_wait_ld();
+            if (a.mode == 0) {
+              const int span = kUM / (int)it.sub;  // rows per slot: 8 .. 128
+              if (span >= 32) {
+                // the warp's 32 rows lie in one slot: butterfly transpose-min,
+                // lane l ends with column c0 + l reduced over the 32 rows
+                unsigned long long v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                  const float dd = xn2 + s_qn2[c0 + j] - 2.0f * __uint_as_float(r[j]);
+                  v[j] = row_ok ? (((unsigned long long)ordered_key(dd) << 32) | (uint32_t)row) : ~0ull;
+                }
+#pragma unroll
+                for (int o = 16; o >= 1; o >>= 1) {
+                  const bool upper = (lane & o) != 0;
+#pragma unroll
+                  for (int i = 0; i < o; ++i) {
+                    const unsigned long long send = upper ? v[i] : v[i + o];
+                    const unsigned long long keep = upper ? v[i + o] : v[i];
+                    const unsigned long long recv = __shfl_xor_sync(HG_FULL, send, o);
+                    v[i] = recv < keep ? recv : keep;
+                  }
+                }
+                const uint32_t slot = t * it.sub + (uint32_t)(quarter * 32 / span);
+                if (c0 + lane < c_hi && v[0] != ~0ull && slot < a.bm_cap)
+                  atomicMin(&a.bm[(uint64_t)s_qidx[c0 + lane] * a.bm_cap + slot], v[0]);
+              } else {
+                const int grp = span;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                  if (c0 + j >= c_hi) break;  // uniform over the warp
+                  unsigned long long key = ~0ull;
+                  if (row_ok) {
+                    const float dd = xn2 + s_qn2[c0 + j] - 2.0f * __uint_as_float(r[j]);
+                    key = ((unsigned long long)ordered_key(dd) << 32) | (uint32_t)row;
+                  }
+                  for (int o = 1; o < grp; o <<= 1) {
+                    const unsigned long long w2 = __shfl_xor_sync(HG_FULL, key, o);
+                    key = w2 < key ? w2 : key;
+                  }
+                  const uint32_t slot = t * it.sub + (uint32_t)((quarter * 32 + lane) / span);
+                  if ((lane & (grp - 1)) == 0 && key != ~0ull && slot < a.bm_cap)
+                    atomicMin(&a.bm[(uint64_t)s_qidx[c0 + j] * a.bm_cap + slot], key);
+                }
+              }
+            } else if (row_ok) {
+#pragma unroll
+              for (int j = 0; j < 32; ++j)
+                if (c0 + j < c_hi) a.dots[(uint64_t)(it.qoff + c0 + j) * a.dots_ld + row] = __uint_as_float(r[j]);
+            }
           }
         }
         tc_fence_before();
@@ -451,7 +536,9 @@ cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q
     attr = true;
   }
   const uint64_t ntiles = (g.nrows + kUM - 1) / kUM;
-  const uint32_t QT = (uint32_t)((g.nq + kUN - 1) / kUN);
+  const int qtile = g.mode == 0 ? kBatchBoundQueries : g.qtile;
+  if (g.mode != 0 && qtile != 64 && qtile != 128 && qtile != 256) return cudaErrorInvalidValue;
+  const uint32_t QT = (uint32_t)((g.nq + qtile - 1) / qtile);
   const uint64_t total =
       g.mode == 0 ? g.nitems : ((ntiles + g.tiles_per_item - 1) / g.tiles_per_item) * (uint64_t)QT;
   if (total == 0) return cudaSuccess;

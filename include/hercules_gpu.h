@@ -196,7 +196,8 @@ HG_API hg_status hg_knn_batch(hg_index *ix, const float *queries, uint32_t nq, c
                               hg_query_stats *stats);
 
 /* Same with queries and outputs in device memory, ordered on `stream`
- * (NULL = the handle's stream); ks stays a host array. */
+ * (NULL = the handle's stream); ks stays a host array; d_queries must be
+ * 16-byte aligned. */
 HG_API hg_status hg_knn_batch_device(hg_index *ix, const float *d_queries, uint32_t nq, const uint32_t *ks,
                                      uint32_t kmax, const hg_knn_opts *opts, float *d_dist_out,
                                      int64_t *d_id_out, void *stream, hg_query_stats *stats);
