@@ -122,16 +122,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(args):
+def dist_setup(args, backend=None):
+    """One process per GPU (torchrun environment); replicas exchange only the
+    step times (max over ranks)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("gloo" if args.impl == "reference" else "nccl",
-                                timeout=datetime.timedelta(seconds=600))
+        if backend is None:
+            backend = "gloo" if args.impl == "reference" else "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world, local
+
+
+def rank_offset(rank):
+    """Query-seed offset of a replica: every rank answers its own queries."""
+    return rank * 7919
 
 
 def barrier(world):
@@ -258,7 +266,7 @@ def main():
     steps, warm, nb = args.steps, args.warmup, args.batch
     t_setup = time.perf_counter()
     X = build_collection(args, torch, H, device)
-    off = rank * 7919
+    off = rank_offset(rank)
     Qb, ks = make_batches(args, torch, H, X, steps + warm, device, offset=off)
     Qe, _ = make_batches(args, torch, H, X, steps + warm, device, offset=off + 5000)
     Qp = make_queries(args, torch, H, X, args.plain_queries, device, offset=off + 9000)
