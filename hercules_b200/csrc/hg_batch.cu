@@ -401,6 +401,39 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_merge(BatchRank a) {
   }
 }
 
+// Survivor pairs into their queries' buckets, 32 pairs per warp step: lanes
+// holding the same query share one atomic (pairs of a query cluster, since
+// the filter emits them tile by tile); empty slots (~0) are skipped.
+__global__ void k_scatter_pairs(const unsigned long long* __restrict__ pairs, const uint32_t* pairs_cnt,
+                                uint32_t pairs_cap, uint32_t* __restrict__ bucket, uint32_t* bucket_cnt,
+                                uint32_t bucket_cap) {
+  const uint32_t n = min(*pairs_cnt, pairs_cap);
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += warps * 32) {
+    const uint32_t i = base + lane;
+    const unsigned long long e = i < n ? pairs[i] : ~0ull;
+    const bool valid = e != ~0ull;
+    const uint32_t q = valid ? (uint32_t)(e >> 32) : 0xffffffffu;
+    const uint32_t same = __match_any_sync(HG_FULL, q);
+    const int leader = __ffs(same) - 1;
+    uint32_t pos = 0;
+    if (valid && lane == leader) pos = atomicAdd(&bucket_cnt[q], (uint32_t)__popc(same));
+    pos = __shfl_sync(HG_FULL, pos, leader) + (uint32_t)__popc(same & ((1u << lane) - 1));
+    if (valid && pos < bucket_cap) bucket[(uint64_t)q * bucket_cap + pos] = (uint32_t)e;
+  }
+}
+
+// The pair list overflowed: every query of the round counts as overflowed.
+__global__ void k_mark_overflow(const uint32_t* pairs_cnt, uint32_t pairs_cap, const uint32_t* qlist, int nlist,
+                                uint32_t* bucket_cnt, uint32_t bucket_cap) {
+  if (*pairs_cnt <= pairs_cap) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nlist; i += gridDim.x * blockDim.x) {
+    const uint32_t q = qlist ? qlist[i] : (uint32_t)i;
+    bucket_cnt[q] = max(bucket_cnt[q], bucket_cap + 1);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -418,6 +451,17 @@ cudaError_t launch_tile_norms(const float4* meta, uint64_t n, float4* tile_meta,
   const uint64_t nt = (n + kBM - 1) / kBM;
   if (!nt) return cudaSuccess;
   k_tile_norms<<<nblk(nt * 32, 256), 256, 0, s>>>(meta, n, tile_meta);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_pairs(const unsigned long long* pairs, const uint32_t* pairs_cnt, uint32_t pairs_cap,
+                                 const uint32_t* qlist, int nlist, uint32_t* bucket, uint32_t* bucket_cnt,
+                                 uint32_t bucket_cap, cudaStream_t s) {
+  // grid-stride, enough threads in flight to hide the bucket atomics' latency
+  k_scatter_pairs<<<2048, 256, 0, s>>>(pairs, pairs_cnt, pairs_cap, bucket, bucket_cnt, bucket_cap);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || nlist == 0) return e;
+  k_mark_overflow<<<nblk(nlist, 256), 256, 0, s>>>(pairs_cnt, pairs_cap, qlist, nlist, bucket_cnt, bucket_cap);
   return cudaGetLastError();
 }
 

@@ -48,9 +48,9 @@ struct BatchGemm {
   uint32_t tiles_per_item;
   float c_acc, c_sq;       // error-bound coefficients: L 2^-20 and (L/8 + 16) 2^-22
   const float* bound;      // B_q
-  uint32_t* bucket;        // [q][bucket_cap] surviving rows
-  uint32_t* bucket_cnt;    // 0 before the launch
-  uint32_t bucket_cap;
+  unsigned long long* pairs;  // survivors (query << 32 | row) in blocks reserved per warp; ~0 = empty slot
+  uint32_t* pairs_cnt;        // slots reserved; 0 before the launch, may end above pairs_cap
+  uint32_t pairs_cap;
   int* err;                // raised (1) when a bounded wait gave up
   // mode 2 (diagnostics): raw dot products q~.x~, [query position][dots_ld]
   float* dots;
@@ -97,5 +97,11 @@ size_t umma_filter_smem();
 cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q_map, const BatchGemm& g, int blocks,
                                cudaStream_t s);
 cudaError_t launch_rerank(const BatchRank& r, int part_blocks, cudaStream_t s);
+// Distributes the filter's survivor pairs into per-query buckets
+// (bucket_cnt[q] counts every pair of q, also beyond bucket_cap); when the
+// pair list overflowed, every query of the round is marked overflowed.
+cudaError_t launch_scatter_pairs(const unsigned long long* pairs, const uint32_t* pairs_cnt, uint32_t pairs_cap,
+                                 const uint32_t* qlist, int nlist, uint32_t* bucket, uint32_t* bucket_cnt,
+                                 uint32_t bucket_cap, cudaStream_t s);
 
 }  // namespace hg

@@ -323,6 +323,7 @@ static void free_device(hg_index* ix) {
   dfree(b.init_cnt);
   dfree(b.bucket);
   dfree(b.bucket_cnt);
+  dfree(b.pairs);
   dfree(b.ok);
   dfree(b.stats);
   dfree(b.heads);
@@ -1315,6 +1316,13 @@ static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket
     b.bm_cap = 0;
     b.parts_kmax = 0;
   }
+  // survivor pairs: room for 16,384 per query of the batch, at most 2^28
+  const uint32_t pairs_cap = (uint32_t)std::min<uint64_t>((uint64_t)b.nq_cap * 16384, 1ull << 28);
+  if (pairs_cap > b.pairs_cap || !b.pairs) {
+    dfree(b.pairs);
+    CK(dalloc(&b.pairs, pairs_cap));
+    b.pairs_cap = pairs_cap;
+  }
   if (kmax > b.parts_kmax || !b.parts) {
     dfree(b.parts);
     CK(dalloc(&b.parts, (size_t)b.nq_cap * hg::kBatchMaxSeg * kmax));
@@ -1471,9 +1479,9 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   g.tiles_per_item = kFilterTilesPerItem;
   filter_coefficients(L, &g.c_acc, &g.c_sq);
   g.bound = b.bound;
-  g.bucket = b.bucket;
-  g.bucket_cnt = b.bucket_cnt;
-  g.bucket_cap = bucket_cap;
+  g.pairs = b.pairs;
+  g.pairs_cnt = b.heads + 1;
+  g.pairs_cap = b.pairs_cap;
   g.err = reinterpret_cast<int*>(b.heads + 3);
   CK(cudaMemsetAsync(b.bm, 0xff, sizeof(unsigned long long) * nq * bm_cap, st));
   CK(cudaMemsetAsync(b.heads, 0, sizeof(uint32_t) * 4, st));
@@ -1522,7 +1530,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   uint64_t launches = 4 + (data_built ? 2 : 0);
   for (int round = 0; round < gemm_rounds_max; ++round) {
     const uint32_t cnt = round == 0 ? nq : (uint32_t)retry.size();
-    launches += round == 0 ? 4 : 5;  // (gather,) filter, re-rank plan / segments / merge
+    launches += round == 0 ? 6 : 7;  // (gather,) filter, scatter, overflow mark, re-rank plan / segments / merge
     if (round > 0) {
       CK(cudaMemcpyAsync(b.qlist, retry.data(), sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice, st));
       CK(hg::launch_rows_to_bf16(d_Q, b.qlist, cnt, (int)L, b.qbf, b.qmeta, st));
@@ -1537,16 +1545,20 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     // a narrow query tile when few queries take part (retry rounds)
     g.qtile = cnt <= 64 ? 64 : (cnt <= 128 ? 128 : hg::kBatchQueryTile);
     CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
+    CK(cudaMemsetAsync(b.heads + 1, 0, sizeof(uint32_t), st));
     HCK(record(ev[2], st));
     CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
     HCK(record(ev[3], st));
+    CK(hg::launch_scatter_pairs(b.pairs, b.heads + 1, b.pairs_cap, round == 0 ? nullptr : b.qlist, (int)cnt,
+                                b.bucket, b.bucket_cnt, bucket_cap, st));
+    HCK(record(ev[5], st));
     CK(hg::launch_rerank(r, sms * kRerankBlocksPerSm, st));
     HCK(record(ev[4], st));
     CK(cudaMemcpyAsync(ok.data(), b.ok, sizeof(int) * nq, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     float tg = 0, tr = 0;
     cudaEventElapsedTime(&tg, ev[2], ev[3]);
-    cudaEventElapsedTime(&tr, ev[3], ev[4]);
+    cudaEventElapsedTime(&tr, ev[3], ev[4]);  // scatter + re-rank
     gemm_ms += tg;
     rerank_ms += tr;
     pairs += (uint64_t)cnt * ix->n;

@@ -100,6 +100,8 @@ struct BatchScratch {
   int* init_cnt = nullptr;
   uint32_t* bucket = nullptr;
   uint32_t* bucket_cnt = nullptr;
+  unsigned long long* pairs = nullptr;  // filter survivors before they are bucketed
+  uint32_t pairs_cap = 0;
   int* ok = nullptr;
   unsigned long long* stats = nullptr;
   uint32_t* heads = nullptr;

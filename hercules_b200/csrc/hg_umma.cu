@@ -40,6 +40,7 @@ constexpr uint32_t kQBytes = kUN * kUK * 2;  // 32 KB per query K block
 constexpr int kResidentKB = 4;               // L <= 256: the query tile stays resident
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s per wait
 constexpr int kErrTimeout = 1;
+constexpr uint32_t kPairBlock = 1024;        // survivor pairs reserved per warp at a time
 
 // shared memory map (offsets from a 1024-byte aligned base)
 constexpr uint32_t kSmQ = 0;                                   // 4 x 32 KB
@@ -337,6 +338,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int half = ew >> 2;
     const float inf = __int_as_float(0x7f800000);
     uint32_t tcount = 0;
+    uint32_t pcur = 0, pend = 0;  // the warp's reserved block of the pair list
     bool ok = true;
     for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
       const Item it = item_of(a, w, QT, ntiles, qtile);
@@ -416,8 +418,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         tc_fence_after();
         const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)b * kUN;
+        // mode 1: survivor masks of the warp's (up to) four 32-column chunks;
+        // the buckets are written after the accumulator is handed back
+        uint32_t masks[4] = {0u, 0u, 0u, 0u};
         if (a.mode == 1) {
-          for (int c0 = c_lo; c0 < c_hi; c0 += 64) {
+#pragma unroll
+          for (int i2 = 0; i2 < 2; ++i2) {
+            const int c0 = c_lo + 64 * i2;
+            if (c0 >= c_hi) break;  // uniform over the warp
             uint32_t r[2][32];
             tc_ld32(tbase + (uint32_t)c0, r[0]);
             tc_ld32(tbase + (uint32_t)(c0 + 32), r[1]);
@@ -444,13 +452,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 uint32_t mask = 0;
 #pragma unroll
                 for (int j = 0; j < 32; ++j) mask |= (v[j] >= h_row) ? (1u << j) : 0u;
-                while (mask) {
-                  const int j = __ffs(mask) - 1;
-                  mask &= mask - 1;
-                  const uint32_t qq = s_qidx[cb + j];
-                  const uint32_t pos = atomicAdd(&a.bucket_cnt[qq], 1u);
-                  if (pos < a.bucket_cap) a.bucket[(uint64_t)qq * a.bucket_cap + pos] = (uint32_t)row;
-                }
+                masks[2 * i2 + hh] = mask;
               }
             }
           }
@@ -513,8 +515,38 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(tempty_bar(b));
+        // survivor pairs into the warp's reserved block of the pair list:
+        // plain stores, one atomic per kPairBlock pairs
+#pragma unroll
+        for (int ci = 0; ci < 4; ++ci) {
+          uint32_t mask = masks[ci];
+          while (__any_sync(HG_FULL, mask != 0)) {
+            const bool has = mask != 0;
+            unsigned long long e = 0;
+            if (has) {
+              const int j = __ffs(mask) - 1;
+              mask &= mask - 1;
+              e = ((unsigned long long)s_qidx[c_lo + 32 * ci + j] << 32) | (uint32_t)row;
+            }
+            const uint32_t bal = __ballot_sync(HG_FULL, has);
+            const uint32_t n = (uint32_t)__popc(bal);
+            if (pcur + n > pend) {
+              // close the block (sentinels in its tail) and reserve the next
+              for (uint32_t i = pcur + lane; i < pend; i += 32) a.pairs[i] = ~0ull;
+              uint32_t nb = 0;
+              if (lane == 0) nb = atomicAdd(a.pairs_cnt, (uint32_t)kPairBlock);
+              nb = __shfl_sync(HG_FULL, nb, 0);
+              pcur = nb;
+              pend = nb + kPairBlock < a.pairs_cap ? nb + kPairBlock : (nb < a.pairs_cap ? a.pairs_cap : nb);
+            }
+            const uint32_t slot = pcur + (uint32_t)__popc(bal & ((1u << lane) - 1));
+            if (has && slot < pend) a.pairs[slot] = e;
+            pcur += n;
+          }
+        }
       }
     }
+    for (uint32_t i = pcur + lane; i < pend; i += 32) a.pairs[i] = ~0ull;  // close the last block
   }
   tc_fence_before();
   __syncthreads();
