@@ -25,7 +25,6 @@
 using hg::Node;
 
 // Launch geometry of the leaf scan.
-constexpr int kEdBlocksPerSm = 4;      // k_ed_stream: 4 x 256 threads per SM
 constexpr int kFilterBlocksPerSm = 8;  // k_lbsax_filter
 
 // ---------------------------------------------------------------------------
@@ -1013,7 +1012,7 @@ static hg_status ensure_scratch(hg_index* ix, int k) {
   dfree(s.err);
   dfree(s.list);
   dfree(s.counters);
-  s.nparts = hg::sm_count(ix->device) * kEdBlocksPerSm * hg::kEdWarps;
+  s.nparts = hg::sm_count(ix->device) * hg::kEdBlocksPerSm * hg::kEdWarps;
   CK(dalloc(&s.lb, nl));
   CK(dalloc(&s.list, ix->n));
   CK(dalloc(&s.counters, 8));
@@ -1087,7 +1086,7 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
   hg::DeviceIndex& d = ix->d;
   const int nl = (int)ix->leaves.size();
   const int sms = hg::sm_count(ix->device);
-  const int ed_blocks = sms * kEdBlocksPerSm;
+  const int ed_blocks = sms * hg::kEdBlocksPerSm;
   hg::EdArgs e{};
   e.rows = d.rows;
   e.ids = d.ids;
@@ -1117,7 +1116,9 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
                              s.cand_lb, s.cand_count, s.unit_prefix, s.bound, s.topk_count, s.counters, st));
     CK(hg::launch_leaf_lb(d_q, e.L, nl, d.leaf_seg_off, d.leaf_points, d.leaf_sk, s.lb, st));
     // the approximate leaf, with an unbounded k-th distance at the start
-    const int a_blocks = std::max(1, std::min(ed_blocks, o.approx_blocks > 0 ? o.approx_blocks : sms));
+        // two blocks per SM: the bound starts at +inf, so more warps would finish
+    // more rows of this leaf before it tightens; fewer leave HBM idle
+    const int a_blocks = std::max(1, std::min(ed_blocks, o.approx_blocks > 0 ? o.approx_blocks : 2 * sms));
     e.list = nullptr;
     e.ident_leaf = s.approx_leaf;
     e.head = s.counters + 0;

@@ -565,8 +565,9 @@ __device__ __forceinline__ int q4_index(int chunk, int half) {
 // bytes of that layout for a series of L floats
 __host__ __device__ inline size_t q4_bytes(int L) { return (size_t)((L / 8 + 31) / 32) * 40 * 2 * 16; }
 // kRowIds: the id of a row is its row index (a matrix without an id map).
-template <bool kRowIds>
-__global__ void __launch_bounds__(kEdThreads, 4) k_ed_stream(EdArgs a) {
+// kLines: 128-byte lines of a row in flight per slot and step
+template <bool kRowIds, int kLines>
+__global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 1 : 4) k_ed_stream(EdArgs a) {
   constexpr int W = kEdThreads / 32;
   __shared__ unsigned long long lists[W][kWarpListCap];
   extern __shared__ float4 qs4[];  // the query, q4_bytes(L) bytes
@@ -648,21 +649,37 @@ __global__ void __launch_bounds__(kEdThreads, 4) k_ed_stream(EdArgs a) {
     }
     if (!__any_sync(HG_FULL, valid)) break;
     const uint32_t bnext = ((iter & 7) == 0) ? ld_volatile(a.bound) : 0x7f800000u;
-    // one line of every owned row: lane j computes chunk ch + j
-    const int c = ch + j;
-    float d = 0.0f;
-    if (valid && c < nch) {
-      const float4* x = reinterpret_cast<const float4*>(a.rows + (uint64_t)row * a.L) + (c << 1);
-      const float4 x0 = __ldcs(x), x1 = __ldcs(x + 1);
-      const float4 q0 = qs4[q4_index(c, 0)], q1 = qs4[q4_index(c, 1)];
-      const float qa[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-      const float xa[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-      d = hg_chunk_d2(qa, xa);
+    // kLines lines of every owned row in flight: lane j computes chunks
+    // ch + 4 l + j (l < kLines); the slot adds them in order
+    const float4* x = reinterpret_cast<const float4*>(a.rows + (uint64_t)row * a.L);
+    float4 xv[kLines][2];
+#pragma unroll
+    for (int l = 0; l < kLines; ++l) {
+      const int c = ch + 4 * l + j;
+      if (valid && c < nch) {
+        xv[l][0] = __ldcs(x + 2 * c);
+        xv[l][1] = __ldcs(x + 2 * c + 1);
+      } else {
+        xv[l][0] = xv[l][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+    float dl[kLines];
+#pragma unroll
+    for (int l = 0; l < kLines; ++l) {
+      const int c = ch + 4 * l + j;
+      dl[l] = 0.0f;
+      if (valid && c < nch) {
+        const float4 q0 = qs4[q4_index(c, 0)], q1 = qs4[q4_index(c, 1)];
+        const float qa[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+        const float xa[8] = {xv[l][0].x, xv[l][0].y, xv[l][0].z, xv[l][0].w,
+                             xv[l][1].x, xv[l][1].y, xv[l][1].z, xv[l][1].w};
+        dl[l] = hg_chunk_d2(qa, xa);
+      }
     }
     bool finished = false;
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const float dt = __shfl_sync(HG_FULL, d, slot_lead + t);
+    for (int t = 0; t < 4 * kLines; ++t) {
+      const float dt = __shfl_sync(HG_FULL, dl[t >> 2], slot_lead + (t & 3));
       if (valid && ch + t < nch) {
         dist = __fadd_rn(dist, dt);
         if (j == 0) ++n_chunks;
@@ -670,7 +687,7 @@ __global__ void __launch_bounds__(kEdThreads, 4) k_ed_stream(EdArgs a) {
       }
     }
     if (valid) {
-      ch += 4;
+      ch += 4 * kLines;
       if (ch >= nch) {
         finished = true;
         valid = false;
@@ -940,24 +957,21 @@ cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s)
   return cudaGetLastError();
 }
 
-cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s) {
+template <bool kRowIds, int kLines>
+static cudaError_t launch_ed(const EdArgs& a, int blocks, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_ed_stream<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q4_bytes(16384));
+    const cudaError_t e = cudaFuncSetAttribute(k_ed_stream<kRowIds, kLines>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q4_bytes(16384));
+    if (e != cudaSuccess) return e;
     attr = true;
   }
-  k_ed_stream<false><<<blocks, kEdThreads, q4_bytes(a.L), s>>>(a);
+  k_ed_stream<kRowIds, kLines><<<blocks, kEdThreads, q4_bytes(a.L), s>>>(a);
   return cudaGetLastError();
 }
-
+cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s) { return launch_ed<false, 2>(a, blocks, s); }
 cudaError_t launch_ed_stream_row_ids(const EdArgs& a, int blocks, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_ed_stream<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q4_bytes(16384));
-    attr = true;
-  }
-  k_ed_stream<true><<<blocks, kEdThreads, q4_bytes(a.L), s>>>(a);
-  return cudaGetLastError();
+  return launch_ed<true, 2>(a, blocks, s);
 }
 
 cudaError_t launch_merge(const unsigned long long* parts, const int* part_count, int nparts, int k,

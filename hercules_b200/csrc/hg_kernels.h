@@ -7,6 +7,7 @@
 namespace hg {
 
 constexpr int kEdWarps = 8;  // warps per block of the distance stream
+constexpr int kEdBlocksPerSm = 4;  // resident blocks per SM of the distance stream
 constexpr int kWarpListCap = 256;  // per-warp candidate buffer (k <= kWarpListCap - 32)
 constexpr int kMaxK = kWarpListCap - 32;
 constexpr int kMaxLeavesSort = 8192;  // single-CTA radix sort capacity

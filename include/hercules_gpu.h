@@ -96,7 +96,7 @@ typedef struct {
   int mode;           /* HG_MODE_* */
   int use_lb_sax;     /* 1: per-row LB_SAX filter before the distance */
   int profile;        /* 1: time every leaf-scan launch with CUDA events */
-  int approx_blocks;  /* blocks of the approximate-leaf scan (0 = one per SM) */
+  int approx_blocks;  /* blocks of the approximate-leaf scan (0 = two per SM) */
   int bucket_cap;     /* HG_MODE_BATCH: filter survivors kept per query before the
                          query falls back to the plain path (0 = 65536) */
   int reserved[3];
