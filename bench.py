@@ -65,6 +65,7 @@ def parse():
     p.add_argument("--cpu-sample-queries", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--ref-queries-per-step", type=int, default=2)
+    p.add_argument("--no-autotune", action="store_true", help="keep the default launch parameters")
     return p.parse_args()
 
 
@@ -288,6 +289,8 @@ def main():
     batch_step(0)  # the first call also builds the BF16 copy of the collection
     torch.cuda.synchronize()
     prep_s = time.perf_counter() - t1
+    # launch parameters tuned on a warm-up batch, before the timed region
+    tuning = ix.tuning() if args.no_autotune else ix.autotune_device(Qb[0].data_ptr(), nb, ks, kmax, stream=stream)
     for i in range(1, warm):
         batch_step(i)
     torch.cuda.synchronize()
@@ -388,7 +391,10 @@ def main():
                                % (args.n, args.L, args.leaf, nb, int(round(100 * args.fresh_frac))),
                    "n": args.n, "L": args.L, "leaf_size": args.leaf, "queries_per_step": nb, "k": list(K_CYCLE),
                    "l2": "inputs (25.6 GB f32 + 12.8 GB bf16) larger than L2; no flush needed",
-                   "parallelism": "replica per GPU" if world > 1 else "single GPU"},
+                   "parallelism": "replica per GPU" if world > 1 else "single GPU",
+                   "tuning": {k: tuning[k] for k in ("filter_tiles_per_item", "bound_tiles_per_item",
+                                                     "rerank_blocks_per_sm", "approx_blocks_per_sm")},
+                   "tuned": not args.no_autotune},
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": nb * args.L * 4,
                 "d2h_bytes_per_step": nb * kmax * (4 + 8)},
         "gpu_launches": int(agg["kernel_launches"]),

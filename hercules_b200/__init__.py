@@ -63,6 +63,15 @@ class KnnOpts(ctypes.Structure):
                 ("approx_blocks", ctypes.c_int), ("bucket_cap", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("filter_tiles_per_item", ctypes.c_uint32), ("bound_tiles_per_item", ctypes.c_uint32),
+                ("rerank_blocks_per_sm", ctypes.c_uint32), ("approx_blocks_per_sm", ctypes.c_uint32),
+                ("batch_ms", ctypes.c_double), ("plain_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _lib = None
 
 # (name, restype, argtypes) for every entry point of include/hercules_gpu.h
@@ -92,6 +101,9 @@ _SIGS = [
     ("hg_knn_batch_device", ctypes.c_int, [_P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, ctypes.POINTER(KnnOpts),
                                            _P, _P, _P, ctypes.POINTER(QueryStats)]),
     ("hg_bf16_dots", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint32, _P, ctypes.c_uint32, _P, _P]),
+    ("hg_tuning_get", ctypes.c_int, [_P, ctypes.POINTER(Tuning)]),
+    ("hg_tuning_set", ctypes.c_int, [_P, ctypes.POINTER(Tuning)]),
+    ("hg_autotune", ctypes.c_int, [_P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, _P, ctypes.POINTER(Tuning)]),
     ("hg_route", ctypes.c_int, [_P, _P, ctypes.c_uint32, _P]),
     ("hg_leaf_lower_bounds", ctypes.c_int, [_P, _P, _P]),
     ("hg_generate_walks", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, _P,
@@ -295,6 +307,26 @@ class HerculesIndex:
                                          ctypes.c_void_p(dist_ptr), ctypes.c_void_p(id_ptr),
                                          ctypes.c_void_p(stream), ctypes.byref(st)))
         return st.as_dict()
+
+    def tuning(self):
+        t = Tuning()
+        _check(lib().hg_tuning_get(self._h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        t = Tuning(**kw)
+        _check(lib().hg_tuning_set(self._h, ctypes.byref(t)))
+
+    def autotune_device(self, q_ptr, nq, ks, kmax, stream=0):
+        """Times candidate launch parameters on device queries and keeps the fastest."""
+        t = Tuning()
+        kp = None
+        if ks is not None:
+            ks = np.ascontiguousarray(ks, dtype=np.uint32)
+            kp = _ptr(ks)
+        _check(lib().hg_autotune(self._h, ctypes.c_void_p(q_ptr), nq, kp, kmax, ctypes.c_void_p(stream),
+                                 ctypes.byref(t)))
+        return t.as_dict()
 
     def route(self, queries):
         q = _f32(queries, self.L)

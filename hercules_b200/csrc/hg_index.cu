@@ -1118,7 +1118,8 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
     // the approximate leaf, with an unbounded k-th distance at the start
         // two blocks per SM: the bound starts at +inf, so more warps would finish
     // more rows of this leaf before it tightens; fewer leave HBM idle
-    const int a_blocks = std::max(1, std::min(ed_blocks, o.approx_blocks > 0 ? o.approx_blocks : 2 * sms));
+    const int a_blocks =
+        std::max(1, std::min(ed_blocks, o.approx_blocks > 0 ? o.approx_blocks : (int)ix->tune.approx_blocks_per_sm * sms));
     e.list = nullptr;
     e.ident_leaf = s.approx_leaf;
     e.head = s.counters + 0;
@@ -1227,11 +1228,8 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
 // batched queries: BF16 tensor-core filter + exact re-rank (hg_batch.cu)
 // ---------------------------------------------------------------------------
 
-constexpr uint32_t kBoundTilesPerItem = 8;
-constexpr uint32_t kFilterTilesPerItem = 32;  // 4096 rows per item: a row chunk stays in L2
 constexpr uint32_t kDefaultBucket = 65536;
 constexpr int kBatchRetries = 3;  // filter rounds after the first for overflowed buckets
-constexpr int kRerankBlocksPerSm = 8;      // k_rerank_part: 8 x 8 warps per SM
 
 // TMA descriptor of a row-major n x L BF16 matrix, boxes of 64 columns
 // (128 bytes, the swizzle span) x box_rows rows, 128-byte swizzle, zero fill
@@ -1445,9 +1443,10 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     const uint32_t tiles = (uint32_t)((sz + T - 1) / T);
     const uint32_t sub = sub_of(tiles);
     const uint32_t use_tiles = std::min<uint32_t>(tiles, bm_cap / sub);
-    for (uint32_t t = 0; t < use_tiles; t += kBoundTilesPerItem)
+    const uint32_t btpi = ix->tune.bound_tiles_per_item;
+    for (uint32_t t = 0; t < use_tiles; t += btpi)
       items.push_back(
-          hg::BatchItem{st0, st0 + sz, i, j - i, t, std::min(use_tiles, t + kBoundTilesPerItem), sub, 0});
+          hg::BatchItem{st0, st0 + sz, i, j - i, t, std::min(use_tiles, t + btpi), sub, 0});
     for (uint32_t x = i; x < j; ++x) slots[perm[x]] = use_tiles * sub;
     i = j;
   }
@@ -1477,7 +1476,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   g.nitems = (uint32_t)items.size();
   g.bm = b.bm;
   g.bm_cap = bm_cap;
-  g.tiles_per_item = kFilterTilesPerItem;
+  g.tiles_per_item = ix->tune.filter_tiles_per_item;
   filter_coefficients(L, &g.c_acc, &g.c_sq);
   g.bound = b.bound;
   g.pairs = b.pairs;
@@ -1553,7 +1552,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     CK(hg::launch_scatter_pairs(b.pairs, b.heads + 1, b.pairs_cap, round == 0 ? nullptr : b.qlist, (int)cnt,
                                 b.bucket, b.bucket_cnt, bucket_cap, st));
     HCK(record(ev[5], st));
-    CK(hg::launch_rerank(r, sms * kRerankBlocksPerSm, st));
+    CK(hg::launch_rerank(r, sms * (int)ix->tune.rerank_blocks_per_sm, st));
     HCK(record(ev[4], st));
     CK(cudaMemcpyAsync(ok.data(), b.ok, sizeof(int) * nq, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -1911,6 +1910,98 @@ hg_status hg_bf16_dots(const float* d_rows, uint64_t n, uint32_t L, const float*
   release();
   if (e != cudaSuccess) return cuda_fail(e, "hg_bf16_dots");
   if (herr) return set_error(HG_ERR_TIMEOUT, "hg_bf16_dots: a tensor-core wait timed out");
+  return HG_OK;
+}
+
+hg_status hg_tuning_get(const hg_index* ix, hg_tuning* out) {
+  if (!ix || !out) return set_error(HG_ERR_ARG, "hg_tuning_get: null argument");
+  *out = ix->tune;
+  return HG_OK;
+}
+
+hg_status hg_tuning_set(hg_index* ix, const hg_tuning* t) {
+  if (!ix || !t) return set_error(HG_ERR_ARG, "hg_tuning_set: null argument");
+  auto bad = [](uint32_t v, uint32_t lo, uint32_t hi) { return v != 0 && (v < lo || v > hi); };
+  if (bad(t->filter_tiles_per_item, 8, 128) || bad(t->bound_tiles_per_item, 2, 64) ||
+      bad(t->rerank_blocks_per_sm, 1, 16) || bad(t->approx_blocks_per_sm, 1, 4))
+    return set_error(HG_ERR_ARG, "hg_tuning_set: a parameter outside its range");
+  if (t->filter_tiles_per_item) ix->tune.filter_tiles_per_item = t->filter_tiles_per_item;
+  if (t->bound_tiles_per_item) ix->tune.bound_tiles_per_item = t->bound_tiles_per_item;
+  if (t->rerank_blocks_per_sm) ix->tune.rerank_blocks_per_sm = t->rerank_blocks_per_sm;
+  if (t->approx_blocks_per_sm) ix->tune.approx_blocks_per_sm = t->approx_blocks_per_sm;
+  return HG_OK;
+}
+
+// Coordinate descent over the launch parameters: each parameter in turn takes
+// every candidate value with the others fixed, timed on the caller's queries
+// (the batched path's phases by their own CUDA events; the plain path on up to
+// 64 of the queries); the fastest value stays.
+hg_status hg_autotune(hg_index* ix, const float* d_queries, uint32_t nq, const uint32_t* ks, uint32_t kmax,
+                      void* stream, hg_tuning* out) {
+  if (!ix || !d_queries || nq == 0 || kmax == 0) return set_error(HG_ERR_ARG, "hg_autotune: bad argument");
+  CK(cudaSetDevice(ix->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : ix->stream;
+  float* d_dist = nullptr;
+  int64_t* d_id = nullptr;
+  CK(dalloc(&d_dist, (size_t)nq * kmax));
+  cudaError_t e = dalloc(&d_id, (size_t)nq * kmax);
+  if (e != cudaSuccess) {
+    dfree(d_dist);
+    return cuda_fail(e, "hg_autotune");
+  }
+  hg_knn_opts o{};
+  hg_status status = HG_OK;
+  auto batch_ms = [&](double* ms) -> hg_status {
+    hg_query_stats sq;
+    hg_status r = knn_batch_impl(ix, d_queries, nq, ks, kmax, o, d_dist, d_id, st, &sq);
+    *ms = sq.device_ms;
+    return r;
+  };
+  const uint32_t np = std::min<uint32_t>(nq, 64), kp = std::min<uint32_t>(kmax, 10);
+  auto plain_ms = [&](double* ms) -> hg_status {
+    hg_query_stats sq;
+    hg_knn_opts po{};
+    po.use_lb_sax = 1;
+    hg_status r = knn_device_impl(ix, d_queries, np, kp, &po, d_dist, d_id, st, &sq);
+    *ms = sq.device_ms;
+    return r;
+  };
+  struct Param {
+    uint32_t* field;
+    std::vector<uint32_t> cand;
+    bool plain;
+  };
+  hg_tuning& t = ix->tune;
+  std::vector<Param> params = {{&t.filter_tiles_per_item, {16, 32, 64}, false},
+                               {&t.bound_tiles_per_item, {4, 8, 16}, false},
+                               {&t.rerank_blocks_per_sm, {4, 8, 16}, false},
+                               {&t.approx_blocks_per_sm, {1, 2, 4}, true}};
+  double warm = 0;
+  status = batch_ms(&warm);  // also builds the BF16 copy on a first call
+  for (auto& p : params) {
+    if (status != HG_OK) break;
+    uint32_t best = *p.field;
+    double best_ms = 1e30;
+    for (uint32_t v : p.cand) {
+      *p.field = v;
+      double ms = 0, ms2 = 0;
+      status = p.plain ? plain_ms(&ms) : batch_ms(&ms);
+      if (status == HG_OK) status = p.plain ? plain_ms(&ms2) : batch_ms(&ms2);
+      if (status != HG_OK) break;
+      ms = std::min(ms, ms2);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = v;
+      }
+    }
+    *p.field = best;
+    if (p.plain) t.plain_ms = best_ms;
+    else t.batch_ms = best_ms;
+  }
+  dfree(d_dist);
+  dfree(d_id);
+  if (status != HG_OK) return status;
+  if (out) *out = t;
   return HG_OK;
 }
 

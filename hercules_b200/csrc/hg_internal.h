@@ -132,4 +132,5 @@ struct hg_index {
   hg::BatchScratch bs;
   cudaStream_t stream = nullptr;
   int max_seg = 0;
+  hg_tuning tune = {32, 8, 8, 2, 0.0, 0.0};  // launch parameters (hg_autotune)
 };

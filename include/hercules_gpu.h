@@ -211,6 +211,33 @@ HG_API hg_status hg_knn_batch_device(hg_index *ix, const float *d_queries, uint3
 HG_API hg_status hg_bf16_dots(const float *d_rows, uint64_t n, uint32_t L, const float *d_queries, uint32_t nq,
                               float *d_dots, void *stream);
 
+/* Launch parameters of the query kernels that depend on the data and the
+ * GPU (no counterpart in the reference: its parallel search takes thread
+ * counts and thresholds on the command line instead).  0 in a field means
+ * "keep the current value". */
+typedef struct {
+  uint32_t filter_tiles_per_item;  /* batched filter: 128-row tiles per work item (8..128) */
+  uint32_t bound_tiles_per_item;   /* batched bound pass: tiles per work item (2..64) */
+  uint32_t rerank_blocks_per_sm;   /* batched re-rank: blocks of 8 warps per SM (1..16) */
+  uint32_t approx_blocks_per_sm;   /* plain path: blocks per SM of the approximate-leaf scan (1..4) */
+  double batch_ms;                 /* hg_autotune: device time of one batch with the chosen values */
+  double plain_ms;                 /* hg_autotune: device time of the plain-path sample */
+} hg_tuning;
+
+/* Current launch parameters of a handle (defaults until tuned or set). */
+HG_API hg_status hg_tuning_get(const hg_index *ix, hg_tuning *out);
+
+/* Sets launch parameters (fields left 0 keep their value). */
+HG_API hg_status hg_tuning_set(hg_index *ix, const hg_tuning *t);
+
+/* Autotuner: times candidate launch parameters on a sample of the caller's
+ * own queries (device memory, 16-byte aligned; nq of them with per-query k
+ * from the host array ks, NULL = kmax), one parameter at a time, keeps the
+ * fastest with the handle and returns them.  Answers do not depend on these
+ * parameters; only the time does.  Allocates its own output buffers. */
+HG_API hg_status hg_autotune(hg_index *ix, const float *d_queries, uint32_t nq, const uint32_t *ks, uint32_t kmax,
+                             void *stream, hg_tuning *out);
+
 /* The approximate leaf of each query: the leaf the query routes to
  * (approximate_knn_search's traversal, hercules_query_engine.c:176-222). */
 HG_API hg_status hg_route(hg_index *ix, const float *queries, uint32_t nq, int32_t *leaf_out);

@@ -135,3 +135,23 @@ def test_batch_edge_cases(hg, gpu_available):
     # empty batch
     d, ids = ix.knn_batch(np.zeros((0, 32), np.float32), 5)
     assert d.shape == (0, 5)
+
+
+def test_autotune_keeps_answers(mid):
+    """The autotuner picks launch parameters from its candidates; answers of
+    both paths are unchanged afterwards."""
+    import torch
+    X, Q, ix = mid
+    before = ix.knn_batch(Q[:64], 10)
+    q = torch.from_numpy(Q[:64]).cuda()
+    t = ix.autotune_device(q.data_ptr(), 64, None, 10)
+    assert t["filter_tiles_per_item"] in (16, 32, 64) and t["bound_tiles_per_item"] in (4, 8, 16)
+    assert t["rerank_blocks_per_sm"] in (4, 8, 16) and t["approx_blocks_per_sm"] in (1, 2, 4)
+    assert t["batch_ms"] > 0 and t["plain_ms"] > 0 and ix.tuning() == t
+    after = ix.knn_batch(Q[:64], 10)
+    assert np.array_equal(bits(before[0]), bits(after[0])) and np.array_equal(before[1], after[1])
+    pd, pi = ix.knn(Q[:16], 10)
+    same_as_plain(ix, Q[:16], np.full(16, 10), after[0][:16], after[1][:16])
+    with pytest.raises(Exception):
+        ix.set_tuning(filter_tiles_per_item=3)
+    ix.set_tuning(filter_tiles_per_item=32, bound_tiles_per_item=8, rerank_blocks_per_sm=8, approx_blocks_per_sm=2)
