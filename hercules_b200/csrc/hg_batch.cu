@@ -46,10 +46,12 @@ constexpr int kBM = kBatchTileRows;
 // One warp per output row w: the BF16 copy of source row src = idx ? idx[w] : w
 // (round to nearest) and, in FP64 rounded up, meta[src] = {|x|^2, |x~|,
 // |x - x~|, 0} (x~ the BF16 row).
-__global__ void k_rows_to_bf16(const float* __restrict__ rows, const uint32_t* __restrict__ idx, uint64_t n, int L,
-                               __nv_bfloat16* __restrict__ out, float4* __restrict__ meta) {
+__global__ void k_rows_to_bf16(const float* __restrict__ rows, const uint32_t* __restrict__ idx, uint64_t n,
+                               const uint32_t* n_dev, int L, __nv_bfloat16* __restrict__ out,
+                               float4* __restrict__ meta) {
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
+  if (n_dev) n = *n_dev;  // at most the n the grid was sized for
   if (w >= n) return;
   const uint64_t src = idx ? idx[w] : w;
   const float4* x = reinterpret_cast<const float4*>(rows + src * L);
@@ -181,10 +183,11 @@ __global__ void __launch_bounds__(1024) k_rerank_plan(BatchRank a) {
   if (tid == 0) carry = 0;
   __syncthreads();
   const float inf = __int_as_float(0x7f800000);
-  for (int base = 0; base < a.nlist; base += 1024) {
+  const int nlist = a.nlist_dev ? (int)*a.nlist_dev : a.nlist;
+  for (int base = 0; base < nlist; base += 1024) {
     const int i = base + tid;
     uint32_t nseg = 0, seg = 0;
-    if (i < a.nlist) {
+    if (i < nlist) {
       const int q = a.qlist ? (int)a.qlist[i] : i;
       const uint32_t n = a.bound[q] < inf ? min(a.bucket_cnt[q], a.bucket_cap) : 0u;
       seg = max((uint32_t)kBatchSegMin, (n + kBatchMaxSeg - 1) / kBatchMaxSeg);
@@ -212,13 +215,13 @@ __global__ void __launch_bounds__(1024) k_rerank_plan(BatchRank a) {
     }
     __syncthreads();
     const uint32_t excl = carry + (wid ? warp_sums[wid - 1] : 0u) + v - nseg;
-    if (i < a.nlist) a.seg_prefix[i] = excl;
+    if (i < nlist) a.seg_prefix[i] = excl;
     __syncthreads();
     if (tid == 1023) carry = excl + nseg;
     __syncthreads();
   }
   if (tid == 0) {
-    a.seg_prefix[a.nlist] = carry;
+    a.seg_prefix[nlist] = carry;
     a.heads[0] = 0;  // work counter of k_rerank_part
   }
 }
@@ -246,7 +249,8 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_part(BatchRank a) {
   const int slot_lead = lane & ~1, j = lane & 1;
   unsigned long long* list = lists[wib];
   const float inf = __int_as_float(0x7f800000);
-  const uint32_t total_items = a.seg_prefix[a.nlist];
+  const int nlist = a.nlist_dev ? (int)*a.nlist_dev : a.nlist;
+  const uint32_t total_items = a.seg_prefix[nlist];
   const int nch = a.L >> 3;
   const uint32_t leaders = 0x55555555u;
   unsigned long long n_rows = 0, n_chunks = 0;
@@ -256,7 +260,7 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_part(BatchRank a) {
     item = __shfl_sync(HG_FULL, item, 0);
     if (item >= total_items) break;
     // list position of the item: the last i with seg_prefix[i] <= item
-    int lo = 0, hi = a.nlist - 1;
+    int lo = 0, hi = nlist - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (a.seg_prefix[mid] <= item) lo = mid;
@@ -353,7 +357,7 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_merge(BatchRank a) {
   __shared__ unsigned long long lists[kRankWarps][kWarpListCap];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int pos = blockIdx.x * kRankWarps + wib;
-  if (pos >= a.nlist) return;
+  if (pos >= (a.nlist_dev ? (int)*a.nlist_dev : a.nlist)) return;
   const int q = a.qlist ? (int)a.qlist[pos] : pos;
   unsigned long long* list = lists[wib];
   const int k = (int)a.kq[q];
@@ -426,12 +430,148 @@ __global__ void k_scatter_pairs(const unsigned long long* __restrict__ pairs, co
 
 // The pair list overflowed: every query of the round counts as overflowed.
 __global__ void k_mark_overflow(const uint32_t* pairs_cnt, uint32_t pairs_cap, const uint32_t* qlist, int nlist,
-                                uint32_t* bucket_cnt, uint32_t bucket_cap) {
+                                const uint32_t* nlist_dev, uint32_t* bucket_cnt, uint32_t bucket_cap) {
   if (*pairs_cnt <= pairs_cap) return;
+  if (nlist_dev) nlist = (int)*nlist_dev;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nlist; i += gridDim.x * blockDim.x) {
     const uint32_t q = qlist ? qlist[i] : (uint32_t)i;
     bucket_cnt[q] = max(bucket_cnt[q], bucket_cap + 1);
   }
+}
+
+// ---------------------------------------------------------------------------
+// device-side control of a batch: grouping, retry lists, verification count
+// ---------------------------------------------------------------------------
+
+// Queries grouped by approximate leaf (one block): per leaf its query count
+// and offset (counting sort; the order inside a leaf is arbitrary), each
+// query's bound slots, and the bound pass's item offsets per leaf (groups of
+// at most kBatchBoundQueries queries x chunks of btpi tiles).
+constexpr int kGroupThreads = 1024;
+__global__ void __launch_bounds__(kGroupThreads) k_group_queries(const int* __restrict__ approx, int nq,
+                                                                 const LeafPlan* __restrict__ plan, int nleaves,
+                                                                 uint32_t btpi, uint32_t* perm, uint32_t* slots,
+                                                                 uint32_t* leaf_qoff, uint32_t* leaf_qcnt,
+                                                                 uint32_t* item_off, uint32_t* nitems) {
+  extern __shared__ uint32_t gsh[];
+  uint32_t* cnt = gsh;            // [nleaves]
+  uint32_t* cur = gsh + nleaves;  // [nleaves]
+  __shared__ uint32_t wsum[2][32];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int i = tid; i < nleaves; i += kGroupThreads) cnt[i] = cur[i] = 0;
+  __syncthreads();
+  for (int q = tid; q < nq; q += kGroupThreads) atomicAdd(&cnt[approx[q]], 1u);
+  __syncthreads();
+  // exclusive scans over the leaves of query counts and item counts; each
+  // thread owns a run of consecutive leaves
+  const int per = (nleaves + kGroupThreads - 1) / kGroupThreads;
+  const int l0 = min(tid * per, nleaves), l1 = min(l0 + per, nleaves);
+  auto items_of = [&](int l) -> uint32_t {
+    const uint32_t c = cnt[l], use = plan[l].use_tiles;
+    if (c == 0 || use == 0) return 0u;
+    return ((c + kBatchBoundQueries - 1) / kBatchBoundQueries) * ((use + btpi - 1) / btpi);
+  };
+  uint32_t sq = 0, si = 0;
+  for (int l = l0; l < l1; ++l) {
+    sq += cnt[l];
+    si += items_of(l);
+  }
+  uint32_t vq = sq, vi = si;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t x = __shfl_up_sync(HG_FULL, vq, o), y = __shfl_up_sync(HG_FULL, vi, o);
+    if (lane >= o) {
+      vq += x;
+      vi += y;
+    }
+  }
+  if (lane == 31) {
+    wsum[0][wid] = vq;
+    wsum[1][wid] = vi;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t x = wsum[0][lane], y = wsum[1][lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t x2 = __shfl_up_sync(HG_FULL, x, o), y2 = __shfl_up_sync(HG_FULL, y, o);
+      if (lane >= o) {
+        x += x2;
+        y += y2;
+      }
+    }
+    wsum[0][lane] = x;
+    wsum[1][lane] = y;
+  }
+  __syncthreads();
+  uint32_t oq = (wid ? wsum[0][wid - 1] : 0u) + vq - sq, oi = (wid ? wsum[1][wid - 1] : 0u) + vi - si;
+  for (int l = l0; l < l1; ++l) {
+    leaf_qoff[l] = oq;
+    leaf_qcnt[l] = cnt[l];
+    item_off[l] = oi;
+    oq += cnt[l];
+    oi += items_of(l);
+  }
+  if (tid == kGroupThreads - 1) *nitems = oi;
+  __syncthreads();
+  for (int q = tid; q < nq; q += kGroupThreads) {
+    const int l = approx[q];
+    const uint32_t pos = atomicAdd(&cur[l], 1u);
+    perm[leaf_qoff[l] + pos] = (uint32_t)q;
+    slots[q] = plan[l].use_tiles * plan[l].sub;
+  }
+}
+
+// The bound pass's work items, one warp per leaf.
+__global__ void k_group_items(const LeafPlan* __restrict__ plan, int nleaves, uint32_t btpi,
+                              const uint32_t* __restrict__ leaf_qoff, const uint32_t* __restrict__ leaf_qcnt,
+                              const uint32_t* __restrict__ item_off, BatchItem* items) {
+  const int l = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (l >= nleaves) return;
+  const LeafPlan p = plan[l];
+  const uint32_t c = leaf_qcnt[l], use = p.use_tiles;
+  if (c == 0 || use == 0) return;
+  const uint32_t per_group = (use + btpi - 1) / btpi;
+  const uint32_t n = ((c + kBatchBoundQueries - 1) / kBatchBoundQueries) * per_group;
+  for (uint32_t i = lane; i < n; i += 32) {
+    const uint32_t g = i / per_group, tb = i % per_group;
+    BatchItem it;
+    it.row_begin = p.start;
+    it.row_end = p.start + p.size;
+    it.q_off = leaf_qoff[l] + g * kBatchBoundQueries;
+    it.q_cnt = min((uint32_t)kBatchBoundQueries, c - g * kBatchBoundQueries);
+    it.tile_lo = tb * btpi;
+    it.tile_hi = min(use, tb * btpi + btpi);
+    it.sub = p.sub;
+    it.pad = 0;
+    items[item_off[l] + i] = it;
+  }
+}
+
+// Queries of a round (list, or 0 .. n) still to retry (ok == 0) go to out.
+__global__ void k_collect_retry(const int* __restrict__ ok, const uint32_t* list, uint32_t n, const uint32_t* n_dev,
+                                uint32_t* out, uint32_t* out_n) {
+  if (n_dev) n = *n_dev;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t q = list ? list[i] : i;
+    if (ok[q] == 0) out[atomicAdd(out_n, 1u)] = q;
+  }
+}
+
+// Phase boundary of a batch: the global timer (ns) into a slot.
+__global__ void k_stamp(unsigned long long* slot) {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  *slot = t;
+}
+
+// Queries the batch did not verify (ok != 1): the plain path answers them.
+__global__ void k_count_unverified(const int* __restrict__ ok, uint32_t nq, uint32_t* out) {
+  uint32_t c = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) c += ok[i] != 1;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(HG_FULL, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
 }
 
 // ---------------------------------------------------------------------------
@@ -441,9 +581,9 @@ __global__ void k_mark_overflow(const uint32_t* pairs_cnt, uint32_t pairs_cap, c
 static inline unsigned nblk(uint64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 cudaError_t launch_rows_to_bf16(const float* rows, const uint32_t* idx, uint64_t n, int L, void* out, float4* meta,
-                                cudaStream_t s) {
+                                cudaStream_t s, const uint32_t* n_dev) {
   if (!n) return cudaSuccess;
-  k_rows_to_bf16<<<nblk(n * 32, 256), 256, 0, s>>>(rows, idx, n, L, static_cast<__nv_bfloat16*>(out), meta);
+  k_rows_to_bf16<<<nblk(n * 32, 256), 256, 0, s>>>(rows, idx, n, n_dev, L, static_cast<__nv_bfloat16*>(out), meta);
   return cudaGetLastError();
 }
 
@@ -455,13 +595,54 @@ cudaError_t launch_tile_norms(const float4* meta, uint64_t n, float4* tile_meta,
 }
 
 cudaError_t launch_scatter_pairs(const unsigned long long* pairs, const uint32_t* pairs_cnt, uint32_t pairs_cap,
-                                 const uint32_t* qlist, int nlist, uint32_t* bucket, uint32_t* bucket_cnt,
-                                 uint32_t bucket_cap, cudaStream_t s) {
+                                 const uint32_t* qlist, int nlist, const uint32_t* nlist_dev, uint32_t* bucket,
+                                 uint32_t* bucket_cnt, uint32_t bucket_cap, cudaStream_t s) {
   // grid-stride, enough threads in flight to hide the bucket atomics' latency
   k_scatter_pairs<<<2048, 256, 0, s>>>(pairs, pairs_cnt, pairs_cap, bucket, bucket_cnt, bucket_cap);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || nlist == 0) return e;
-  k_mark_overflow<<<nblk(nlist, 256), 256, 0, s>>>(pairs_cnt, pairs_cap, qlist, nlist, bucket_cnt, bucket_cap);
+  k_mark_overflow<<<nblk(nlist, 256), 256, 0, s>>>(pairs_cnt, pairs_cap, qlist, nlist, nlist_dev, bucket_cnt,
+                                                   bucket_cap);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_group_queries(const int* approx, int nq, const LeafPlan* plan, int nleaves, uint32_t btpi,
+                                 uint32_t* perm, uint32_t* slots, uint32_t* leaf_qoff, uint32_t* leaf_qcnt,
+                                 uint32_t* item_off, uint32_t* nitems, BatchItem* items, cudaStream_t s) {
+  const size_t smem = sizeof(uint32_t) * 2 * (size_t)nleaves;
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e = cudaFuncSetAttribute(k_group_queries, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)(sizeof(uint32_t) * 2 * kMaxLeavesSort));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_group_queries<<<1, kGroupThreads, smem, s>>>(approx, nq, plan, nleaves, btpi, perm, slots, leaf_qoff, leaf_qcnt,
+                                                 item_off, nitems);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_group_items<<<nblk((uint64_t)nleaves * 32, 256), 256, 0, s>>>(plan, nleaves, btpi, leaf_qoff, leaf_qcnt,
+                                                                 item_off, items);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_collect_retry(const int* ok, const uint32_t* list, uint32_t n, const uint32_t* n_dev,
+                                 uint32_t* out, uint32_t* out_n, cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  const unsigned g = nblk(n, 256) < 1024 ? nblk(n, 256) : 1024;
+  k_collect_retry<<<g, 256, 0, s>>>(ok, list, n, n_dev, out, out_n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stamp(unsigned long long* slot, cudaStream_t s) {
+  k_stamp<<<1, 1, 0, s>>>(slot);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_unverified(const int* ok, uint32_t nq, uint32_t* out, cudaStream_t s) {
+  if (!nq) return cudaSuccess;
+  const unsigned g = nblk(nq, 256) < 1024 ? nblk(nq, 256) : 1024;
+  k_count_unverified<<<g, 256, 0, s>>>(ok, nq, out);
   return cudaGetLastError();
 }
 

@@ -27,6 +27,12 @@ struct BatchItem {
   uint32_t pad;
 };
 
+// Rows of one leaf and its bound-pass plan (slots per tile and tiles used).
+struct LeafPlan {
+  uint64_t start;
+  uint32_t size, use_tiles, sub, pad;
+};
+
 // Arguments of the tensor-core filter (hg_umma.cu); the BF16 rows and the
 // BF16 queries (in tile order) reach it as TMA descriptors.
 struct BatchGemm {
@@ -38,10 +44,12 @@ struct BatchGemm {
   const uint32_t* qperm;   // query of each tile column (position in the BF16 query matrix)
   int nq;
   int mode;  // 0: bound pass over the items; 1: filter over every row; 2: raw products
-  int qtile; // modes 1 and 2: queries per tile (MMA N): 64, 128 or 256
+  int qtile; // modes 1 and 2: queries per tile (MMA N): 64, 128, 256, or 0 = by the query count
+  const uint32_t* nq_dev;   // if set: the query count (<= nq) read on the device
   // mode 0
   const BatchItem* items;
   uint32_t nitems;
+  const uint32_t* nitems_dev;  // if set: the item count read on the device
   unsigned long long* bm;  // [q][bm_cap] (ordered d~ << 32 | row), ~0 before the launch
   uint32_t bm_cap;
   // mode 1
@@ -80,7 +88,8 @@ struct BatchRank {
   unsigned long long* stats;  // [0] rows re-ranked [1] chunks [2] filter survivors
   // re-rank of the queries qlist[0 .. nlist) (qlist null: 0 .. nlist)
   const uint32_t* qlist;
-  int nlist;
+  int nlist;                  // the list's size, or its capacity when nlist_dev is set
+  const uint32_t* nlist_dev;  // if set: the list's size read on the device
   uint32_t* seg_rows;         // [list position] rows per segment
   uint32_t* seg_prefix;       // [nlist + 1] exclusive prefix of segments
   uint32_t* qbound;           // [q] running k-th distance (float bits)
@@ -89,8 +98,16 @@ struct BatchRank {
   uint32_t* heads;            // [0] segment counter
 };
 
+// n_dev (optional): the row count read on the device, at most n
 cudaError_t launch_rows_to_bf16(const float* rows, const uint32_t* idx, uint64_t n, int L, void* out, float4* meta,
-                                cudaStream_t s);
+                                cudaStream_t s, const uint32_t* n_dev = nullptr);
+cudaError_t launch_group_queries(const int* approx, int nq, const LeafPlan* plan, int nleaves, uint32_t btpi,
+                                 uint32_t* perm, uint32_t* slots, uint32_t* leaf_qoff, uint32_t* leaf_qcnt,
+                                 uint32_t* item_off, uint32_t* nitems, BatchItem* items, cudaStream_t s);
+cudaError_t launch_collect_retry(const int* ok, const uint32_t* list, uint32_t n, const uint32_t* n_dev,
+                                 uint32_t* out, uint32_t* out_n, cudaStream_t s);
+cudaError_t launch_count_unverified(const int* ok, uint32_t nq, uint32_t* out, cudaStream_t s);
+cudaError_t launch_stamp(unsigned long long* slot, cudaStream_t s);  // global-timer stamp (ns)
 cudaError_t launch_tile_norms(const float4* meta, uint64_t n, float4* tile_meta, cudaStream_t s);
 cudaError_t launch_bound_select(const BatchRank& r, cudaStream_t s);
 size_t umma_filter_smem();
@@ -101,7 +118,7 @@ cudaError_t launch_rerank(const BatchRank& r, int part_blocks, cudaStream_t s);
 // (bucket_cnt[q] counts every pair of q, also beyond bucket_cap); when the
 // pair list overflowed, every query of the round is marked overflowed.
 cudaError_t launch_scatter_pairs(const unsigned long long* pairs, const uint32_t* pairs_cnt, uint32_t pairs_cap,
-                                 const uint32_t* qlist, int nlist, uint32_t* bucket, uint32_t* bucket_cnt,
-                                 uint32_t bucket_cap, cudaStream_t s);
+                                 const uint32_t* qlist, int nlist, const uint32_t* nlist_dev, uint32_t* bucket,
+                                 uint32_t* bucket_cnt, uint32_t bucket_cap, cudaStream_t s);
 
 }  // namespace hg

@@ -332,6 +332,17 @@ static void free_device(hg_index* ix) {
   dfree(b.qbound);
   dfree(b.parts);
   dfree(b.part_cnt);
+  dfree(b.qlist2);
+  dfree(b.ctrl);
+  dfree(b.qin);
+  dfree(b.out_dist);
+  dfree(b.out_id);
+  dfree(b.leaf_plan);
+  dfree(b.leaf_qoff);
+  dfree(b.leaf_qcnt);
+  dfree(b.item_off);
+  if (b.graph) cudaGraphExecDestroy(b.graph);
+  dfree(b.stamps);
   b = hg::BatchScratch{};
 }
 
@@ -1167,7 +1178,7 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
 
 static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, const uint32_t* ks, uint32_t kmax,
                                 const hg_knn_opts& o, float* d_dist, int64_t* d_id, cudaStream_t st,
-                                hg_query_stats* stats);
+                                hg_query_stats* stats, bool host_io = false);
 
 static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t nq, uint32_t k,
                                  const hg_knn_opts* opts, float* d_dist, int64_t* d_id, cudaStream_t st,
@@ -1311,6 +1322,7 @@ static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket
     CK(dalloc(&b.qbound, nq));
     CK(dalloc(&b.part_cnt, (size_t)nq * hg::kBatchMaxSeg));
     b.nq_cap = nq;
+    ++b.gen;  // a captured pipeline holds the old addresses
     b.bucket_cap = 0;
     b.bm_cap = 0;
     b.parts_kmax = 0;
@@ -1321,30 +1333,36 @@ static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket
     dfree(b.pairs);
     CK(dalloc(&b.pairs, pairs_cap));
     b.pairs_cap = pairs_cap;
+    ++b.gen;  // a captured pipeline holds the old addresses
   }
   if (kmax > b.parts_kmax || !b.parts) {
     dfree(b.parts);
     CK(dalloc(&b.parts, (size_t)b.nq_cap * hg::kBatchMaxSeg * kmax));
     b.parts_kmax = kmax;
+    ++b.gen;  // a captured pipeline holds the old addresses
   }
   if (!b.stats) {
     CK(dalloc(&b.stats, 8));
     CK(dalloc(&b.heads, 4));
+    ++b.gen;  // a captured pipeline holds the old addresses
   }
   if ((uint64_t)b.nq_cap * bucket_cap > (uint64_t)b.nq_cap * b.bucket_cap || !b.bucket) {
     dfree(b.bucket);
     CK(dalloc(&b.bucket, (size_t)b.nq_cap * bucket_cap));
     b.bucket_cap = bucket_cap;
+    ++b.gen;  // a captured pipeline holds the old addresses
   }
   if (bm_cap > b.bm_cap || !b.bm) {
     dfree(b.bm);
     CK(dalloc(&b.bm, (size_t)b.nq_cap * bm_cap));
     b.bm_cap = bm_cap;
+    ++b.gen;  // a captured pipeline holds the old addresses
   }
   if (nitems > b.items_cap || !b.items) {
     dfree(b.items);
     CK(dalloc(&b.items, std::max<uint32_t>(nitems, 1)));
     b.items_cap = std::max<uint32_t>(nitems, 1);
+    ++b.gen;  // a captured pipeline holds the old addresses
   }
   return HG_OK;
 }
@@ -1362,10 +1380,175 @@ static hg_status record(cudaEvent_t e, cudaStream_t st) {
   return HG_OK;
 }
 
-// Batched exact k-NN over device queries; ks is a host array (or null).
+// Bound-pass plan of every leaf for `want` candidate rows per query: slots
+// per 128-row tile (enough for `want` where the leaf has the rows, at most
+// kBatchMaxSlots per query) and the tiles used.
+static hg_status ensure_leaf_plan(hg_index* ix, uint64_t want, cudaStream_t st) {
+  hg::BatchScratch& b = ix->bs;
+  const int nl = (int)ix->leaves.size();
+  if (b.leaf_plan && b.plan_want == want) return HG_OK;
+  const uint32_t T = hg::kBatchTileRows;
+  auto sub_of = [&](uint32_t tiles) {
+    uint32_t sub = 1;
+    while (sub < 16 && (uint64_t)std::max<uint32_t>(tiles, 1) * sub < want) sub <<= 1;
+    return sub;
+  };
+  std::vector<hg::LeafPlan> plan(nl);
+  uint32_t bm_cap = 1;
+  for (int l = 0; l < nl; ++l) {
+    const Node& nd = ix->nodes[ix->leaves[l]];
+    const uint32_t tiles = (uint32_t)((nd.node_size + T - 1) / T);
+    plan[l].start = nd.file_pos;
+    plan[l].size = nd.node_size;
+    plan[l].sub = sub_of(tiles);
+    plan[l].pad = 0;
+    bm_cap = std::max<uint32_t>(bm_cap, (uint32_t)std::min<uint64_t>(hg::kBatchMaxSlots, (uint64_t)tiles * plan[l].sub));
+  }
+  uint32_t max_use = 0;
+  for (int l = 0; l < nl; ++l) {
+    const uint32_t tiles = (plan[l].size + T - 1) / T;
+    plan[l].use_tiles = std::min<uint32_t>(tiles, bm_cap / plan[l].sub);
+    max_use = std::max(max_use, plan[l].use_tiles);
+  }
+  if (!b.leaf_plan) {
+    CK(dalloc(&b.leaf_plan, nl));
+    CK(dalloc(&b.leaf_qoff, nl + 1));
+    CK(dalloc(&b.leaf_qcnt, nl + 1));
+    CK(dalloc(&b.item_off, nl + 1));
+  }
+  CK(cudaMemcpyAsync(b.leaf_plan, plan.data(), sizeof(hg::LeafPlan) * nl, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  b.plan_want = want;
+  b.plan_bm_cap = bm_cap;
+  b.plan_max_use = max_use;
+  ++b.gen;
+  return HG_OK;
+}
+
+// Everything of one batch after the queries are in b.qin and their k in
+// b.kq, as one stream-ordered sequence with no host decision inside (so it
+// can be captured in a CUDA graph): routing and grouping on the device, the
+// bound pass, 1 + kBatchRetries filter rounds whose query lists are built on
+// the device (an empty round costs a few microseconds), the count of queries
+// left unverified.  Events gev[0..] mark the phases.
+static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_t bucket_cap, const CUtensorMap& qmap,
+                               cudaStream_t st, uint64_t* launches) {
+  hg::BatchScratch& b = ix->bs;
+  const uint32_t L = ix->L;
+  const int sms = hg::sm_count(ix->device);
+  const int nl = (int)ix->leaves.size();
+  auto stamp = [&](int i) { return hg::launch_stamp(b.stamps + i, st); };
+  CK(stamp(0));
+  CK(cudaMemsetAsync(b.ctrl, 0, sizeof(uint32_t) * 16, st));
+  CK(cudaMemsetAsync(b.heads, 0, sizeof(uint32_t) * 4, st));
+  CK(cudaMemsetAsync(b.stats, 0, sizeof(unsigned long long) * 8, st));
+  CK(cudaMemsetAsync(b.bm, 0xff, sizeof(unsigned long long) * nq * b.plan_bm_cap, st));
+  // 1. approximate leaves, grouping
+  CK(hg::launch_route_queries(b.qin, (int)nq, (int)L, index_tree(ix), b.approx, st));
+  CK(hg::launch_group_queries(b.approx, (int)nq, b.leaf_plan, nl, ix->tune.bound_tiles_per_item, b.qperm, b.slots,
+                              b.leaf_qoff, b.leaf_qcnt, b.item_off, b.ctrl + 0, b.items, st));
+  CK(hg::launch_rows_to_bf16(b.qin, b.qperm, nq, (int)L, b.qbf, b.qmeta, st));
+  // 2. bound pass
+  hg::BatchGemm g{};
+  g.L = (int)L;
+  g.nrows = ix->n;
+  g.xmeta = ix->bd.xmeta;
+  g.tile_meta = ix->bd.tile_meta;
+  g.qmeta = b.qmeta;
+  g.qperm = b.qperm;
+  g.nq = (int)nq;
+  g.mode = 0;
+  g.qtile = hg::kBatchQueryTile;
+  g.items = b.items;
+  g.nitems = b.items_cap;
+  g.nitems_dev = b.ctrl + 0;
+  g.bm = b.bm;
+  g.bm_cap = b.plan_bm_cap;
+  g.tiles_per_item = ix->tune.filter_tiles_per_item;
+  filter_coefficients(L, &g.c_acc, &g.c_sq);
+  g.bound = b.bound;
+  g.pairs = b.pairs;
+  g.pairs_cnt = b.heads + 1;
+  g.pairs_cap = b.pairs_cap;
+  g.err = reinterpret_cast<int*>(b.heads + 3);
+  CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
+  hg::BatchRank r{};
+  r.rows = ix->d.rows;
+  r.ids = ix->d.ids;
+  r.Q = b.qin;
+  r.L = (int)L;
+  r.nq = (int)nq;
+  r.kq = b.kq;
+  r.kmax = (int)kmax;
+  r.bm = b.bm;
+  r.bm_cap = b.plan_bm_cap;
+  r.slots_of_query = b.slots;
+  r.bound = b.bound;
+  r.init = b.init;
+  r.init_cnt = b.init_cnt;
+  r.bucket = b.bucket;
+  r.bucket_cnt = b.bucket_cnt;
+  r.bucket_cap = bucket_cap;
+  r.dist_out = b.out_dist;
+  r.id_out = b.out_id;
+  r.ok_out = b.ok;
+  r.stats = b.stats;
+  r.seg_rows = b.seg_rows;
+  r.seg_prefix = b.seg_prefix;
+  r.qbound = b.qbound;
+  r.parts = b.parts;
+  r.part_cnt = b.part_cnt;
+  r.heads = b.heads + 2;
+  r.qlist = nullptr;
+  r.nlist = (int)nq;
+  r.nlist_dev = nullptr;
+  CK(hg::launch_bound_select(r, st));
+  CK(stamp(1));
+  *launches = 8;  // route, group (2), conversion, bound pass, bound selection
+  // 3-5. certified filter, exact re-rank, verification; queries whose bucket
+  // overflowed are retried with the bound their first survivors gave
+  uint32_t* lists[2] = {b.qlist, b.qlist2};
+  for (int round = 0; round <= kBatchRetries; ++round) {
+    const uint32_t* list_in = round == 0 ? nullptr : lists[(round - 1) & 1];
+    const uint32_t* n_dev = round == 0 ? nullptr : b.ctrl + 4 + round;
+    if (round > 0) {
+      CK(hg::launch_rows_to_bf16(b.qin, list_in, nq, (int)L, b.qbf, b.qmeta, st, n_dev));
+      ++*launches;
+    }
+    g.mode = 1;
+    g.qperm = round == 0 ? b.qperm : list_in;
+    g.nq_dev = n_dev;
+    g.qtile = round == 0 ? hg::kBatchQueryTile : 0;
+    CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
+    CK(cudaMemsetAsync(b.heads + 1, 0, sizeof(uint32_t), st));
+    CK(stamp(2 + 3 * round));
+    CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
+    CK(stamp(3 + 3 * round));
+    CK(hg::launch_scatter_pairs(b.pairs, b.heads + 1, b.pairs_cap, list_in, (int)nq, n_dev, b.bucket, b.bucket_cnt,
+                                bucket_cap, st));
+    r.qlist = list_in;
+    r.nlist = (int)nq;
+    r.nlist_dev = n_dev;
+    CK(hg::launch_rerank(r, sms * (int)ix->tune.rerank_blocks_per_sm, st));
+    CK(stamp(4 + 3 * round));
+    *launches += 9;  // filter, scatter, overflow mark, re-rank plan / segments / merge
+    if (round < kBatchRetries) {
+      CK(hg::launch_collect_retry(b.ok, list_in, nq, n_dev, lists[round & 1], b.ctrl + 4 + round + 1, st));
+      ++*launches;
+    }
+  }
+  CK(hg::launch_count_unverified(b.ok, nq, b.ctrl + 3, st));
+  CK(stamp(15));
+  *launches += 2;
+  return HG_OK;
+}
+
+// Batched exact k-NN; ks is a host array (or null).  Queries and answers are
+// device buffers, or host buffers with host_io (copied straight into and out
+// of the handle's fixed buffers: no allocation per call).
 static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, const uint32_t* ks, uint32_t kmax,
                                 const hg_knn_opts& o, float* d_dist, int64_t* d_id, cudaStream_t st,
-                                hg_query_stats* stats) {
+                                hg_query_stats* stats, bool host_io) {
   if (!ix || (!d_Q && nq)) return set_error(HG_ERR_ARG, "hg_knn_batch: null argument");
   if (kmax == 0) return set_error(HG_ERR_ARG, "hg_knn_batch: k must be positive");
   if ((int)kmax > hg::kMaxK) return set_error(HG_ERR_LIMIT, "hg_knn_batch: k above 224");
@@ -1373,7 +1556,8 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   if (ix->leaves.size() > (size_t)hg::kMaxLeavesSort)
     return set_error(HG_ERR_LIMIT, "hg_knn_batch: more than 8192 leaves");
   if (nq > (1u << 24)) return set_error(HG_ERR_LIMIT, "hg_knn_batch: more than 2^24 queries");
-  if (((uintptr_t)d_Q & 15) != 0) return set_error(HG_ERR_ARG, "hg_knn_batch: queries must be 16-byte aligned");
+  if (!host_io && ((uintptr_t)d_Q & 15) != 0)
+    return set_error(HG_ERR_ARG, "hg_knn_batch: queries must be 16-byte aligned");
   std::vector<uint32_t> kq(nq, kmax);
   if (ks)
     for (uint32_t i = 0; i < nq; ++i) {
@@ -1388,214 +1572,122 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   const bool data_built = ix->bd.xbf == nullptr;
   HCK(ensure_batch_data(ix, st));
   const uint32_t L = ix->L;
-  const int sms = hg::sm_count(ix->device);
   const uint32_t bucket_cap = o.bucket_cap > 0 ? (uint32_t)o.bucket_cap : kDefaultBucket;
   hg::BatchScratch& b = ix->bs;
-  HCK(ensure_batch_scratch(ix, std::max(nq, b.nq_cap), bucket_cap, 1, 1, kmax));
-
-  cudaEvent_t ev[6];
-  for (auto& e : ev) CK(cudaEventCreate(&e));
-  struct EvGuard {
-    cudaEvent_t* e;
-    ~EvGuard() {
-      for (int i = 0; i < 6; ++i) cudaEventDestroy(e[i]);
-    }
-  } guard{ev};
-  HCK(record(ev[0], st));
-  // 1. approximate leaves
-  CK(hg::launch_route_queries(d_Q, (int)nq, (int)L, index_tree(ix), b.approx, st));
-  std::vector<int> approx(nq);
-  CK(cudaMemcpyAsync(approx.data(), b.approx, sizeof(int) * nq, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-
-  // queries grouped by approximate leaf; slots per tile for the bound pass
-  const uint32_t T = hg::kBatchTileRows;
-  std::vector<uint32_t> perm(nq);
-  for (uint32_t i = 0; i < nq; ++i) perm[i] = i;
-  std::stable_sort(perm.begin(), perm.end(), [&](uint32_t a, uint32_t c) { return approx[a] < approx[c]; });
-  auto leaf_rows = [&](int li, uint64_t* start, uint64_t* size) {
-    const Node& nd = ix->nodes[ix->leaves[li]];
-    *start = nd.file_pos;
-    *size = nd.node_size;
-  };
-  // bound slots per tile, per leaf: enough slots for max(2k + 32, 256) candidate rows
-  // where the leaf has them, at most kBatchMaxSlots per query
-  const uint64_t want = std::max<uint64_t>(2ull * kmax + 32, 256);
-  auto sub_of = [&](uint32_t tiles) {
-    uint32_t sub = 1;
-    while (sub < 16 && (uint64_t)std::max<uint32_t>(tiles, 1) * sub < want) sub <<= 1;
-    return sub;
-  };
-  uint32_t bm_cap = 1;
-  for (uint32_t i = 0; i < nq; ++i) {
-    uint64_t st0, sz;
-    leaf_rows(approx[i], &st0, &sz);
-    const uint32_t tiles = (uint32_t)((sz + T - 1) / T);
-    bm_cap = std::max<uint32_t>(bm_cap, (uint32_t)std::min<uint64_t>(hg::kBatchMaxSlots, (uint64_t)tiles * sub_of(tiles)));
+  HCK(ensure_leaf_plan(ix, std::max<uint64_t>(2ull * kmax + 32, 256), st));
+  const uint32_t btpi = ix->tune.bound_tiles_per_item;
+  const uint32_t items_cap =
+      (uint32_t)(((uint64_t)(nq + hg::kBatchBoundQueries - 1) / hg::kBatchBoundQueries + ix->leaves.size()) *
+                 ((b.plan_max_use + btpi - 1) / btpi));
+  HCK(ensure_batch_scratch(ix, std::max(nq, b.nq_cap), bucket_cap, b.plan_bm_cap, items_cap, kmax));
+  if (!b.ctrl) {
+    CK(dalloc(&b.ctrl, 16));
+    CK(dalloc(&b.stamps, 16));
   }
-  std::vector<hg::BatchItem> items;
-  std::vector<uint32_t> slots(nq);
-  for (uint32_t i = 0; i < nq;) {
-    uint32_t j = i;
-    while (j < nq && approx[perm[j]] == approx[perm[i]] && j - i < (uint32_t)hg::kBatchBoundQueries) ++j;
-    uint64_t st0, sz;
-    leaf_rows(approx[perm[i]], &st0, &sz);
-    const uint32_t tiles = (uint32_t)((sz + T - 1) / T);
-    const uint32_t sub = sub_of(tiles);
-    const uint32_t use_tiles = std::min<uint32_t>(tiles, bm_cap / sub);
-    const uint32_t btpi = ix->tune.bound_tiles_per_item;
-    for (uint32_t t = 0; t < use_tiles; t += btpi)
-      items.push_back(
-          hg::BatchItem{st0, st0 + sz, i, j - i, t, std::min(use_tiles, t + btpi), sub, 0});
-    for (uint32_t x = i; x < j; ++x) slots[perm[x]] = use_tiles * sub;
-    i = j;
+  if (!b.qlist2 || !b.qin || b.out_kmax < kmax) {
+    dfree(b.qlist2);
+    dfree(b.qin);
+    dfree(b.out_dist);
+    dfree(b.out_id);
+    CK(dalloc(&b.qlist2, b.nq_cap));
+    CK(dalloc(&b.qin, (size_t)b.nq_cap * L));
+    CK(dalloc(&b.out_dist, (size_t)b.nq_cap * kmax));
+    CK(dalloc(&b.out_id, (size_t)b.nq_cap * kmax));
+    b.out_kmax = kmax;
+    ++b.gen;
   }
-  HCK(ensure_batch_scratch(ix, b.nq_cap, bucket_cap, bm_cap, (uint32_t)items.size(), kmax));
-  CK(cudaMemcpyAsync(b.qperm, perm.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
+  // inputs at fixed addresses: the queries and their k
+  CK(cudaMemcpyAsync(b.qin, d_Q, sizeof(float) * nq * L,
+                     host_io ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
   CK(cudaMemcpyAsync(b.kq, kq.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(b.slots, slots.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
-  if (!items.empty())
-    CK(cudaMemcpyAsync(b.items, items.data(), sizeof(hg::BatchItem) * items.size(), cudaMemcpyHostToDevice, st));
-  // BF16 queries in processing order (tile columns), norms by query
-  CK(hg::launch_rows_to_bf16(d_Q, b.qperm, nq, (int)L, b.qbf, b.qmeta, st));
   CUtensorMap qmap;
   HCK(encode_bf16_map(&qmap, b.qbf, nq, L, hg::kBatchQueryTile));
-
-  // 2. bound pass
-  hg::BatchGemm g{};
-  g.L = (int)L;
-  g.nrows = ix->n;
-  g.xmeta = ix->bd.xmeta;
-  g.tile_meta = ix->bd.tile_meta;
-  g.qmeta = b.qmeta;
-  g.qperm = b.qperm;
-  g.nq = (int)nq;
-  g.mode = 0;
-  g.qtile = hg::kBatchQueryTile;
-  g.items = b.items;
-  g.nitems = (uint32_t)items.size();
-  g.bm = b.bm;
-  g.bm_cap = bm_cap;
-  g.tiles_per_item = ix->tune.filter_tiles_per_item;
-  filter_coefficients(L, &g.c_acc, &g.c_sq);
-  g.bound = b.bound;
-  g.pairs = b.pairs;
-  g.pairs_cnt = b.heads + 1;
-  g.pairs_cap = b.pairs_cap;
-  g.err = reinterpret_cast<int*>(b.heads + 3);
-  CK(cudaMemsetAsync(b.bm, 0xff, sizeof(unsigned long long) * nq * bm_cap, st));
-  CK(cudaMemsetAsync(b.heads, 0, sizeof(uint32_t) * 4, st));
-  CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
-  CK(cudaMemsetAsync(b.stats, 0, sizeof(unsigned long long) * 8, st));
-  CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
-  hg::BatchRank r{};
-  r.rows = ix->d.rows;
-  r.ids = ix->d.ids;
-  r.Q = d_Q;
-  r.L = (int)L;
-  r.nq = (int)nq;
-  r.kq = b.kq;
-  r.kmax = (int)kmax;
-  r.bm = b.bm;
-  r.bm_cap = bm_cap;
-  r.slots_of_query = b.slots;
-  r.bound = b.bound;
-  r.init = b.init;
-  r.init_cnt = b.init_cnt;
-  r.bucket = b.bucket;
-  r.bucket_cnt = b.bucket_cnt;
-  r.bucket_cap = bucket_cap;
-  r.dist_out = d_dist;
-  r.id_out = d_id;
-  r.ok_out = b.ok;
-  r.stats = b.stats;
-  r.seg_rows = b.seg_rows;
-  r.seg_prefix = b.seg_prefix;
-  r.qbound = b.qbound;
-  r.parts = b.parts;
-  r.part_cnt = b.part_cnt;
-  r.heads = b.heads + 2;
-  r.qlist = nullptr;
-  r.nlist = (int)nq;
-  CK(hg::launch_bound_select(r, st));
-  HCK(record(ev[1], st));
-  // 3-5. certified filter, exact re-rank, verification; a query whose bucket
-  // overflowed is retried with the bound its first survivors gave
-  const int gemm_rounds_max = 1 + kBatchRetries;
-  std::vector<int> ok(nq);
-  std::vector<uint32_t> retry;
-  double gemm_ms = 0, rerank_ms = 0;
-  uint64_t pairs = 0, retried = 0;
-  // route, query conversion, bound pass, bound selection
-  uint64_t launches = 4 + (data_built ? 2 : 0);
-  for (int round = 0; round < gemm_rounds_max; ++round) {
-    const uint32_t cnt = round == 0 ? nq : (uint32_t)retry.size();
-    launches += round == 0 ? 6 : 7;  // (gather,) filter, scatter, overflow mark, re-rank plan / segments / merge
-    if (round > 0) {
-      CK(cudaMemcpyAsync(b.qlist, retry.data(), sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice, st));
-      CK(hg::launch_rows_to_bf16(d_Q, b.qlist, cnt, (int)L, b.qbf, b.qmeta, st));
-      HCK(encode_bf16_map(&qmap, b.qbf, cnt, L, hg::kBatchQueryTile));
-      g.qperm = b.qlist;
-      r.qlist = b.qlist;
-      retried += cnt;
+  // the pipeline, captured once per shape in a CUDA graph and replayed
+  const uint64_t key[8] = {nq, kmax, bucket_cap, b.gen, ix->tune.filter_tiles_per_item, ix->tune.bound_tiles_per_item,
+                           ix->tune.rerank_blocks_per_sm, 1};
+  uint64_t launches = 0;
+  if (!b.graph || memcmp(key, b.graph_key, sizeof key) != 0) {
+    if (b.graph) {
+      cudaGraphExecDestroy(b.graph);
+      b.graph = nullptr;
     }
-    g.nq = (int)cnt;
-    r.nlist = (int)cnt;
-    g.mode = 1;
-    // a narrow query tile when few queries take part (retry rounds)
-    g.qtile = cnt <= 64 ? 64 : (cnt <= 128 ? 128 : hg::kBatchQueryTile);
-    CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
-    CK(cudaMemsetAsync(b.heads + 1, 0, sizeof(uint32_t), st));
-    HCK(record(ev[2], st));
-    CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
-    HCK(record(ev[3], st));
-    CK(hg::launch_scatter_pairs(b.pairs, b.heads + 1, b.pairs_cap, round == 0 ? nullptr : b.qlist, (int)cnt,
-                                b.bucket, b.bucket_cnt, bucket_cap, st));
-    HCK(record(ev[5], st));
-    CK(hg::launch_rerank(r, sms * (int)ix->tune.rerank_blocks_per_sm, st));
-    HCK(record(ev[4], st));
-    CK(cudaMemcpyAsync(ok.data(), b.ok, sizeof(int) * nq, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    float tg = 0, tr = 0;
-    cudaEventElapsedTime(&tg, ev[2], ev[3]);
-    cudaEventElapsedTime(&tr, ev[3], ev[4]);  // scatter + re-rank
-    gemm_ms += tg;
-    rerank_ms += tr;
-    pairs += (uint64_t)cnt * ix->n;
-    std::vector<uint32_t> next;
-    const uint32_t* lst = round == 0 ? nullptr : retry.data();
-    for (uint32_t i = 0; i < cnt; ++i) {
-      const uint32_t q = lst ? lst[i] : i;
-      if (ok[q] == 0) next.push_back(q);
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+    const hg_status s = enqueue_batch(ix, nq, kmax, bucket_cap, qmap, st, &launches);
+    const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (s != HG_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return s;
     }
-    retry.swap(next);
-    if (retry.empty()) break;
+    CK(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&b.graph, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(ie);
+    memcpy(b.graph_key, key, sizeof key);
+    b.graph_launches = launches;
   }
-  unsigned long long hs[8];
+  launches = b.graph_launches;
+  CK(cudaGraphLaunch(b.graph, st));
+  unsigned long long hs[8], ts[16];
+  uint32_t ctrl[16];
   uint32_t dev_err = 0;
+  CK(cudaMemcpyAsync(ts, b.stamps, sizeof ts, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(hs, b.stats, sizeof hs, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(ctrl, b.ctrl, sizeof ctrl, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(&dev_err, b.heads + 3, sizeof dev_err, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   if (dev_err) return set_error(HG_ERR_TIMEOUT, "hg_knn_batch: a tensor-core filter wait timed out");
   // queries that did not verify: the plain path
-  HCK(record(ev[2], st));
-  hg_knn_opts po{};
-  po.mode = HG_MODE_PLAIN;
-  po.use_lb_sax = 1;
+  cudaEvent_t fb0 = nullptr, fb1 = nullptr;
+  CK(cudaEventCreate(&fb0));
+  CK(cudaEventCreate(&fb1));
+  CK(cudaEventRecord(fb0, st));
   uint64_t fallbacks = 0;
-  for (uint32_t q = 0; q < nq; ++q) {
-    if (ok[q] == 1) continue;
-    ++fallbacks;
-    HCK(knn_one(ix, d_Q + (uint64_t)q * L, (int)kq[q], po, d_dist + (uint64_t)q * kmax, d_id + (uint64_t)q * kmax,
-                st, nullptr));
+  hg_status fs = HG_OK;
+  if (ctrl[3] > 0) {
+    std::vector<int> ok(nq);
+    CK(cudaMemcpy(ok.data(), b.ok, sizeof(int) * nq, cudaMemcpyDeviceToHost));
+    hg_knn_opts po{};
+    po.mode = HG_MODE_PLAIN;
+    po.use_lb_sax = 1;
+    for (uint32_t q = 0; q < nq && fs == HG_OK; ++q) {
+      if (ok[q] == 1) continue;
+      ++fallbacks;
+      fs = knn_one(ix, b.qin + (uint64_t)q * L, (int)kq[q], po, b.out_dist + (uint64_t)q * kmax,
+                   b.out_id + (uint64_t)q * kmax, st, nullptr);
+    }
   }
-  HCK(record(ev[3], st));
-  CK(cudaStreamSynchronize(st));
+  cudaEventRecord(fb1, st);
+  if (fs == HG_OK) {
+    const cudaMemcpyKind kind = host_io ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    cudaError_t ce = cudaSuccess;
+    if (d_dist) ce = cudaMemcpyAsync(d_dist, b.out_dist, sizeof(float) * nq * kmax, kind, st);
+    if (ce == cudaSuccess && d_id) ce = cudaMemcpyAsync(d_id, b.out_id, sizeof(int64_t) * nq * kmax, kind, st);
+    if (ce != cudaSuccess) fs = cuda_fail(ce, "hg_knn_batch");
+  }
+  cudaStreamSynchronize(st);
+  if (fs != HG_OK) {
+    cudaEventDestroy(fb0);
+    cudaEventDestroy(fb1);
+    return fs;
+  }
   if (stats) {
-    float t01 = 0, tf = 0, t03 = 0;
-    cudaEventElapsedTime(&t01, ev[0], ev[1]);
-    cudaEventElapsedTime(&tf, ev[2], ev[3]);
-    cudaEventElapsedTime(&t03, ev[0], ev[3]);
+    auto span = [&](int i, int j) { return (double)(ts[j] - ts[i]) * 1e-6; };  // ms
+    float tf = 0;
+    double gemm = 0, rerank = 0;
+    uint64_t pairs = 0, retried = 0;
+    const double t01 = span(0, 1);
+    for (int round = 0; round <= kBatchRetries; ++round) {
+      const double tg = span(2 + 3 * round, 3 + 3 * round), tr = span(3 + 3 * round, 4 + 3 * round);
+      const uint64_t cnt = round == 0 ? nq : ctrl[4 + round];
+      if (round > 0) retried += cnt;
+      if (cnt == 0 && round > 0) continue;
+      gemm += tg;
+      rerank += tr;
+      pairs += cnt * ix->n;
+    }
+    cudaEventElapsedTime(&tf, fb0, fb1);
+    const double t0e = span(0, 15) + (fallbacks ? tf : 0.0);
     stats->queries = nq;
     stats->rows_visited = hs[0];
     stats->chunks_loaded = hs[1];
@@ -1604,12 +1696,14 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     stats->fallback_queries = fallbacks;
     stats->retried_queries = retried;
     stats->bound_ms = t01;
-    stats->gemm_ms = gemm_ms;
-    stats->rerank_ms = rerank_ms;
-    stats->fallback_ms = tf;
-    stats->device_ms = t03;
-    stats->kernel_launches = launches + 9 * fallbacks;
+    stats->gemm_ms = gemm;
+    stats->rerank_ms = rerank;
+    stats->fallback_ms = fallbacks ? tf : 0.0;
+    stats->device_ms = t0e;
+    stats->kernel_launches = launches + (data_built ? 2 : 0) + 9 * fallbacks;
   }
+  cudaEventDestroy(fb0);
+  cudaEventDestroy(fb1);
   return HG_OK;
 }
 
@@ -1808,35 +1902,9 @@ hg_status hg_knn_batch_device(hg_index* ix, const float* d_queries, uint32_t nq,
 hg_status hg_knn_batch(hg_index* ix, const float* queries, uint32_t nq, const uint32_t* ks, uint32_t kmax,
                        const hg_knn_opts* opts, float* dist_out, int64_t* id_out, hg_query_stats* stats) {
   if (!ix || (!queries && nq)) return set_error(HG_ERR_ARG, "hg_knn_batch: null argument");
-  if (nq == 0 || kmax == 0) {
-    hg_knn_opts o{};
-    return knn_batch_impl(ix, nullptr, 0, ks, kmax, o, nullptr, nullptr, nullptr, stats);
-  }
-  CK(cudaSetDevice(ix->device));
-  float* d_q = nullptr;
-  float* d_dist = nullptr;
-  int64_t* d_id = nullptr;
-  const size_t nout = (size_t)nq * kmax;
-  cudaError_t e = dalloc(&d_q, (size_t)nq * ix->L);
-  if (e == cudaSuccess) e = dalloc(&d_dist, nout);
-  if (e == cudaSuccess) e = dalloc(&d_id, nout);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_q, queries, sizeof(float) * nq * ix->L, cudaMemcpyHostToDevice, ix->stream);
-  hg_status s = e == cudaSuccess ? HG_OK : cuda_fail(e, "hg_knn_batch");
   hg_knn_opts o{};
   if (opts) o = *opts;
-  if (s == HG_OK) s = knn_batch_impl(ix, d_q, nq, ks, kmax, o, d_dist, d_id, ix->stream, stats);
-  if (s == HG_OK) {
-    if (id_out) e = cudaMemcpyAsync(id_out, d_id, sizeof(int64_t) * nout, cudaMemcpyDeviceToHost, ix->stream);
-    if (e == cudaSuccess && dist_out)
-      e = cudaMemcpyAsync(dist_out, d_dist, sizeof(float) * nout, cudaMemcpyDeviceToHost, ix->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
-    if (e != cudaSuccess) s = cuda_fail(e, "hg_knn_batch");
-  }
-  if (d_q) cudaFree(d_q);
-  if (d_dist) cudaFree(d_dist);
-  if (d_id) cudaFree(d_id);
-  return s;
+  return knn_batch_impl(ix, queries, nq, ks, kmax, o, dist_out, id_out, nullptr, stats, true);
 }
 
 hg_status hg_bf16_dots(const float* d_rows, uint64_t n, uint32_t L, const float* d_queries, uint32_t nq,

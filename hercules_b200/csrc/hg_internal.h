@@ -112,6 +112,26 @@ struct BatchScratch {
   uint32_t* qbound = nullptr;
   unsigned long long* parts = nullptr;
   int* part_cnt = nullptr;
+  // device-side control of a batch
+  uint32_t* qlist2 = nullptr;    // second retry list (rounds alternate)
+  uint32_t* ctrl = nullptr;      // [0] bound items [3] unverified queries [4 + r] queries of round r
+  float* qin = nullptr;          // the batch's queries (fixed address for the graph)
+  float* out_dist = nullptr;     // the batch's answers before they are copied out
+  int64_t* out_id = nullptr;
+  uint32_t out_kmax = 0;
+  // bound-pass plan per leaf, for the `want` slots it was made for
+  LeafPlan* leaf_plan = nullptr;
+  uint32_t* leaf_qoff = nullptr;
+  uint32_t* leaf_qcnt = nullptr;
+  uint32_t* item_off = nullptr;
+  uint64_t plan_want = 0;
+  uint32_t plan_bm_cap = 0, plan_max_use = 0;
+  uint64_t gen = 0;              // bumped whenever a buffer above moves
+  // the captured batch pipeline and the key it was captured for
+  cudaGraphExec_t graph = nullptr;
+  uint64_t graph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  uint64_t graph_launches = 0;   // kernels in the captured pipeline
+  unsigned long long* stamps = nullptr;  // [16] global-timer stamps at the phase boundaries
 };
 
 }  // namespace hg

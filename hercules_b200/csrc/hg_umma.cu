@@ -176,7 +176,8 @@ struct Item {
   uint32_t sub;
 };
 
-__device__ __forceinline__ Item item_of(const BatchGemm& a, uint32_t w, uint32_t QT, uint64_t ntiles, int qtile) {
+__device__ __forceinline__ Item item_of(const BatchGemm& a, uint32_t w, uint32_t QT, uint64_t ntiles, int qtile,
+                                        int nq) {
   Item it;
   if (a.mode == 0) {
     const BatchItem b = a.items[w];
@@ -192,7 +193,7 @@ __device__ __forceinline__ Item item_of(const BatchGemm& a, uint32_t w, uint32_t
     it.rb = 0;
     it.re = a.nrows;
     it.qoff = qt * (uint32_t)qtile;
-    it.qcnt = (uint32_t)min(a.nq - (int)it.qoff, qtile);
+    it.qcnt = (uint32_t)min(nq - (int)it.qoff, qtile);
     it.t_lo = chunk * a.tiles_per_item;
     const uint64_t th = (uint64_t)it.t_lo + a.tiles_per_item;
     it.t_hi = (uint32_t)(th < ntiles ? th : ntiles);
@@ -226,12 +227,16 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int nkb = (a.L + kUK - 1) / kUK;
   const bool resident = nkb <= kResidentKB;
   const uint32_t nst = resident ? kAStages : kResidentKB;  // streamed: one query slot per stage
-  // queries per tile (MMA N): 64 in the bound pass, else the launch's choice
-  const int qtile = a.mode == 0 ? kBatchBoundQueries : a.qtile;
-  const uint32_t QT = (uint32_t)((a.nq + qtile - 1) / qtile);
+  // query count (read on the device for rounds planned there) and queries
+  // per tile (MMA N): 64 in the bound pass, else the launch's choice or, for
+  // 0, the narrowest of 64 / 128 / 256 that holds the queries
+  const int nq = a.nq_dev ? (int)min((uint32_t)a.nq, *a.nq_dev) : a.nq;
+  const int qtile = a.mode == 0 ? kBatchBoundQueries
+                                : (a.qtile ? a.qtile : (nq <= 64 ? 64 : (nq <= 128 ? 128 : kUN)));
+  const uint32_t QT = (uint32_t)((nq + qtile - 1) / qtile);
   const uint64_t ntiles = (a.nrows + kUM - 1) / kUM;
   const uint32_t nchunks = (uint32_t)((ntiles + a.tiles_per_item - 1) / a.tiles_per_item);
-  const uint32_t total = a.mode == 0 ? a.nitems : nchunks * QT;
+  const uint32_t total = a.mode == 0 ? (a.nitems_dev ? *a.nitems_dev : a.nitems) : nchunks * QT;
 
   if (tid == 0) {
     for (int s = 0; s < kAStages; ++s) {
@@ -264,7 +269,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t g = 0, it_n = 0;
       bool ok = true;
       for (uint32_t w = blockIdx.x; ok && w < total; w += gridDim.x, ++it_n) {
-        const Item it = item_of(a, w, QT, ntiles, qtile);
+        const Item it = item_of(a, w, QT, ntiles, qtile, nq);
         if (resident) {
           ok = mbar_wait(qempty_bar, (it_n & 1) ^ 1, abort_flag, a.err);
           if (!ok) break;
@@ -297,7 +302,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t g = 0, tcount = 0, it_n = 0;
       bool ok = true;
       for (uint32_t w = blockIdx.x; ok && w < total; w += gridDim.x, ++it_n) {
-        const Item it = item_of(a, w, QT, ntiles, qtile);
+        const Item it = item_of(a, w, QT, ntiles, qtile, nq);
         if (resident) {
           ok = mbar_wait(qfull_bar, it_n & 1, abort_flag, a.err);
           if (!ok) break;
@@ -341,7 +346,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t pcur = 0, pend = 0;  // the warp's reserved block of the pair list
     bool ok = true;
     for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
-      const Item it = item_of(a, w, QT, ntiles, qtile);
+      const Item it = item_of(a, w, QT, ntiles, qtile, nq);
       // item boundary: every epilogue warp is done with the previous item
       // and all of them learn whether any gave up
       if (lane == 0) s_okw[ew] = ok ? 1 : 0;
@@ -568,13 +573,17 @@ cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q
     attr = true;
   }
   const uint64_t ntiles = (g.nrows + kUM - 1) / kUM;
-  const int qtile = g.mode == 0 ? kBatchBoundQueries : g.qtile;
-  if (g.mode != 0 && qtile != 64 && qtile != 128 && qtile != 256) return cudaErrorInvalidValue;
-  const uint32_t QT = (uint32_t)((g.nq + qtile - 1) / qtile);
-  const uint64_t total =
-      g.mode == 0 ? g.nitems : ((ntiles + g.tiles_per_item - 1) / g.tiles_per_item) * (uint64_t)QT;
-  if (total == 0) return cudaSuccess;
-  const int grid = (int)(total < (uint64_t)blocks ? total : (uint64_t)blocks);
+  if (g.mode != 0 && g.qtile != 0 && g.qtile != 64 && g.qtile != 128 && g.qtile != 256) return cudaErrorInvalidValue;
+  // counts read on the device: every CTA starts and leaves when out of items
+  int grid = blocks;
+  if (!(g.mode == 0 ? g.nitems_dev : g.nq_dev)) {
+    const int qtile = g.mode == 0 ? kBatchBoundQueries : (g.qtile ? g.qtile : (g.nq <= 64 ? 64 : (g.nq <= 128 ? 128 : kUN)));
+    const uint32_t QT = (uint32_t)((g.nq + qtile - 1) / qtile);
+    const uint64_t total =
+        g.mode == 0 ? g.nitems : ((ntiles + g.tiles_per_item - 1) / g.tiles_per_item) * (uint64_t)QT;
+    if (total == 0) return cudaSuccess;
+    grid = (int)(total < (uint64_t)blocks ? total : (uint64_t)blocks);
+  }
   k_umma_filter<<<grid, kThreads, kDynSmem, s>>>(rows_map, q_map, g);
   return cudaGetLastError();
 }
