@@ -62,6 +62,10 @@ def parse():
     p.add_argument("--fresh-frac", type=float, default=0.1)
     p.add_argument("--plain-queries", type=int, default=128, help="queries through the plain path")
     p.add_argument("--plain-k", type=int, default=10)
+    p.add_argument("--data", choices=["walks", "unit"], default="walks",
+                   help="z-normalised random walks, or unit-normalised Gaussian vectors")
+    p.add_argument("--sigma2", default="0.01,0.1,1.0", help="noise levels of the noisy queries, in equal shares")
+    p.add_argument("--ks", default="1,10,100", help="k of the batched queries, cycling")
     p.add_argument("--cpu-sample-queries", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--ref-queries-per-step", type=int, default=2)
@@ -69,9 +73,12 @@ def parse():
     return p.parse_args()
 
 
-def sigma2_for(nq, offset=0):
-    cyc = np.array([0.01, 0.1, 1.0])
-    return cyc[(np.arange(nq) + offset) % 3]
+SIGMA2 = (0.01, 0.1, 1.0)
+
+
+def sigma2_for(nq, offset=0, levels=SIGMA2):
+    cyc = np.array(levels, dtype=np.float64)
+    return cyc[(np.arange(nq) + offset) % len(cyc)]
 
 
 class ClockSampler:
@@ -184,17 +191,29 @@ def profile_json(name):
 def build_collection(args, torch, H, device):
     n, L = args.n, args.L
     X = torch.empty((n, L), dtype=torch.float32, device=device)
-    H.generate_walks_device(DATA_SEED, n, L, X.data_ptr(), device=device)
+    if args.data == "unit":
+        H.generate_unit_vectors_device(DATA_SEED, n, L, X.data_ptr(), device=device)
+    else:
+        H.generate_walks_device(DATA_SEED, n, L, X.data_ptr(), device=device)
     torch.cuda.synchronize()
     return X
 
 
 def make_queries(args, torch, H, X, nq, device, offset):
     Q = torch.empty((nq, args.L), dtype=torch.float32, device=device)
-    H.generate_queries_device(QUERY_SEED + offset, X.data_ptr(), args.n, args.L, sigma2_for(nq), Q.data_ptr(),
-                              device=device)
+    gen = H.generate_unit_queries_device if args.data == "unit" else H.generate_queries_device
+    gen(QUERY_SEED + offset, X.data_ptr(), args.n, args.L, sigma2_for(nq, levels=levels_of(args)), Q.data_ptr(),
+        device=device)
     torch.cuda.synchronize()
     return Q
+
+
+def levels_of(args):
+    return tuple(float(x) for x in args.sigma2.split(","))
+
+
+def ks_of(args):
+    return tuple(int(x) for x in args.ks.split(","))
 
 
 def make_batches(args, torch, H, X, nbatches, device, offset):
@@ -203,14 +222,16 @@ def make_batches(args, torch, H, X, nbatches, device, offset):
     nb = args.batch
     nf = int(round(nb * args.fresh_frac))
     Q = torch.empty((nbatches, nb, args.L), dtype=torch.float32, device=device)
+    gen = H.generate_unit_queries_device if args.data == "unit" else H.generate_queries_device
+    fresh = H.generate_unit_vectors_device if args.data == "unit" else H.generate_walks_device
     for i in range(nbatches):
-        H.generate_queries_device(QUERY_SEED + offset + i, X.data_ptr(), args.n, args.L, sigma2_for(nb - nf),
-                                  Q[i].data_ptr(), device=device)
+        gen(QUERY_SEED + offset + i, X.data_ptr(), args.n, args.L, sigma2_for(nb - nf, levels=levels_of(args)),
+            Q[i].data_ptr(), device=device)
         if nf:
-            H.generate_walks_device(FRESH_SEED + offset, nf, args.L, Q[i, nb - nf:].data_ptr(),
-                                    first=(offset + i) * nf, device=device)
+            fresh(FRESH_SEED + offset, nf, args.L, Q[i, nb - nf:].data_ptr(), first=(offset + i) * nf, device=device)
     torch.cuda.synchronize()
-    ks = np.array(K_CYCLE, np.uint32)[np.arange(nb) % len(K_CYCLE)]
+    kc = ks_of(args)
+    ks = np.array(kc, np.uint32)[np.arange(nb) % len(kc)]
     return Q, ks
 
 
@@ -386,11 +407,16 @@ def main():
         "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "bf16 filter (fp32 accumulate) + f32 exact re-rank",
         "data": "synthetic (seeded z-normalised random walks; noisy and fresh queries)",
-        "config": {"workload": "batched exact k-NN, %d x %d float32, leaf %d, %d queries/step, k cycling 1/10/100, "
-                               "sigma2 thirds 0.01/0.1/1.0 + %d%% fresh walks"
-                               % (args.n, args.L, args.leaf, nb, int(round(100 * args.fresh_frac))),
-                   "n": args.n, "L": args.L, "leaf_size": args.leaf, "queries_per_step": nb, "k": list(K_CYCLE),
-                   "l2": "inputs (25.6 GB f32 + 12.8 GB bf16) larger than L2; no flush needed",
+        "config": {"workload": "batched exact k-NN, %d x %d float32 %s, leaf %d, %d queries/step, k cycling %s, "
+                               "sigma2 in equal shares %s + %d%% fresh %s"
+                               % (args.n, args.L, "z-normalised random walks" if args.data == "walks" else
+                                  "unit-normalised Gaussian vectors", args.leaf, nb, "/".join(map(str, ks_of(args))),
+                                  "/".join(map(str, levels_of(args))), int(round(100 * args.fresh_frac)),
+                                  "walks" if args.data == "walks" else "vectors"),
+                   "n": args.n, "L": args.L, "leaf_size": args.leaf, "queries_per_step": nb, "k": list(ks_of(args)),
+                   "data": args.data,
+                   "l2": "inputs (%.1f GB f32 + %.1f GB bf16) larger than L2; no flush needed"
+              % (args.n * args.L * 4 / 1e9, args.n * args.L * 2 / 1e9),
                    "parallelism": "replica per GPU" if world > 1 else "single GPU",
                    "tuning": {k: tuning[k] for k in ("filter_tiles_per_item", "bound_tiles_per_item",
                                                      "rerank_blocks_per_sm", "approx_blocks_per_sm")},

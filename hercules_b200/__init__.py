@@ -110,6 +110,10 @@ _SIGS = [
                                          ctypes.c_int, ctypes.c_int]),
     ("hg_generate_queries", ctypes.c_int, [ctypes.c_uint64, _P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
                                            _P, _P, _P, ctypes.c_int, ctypes.c_int]),
+    ("hg_generate_unit_vectors", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
+                                                _P, ctypes.c_int, ctypes.c_int]),
+    ("hg_generate_unit_queries", ctypes.c_int, [ctypes.c_uint64, _P, ctypes.c_uint64, ctypes.c_uint32,
+                                                ctypes.c_uint32, _P, _P, _P, ctypes.c_int, ctypes.c_int]),
     ("hg_sax_breakpoints", ctypes.c_int, [_P]),
     ("hg_pscan_noalloc", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint32, _P, ctypes.c_uint32, _P, _P, _P]),
 ]
@@ -376,6 +380,32 @@ def generate_queries_device(seed, data_ptr, n, L, sigma2, out_ptr, base_ptr=None
     _check(lib().hg_generate_queries(seed, ctypes.c_void_p(data_ptr), n, L, s2.shape[0], _ptr(s2),
                                      ctypes.c_void_p(out_ptr), ctypes.c_void_p(base_ptr) if base_ptr else None,
                                      1, device))
+
+
+def generate_unit_vectors(seed, n, L, first=0):
+    """Host-side unit-normalised Gaussian rows (same bits as the GPU generator)."""
+    out = np.zeros((n, L), dtype=np.float32)
+    _check(lib().hg_generate_unit_vectors(seed, first, n, L, _ptr(out), 0, 0))
+    return out
+
+
+def generate_unit_vectors_device(seed, n, L, out_ptr, first=0, device=0):
+    _check(lib().hg_generate_unit_vectors(seed, first, n, L, ctypes.c_void_p(out_ptr), 1, device))
+
+
+def generate_unit_queries(seed, data, sigma2):
+    data = _f32(data)
+    n, L = data.shape
+    s2 = np.ascontiguousarray(sigma2, dtype=np.float64)
+    out = np.zeros((s2.shape[0], L), dtype=np.float32)
+    _check(lib().hg_generate_unit_queries(seed, _ptr(data), n, L, s2.shape[0], _ptr(s2), _ptr(out), None, 0, 0))
+    return out
+
+
+def generate_unit_queries_device(seed, data_ptr, n, L, sigma2, out_ptr, device=0):
+    s2 = np.ascontiguousarray(sigma2, dtype=np.float64)
+    _check(lib().hg_generate_unit_queries(seed, ctypes.c_void_p(data_ptr), n, L, s2.shape[0], _ptr(s2),
+                                          ctypes.c_void_p(out_ptr), None, 1, device))
 
 
 def sax_breakpoints():

@@ -155,6 +155,26 @@ HG_HD void random_walk(uint64_t seed, uint64_t id, int L, float* out) {
   znorm(out, L);
 }
 
+// L2 normalisation in float: sequential sum of squares, sqrt, divide.
+HG_HD void l2norm(float* v, int L) {
+  float ss = 0.0f;
+  for (int i = 0; i < L; ++i) ss = HG_FADD(ss, HG_FMUL(v[i], v[i]));
+  const float nrm = HG_FSQRT(ss);
+  if (nrm > 0.0f)
+    for (int i = 0; i < L; ++i) v[i] = HG_FDIV(v[i], nrm);
+}
+
+// Row `id` of the unit-normalised Gaussian stream `seed`: N(0, I) then L2
+// normalisation (the short-series vector shape; L a multiple of 4).
+HG_HD void gaussian_unit(uint64_t seed, uint64_t id, int L, float* out) {
+  for (int b = 0; b < L / 4; ++b) {
+    double z[4];
+    normal4(seed, id, (uint32_t)b, kTagWalk, z);
+    for (int j = 0; j < 4; ++j) out[4 * b + j] = (float)z[j];
+  }
+  l2norm(out, L);
+}
+
 // The dataset row a noisy query starts from.
 HG_HD uint64_t pick_row(uint64_t seed, uint64_t qid, uint64_t n) {
   uint32_t o[4];
@@ -165,14 +185,17 @@ HG_HD uint64_t pick_row(uint64_t seed, uint64_t qid, uint64_t n) {
 
 // Query `qid`: dataset row `base` plus N(0, sigma2) noise per point, then
 // z-normalised (the workload of the noisy-query configurations).
-HG_HD void noisy_query(uint64_t seed, uint64_t qid, const float* base, int L, double sigma2, float* out) {
+// unit = 1: L2-normalised instead (queries of the unit-vector shape).
+HG_HD void noisy_query(uint64_t seed, uint64_t qid, const float* base, int L, double sigma2, float* out,
+                       int unit = 0) {
   double sigma = HG_DSQRT(sigma2);
   for (int b = 0; b < L / 4; ++b) {
     double z[4];
     normal4(seed, qid, (uint32_t)b, kTagNoise, z);
     for (int j = 0; j < 4; ++j) out[4 * b + j] = HG_FADD(base[4 * b + j], (float)HG_DMUL(sigma, z[j]));
   }
-  znorm(out, L);
+  if (unit) l2norm(out, L);
+  else znorm(out, L);
 }
 
 }  // namespace hg

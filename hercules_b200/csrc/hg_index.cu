@@ -2108,21 +2108,25 @@ hg_status hg_leaf_lower_bounds(hg_index* ix, const float* query, float* lb_out) 
   return e == cudaSuccess ? HG_OK : cuda_fail(e, "hg_leaf_lower_bounds");
 }
 
-hg_status hg_generate_walks(uint64_t seed, uint64_t first, uint64_t n, uint32_t L, float* out, int on_device,
-                            int device) {
+static hg_status generate_rows(uint64_t seed, uint64_t first, uint64_t n, uint32_t L, float* out, int on_device,
+                               int device, int unit) {
   if (!out || L == 0 || L % 4 != 0) return set_error(HG_ERR_ARG, "hg_generate_walks: L must be a multiple of 4");
   if (on_device) {
     CK(cudaSetDevice(device));
-    CK(hg::launch_generate_walks(seed, first, n, (int)L, out, 0));
+    CK(hg::launch_generate_walks(seed, first, n, (int)L, out, 0, unit));
     CK(cudaStreamSynchronize(0));
     return HG_OK;
   }
-  parallel_for(n, [=](uint64_t i) { hg::random_walk(seed, first + i, (int)L, out + i * L); });
+  parallel_for(n, [=](uint64_t i) {
+    if (unit) hg::gaussian_unit(seed, first + i, (int)L, out + i * L);
+    else hg::random_walk(seed, first + i, (int)L, out + i * L);
+  });
   return HG_OK;
 }
 
-hg_status hg_generate_queries(uint64_t seed, const float* data, uint64_t n, uint32_t L, uint32_t nq,
-                              const double* sigma2, float* out, uint64_t* base_ids, int on_device, int device) {
+static hg_status generate_queries(uint64_t seed, const float* data, uint64_t n, uint32_t L, uint32_t nq,
+                                  const double* sigma2, float* out, uint64_t* base_ids, int on_device, int device,
+                                  int unit) {
   if (!data || !out || !sigma2 || n == 0 || L == 0 || L % 4 != 0)
     return set_error(HG_ERR_ARG, "hg_generate_queries: bad argument");
   if (on_device) {
@@ -2130,7 +2134,7 @@ hg_status hg_generate_queries(uint64_t seed, const float* data, uint64_t n, uint
     double* d_s = nullptr;
     CK(dalloc(&d_s, nq));
     cudaError_t e = cudaMemcpy(d_s, sigma2, sizeof(double) * nq, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = hg::launch_generate_queries(seed, data, n, (int)L, (int)nq, d_s, out, base_ids, 0);
+    if (e == cudaSuccess) e = hg::launch_generate_queries(seed, data, n, (int)L, (int)nq, d_s, out, base_ids, 0, unit);
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     cudaFree(d_s);
     return e == cudaSuccess ? HG_OK : cuda_fail(e, "hg_generate_queries");
@@ -2138,9 +2142,29 @@ hg_status hg_generate_queries(uint64_t seed, const float* data, uint64_t n, uint
   parallel_for(nq, [=](uint64_t j) {
     const uint64_t b = hg::pick_row(seed, j, n);
     if (base_ids) base_ids[j] = b;
-    hg::noisy_query(seed, j, data + b * L, (int)L, sigma2[j], out + j * L);
+    hg::noisy_query(seed, j, data + b * L, (int)L, sigma2[j], out + j * L, unit);
   });
   return HG_OK;
+}
+
+hg_status hg_generate_walks(uint64_t seed, uint64_t first, uint64_t n, uint32_t L, float* out, int on_device,
+                            int device) {
+  return generate_rows(seed, first, n, L, out, on_device, device, 0);
+}
+
+hg_status hg_generate_queries(uint64_t seed, const float* data, uint64_t n, uint32_t L, uint32_t nq,
+                              const double* sigma2, float* out, uint64_t* base_ids, int on_device, int device) {
+  return generate_queries(seed, data, n, L, nq, sigma2, out, base_ids, on_device, device, 0);
+}
+
+hg_status hg_generate_unit_vectors(uint64_t seed, uint64_t first, uint64_t n, uint32_t L, float* out, int on_device,
+                                   int device) {
+  return generate_rows(seed, first, n, L, out, on_device, device, 1);
+}
+
+hg_status hg_generate_unit_queries(uint64_t seed, const float* data, uint64_t n, uint32_t L, uint32_t nq,
+                                   const double* sigma2, float* out, uint64_t* base_ids, int on_device, int device) {
+  return generate_queries(seed, data, n, L, nq, sigma2, out, base_ids, on_device, device, 1);
 }
 
 hg_status hg_sax_breakpoints(float* out255) {

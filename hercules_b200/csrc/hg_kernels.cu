@@ -835,20 +835,21 @@ __global__ void k_emit(const unsigned long long* topk, const int* topk_count, in
 // data generation
 // ---------------------------------------------------------------------------
 
-__global__ void k_generate_walks(uint64_t seed, uint64_t first, uint64_t n, int L, float* out) {
+__global__ void k_generate_walks(uint64_t seed, uint64_t first, uint64_t n, int L, float* out, int unit) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   // each thread writes its own row; the L2 merges the partial sectors
-  random_walk(seed, first + i, L, out + i * (uint64_t)L);
+  if (unit) gaussian_unit(seed, first + i, L, out + i * (uint64_t)L);
+  else random_walk(seed, first + i, L, out + i * (uint64_t)L);
 }
 
 __global__ void k_generate_queries(uint64_t seed, const float* data, uint64_t n, int L, int nq,
-                                   const double* sigma2, float* out, uint64_t* base_ids) {
+                                   const double* sigma2, float* out, uint64_t* base_ids, int unit) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nq) return;
   const uint64_t b = pick_row(seed, (uint64_t)j, n);
   if (base_ids) base_ids[j] = b;
-  noisy_query(seed, (uint64_t)j, data + b * (uint64_t)L, L, sigma2[j], out + (uint64_t)j * L);
+  noisy_query(seed, (uint64_t)j, data + b * (uint64_t)L, L, sigma2[j], out + (uint64_t)j * L, unit);
 }
 
 // ---------------------------------------------------------------------------
@@ -994,16 +995,16 @@ cudaError_t launch_emit(const unsigned long long* topk, const int* topk_count, i
 }
 
 cudaError_t launch_generate_walks(uint64_t seed, uint64_t first, uint64_t n, int L, float* out,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, int unit) {
   if (!n) return cudaSuccess;
-  k_generate_walks<<<blocks_for(n, 128), 128, 0, s>>>(seed, first, n, L, out);
+  k_generate_walks<<<blocks_for(n, 128), 128, 0, s>>>(seed, first, n, L, out, unit);
   return cudaGetLastError();
 }
 
 cudaError_t launch_generate_queries(uint64_t seed, const float* data, uint64_t n, int L, int nq,
-                                    const double* sigma2, float* out, uint64_t* base_ids, cudaStream_t s) {
+                                    const double* sigma2, float* out, uint64_t* base_ids, cudaStream_t s, int unit) {
   if (!nq) return cudaSuccess;
-  k_generate_queries<<<blocks_for(nq, 64), 64, 0, s>>>(seed, data, n, L, nq, sigma2, out, base_ids);
+  k_generate_queries<<<blocks_for(nq, 64), 64, 0, s>>>(seed, data, n, L, nq, sigma2, out, base_ids, unit);
   return cudaGetLastError();
 }
 

@@ -109,9 +109,11 @@ cudaError_t launch_emit(const unsigned long long* topk, const int* topk_count, i
                         int64_t* id_out, cudaStream_t s);
 
 // data
+// unit = 1: unit-normalised Gaussian rows / L2-normalised noisy queries
 cudaError_t launch_generate_walks(uint64_t seed, uint64_t first, uint64_t n, int L, float* out,
-                                  cudaStream_t s);
+                                  cudaStream_t s, int unit = 0);
 cudaError_t launch_generate_queries(uint64_t seed, const float* data, uint64_t n, int L, int nq,
-                                    const double* sigma2, float* out, uint64_t* base_ids, cudaStream_t s);
+                                    const double* sigma2, float* out, uint64_t* base_ids, cudaStream_t s,
+                                    int unit = 0);
 
 }  // namespace hg

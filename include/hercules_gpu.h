@@ -262,6 +262,19 @@ HG_API hg_status hg_generate_queries(uint64_t seed, const float *data, uint64_t 
                               uint32_t nq, const double *sigma2, float *out, uint64_t *base_ids,
                               int on_device, int device);
 
+/* Unit vectors: rows [first, first+n) of stream `seed`, each N(0, I) (the
+ * same Philox + Box-Muller draws) then L2-normalised in float -- the
+ * short-series vector shape of the benchmark configurations (no reference
+ * counterpart: the reference generator makes random walks only). */
+HG_API hg_status hg_generate_unit_vectors(uint64_t seed, uint64_t first, uint64_t n, uint32_t L, float *out,
+                                          int out_on_device, int device);
+
+/* hg_generate_queries for unit vectors: row pick(j) plus N(0, sigma2[j])
+ * noise, then L2-normalised. */
+HG_API hg_status hg_generate_unit_queries(uint64_t seed, const float *data, uint64_t n, uint32_t L, uint32_t nq,
+                                          const double *sigma2, float *out, uint64_t *base_ids, int on_device,
+                                          int device);
+
 /* The 255 iSAX breakpoints of cardinality 256 used by this library. */
 HG_API hg_status hg_sax_breakpoints(float *out255);
 

@@ -155,3 +155,17 @@ def test_autotune_keeps_answers(mid):
     with pytest.raises(Exception):
         ix.set_tuning(filter_tiles_per_item=3)
     ix.set_tuning(filter_tiles_per_item=32, bound_tiles_per_item=8, rerank_blocks_per_sm=8, approx_blocks_per_sm=2)
+
+
+def test_batch_unit_vectors(hg, gpu_available, oracle_mod):
+    """Unit-normalised Gaussian vectors (norms 1, not sqrt(L)): the batched
+    answers equal the plain path's and the oracle's."""
+    X = hg.generate_unit_vectors(91, 60_000, 96)
+    Q = hg.generate_unit_queries(92, X, np.full(40, 0.1))
+    ix = hg.HerculesIndex.build(X, 5_000)
+    ks = np.array([1, 10, 100, 10] * 10, np.uint32)
+    d, ids, st = ix.knn_batch(Q, ks, stats=True)
+    same_as_plain(ix, Q, ks, d, ids)
+    assert st["fallback_queries"] <= 4, st
+    od, oid = oracle_mod.pscan(X, Q[1], 10)
+    assert np.array_equal(bits(d[1, :10]), bits(od)) and np.array_equal(ids[1, :10], oid)

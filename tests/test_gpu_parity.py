@@ -229,3 +229,18 @@ def test_cli_is_a_drop_in_for_the_reference_cli(hg, tmp_path, gpu_available):
         for r_ in range(g["k"]):
             assert got[("Query_exact_distance", j + 1, r_ + 1)] == g["answers"]["exact_distance"][j][r_]
             assert got[("Query_exact_node_file_pos", j + 1, r_ + 1)] == g["answers"]["exact_node_file_pos"][j][r_]
+
+
+def test_device_unit_generator_matches_host(hg, gpu_available):
+    import torch
+    n, L = 500, 96
+    t = torch.empty((n, L), dtype=torch.float32, device="cuda")
+    hg.generate_unit_vectors_device(77, n, L, t.data_ptr())
+    torch.cuda.synchronize()
+    host = hg.generate_unit_vectors(77, n, L)
+    assert np.array_equal(t.cpu().numpy().view(np.uint32), host.view(np.uint32))
+    sig = np.full(12, 0.1)
+    qd = torch.empty((12, L), dtype=torch.float32, device="cuda")
+    hg.generate_unit_queries_device(8, t.data_ptr(), n, L, sig, qd.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(qd.cpu().numpy().view(np.uint32), hg.generate_unit_queries(8, host, sig).view(np.uint32))
