@@ -1023,7 +1023,7 @@ static hg_status ensure_scratch(hg_index* ix, int k) {
   dfree(s.err);
   dfree(s.list);
   dfree(s.counters);
-  s.nparts = hg::sm_count(ix->device) * hg::kEdBlocksPerSm * hg::kEdWarps;
+  s.nparts = hg::sm_count(ix->device) * hg::ed_blocks_per_sm((int)ix->L) * hg::kEdWarps;
   CK(dalloc(&s.lb, nl));
   CK(dalloc(&s.list, ix->n));
   CK(dalloc(&s.counters, 8));
@@ -1097,7 +1097,7 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
   hg::DeviceIndex& d = ix->d;
   const int nl = (int)ix->leaves.size();
   const int sms = hg::sm_count(ix->device);
-  const int ed_blocks = sms * hg::kEdBlocksPerSm;
+  const int ed_blocks = sms * hg::ed_blocks_per_sm((int)ix->L);
   hg::EdArgs e{};
   e.rows = d.rows;
   e.ids = d.ids;
@@ -1373,11 +1373,6 @@ static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket
 static void filter_coefficients(uint32_t L, float* c_acc, float* c_sq) {
   *c_acc = std::nextafter((float)(L * std::ldexp(1.0, -20)), INFINITY);
   *c_sq = std::nextafter((float)((L / 8.0 + 16.0) * std::ldexp(1.0, -22)), INFINITY);
-}
-
-static hg_status record(cudaEvent_t e, cudaStream_t st) {
-  CK(cudaEventRecord(e, st));
-  return HG_OK;
 }
 
 // Bound-pass plan of every leaf for `want` candidate rows per query: slots

@@ -565,14 +565,21 @@ __device__ __forceinline__ int q4_index(int chunk, int half) {
 // bytes of that layout for a series of L floats
 __host__ __device__ inline size_t q4_bytes(int L) { return (size_t)((L / 8 + 31) / 32) * 40 * 2 * 16; }
 // kRowIds: the id of a row is its row index (a matrix without an id map).
-// kLines: 128-byte lines of a row in flight per slot and step
-template <bool kRowIds, int kLines>
-__global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 1 : 4) k_ed_stream(EdArgs a) {
+// kSlot: lanes per row (a slot); kLines: 32-byte chunks per lane of a row in
+// flight per step, so a slot reads kSlot * kLines * 32 bytes of its row per
+// step.  Short series use 4-lane slots (8 rows per warp, 128-byte lines);
+// long series, few candidate rows per query, use wider slots.
+template <int kSlot>
+__host__ __device__ constexpr uint32_t slot_leaders() {
+  return kSlot == 32 ? 0x1u : (kSlot == 16 ? 0x10001u : (kSlot == 8 ? 0x01010101u : 0x11111111u));
+}
+template <bool kRowIds, int kLines, int kSlot>
+__global__ void __launch_bounds__(kEdThreads, 4) k_ed_stream(EdArgs a) {
   constexpr int W = kEdThreads / 32;
   __shared__ unsigned long long lists[W][kWarpListCap];
   extern __shared__ float4 qs4[];  // the query, q4_bytes(L) bytes
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int slot_lead = lane & ~3, j = lane & 3;
+  const int slot_lead = lane & ~(kSlot - 1), j = lane & (kSlot - 1);
   unsigned long long* list = lists[wib];
   for (int i = lane; i < kWarpListCap; i += 32) list[i] = ~0ull;
   for (int i = threadIdx.x; i < (a.L >> 2); i += blockDim.x)
@@ -592,17 +599,19 @@ __global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 1 : 4) k_ed_stream(Ed
   }
   const uint32_t nwarps = gridDim.x * W;
   const uint32_t gw = blockIdx.x * W + wib;
-  const uint32_t lt = (1u << lane) - 1;
-  const uint32_t leaders = 0x11111111u;
-  // batch b of this warp covers entries [(gw + b * nwarps) * 32, +32)
+  const uint32_t leaders = slot_leaders<kSlot>();
+  // batch b of this warp covers entries [(gw + b * nwarps) * bs, +bs): bs
+  // spreads a short list over all warps (a few long rows keep every warp busy)
+  const uint32_t per_warp = (uint32_t)(((uint64_t)total + nwarps - 1) / nwarps);
+  const uint32_t bs = per_warp < 1u ? 1u : (per_warp > 32u ? 32u : per_warp);
   auto entry = [&](uint32_t batch) -> uint32_t {
-    const uint64_t idx = (uint64_t)batch * 32 + lane;
-    if (idx >= total) return 0xffffffffu;
+    const uint64_t idx = (uint64_t)batch * bs + lane;
+    if ((uint32_t)lane >= bs || idx >= total) return 0xffffffffu;
     return a.list ? a.list[idx] : (uint32_t)(first + idx);
   };
   auto count_of = [&](uint32_t batch) -> uint32_t {
-    const uint64_t b0 = (uint64_t)batch * 32;
-    return b0 < total ? (uint32_t)(total - b0 < 32 ? total - b0 : 32) : 0u;
+    const uint64_t b0 = (uint64_t)batch * bs;
+    return b0 < total ? (uint32_t)(total - b0 < bs ? total - b0 : bs) : 0u;
   };
   uint32_t batch = gw;
   uint32_t cur = entry(batch);  // lane i holds entry i of the current batch
@@ -655,7 +664,7 @@ __global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 1 : 4) k_ed_stream(Ed
     float4 xv[kLines][2];
 #pragma unroll
     for (int l = 0; l < kLines; ++l) {
-      const int c = ch + 4 * l + j;
+      const int c = ch + kSlot * l + j;
       if (valid && c < nch) {
         xv[l][0] = __ldcs(x + 2 * c);
         xv[l][1] = __ldcs(x + 2 * c + 1);
@@ -666,7 +675,7 @@ __global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 1 : 4) k_ed_stream(Ed
     float dl[kLines];
 #pragma unroll
     for (int l = 0; l < kLines; ++l) {
-      const int c = ch + 4 * l + j;
+      const int c = ch + kSlot * l + j;
       dl[l] = 0.0f;
       if (valid && c < nch) {
         const float4 q0 = qs4[q4_index(c, 0)], q1 = qs4[q4_index(c, 1)];
@@ -678,8 +687,8 @@ __global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 1 : 4) k_ed_stream(Ed
     }
     bool finished = false;
 #pragma unroll
-    for (int t = 0; t < 4 * kLines; ++t) {
-      const float dt = __shfl_sync(HG_FULL, dl[t >> 2], slot_lead + (t & 3));
+    for (int t = 0; t < kSlot * kLines; ++t) {
+      const float dt = __shfl_sync(HG_FULL, dl[t / kSlot], slot_lead + (t % kSlot));
       if (valid && ch + t < nch) {
         dist = __fadd_rn(dist, dt);
         if (j == 0) ++n_chunks;
@@ -687,7 +696,7 @@ __global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 1 : 4) k_ed_stream(Ed
       }
     }
     if (valid) {
-      ch += 4 * kLines;
+      ch += kSlot * kLines;
       if (ch >= nch) {
         finished = true;
         valid = false;
@@ -958,21 +967,37 @@ cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s)
   return cudaGetLastError();
 }
 
-template <bool kRowIds, int kLines>
+template <bool kRowIds, int kLines, int kSlot>
 static cudaError_t launch_ed(const EdArgs& a, int blocks, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
-    const cudaError_t e = cudaFuncSetAttribute(k_ed_stream<kRowIds, kLines>,
+    const cudaError_t e = cudaFuncSetAttribute(k_ed_stream<kRowIds, kLines, kSlot>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q4_bytes(16384));
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k_ed_stream<kRowIds, kLines><<<blocks, kEdThreads, q4_bytes(a.L), s>>>(a);
+  k_ed_stream<kRowIds, kLines, kSlot><<<blocks, kEdThreads, q4_bytes(a.L), s>>>(a);
   return cudaGetLastError();
 }
-cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s) { return launch_ed<false, 2>(a, blocks, s); }
+// long series (L >= 4096): few candidate rows per query, each long, so
+// more lanes per row keep more of each row in flight
+#ifndef HG_ED_LONG_LINES
+#define HG_ED_LONG_LINES 2
+#endif
+#ifndef HG_ED_LONG_SLOT
+#define HG_ED_LONG_SLOT 8
+#endif
+cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s) {
+  return a.L >= 4096 ? launch_ed<false, HG_ED_LONG_LINES, HG_ED_LONG_SLOT>(a, blocks, s) : launch_ed<false, 2, 4>(a, blocks, s);
+}
 cudaError_t launch_ed_stream_row_ids(const EdArgs& a, int blocks, cudaStream_t s) {
-  return launch_ed<true, 2>(a, blocks, s);
+  return a.L >= 4096 ? launch_ed<true, HG_ED_LONG_LINES, HG_ED_LONG_SLOT>(a, blocks, s) : launch_ed<true, 2, 4>(a, blocks, s);
+}
+int ed_blocks_per_sm(int L) {
+  // shared memory per block: the staged query + 8 per-warp lists of 2 KB
+  const size_t per_block = q4_bytes(L) + (size_t)kEdWarps * kWarpListCap * 8 + 1024;
+  const int fit = (int)((size_t)227 * 1024 / per_block);
+  return fit < 1 ? 1 : (fit < kEdBlocksPerSm ? fit : kEdBlocksPerSm);
 }
 
 cudaError_t launch_merge(const unsigned long long* parts, const int* part_count, int nparts, int k,

@@ -100,6 +100,8 @@ cudaError_t launch_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_pr
                               int* topk_count, uint32_t* counters, cudaStream_t s);
 cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s);
 cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s);
+// resident blocks per SM of the distance stream for series length L
+int ed_blocks_per_sm(int L);
 // the same with id = row index (EdArgs::ids unused)
 cudaError_t launch_ed_stream_row_ids(const EdArgs& a, int blocks, cudaStream_t s);
 cudaError_t launch_merge(const unsigned long long* parts, const int* part_count, int nparts, int k,

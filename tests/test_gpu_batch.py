@@ -114,7 +114,7 @@ def test_batch_reference_configs(hg, gpu_available, name):
         same_as_plain(ix, Q, np.full(len(Q), k), d, ids)
 
 
-@pytest.mark.parametrize("L,n,leaf", [(16, 3000, 100), (1024, 6000, 500)])
+@pytest.mark.parametrize("L,n,leaf", [(16, 3000, 100), (1024, 6000, 500), (4096, 3000, 300), (16384, 1000, 100)])
 def test_batch_other_lengths(hg, gpu_available, L, n, leaf):
     X = hg.generate_walks(51, n, L)
     Q = hg.generate_queries(52, X, np.array([0.01, 0.1, 1.0] * 4))

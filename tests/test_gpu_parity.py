@@ -183,19 +183,22 @@ def test_edge_cases(hg, oracle_mod, gpu_available):
     assert np.array_equal(bits(d[0][ok]), bits(od[:43]))
 
 
-@pytest.mark.parametrize("L,n,leaf", [(16, 3000, 100), (1024, 3000, 250)])
+@pytest.mark.parametrize("L,n,leaf", [(16, 3000, 100), (1024, 3000, 250), (4096, 2000, 200), (16384, 800, 100)])
 def test_other_lengths(hg, oracle_mod, gpu_available, L, n, leaf):
+    """Short and long series (L >= 4096 runs the distance stream with 8-lane
+    slots, each list spread over every warp)."""
     X = hg.generate_walks(51, n, L)
-    Q = hg.generate_queries(52, X, np.array([0.01, 0.1, 1.0]))
+    Q = hg.generate_queries(52, X, np.array([0.01, 0.1, 1.0] * 3))
     ix = hg.HerculesIndex.build(X, leaf)
     oi = oracle_mod.OracleIndex.build(X, leaf)
     assert ix.leaves() == oi.leaves()
     ids_map = oi.row_ids()
-    d, ids = ix.knn(Q, 10, use_lb_sax=True)
-    for j, q in enumerate(Q):
-        od, orow, _, _ = oi.knn(q, 10)
-        assert np.array_equal(bits(d[j]), bits(od))
-        assert np.array_equal(ids[j], ids_map[orow])
+    for k, lbsax in ((10, True), (1, False), (100, True)):
+        d, ids = ix.knn(Q, k, use_lb_sax=lbsax)
+        for j, q in enumerate(Q):
+            od, orow, _, _ = oi.knn(q, k)
+            assert np.array_equal(bits(d[j]), bits(od)), (k, j)
+            assert np.array_equal(ids[j], ids_map[orow]), (k, j)
 
 
 def test_cli_is_a_drop_in_for_the_reference_cli(hg, tmp_path, gpu_available):
