@@ -1997,8 +1997,8 @@ hg_status hg_tuning_set(hg_index* ix, const hg_tuning* t) {
 
 // Coordinate descent over the launch parameters: each parameter in turn takes
 // every candidate value with the others fixed, timed on the caller's queries
-// (the batched path's phases by their own CUDA events; the plain path on up to
-// 64 of the queries); the fastest value stays.
+// (the batched call's device time from its %globaltimer stamps; the plain path
+// on up to 64 of the queries, k <= 10); the fastest of two runs per value stays.
 hg_status hg_autotune(hg_index* ix, const float* d_queries, uint32_t nq, const uint32_t* ks, uint32_t kmax,
                       void* stream, hg_tuning* out) {
   if (!ix || !d_queries || nq == 0 || kmax == 0) return set_error(HG_ERR_ARG, "hg_autotune: bad argument");
