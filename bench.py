@@ -235,6 +235,56 @@ def make_batches(args, torch, H, X, nbatches, device, offset):
     return Q, ks
 
 
+def fp64_oracle_check(args, torch, H, Q, ks, D, I, device, nsample=32):
+    """FP64 brute force over the whole collection (regenerated chunk by chunk
+    from the same seed) for the first nsample queries of a timed batch:
+    recall of the returned ids against the FP64 k nearest, and the relative
+    error of the returned FP32 distances against the FP64 distances of the
+    same rows."""
+    s = min(nsample, Q.shape[0])
+    n, L = args.n, args.L
+    q = Q[:s].double()
+    kq = torch.as_tensor(ks[:s].astype(np.int64), device=q.device)
+    kmax = int(kq.max())
+    ours = I[:s, :kmax]
+    ours_d = D[:s, :kmax].double()
+    gen = H.generate_unit_vectors_device if args.data == "unit" else H.generate_walks_device
+    chunk = max(1, min(n, (1 << 28) // L))
+    buf = torch.empty((chunk, L), dtype=torch.float32, device=device)
+    best_d = torch.full((s, kmax), float("inf"), dtype=torch.float64, device=device)
+    best_i = torch.full((s, kmax), -1, dtype=torch.int64, device=device)
+    d64_ours = torch.full((s, kmax), float("nan"), dtype=torch.float64, device=device)
+    qn = (q * q).sum(1)
+    for first in range(0, n, chunk):
+        m = min(chunk, n - first)
+        gen(DATA_SEED, m, L, buf.data_ptr(), first=first, device=device)
+        x = buf[:m].double()
+        d = (qn[:, None] + (x * x).sum(1)[None, :] - 2.0 * (q @ x.T)).clamp_min_(0.0)
+        ids = torch.arange(first, first + m, device=device)
+        cd = torch.cat([best_d, d], 1)
+        ci = torch.cat([best_i, ids[None, :].expand(s, m)], 1)
+        best_d, pos = torch.topk(cd, kmax, dim=1, largest=False, sorted=True)
+        best_i = torch.gather(ci, 1, pos)
+        inside = (ours >= first) & (ours < first + m)
+        if inside.any():
+            rr, cc = inside.nonzero(as_tuple=True)
+            d64_ours[rr, cc] = d[rr, ours[rr, cc] - first]
+    torch.cuda.synchronize()
+    hits, total, max_rel = 0, 0, 0.0
+    for j in range(s):
+        k = int(kq[j])
+        a = set(ours[j, :k].tolist())
+        b = set(best_i[j, :k].tolist())
+        hits += len(a & b)
+        total += k
+        d64 = d64_ours[j, :k]
+        rel = ((ours_d[j, :k] - d64).abs() / d64.clamp_min(1e-30)).max()
+        max_rel = max(max_rel, float(rel))
+    return {"queries": s, "pairs": total, "recall_vs_fp64_topk": round(hits / max(total, 1), 6),
+            "max_rel_err_vs_fp64": max_rel,
+            "how": "FP64 brute force over all %d rows, regenerated from the data seed in chunks" % n}
+
+
 def cpu_reference_run(args, index_dir, queries_host, threads, extra=(), k=10):
     """Runs the reference CLI over the written index; per-query seconds from
     its own Query_total_time_secs lines."""
@@ -326,6 +376,7 @@ def main():
         st = batch_step(i)
         for kk, v in st.items():
             agg[kk] = agg.get(kk, 0) + v
+        agg["err_max_max"] = max(agg.get("err_max_max", 0.0), st["err_max"])
     e1.record()
     torch.cuda.synchronize()
     ck = clocks.stop()
@@ -347,6 +398,9 @@ def main():
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, device=torch.device("cuda", device))
     e2e_value = total_q / e2e_s
+
+    # answers of the last timed batch against an FP64 brute force
+    fp64 = fp64_oracle_check(args, torch, H, Qb[warm + steps - 1], ks, D, I, device)
 
     # the plain per-query path on the same collection, every scan launch timed
     pk = args.plain_k
@@ -431,6 +485,11 @@ def main():
                   "batched_over_plain": round(value / plain_qps, 2) if plain_qps > 0 else None},
         "cpu_baseline": cpu_baseline,
         "clocks": ck,
+        "certified_bound": {"err_mean": agg["err_mean"] / steps, "err_max": agg["err_max_max"],
+                            "err_over_bound_mean": agg["err_over_bound"] / steps,
+                            "what": "err(q, work item) of the filter pass over every row: "
+                                    "d~ - err <= B_q keeps every row within B_q"},
+        "fp64_oracle": fp64,
         "stats": {"survivors_per_query": agg["survivors"] / (nb * steps),
                   "survivor_fraction": agg["survivors"] / max(agg["bf16_pairs"], 1),
                   "rerank_rows_per_query": agg["rows_visited"] / (nb * steps),

@@ -343,6 +343,7 @@ static void free_device(hg_index* ix) {
   dfree(b.item_off);
   if (b.graph) cudaGraphExecDestroy(b.graph);
   dfree(b.stamps);
+  dfree(b.errstat);
   b = hg::BatchScratch{};
 }
 
@@ -1514,6 +1515,8 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
     g.qperm = round == 0 ? b.qperm : list_in;
     g.nq_dev = n_dev;
     g.qtile = round == 0 ? hg::kBatchQueryTile : 0;
+    g.errstat = round == 0 ? b.errstat : nullptr;
+    if (round == 0) CK(cudaMemsetAsync(b.errstat, 0, 5 * sizeof(double), st));
     CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
     CK(cudaMemsetAsync(b.heads + 1, 0, sizeof(uint32_t), st));
     CK(stamp(2 + 3 * round));
@@ -1578,6 +1581,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   if (!b.ctrl) {
     CK(dalloc(&b.ctrl, 16));
     CK(dalloc(&b.stamps, 16));
+    CK(dalloc(&b.errstat, 5));
   }
   if (!b.qlist2 || !b.qin || b.out_kmax < kmax) {
     dfree(b.qlist2);
@@ -1626,7 +1630,9 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   unsigned long long hs[8], ts[16];
   uint32_t ctrl[16];
   uint32_t dev_err = 0;
+  double es[5];
   CK(cudaMemcpyAsync(ts, b.stamps, sizeof ts, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(es, b.errstat, sizeof es, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(hs, b.stats, sizeof hs, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(ctrl, b.ctrl, sizeof ctrl, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(&dev_err, b.heads + 3, sizeof dev_err, cudaMemcpyDeviceToHost, st));
@@ -1696,6 +1702,9 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     stats->fallback_ms = fallbacks ? tf : 0.0;
     stats->device_ms = t0e;
     stats->kernel_launches = launches + (data_built ? 2 : 0) + 9 * fallbacks;
+    stats->err_mean = es[2] > 0 ? es[0] / es[2] : 0.0;
+    stats->err_max = es[4];
+    stats->err_over_bound = es[3] > 0 ? es[1] / es[3] : 0.0;
   }
   cudaEventDestroy(fb0);
   cudaEventDestroy(fb1);

@@ -132,6 +132,7 @@ struct BatchScratch {
   uint64_t graph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   uint64_t graph_launches = 0;   // kernels in the captured pipeline
   unsigned long long* stamps = nullptr;  // [16] global-timer stamps at the phase boundaries
+  double* errstat = nullptr;             // [5] certified bounds of the first filter pass (BatchGemm::errstat)
 };
 
 }  // namespace hg

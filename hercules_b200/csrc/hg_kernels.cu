@@ -574,7 +574,7 @@ __host__ __device__ constexpr uint32_t slot_leaders() {
   return kSlot == 32 ? 0x1u : (kSlot == 16 ? 0x10001u : (kSlot == 8 ? 0x01010101u : 0x11111111u));
 }
 template <bool kRowIds, int kLines, int kSlot>
-__global__ void __launch_bounds__(kEdThreads, 4) k_ed_stream(EdArgs a) {
+__global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 3 : 4) k_ed_stream(EdArgs a) {
   constexpr int W = kEdThreads / 32;
   __shared__ unsigned long long lists[W][kWarpListCap];
   extern __shared__ float4 qs4[];  // the query, q4_bytes(L) bytes
@@ -626,9 +626,19 @@ __global__ void __launch_bounds__(kEdThreads, 4) k_ed_stream(EdArgs a) {
   float B = __int_as_float((int)ld_volatile(a.bound));
   bool valid = false;  // slot-uniform
   uint32_t row = 0;
-  int ch = 0;
+  int ch = 0;  // a multiple of kStep: the query offsets below stay inside one 32-chunk group
   float dist = 0.0f;
-  unsigned long long n_chunks = 0, n_done = 0, n_rows = 0;
+  const float4* x = nullptr;
+  uint32_t n_chunks = 0, n_done = 0, n_rows = 0;  // this lane's (slot leaders only)
+  constexpr int kStep = kSlot * kLines;  // chunks of a row per step
+  static_assert(32 % kStep == 0, "a step stays inside one 32-chunk group of the staged query");
+  // staged-query float4 index of chunk ch + kSlot l + j: base(ch) + qoff[l]
+  int qoff[kLines];
+#pragma unroll
+  for (int l = 0; l < kLines; ++l) {
+    const int o = kSlot * l + j;
+    qoff[l] = 2 * (o + (o >> 2));
+  }
   for (int iter = 1;; ++iter) {
     // refill the slots without a row
     uint32_t need = __ballot_sync(HG_FULL, !valid) & leaders;
@@ -651,6 +661,7 @@ __global__ void __launch_bounds__(kEdThreads, 4) k_ed_stream(EdArgs a) {
         valid = true;
         dist = 0.0f;
         ch = 0;
+        x = reinterpret_cast<const float4*>(a.rows + (uint64_t)row * a.L) + 2 * j;
         if (j == 0) ++n_rows;
       }
       cur_used += take;
@@ -658,51 +669,68 @@ __global__ void __launch_bounds__(kEdThreads, 4) k_ed_stream(EdArgs a) {
     }
     if (!__any_sync(HG_FULL, valid)) break;
     const uint32_t bnext = ((iter & 7) == 0) ? ld_volatile(a.bound) : 0x7f800000u;
-    // kLines lines of every owned row in flight: lane j computes chunks
-    // ch + 4 l + j (l < kLines); the slot adds them in order
-    const float4* x = reinterpret_cast<const float4*>(a.rows + (uint64_t)row * a.L);
+    // kLines chunks of every owned row in flight: lane j computes chunks
+    // ch + kSlot l + j (l < kLines); chunks past the row's end count as 0
     float4 xv[kLines][2];
+    bool in[kLines];
 #pragma unroll
     for (int l = 0; l < kLines; ++l) {
-      const int c = ch + kSlot * l + j;
-      if (valid && c < nch) {
-        xv[l][0] = __ldcs(x + 2 * c);
-        xv[l][1] = __ldcs(x + 2 * c + 1);
-      } else {
-        xv[l][0] = xv[l][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+      in[l] = valid && ch + kSlot * l + j < nch;
+      if (in[l]) {
+        xv[l][0] = __ldcs(x + 2 * kSlot * l);
+        xv[l][1] = __ldcs(x + 2 * kSlot * l + 1);
       }
     }
+    // a slot without a row (its ch may equal nch) reads the first chunks:
+    // every index stays inside the staged query
+    const int cq = valid ? ch : 0;
+    const int qb = 2 * ((cq >> 5) * 40 + (cq & 31) + ((cq & 31) >> 2));
     float dl[kLines];
 #pragma unroll
     for (int l = 0; l < kLines; ++l) {
-      const int c = ch + kSlot * l + j;
-      dl[l] = 0.0f;
-      if (valid && c < nch) {
-        const float4 q0 = qs4[q4_index(c, 0)], q1 = qs4[q4_index(c, 1)];
-        const float qa[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-        const float xa[8] = {xv[l][0].x, xv[l][0].y, xv[l][0].z, xv[l][0].w,
-                             xv[l][1].x, xv[l][1].y, xv[l][1].z, xv[l][1].w};
-        dl[l] = hg_chunk_d2(qa, xa);
-      }
+      const float4 q0 = qs4[qb + qoff[l]], q1 = qs4[qb + qoff[l] + 1];
+      const float qa[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+      const float xa[8] = {xv[l][0].x, xv[l][0].y, xv[l][0].z, xv[l][0].w,
+                           xv[l][1].x, xv[l][1].y, xv[l][1].z, xv[l][1].w};
+      const float d = hg_chunk_d2(qa, xa);
+      dl[l] = in[l] ? d : 0.0f;
+    }
+    // the slot adds the step's chunk sums in order (adding 0 leaves a sum
+    // unchanged); one abandon test per step, since the step's lines are
+    // already loaded
+    float part[kStep];
+    float acc = dist;
+#pragma unroll
+    for (int t = 0; t < kStep; ++t) {
+      acc = __fadd_rn(acc, __shfl_sync(HG_FULL, dl[t / kSlot], slot_lead + (t % kSlot)));
+      part[t] = acc;
     }
     bool finished = false;
-#pragma unroll
-    for (int t = 0; t < kSlot * kLines; ++t) {
-      const float dt = __shfl_sync(HG_FULL, dl[t / kSlot], slot_lead + (t % kSlot));
-      if (valid && ch + t < nch) {
-        dist = __fadd_rn(dist, dt);
-        if (j == 0) ++n_chunks;
-        if (dist > B) valid = false;  // abandoned
-      }
-    }
     if (valid) {
-      ch += kSlot * kLines;
-      if (ch >= nch) {
-        finished = true;
+      if (acc > B) {
+        // abandoned: the reference reads up to the first chunk whose sum
+        // exceeds the bound (the partial sums never decrease)
+        if (j == 0) {
+          int used = 1;
+#pragma unroll
+          for (int t = 0; t < kStep; ++t) used += part[t] <= B ? 1 : 0;
+          n_chunks += (uint32_t)(ch + used);
+        }
         valid = false;
+      } else {
+        dist = acc;
+        ch += kStep;
+        x += 2 * kStep;
+        if (ch >= nch) {
+          finished = true;
+          valid = false;
+          if (j == 0) {
+            n_chunks += (uint32_t)nch;
+            ++n_done;
+          }
+        }
       }
     }
-    if (finished && j == 0) ++n_done;
     const bool take = finished && j == 0 && dist <= B && dist <= T;
     warp_list_add(list, cnt, T, a.k, a.bound, take, dist,
                   take ? (kRowIds ? row : (uint32_t)a.ids[row]) : 0u);
@@ -712,17 +740,18 @@ __global__ void __launch_bounds__(kEdThreads, 4) k_ed_stream(EdArgs a) {
   if (cnt == a.k && lane == 0) atomicMin(a.bound, (uint32_t)(list[a.k - 1] >> 32));
   unsigned long long* out = a.parts + (uint64_t)gw * kWarpListCap;
   for (int i = lane; i < cnt; i += 32) out[i] = list[i];
+  unsigned long long s_chunks = n_chunks, s_done = n_done, s_rows = n_rows;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    n_chunks += __shfl_xor_sync(HG_FULL, n_chunks, o);
-    n_done += __shfl_xor_sync(HG_FULL, n_done, o);
-    n_rows += __shfl_xor_sync(HG_FULL, n_rows, o);
+    s_chunks += __shfl_xor_sync(HG_FULL, s_chunks, o);
+    s_done += __shfl_xor_sync(HG_FULL, s_done, o);
+    s_rows += __shfl_xor_sync(HG_FULL, s_rows, o);
   }
   if (lane == 0) {
     a.part_count[gw] = cnt;
-    atomicAdd(&a.stats[1], n_chunks);
-    atomicAdd(&a.stats[4], n_done);
-    atomicAdd(&a.stats[5], n_rows);
+    atomicAdd(&a.stats[1], s_chunks);
+    atomicAdd(&a.stats[4], s_done);
+    atomicAdd(&a.stats[5], s_rows);
   }
 }
 
@@ -987,17 +1016,25 @@ static cudaError_t launch_ed(const EdArgs& a, int blocks, cudaStream_t s) {
 #ifndef HG_ED_LONG_SLOT
 #define HG_ED_LONG_SLOT 8
 #endif
+#ifndef HG_ED_SHORT_LINES
+#define HG_ED_SHORT_LINES 2
+#endif
 cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s) {
-  return a.L >= 4096 ? launch_ed<false, HG_ED_LONG_LINES, HG_ED_LONG_SLOT>(a, blocks, s) : launch_ed<false, 2, 4>(a, blocks, s);
+  return a.L >= 4096 ? launch_ed<false, HG_ED_LONG_LINES, HG_ED_LONG_SLOT>(a, blocks, s)
+                     : launch_ed<false, HG_ED_SHORT_LINES, 4>(a, blocks, s);
 }
 cudaError_t launch_ed_stream_row_ids(const EdArgs& a, int blocks, cudaStream_t s) {
-  return a.L >= 4096 ? launch_ed<true, HG_ED_LONG_LINES, HG_ED_LONG_SLOT>(a, blocks, s) : launch_ed<true, 2, 4>(a, blocks, s);
+  return a.L >= 4096 ? launch_ed<true, HG_ED_LONG_LINES, HG_ED_LONG_SLOT>(a, blocks, s)
+                     : launch_ed<true, HG_ED_SHORT_LINES, 4>(a, blocks, s);
 }
 int ed_blocks_per_sm(int L) {
   // shared memory per block: the staged query + 8 per-warp lists of 2 KB
   const size_t per_block = q4_bytes(L) + (size_t)kEdWarps * kWarpListCap * 8 + 1024;
   const int fit = (int)((size_t)227 * 1024 / per_block);
-  return fit < 1 ? 1 : (fit < kEdBlocksPerSm ? fit : kEdBlocksPerSm);
+  // registers: more than two lines per step leave room for 3 blocks
+  const int lines = L >= 4096 ? HG_ED_LONG_LINES : HG_ED_SHORT_LINES;
+  const int cap = lines > 2 ? 3 : kEdBlocksPerSm;
+  return fit < 1 ? 1 : (fit < cap ? fit : cap);
 }
 
 cudaError_t launch_merge(const unsigned long long* parts, const int* part_count, int nparts, int k,

@@ -345,6 +345,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t tcount = 0;
     uint32_t pcur = 0, pend = 0;  // the warp's reserved block of the pair list
     bool ok = true;
+    // the certified bounds this thread's columns used (a.errstat)
+    float e_sum = 0.0f, e_rel = 0.0f, e_max = 0.0f;
+    uint32_t e_cnt = 0, e_rcnt = 0;
     for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
       const Item it = item_of(a, w, QT, ntiles, qtile, nq);
       // item boundary: every epilogue warp is done with the previous item
@@ -391,6 +394,15 @@ __global__ void __launch_bounds__(kThreads, 1)
           const float err = 2.000002f * (qm.y * tm.z + qm.z * tm.y + qm.z * tm.z + a.c_acc * qm.y * tm.y) +
                             a.c_sq * (qm.x + tm.x + qb) + 1e-5f;
           tv = 0.5f * (qm.x - qb - err);
+          if (a.errstat) {
+            e_sum += err;
+            e_max = fmaxf(e_max, err);
+            ++e_cnt;
+            if (qb > 0.0f) {
+              e_rel += err / qb;
+              ++e_rcnt;
+            }
+          }
         }
         s_thr[etid] = tv;
       }
@@ -552,6 +564,27 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
     for (uint32_t i = pcur + lane; i < pend; i += 32) a.pairs[i] = ~0ull;  // close the last block
+    if (a.errstat) {
+      double ds = e_sum, dr = e_rel;
+      uint32_t c = e_cnt, rc = e_rcnt;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        ds += __shfl_xor_sync(HG_FULL, ds, o);
+        dr += __shfl_xor_sync(HG_FULL, dr, o);
+        c += __shfl_xor_sync(HG_FULL, c, o);
+        rc += __shfl_xor_sync(HG_FULL, rc, o);
+        e_max = fmaxf(e_max, __shfl_xor_sync(HG_FULL, e_max, o));
+      }
+      if (lane == 0 && c) {
+        atomicAdd(&a.errstat[0], ds);
+        atomicAdd(&a.errstat[1], dr);
+        atomicAdd(&a.errstat[2], (double)c);
+        atomicAdd(&a.errstat[3], (double)rc);
+        // err >= 0: the order of the bit patterns is the order of the values
+        atomicMax(reinterpret_cast<unsigned long long*>(&a.errstat[4]),
+                  (unsigned long long)__double_as_longlong((double)e_max));
+      }
+    }
   }
   tc_fence_before();
   __syncthreads();

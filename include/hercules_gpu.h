@@ -84,6 +84,11 @@ typedef struct {
   double rerank_ms;           /* device time: exact re-rank of the survivors */
   double fallback_ms;         /* device time: plain path for the fallback queries */
   uint64_t kernel_launches;   /* kernels this library launched for the call */
+  /* batched path: the certified error bound err(q, item) of the filter pass
+   * over every row, over its (work item, query) pairs with a finite bound */
+  double err_mean;            /* mean err */
+  double err_max;             /* largest err */
+  double err_over_bound;      /* mean err / B_q (B_q > 0) */
 } hg_query_stats;
 
 /* Search mode. */

@@ -45,6 +45,10 @@ def test_batch_matches_plain_uniform_k(mid, k):
     # the filter, not the fallback, answered nearly every query
     assert st["fallback_queries"] <= len(Q) // 20, st
     assert st["survivors"] > 0 and st["bf16_pairs"] == len(Q) * X.shape[0]
+    # the certified bound the filter used: positive, and at L = 256 on
+    # z-normalised walks well below the plain 2u|q||x| bound (4.0)
+    assert 0 < st["err_mean"] <= st["err_max"] < 4.0, st
+    assert st["err_over_bound"] > 0, st
 
 
 def test_batch_mixed_k(mid):
