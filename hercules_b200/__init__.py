@@ -61,7 +61,8 @@ class QueryStats(ctypes.Structure):
 
 class KnnOpts(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("use_lb_sax", ctypes.c_int), ("profile", ctypes.c_int),
-                ("approx_blocks", ctypes.c_int), ("bucket_cap", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+                ("approx_blocks", ctypes.c_int), ("bucket_cap", ctypes.c_int), ("dense_filter", ctypes.c_int),
+                ("reserved", ctypes.c_int * 2)]
 
 
 class Tuning(ctypes.Structure):
@@ -284,10 +285,11 @@ class HerculesIndex:
                                    ctypes.byref(st)))
         return st.as_dict()
 
-    def knn_batch(self, queries, k, stats=False, bucket_cap=0):
+    def knn_batch(self, queries, k, stats=False, bucket_cap=0, dense_filter=False):
         """Batched exact k-NN (BF16 tensor-core filter + exact re-rank); k is
         an int or one k per query.  Outputs are nq x max(k); entries past a
-        query's k are +inf / -1."""
+        query's k are +inf / -1.  dense_filter: filter every row against every
+        query (no LB_EAPCA leaf pruning first); the answers are the same."""
         q = _f32(queries, self.L)
         nq = q.shape[0]
         ks = np.broadcast_to(np.asarray(k, dtype=np.uint32), (nq,)).copy()
@@ -295,15 +297,15 @@ class HerculesIndex:
         d = np.zeros((nq, kmax), dtype=np.float32)
         ids = np.zeros((nq, kmax), dtype=np.int64)
         st = QueryStats()
-        opts = KnnOpts(MODE_BATCH, 1, 0, 0, bucket_cap)
+        opts = KnnOpts(MODE_BATCH, 1, 0, 0, bucket_cap, int(bool(dense_filter)))
         _check(lib().hg_knn_batch(self._h, _ptr(q), nq, _ptr(ks), kmax, ctypes.byref(opts), _ptr(d), _ptr(ids),
                                   ctypes.byref(st)))
         return (d, ids, st.as_dict()) if stats else (d, ids)
 
-    def knn_batch_device(self, q_ptr, nq, ks, kmax, dist_ptr, id_ptr, stream=0, bucket_cap=0):
+    def knn_batch_device(self, q_ptr, nq, ks, kmax, dist_ptr, id_ptr, stream=0, bucket_cap=0, dense_filter=False):
         """Device-resident batched variant; ks is a host array (or None)."""
         st = QueryStats()
-        opts = KnnOpts(MODE_BATCH, 1, 0, 0, bucket_cap)
+        opts = KnnOpts(MODE_BATCH, 1, 0, 0, bucket_cap, int(bool(dense_filter)))
         kp = None
         if ks is not None:
             ks = np.ascontiguousarray(ks, dtype=np.uint32)

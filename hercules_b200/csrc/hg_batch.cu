@@ -543,8 +543,108 @@ __global__ void k_group_items(const LeafPlan* __restrict__ plan, int nleaves, ui
     it.tile_lo = tb * btpi;
     it.tile_hi = min(use, tb * btpi + btpi);
     it.sub = p.sub;
-    it.pad = 0;
+    it.row_skip = 0;
     items[item_off[l] + i] = it;
+  }
+}
+
+// The pruned filter's layout (one block): per leaf, its kept queries get a
+// run of the query panel (exclusive scan of the counts) and its work items
+// a run of the item list (query tiles of kBatchQueryTile x chunks of tpi
+// 128-row tiles on the global tile grid).  ctl[0] = items, ctl[1] = panel
+// rows, ctl[2] = the dense pass's query count: 0, or nq when the panel or
+// the item list would overflow (the dense pass then filters every row).
+// pairs = sum over leaves of kept queries x leaf rows.
+__global__ void __launch_bounds__(kGroupThreads) k_group_pruned(const uint32_t* __restrict__ leaf_cnt,
+                                                                const LeafPlan* __restrict__ plan, int nleaves,
+                                                                uint32_t tpi, uint32_t panel_cap, uint32_t items_cap,
+                                                                uint32_t nq, uint32_t* leaf_poff, uint32_t* leaf_ioff,
+                                                                uint32_t* ctl, unsigned long long* pairs) {
+  __shared__ unsigned long long wsum[3][32];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  auto items_of = [&](int l) -> unsigned long long {
+    const uint32_t c = leaf_cnt[l];
+    if (c == 0 || plan[l].size == 0) return 0ull;
+    const uint64_t t0 = plan[l].start / kBM, t1 = (plan[l].start + plan[l].size + kBM - 1) / kBM;
+    return (unsigned long long)((c + kBatchQueryTile - 1) / kBatchQueryTile) * ((t1 - t0 + tpi - 1) / tpi);
+  };
+  const int per = (nleaves + kGroupThreads - 1) / kGroupThreads;
+  const int l0 = min(tid * per, nleaves), l1 = min(l0 + per, nleaves);
+  unsigned long long sq = 0, si = 0, sp = 0;
+  for (int l = l0; l < l1; ++l) {
+    sq += leaf_cnt[l];
+    si += items_of(l);
+    sp += (unsigned long long)leaf_cnt[l] * plan[l].size;
+  }
+  unsigned long long v[3] = {sq, si, sp};
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const unsigned long long x = __shfl_up_sync(HG_FULL, v[i], o);
+      if (lane >= o) v[i] += x;
+    }
+  }
+  if (lane == 31)
+    for (int i = 0; i < 3; ++i) wsum[i][wid] = v[i];
+  __syncthreads();
+  if (wid == 0) {
+    unsigned long long x[3] = {wsum[0][lane], wsum[1][lane], wsum[2][lane]};
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const unsigned long long y = __shfl_up_sync(HG_FULL, x[i], o);
+        if (lane >= o) x[i] += y;
+      }
+    }
+    for (int i = 0; i < 3; ++i) wsum[i][lane] = x[i];
+  }
+  __syncthreads();
+  unsigned long long oq = (wid ? wsum[0][wid - 1] : 0ull) + v[0] - sq;
+  unsigned long long oi = (wid ? wsum[1][wid - 1] : 0ull) + v[1] - si;
+  for (int l = l0; l < l1; ++l) {
+    leaf_poff[l] = (uint32_t)oq;
+    leaf_ioff[l] = (uint32_t)oi;
+    oq += leaf_cnt[l];
+    oi += items_of(l);
+  }
+  if (tid == kGroupThreads - 1) {
+    const unsigned long long tq = wsum[0][31], ti = wsum[1][31], tp = wsum[2][31];
+    const bool fits = tq <= panel_cap && ti <= items_cap;
+    ctl[0] = fits ? (uint32_t)ti : 0u;
+    ctl[1] = fits ? (uint32_t)tq : 0u;
+    ctl[2] = fits ? 0u : nq;
+    *pairs = fits ? tp : 0ull;
+  }
+}
+
+// The pruned filter's panel list and work items, one block per leaf.
+__global__ void k_emit_pruned(const uint32_t* __restrict__ leaf_cnt, const uint32_t* __restrict__ leaf_q,
+                              uint32_t stride, const uint32_t* __restrict__ leaf_poff,
+                              const uint32_t* __restrict__ leaf_ioff, const LeafPlan* __restrict__ plan, uint32_t tpi,
+                              const uint32_t* __restrict__ ctl, uint32_t* panel_list, BatchItem* items) {
+  const int l = blockIdx.x;
+  const uint32_t c = leaf_cnt[l];
+  if (ctl[0] == 0 || c == 0 || plan[l].size == 0) return;
+  const uint32_t po = leaf_poff[l], io = leaf_ioff[l];
+  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) panel_list[po + i] = leaf_q[(uint64_t)l * stride + i];
+  const uint64_t start = plan[l].start, end = start + plan[l].size;
+  const uint64_t t0 = start / kBM, t1 = (end + kBM - 1) / kBM;
+  const uint32_t ntile = (uint32_t)(t1 - t0), nch = (ntile + tpi - 1) / tpi;
+  const uint32_t nqt = (c + kBatchQueryTile - 1) / kBatchQueryTile;
+  for (uint32_t i = threadIdx.x; i < nch * nqt; i += blockDim.x) {
+    const uint32_t ch = i / nqt, qt = i % nqt;
+    BatchItem it;
+    it.row_begin = t0 * kBM;
+    it.row_end = end;
+    it.q_off = po + qt * kBatchQueryTile;
+    it.q_cnt = min((uint32_t)kBatchQueryTile, c - qt * kBatchQueryTile);
+    it.tile_lo = ch * tpi;
+    it.tile_hi = min(ntile, ch * tpi + tpi);
+    it.sub = 1;
+    it.row_skip = (uint32_t)(start - t0 * kBM);
+    items[io + i] = it;
   }
 }
 
@@ -623,6 +723,20 @@ cudaError_t launch_group_queries(const int* approx, int nq, const LeafPlan* plan
   if (e != cudaSuccess) return e;
   k_group_items<<<nblk((uint64_t)nleaves * 32, 256), 256, 0, s>>>(plan, nleaves, btpi, leaf_qoff, leaf_qcnt,
                                                                  item_off, items);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_group_pruned(const uint32_t* leaf_cnt, const uint32_t* leaf_q, uint32_t stride,
+                                const LeafPlan* plan, int nleaves, uint32_t tpi, uint32_t panel_cap,
+                                uint32_t items_cap, uint32_t nq, uint32_t* leaf_poff, uint32_t* leaf_ioff,
+                                uint32_t* ctl, unsigned long long* pairs, uint32_t* panel_list, BatchItem* items,
+                                cudaStream_t s) {
+  k_group_pruned<<<1, kGroupThreads, 0, s>>>(leaf_cnt, plan, nleaves, tpi, panel_cap, items_cap, nq, leaf_poff,
+                                             leaf_ioff, ctl, pairs);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || nleaves == 0) return e;
+  k_emit_pruned<<<nleaves, 256, 0, s>>>(leaf_cnt, leaf_q, stride, leaf_poff, leaf_ioff, plan, tpi, ctl, panel_list,
+                                        items);
   return cudaGetLastError();
 }
 

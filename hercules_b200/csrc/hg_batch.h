@@ -20,11 +20,11 @@ constexpr int kBatchSegMin = 256;     // rows per re-rank segment, at least
 // [row_begin, row_end) (one approximate leaf) against queries
 // qperm[q_off .. q_off + q_cnt).
 struct BatchItem {
-  uint64_t row_begin, row_end;
+  uint64_t row_begin, row_end;  // tile t covers rows row_begin + 128 t .. +127, valid below row_end
   uint32_t q_off, q_cnt;
   uint32_t tile_lo, tile_hi;
-  uint32_t sub;  // bound slots per tile: 1, 2, 4, 8 or 16
-  uint32_t pad;
+  uint32_t sub;       // bound slots per tile: 1, 2, 4, 8 or 16 (bound pass)
+  uint32_t row_skip;  // rows of the first tile before the item's rows (pruned filter: tiles on the 128-row grid)
 };
 
 // Rows of one leaf and its bound-pass plan (slots per tile and tiles used).
@@ -43,7 +43,8 @@ struct BatchGemm {
   const float4* qmeta;      // per query: |q|^2, |q~|, |q - q~|, 0
   const uint32_t* qperm;   // query of each tile column (position in the BF16 query matrix)
   int nq;
-  int mode;  // 0: bound pass over the items; 1: filter over every row; 2: raw products
+  int mode;  // 0: bound pass over the items; 1: filter over every row; 2: raw products;
+             // 3: filter over the items (leaves x the queries whose LB_EAPCA is within their bound)
   int qtile; // modes 1 and 2: queries per tile (MMA N): 64, 128, 256, or 0 = by the query count
   const uint32_t* nq_dev;   // if set: the query count (<= nq) read on the device
   // mode 0
@@ -108,6 +109,13 @@ cudaError_t launch_rows_to_bf16(const float* rows, const uint32_t* idx, uint64_t
 cudaError_t launch_group_queries(const int* approx, int nq, const LeafPlan* plan, int nleaves, uint32_t btpi,
                                  uint32_t* perm, uint32_t* slots, uint32_t* leaf_qoff, uint32_t* leaf_qcnt,
                                  uint32_t* item_off, uint32_t* nitems, BatchItem* items, cudaStream_t s);
+// the pruned filter's query panel list and work items from the kept
+// (leaf, query) pairs (k_group_pruned, k_emit_pruned)
+cudaError_t launch_group_pruned(const uint32_t* leaf_cnt, const uint32_t* leaf_q, uint32_t stride,
+                                const LeafPlan* plan, int nleaves, uint32_t tpi, uint32_t panel_cap,
+                                uint32_t items_cap, uint32_t nq, uint32_t* leaf_poff, uint32_t* leaf_ioff,
+                                uint32_t* ctl, unsigned long long* pairs, uint32_t* panel_list, BatchItem* items,
+                                cudaStream_t s);
 cudaError_t launch_collect_retry(const int* ok, const uint32_t* list, uint32_t n, const uint32_t* n_dev,
                                  uint32_t* out, uint32_t* out_n, cudaStream_t s);
 cudaError_t launch_count_unverified(const int* ok, uint32_t nq, uint32_t* out, cudaStream_t s);

@@ -344,6 +344,15 @@ static void free_device(hg_index* ix) {
   if (b.graph) cudaGraphExecDestroy(b.graph);
   dfree(b.stamps);
   dfree(b.errstat);
+  dfree(b.leaf_cnt);
+  dfree(b.leaf_q);
+  dfree(b.leaf_poff);
+  dfree(b.leaf_ioff);
+  dfree(b.panel_list);
+  dfree(b.panel_bf);
+  dfree(b.items3);
+  dfree(b.pctl);
+  dfree(b.ppairs);
   b = hg::BatchScratch{};
 }
 
@@ -1368,6 +1377,53 @@ static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket
   return HG_OK;
 }
 
+// Buffers of the pruned filter for b.nq_cap queries; *ok = false when they
+// would not fit their limits (the batch then filters every row): the kept
+// (leaf, query) lists within 1 GiB, the query panel within 2 GiB or one
+// copy of the batch, whichever is larger.
+static hg_status ensure_prune_scratch(hg_index* ix, bool* ok) {
+  hg::BatchScratch& b = ix->bs;
+  const uint64_t nl = ix->leaves.size(), nq = b.nq_cap, L = ix->L;
+  *ok = nl > 0 && nl * nq * 4 <= (1ull << 30);
+  if (!*ok) return HG_OK;
+  if (b.prune_nq >= nq && b.leaf_q) return HG_OK;
+  dfree(b.leaf_cnt);
+  dfree(b.leaf_q);
+  dfree(b.leaf_poff);
+  dfree(b.leaf_ioff);
+  dfree(b.panel_list);
+  dfree(b.panel_bf);
+  dfree(b.items3);
+  dfree(b.pctl);
+  dfree(b.ppairs);
+  b.prune_nq = 0;
+  const uint64_t panel = std::min<uint64_t>(nl * nq, std::max<uint64_t>(nq, (2ull << 30) / (2 * L)));
+  // items for the narrowest work item (8 tiles): chunks of every leaf x its query tiles
+  const uint64_t ntiles = (ix->n + hg::kBatchTileRows - 1) / hg::kBatchTileRows;
+  const uint64_t items = (ntiles / 8 + 2 * nl) * ((nq + hg::kBatchQueryTile - 1) / hg::kBatchQueryTile);
+  if (panel >= (1ull << 32) || items >= (1ull << 31)) {
+    *ok = false;
+    return HG_OK;
+  }
+  CK(dalloc(&b.leaf_cnt, nl));
+  CK(dalloc(&b.leaf_q, nl * nq));
+  CK(dalloc(&b.leaf_poff, nl));
+  CK(dalloc(&b.leaf_ioff, nl));
+  CK(dalloc(&b.panel_list, panel));
+  uint16_t* p = nullptr;
+  CK(dalloc(&p, panel * L));
+  b.panel_bf = p;
+  CK(dalloc(&b.items3, items));
+  CK(dalloc(&b.pctl, 4));
+  CK(dalloc(&b.ppairs, 1));
+  b.panel_cap = (uint32_t)panel;
+  b.items3_cap = (uint32_t)items;
+  HCK(encode_bf16_map(&b.panel_map, b.panel_bf, panel, (uint32_t)L, hg::kBatchQueryTile));
+  b.prune_nq = (uint32_t)nq;
+  ++b.gen;  // a captured pipeline holds the old addresses
+  return HG_OK;
+}
+
 // Error-bound coefficients of the BF16 filter for series length L (see
 // hg_batch.cu): c_acc = L 2^-20 (FP32 accumulation on the tensor cores) and
 // c_sq = (L/8 + 16) 2^-22, both rounded up to float.
@@ -1428,7 +1484,7 @@ static hg_status ensure_leaf_plan(hg_index* ix, uint64_t want, cudaStream_t st) 
 // the device (an empty round costs a few microseconds), the count of queries
 // left unverified.  Events gev[0..] mark the phases.
 static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_t bucket_cap, const CUtensorMap& qmap,
-                               cudaStream_t st, uint64_t* launches) {
+                               bool prune, cudaStream_t st, uint64_t* launches) {
   hg::BatchScratch& b = ix->bs;
   const uint32_t L = ix->L;
   const int sms = hg::sm_count(ix->device);
@@ -1499,8 +1555,22 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
   r.nlist = (int)nq;
   r.nlist_dev = nullptr;
   CK(hg::launch_bound_select(r, st));
-  CK(stamp(1));
   *launches = 8;  // route, group (2), conversion, bound pass, bound selection
+  // 3a. the leaves each query must filter (LB_EAPCA within B_q), each leaf's
+  // queries laid out contiguously in a BF16 panel, and the work items
+  const hg::DeviceIndex& d = ix->d;
+  if (prune) {
+    CK(cudaMemsetAsync(b.leaf_cnt, 0, sizeof(uint32_t) * nl, st));
+    CK(cudaMemsetAsync(b.ppairs, 0, sizeof(unsigned long long), st));
+    CK(hg::launch_leaf_keep(b.qin, (int)L, (int)nq, d.leaf_seg_off, d.leaf_points, d.leaf_sk, d.leaf_size, nl, b.bound,
+                            b.leaf_cnt, b.leaf_q, b.prune_nq, st));
+    CK(hg::launch_group_pruned(b.leaf_cnt, b.leaf_q, b.prune_nq, b.leaf_plan, nl, ix->tune.filter_tiles_per_item,
+                               b.panel_cap, b.items3_cap, nq, b.leaf_poff, b.leaf_ioff, b.pctl, b.ppairs,
+                               b.panel_list, b.items3, st));
+    CK(hg::launch_rows_to_bf16(b.qin, b.panel_list, b.panel_cap, (int)L, b.panel_bf, b.qmeta, st, b.pctl + 1));
+    *launches += 4;
+  }
+  CK(stamp(1));
   // 3-5. certified filter, exact re-rank, verification; queries whose bucket
   // overflowed are retried with the bound their first survivors gave
   uint32_t* lists[2] = {b.qlist, b.qlist2};
@@ -1511,15 +1581,28 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
       CK(hg::launch_rows_to_bf16(b.qin, list_in, nq, (int)L, b.qbf, b.qmeta, st, n_dev));
       ++*launches;
     }
-    g.mode = 1;
-    g.qperm = round == 0 ? b.qperm : list_in;
-    g.nq_dev = n_dev;
-    g.qtile = round == 0 ? hg::kBatchQueryTile : 0;
     g.errstat = round == 0 ? b.errstat : nullptr;
     if (round == 0) CK(cudaMemsetAsync(b.errstat, 0, 5 * sizeof(double), st));
     CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
     CK(cudaMemsetAsync(b.heads + 1, 0, sizeof(uint32_t), st));
     CK(stamp(2 + 3 * round));
+    if (round == 0 && prune) {
+      // the kept (leaf, query) pairs; the dense pass below runs only when
+      // the panel overflowed (its query count is then nq, else 0)
+      g.mode = 3;
+      g.items = b.items3;
+      g.nitems = b.items3_cap;
+      g.nitems_dev = b.pctl + 0;
+      g.qperm = b.panel_list;
+      g.nq_dev = nullptr;
+      g.qtile = hg::kBatchQueryTile;
+      CK(hg::launch_umma_filter(ix->bd.rows_map, b.panel_map, g, sms, st));
+      ++*launches;
+    }
+    g.mode = 1;
+    g.qperm = round == 0 ? b.qperm : list_in;
+    g.nq_dev = round == 0 ? (prune ? b.pctl + 2 : nullptr) : n_dev;
+    g.qtile = round == 0 ? hg::kBatchQueryTile : 0;
     CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
     CK(stamp(3 + 3 * round));
     CK(hg::launch_scatter_pairs(b.pairs, b.heads + 1, b.pairs_cap, list_in, (int)nq, n_dev, b.bucket, b.bucket_cnt,
@@ -1602,8 +1685,10 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   CUtensorMap qmap;
   HCK(encode_bf16_map(&qmap, b.qbf, nq, L, hg::kBatchQueryTile));
   // the pipeline, captured once per shape in a CUDA graph and replayed
+  bool prune = false;
+  if (!o.dense_filter) HCK(ensure_prune_scratch(ix, &prune));
   const uint64_t key[8] = {nq, kmax, bucket_cap, b.gen, ix->tune.filter_tiles_per_item, ix->tune.bound_tiles_per_item,
-                           ix->tune.rerank_blocks_per_sm, 1};
+                           ix->tune.rerank_blocks_per_sm, prune ? 2u : 1u};
   uint64_t launches = 0;
   if (!b.graph || memcmp(key, b.graph_key, sizeof key) != 0) {
     if (b.graph) {
@@ -1612,7 +1697,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     }
     cudaGraph_t graph = nullptr;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-    const hg_status s = enqueue_batch(ix, nq, kmax, bucket_cap, qmap, st, &launches);
+    const hg_status s = enqueue_batch(ix, nq, kmax, bucket_cap, qmap, prune, st, &launches);
     const cudaError_t ce = cudaStreamEndCapture(st, &graph);
     if (s != HG_OK) {
       if (graph) cudaGraphDestroy(graph);
@@ -1631,6 +1716,12 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   uint32_t ctrl[16];
   uint32_t dev_err = 0;
   double es[5];
+  uint32_t pc[4] = {0, 0, 0, 0};
+  unsigned long long pp = 0;
+  if (prune) {
+    CK(cudaMemcpyAsync(pc, b.pctl, sizeof pc, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&pp, b.ppairs, sizeof pp, cudaMemcpyDeviceToHost, st));
+  }
   CK(cudaMemcpyAsync(ts, b.stamps, sizeof ts, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(es, b.errstat, sizeof es, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(hs, b.stats, sizeof hs, cudaMemcpyDeviceToHost, st));
@@ -1685,7 +1776,9 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
       if (cnt == 0 && round > 0) continue;
       gemm += tg;
       rerank += tr;
-      pairs += cnt * ix->n;
+      // round 0 with pruning: the kept pairs, plus every pair if the dense
+      // pass ran instead
+      pairs += (round == 0 && prune) ? pp + (uint64_t)pc[2] * ix->n : cnt * ix->n;
     }
     cudaEventElapsedTime(&tf, fb0, fb1);
     const double t0e = span(0, 15) + (fallbacks ? tf : 0.0);

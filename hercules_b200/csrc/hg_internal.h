@@ -133,6 +133,20 @@ struct BatchScratch {
   uint64_t graph_launches = 0;   // kernels in the captured pipeline
   unsigned long long* stamps = nullptr;  // [16] global-timer stamps at the phase boundaries
   double* errstat = nullptr;             // [5] certified bounds of the first filter pass (BatchGemm::errstat)
+  // pruned filter: the (leaf, query) pairs LB_EAPCA keeps, their query panel
+  // (each leaf's queries contiguous, BF16) and work items
+  uint32_t prune_nq = 0;                 // queries the buffers hold (0: not allocated)
+  uint32_t* leaf_cnt = nullptr;          // [leaves] kept queries
+  uint32_t* leaf_q = nullptr;            // [leaves][prune_nq] their ids
+  uint32_t* leaf_poff = nullptr;         // [leaves] panel offset
+  uint32_t* leaf_ioff = nullptr;         // [leaves] item offset
+  uint32_t* panel_list = nullptr;        // [panel_cap] query of each panel row
+  void* panel_bf = nullptr;              // [panel_cap][L] BF16
+  BatchItem* items3 = nullptr;           // [items3_cap]
+  uint32_t panel_cap = 0, items3_cap = 0;
+  uint32_t* pctl = nullptr;              // [4] items, panel rows, dense-pass queries
+  unsigned long long* ppairs = nullptr;  // (query, row) pairs of the pruned pass
+  CUtensorMap panel_map;                 // TMA descriptor of panel_bf (64 x 256 boxes)
 };
 
 }  // namespace hg

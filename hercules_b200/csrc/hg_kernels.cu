@@ -278,6 +278,45 @@ __global__ void k_leaf_lb(const float* __restrict__ q, int L, int nleaves, const
   if ((threadIdx.x & 31) == 0) lb[w] = sum;
 }
 
+// Leaves each query of a batch must filter: one block per query, a warp per
+// leaf computes LB_EAPCA exactly as k_leaf_lb (the reference arithmetic of
+// calculate_node_min_distance) and keeps the leaf when
+//     LB <= B_q (1 + 2^-10) + L 2^-20,
+// B_q the query's bound (+inf keeps every leaf).  The plain path scans only
+// leaves with LB <= its running bound <= B_q, so the kept leaves include
+// every leaf it scans; the margins cover the rounding of B_q's product.
+// Kept (leaf, query) pairs go to leaf_q[leaf * stride + i], counted in
+// leaf_cnt[leaf].
+__global__ void k_leaf_keep(const float* __restrict__ Q, int L, int nq, const int* __restrict__ seg_off,
+                            const short* __restrict__ points, const float* __restrict__ sk,
+                            const uint32_t* __restrict__ leaf_size, int nleaves, const float* __restrict__ bound,
+                            uint32_t* leaf_cnt, uint32_t* leaf_q, uint32_t stride) {
+  extern __shared__ float qs[];
+  const int q = blockIdx.x;
+  if (q >= nq) return;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) qs[i] = Q[(uint64_t)q * L + i];
+  __syncthreads();
+  const float B = bound[q];
+  const float lim = B < __int_as_float(0x7f800000)
+                        ? __fadd_ru(__fmul_ru(B, 1.0f + 0x1p-10f), __fmul_ru((float)L, 0x1p-20f))
+                        : __int_as_float(0x7f800000);
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int w = threadIdx.x >> 5; w < nleaves; w += nw) {
+    if (leaf_size[w] == 0) continue;
+    const int off = seg_off[w], nseg = seg_off[w + 1] - off;
+    float sum = 0.0f;
+    int start = 0;
+    for (int s = 0; s < nseg && sum <= lim; ++s) {
+      const int end = points[off + s];
+      float m, sd;
+      warp_mean_stdev(qs, start, end, &m, &sd);
+      sum = __fadd_rn(sum, hg_eapca_term(m, sd, sk + 4 * (off + s), end - start));
+      start = end;
+    }
+    if (lane == 0 && sum <= lim) leaf_q[(uint64_t)w * stride + atomicAdd(&leaf_cnt[w], 1u)] = (uint32_t)q;
+  }
+}
+
 // Candidate leaves: LB_EAPCA <= current bound, not the approximate leaf, not
 // empty; ordered by LB with a stable LSD radix sort (4-bit digits, 8 passes)
 // in one CTA; then the exclusive prefix of their tile counts.
@@ -967,6 +1006,20 @@ cudaError_t launch_leaf_lb(const float* q, int L, int nleaves, const int* seg_of
   }
   k_leaf_lb<<<blocks_for((uint64_t)nleaves * 32, 256), 256, sizeof(float) * L, s>>>(q, L, nleaves, seg_off,
                                                                                   points, sk, lb_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_leaf_keep(const float* Q, int L, int nq, const int* seg_off, const short* points, const float* sk,
+                             const uint32_t* leaf_size, int nleaves, const float* bound, uint32_t* leaf_cnt,
+                             uint32_t* leaf_q, uint32_t stride, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_leaf_keep, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
+    attr = true;
+  }
+  if (nq <= 0) return cudaSuccess;
+  k_leaf_keep<<<nq, 256, sizeof(float) * L, s>>>(Q, L, nq, seg_off, points, sk, leaf_size, nleaves, bound, leaf_cnt,
+                                                 leaf_q, stride);
   return cudaGetLastError();
 }
 

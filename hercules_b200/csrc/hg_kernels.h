@@ -100,6 +100,11 @@ cudaError_t launch_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_pr
                               int* topk_count, uint32_t* counters, cudaStream_t s);
 cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s);
 cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s);
+// batched path: the (leaf, query) pairs whose LB_EAPCA is within the query's
+// bound (k_leaf_keep)
+cudaError_t launch_leaf_keep(const float* Q, int L, int nq, const int* seg_off, const short* points, const float* sk,
+                             const uint32_t* leaf_size, int nleaves, const float* bound, uint32_t* leaf_cnt,
+                             uint32_t* leaf_q, uint32_t stride, cudaStream_t s);
 // resident blocks per SM of the distance stream for series length L
 int ed_blocks_per_sm(int L);
 // the same with id = row index (EdArgs::ids unused)

@@ -13,9 +13,11 @@
 //               tile's rows) and columns 128 ((w - 4) / 4) .. +127 (queries).
 // Work items are (128-row tiles, query tile) pairs in a static round robin:
 // mode 1 walks row chunks x query tiles (a chunk's query tiles run side by
-// side so the chunk is read from HBM once); mode 0 walks the host's items
-// (approximate leaves x the queries routed there); mode 2 writes the raw dot
-// products (diagnostics).  Every mbarrier wait gives up after kWaitNs of
+// side so the chunk is read from HBM once); mode 0 walks an item list
+// (approximate leaves x the queries routed there) for the bound pass; mode 3
+// walks an item list (leaves x the queries that LB_EAPCA keeps for them) with
+// mode 1's screening epilogue; mode 2 writes the raw dot products
+// (diagnostics).  Every mbarrier wait gives up after kWaitNs of
 // global time: the CTA then raises *err, drains its copies and MMAs, frees
 // TMEM and returns.
 #include <cuda.h>
@@ -170,7 +172,8 @@ __device__ __forceinline__ uint32_t ordered_key(float f) {
 }
 
 struct Item {
-  uint64_t rb, re;  // rows of the item
+  uint64_t rb, re;  // tile t covers rows rb + 128 t .., valid in [vb, re)
+  uint64_t vb;
   uint32_t qoff, qcnt;
   uint32_t t_lo, t_hi;
   uint32_t sub;
@@ -179,10 +182,11 @@ struct Item {
 __device__ __forceinline__ Item item_of(const BatchGemm& a, uint32_t w, uint32_t QT, uint64_t ntiles, int qtile,
                                         int nq) {
   Item it;
-  if (a.mode == 0) {
+  if (a.mode == 0 || a.mode == 3) {
     const BatchItem b = a.items[w];
     it.rb = b.row_begin;
     it.re = b.row_end;
+    it.vb = b.row_begin + b.row_skip;
     it.qoff = b.q_off;
     it.qcnt = b.q_cnt;
     it.t_lo = b.tile_lo;
@@ -192,6 +196,7 @@ __device__ __forceinline__ Item item_of(const BatchGemm& a, uint32_t w, uint32_t
     const uint32_t chunk = w / QT, qt = w % QT;
     it.rb = 0;
     it.re = a.nrows;
+    it.vb = 0;
     it.qoff = qt * (uint32_t)qtile;
     it.qcnt = (uint32_t)min(nq - (int)it.qoff, qtile);
     it.t_lo = chunk * a.tiles_per_item;
@@ -231,12 +236,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   // per tile (MMA N): 64 in the bound pass, else the launch's choice or, for
   // 0, the narrowest of 64 / 128 / 256 that holds the queries
   const int nq = a.nq_dev ? (int)min((uint32_t)a.nq, *a.nq_dev) : a.nq;
+  const bool listed = a.mode == 0 || a.mode == 3;  // items from a.items
+  const bool screen = a.mode == 1 || a.mode == 3;  // threshold epilogue, survivor pairs
   const int qtile = a.mode == 0 ? kBatchBoundQueries
                                 : (a.qtile ? a.qtile : (nq <= 64 ? 64 : (nq <= 128 ? 128 : kUN)));
   const uint32_t QT = (uint32_t)((nq + qtile - 1) / qtile);
   const uint64_t ntiles = (a.nrows + kUM - 1) / kUM;
   const uint32_t nchunks = (uint32_t)((ntiles + a.tiles_per_item - 1) / a.tiles_per_item);
-  const uint32_t total = a.mode == 0 ? (a.nitems_dev ? *a.nitems_dev : a.nitems) : nchunks * QT;
+  const uint32_t total = listed ? (a.nitems_dev ? min(a.nitems, *a.nitems_dev) : a.nitems) : nchunks * QT;
 
   if (tid == 0) {
     for (int s = 0; s < kAStages; ++s) {
@@ -365,14 +372,14 @@ __global__ void __launch_bounds__(kThreads, 1)
       if ((uint32_t)etid < it.qcnt) {
         q = a.qperm[it.qoff + etid];
         qm = a.qmeta[q];
-        if (a.mode == 1) {
+        if (screen) {
           const float b = a.bound[q];
           qb = b < inf ? b : -1.0f;
         }
       }
       s_qidx[etid] = q;
       s_qn2[etid] = qm.x;
-      if (a.mode == 1) {
+      if (screen) {
         // norm maxima over the item's rows (its 128-row tiles), then the
         // column's threshold: keep (row, q) when acc - t_q >= |x|^2 / 2 with
         // t_q = (|q|^2 - B - err) / 2
@@ -415,13 +422,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       auto prefetch = [&](uint32_t t) {
         if (t >= it.t_hi) return;
         const uint64_t rw = it.rb + (uint64_t)t * kUM + quarter * 32 + lane;
-        xn_next = (rw < it.re && rw < a.nrows) ? a.xmeta[rw].x : 0.0f;
+        xn_next = (rw >= it.vb && rw < it.re && rw < a.nrows) ? a.xmeta[rw].x : 0.0f;
       };
       prefetch(it.t_lo);
       for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t, ++tcount) {
         const int b = (int)(tcount & 1);
         const uint64_t row = it.rb + (uint64_t)t * kUM + quarter * 32 + lane;
-        const bool row_ok = row < it.re && row < a.nrows;
+        const bool row_ok = row >= it.vb && row < it.re && row < a.nrows;
         const float xn2 = xn_next;
         prefetch(t + 1);
         const float h_row = row_ok ? 0.5f * xn2 : inf;
@@ -438,7 +445,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         // mode 1: survivor masks of the warp's (up to) four 32-column chunks;
         // the buckets are written after the accumulator is handed back
         uint32_t masks[4] = {0u, 0u, 0u, 0u};
-        if (a.mode == 1) {
+        if (screen) {
 #pragma unroll
           for (int i2 = 0; i2 < 2; ++i2) {
             const int c0 = c_lo + 64 * i2;
@@ -609,11 +616,12 @@ cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q
   if (g.mode != 0 && g.qtile != 0 && g.qtile != 64 && g.qtile != 128 && g.qtile != 256) return cudaErrorInvalidValue;
   // counts read on the device: every CTA starts and leaves when out of items
   int grid = blocks;
-  if (!(g.mode == 0 ? g.nitems_dev : g.nq_dev)) {
+  const bool listed = g.mode == 0 || g.mode == 3;
+  if (!(listed ? g.nitems_dev : g.nq_dev)) {
     const int qtile = g.mode == 0 ? kBatchBoundQueries : (g.qtile ? g.qtile : (g.nq <= 64 ? 64 : (g.nq <= 128 ? 128 : kUN)));
     const uint32_t QT = (uint32_t)((g.nq + qtile - 1) / qtile);
     const uint64_t total =
-        g.mode == 0 ? g.nitems : ((ntiles + g.tiles_per_item - 1) / g.tiles_per_item) * (uint64_t)QT;
+        listed ? g.nitems : ((ntiles + g.tiles_per_item - 1) / g.tiles_per_item) * (uint64_t)QT;
     if (total == 0) return cudaSuccess;
     grid = (int)(total < (uint64_t)blocks ? total : (uint64_t)blocks);
   }

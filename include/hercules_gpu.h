@@ -104,7 +104,9 @@ typedef struct {
   int approx_blocks;  /* blocks of the approximate-leaf scan (0 = two per SM) */
   int bucket_cap;     /* HG_MODE_BATCH: filter survivors kept per query before the
                          query falls back to the plain path (0 = 65536) */
-  int reserved[3];
+  int dense_filter;   /* HG_MODE_BATCH: 1 = filter every row against every query
+                         (no LB_EAPCA leaf pruning before the filter) */
+  int reserved[2];
 } hg_knn_opts;
 
 /* ---- status ----------------------------------------------------------- */

@@ -44,11 +44,25 @@ def test_batch_matches_plain_uniform_k(mid, k):
     same_as_plain(ix, Q, np.full(len(Q), k), d, ids)
     # the filter, not the fallback, answered nearly every query
     assert st["fallback_queries"] <= len(Q) // 20, st
-    assert st["survivors"] > 0 and st["bf16_pairs"] == len(Q) * X.shape[0]
+    # LB_EAPCA keeps only part of the (query, leaf) pairs for the filter
+    assert st["survivors"] > 0 and 0 < st["bf16_pairs"] <= len(Q) * X.shape[0]
     # the certified bound the filter used: positive, and at L = 256 on
     # z-normalised walks well below the plain 2u|q||x| bound (4.0)
     assert 0 < st["err_mean"] <= st["err_max"] < 4.0, st
     assert st["err_over_bound"] > 0, st
+
+
+def test_pruned_filter_equals_dense_filter(mid):
+    """Filtering only the leaves whose LB_EAPCA is within a query's bound
+    gives the same answers as filtering every row, with fewer pairs."""
+    X, Q, ix = mid
+    ks = np.array([1, 10, 100, 5] * (len(Q) // 4) + [10] * (len(Q) % 4), np.uint32)
+    d1, i1, s1 = ix.knn_batch(Q, ks, stats=True)
+    d2, i2, s2 = ix.knn_batch(Q, ks, stats=True, dense_filter=True)
+    assert np.array_equal(bits(d1), bits(d2)) and np.array_equal(i1, i2)
+    assert s2["bf16_pairs"] >= len(Q) * X.shape[0]
+    assert s1["bf16_pairs"] < s2["bf16_pairs"], (s1["bf16_pairs"], s2["bf16_pairs"])
+    same_as_plain(ix, Q, ks, d1, i1)
 
 
 def test_batch_mixed_k(mid):
