@@ -61,6 +61,7 @@ struct BatchGemm {
   uint32_t* pairs_cnt;        // slots reserved; 0 before the launch, may end above pairs_cap
   uint32_t pairs_cap;
   int* err;                // raised (1) when a bounded wait gave up
+  uint32_t* queue;         // if set: the work-item counter (0 before the launch); else a static round robin
   // if set (mode 1): the certified bounds used, [0] sum of err, [1] sum of
   // err / B_q (B_q > 0), [2] (item, query) pairs, [3] pairs with B_q > 0,
   // [4] the largest err; zeroed before the launch

@@ -344,6 +344,7 @@ static void free_device(hg_index* ix) {
   if (b.graph) cudaGraphExecDestroy(b.graph);
   dfree(b.stamps);
   dfree(b.errstat);
+  dfree(b.queues);
   dfree(b.leaf_cnt);
   dfree(b.leaf_q);
   dfree(b.leaf_poff);
@@ -1494,6 +1495,7 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
   CK(cudaMemsetAsync(b.ctrl, 0, sizeof(uint32_t) * 16, st));
   CK(cudaMemsetAsync(b.heads, 0, sizeof(uint32_t) * 4, st));
   CK(cudaMemsetAsync(b.stats, 0, sizeof(unsigned long long) * 8, st));
+  CK(cudaMemsetAsync(b.queues, 0, sizeof(uint32_t) * 8, st));
   CK(cudaMemsetAsync(b.bm, 0xff, sizeof(unsigned long long) * nq * b.plan_bm_cap, st));
   // 1. approximate leaves, grouping
   CK(hg::launch_route_queries(b.qin, (int)nq, (int)L, index_tree(ix), b.approx, st));
@@ -1523,6 +1525,7 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
   g.pairs_cnt = b.heads + 1;
   g.pairs_cap = b.pairs_cap;
   g.err = reinterpret_cast<int*>(b.heads + 3);
+  g.queue = b.queues + 0;
   CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
   hg::BatchRank r{};
   r.rows = ix->d.rows;
@@ -1596,6 +1599,7 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
       g.qperm = b.panel_list;
       g.nq_dev = nullptr;
       g.qtile = hg::kBatchQueryTile;
+      g.queue = b.queues + 1;
       CK(hg::launch_umma_filter(ix->bd.rows_map, b.panel_map, g, sms, st));
       ++*launches;
     }
@@ -1603,6 +1607,7 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
     g.qperm = round == 0 ? b.qperm : list_in;
     g.nq_dev = round == 0 ? (prune ? b.pctl + 2 : nullptr) : n_dev;
     g.qtile = round == 0 ? hg::kBatchQueryTile : 0;
+    g.queue = b.queues + 2 + round;
     CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
     CK(stamp(3 + 3 * round));
     CK(hg::launch_scatter_pairs(b.pairs, b.heads + 1, b.pairs_cap, list_in, (int)nq, n_dev, b.bucket, b.bucket_cnt,
@@ -1665,6 +1670,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     CK(dalloc(&b.ctrl, 16));
     CK(dalloc(&b.stamps, 16));
     CK(dalloc(&b.errstat, 5));
+    CK(dalloc(&b.queues, 8));
   }
   if (!b.qlist2 || !b.qin || b.out_kmax < kmax) {
     dfree(b.qlist2);

@@ -133,6 +133,7 @@ struct BatchScratch {
   uint64_t graph_launches = 0;   // kernels in the captured pipeline
   unsigned long long* stamps = nullptr;  // [16] global-timer stamps at the phase boundaries
   double* errstat = nullptr;             // [5] certified bounds of the first filter pass (BatchGemm::errstat)
+  uint32_t* queues = nullptr;            // [8] work-item counters of the filter launches
   // pruned filter: the (leaf, query) pairs LB_EAPCA keeps, their query panel
   // (each leaf's queries contiguous, BF16) and work items
   uint32_t prune_nq = 0;                 // queries the buffers hold (0: not allocated)

@@ -304,14 +304,20 @@ __global__ void k_leaf_keep(const float* __restrict__ Q, int L, int nq, const in
   for (int w = threadIdx.x >> 5; w < nleaves; w += nw) {
     if (leaf_size[w] == 0) continue;
     const int off = seg_off[w], nseg = seg_off[w + 1] - off;
+    // lane s: the term of segment s (hg_mean_stdev is warp_mean_stdev's
+    // arithmetic); the terms are then added in segment order
     float sum = 0.0f;
-    int start = 0;
-    for (int s = 0; s < nseg && sum <= lim; ++s) {
-      const int end = points[off + s];
-      float m, sd;
-      warp_mean_stdev(qs, start, end, &m, &sd);
-      sum = __fadd_rn(sum, hg_eapca_term(m, sd, sk + 4 * (off + s), end - start));
-      start = end;
+    for (int s0 = 0; s0 < nseg && sum <= lim; s0 += 32) {
+      const int s = s0 + lane;
+      float term = 0.0f;
+      if (s < nseg) {
+        const int start = s == 0 ? 0 : points[off + s - 1], end = points[off + s];
+        float m, sd;
+        hg_mean_stdev(qs, start, end, &m, &sd);
+        term = hg_eapca_term(m, sd, sk + 4 * (off + s), end - start);
+      }
+      const int n = min(32, nseg - s0);
+      for (int j = 0; j < n; ++j) sum = __fadd_rn(sum, __shfl_sync(HG_FULL, term, j));
     }
     if (lane == 0 && sum <= lim) leaf_q[(uint64_t)w * stride + atomicAdd(&leaf_cnt[w], 1u)] = (uint32_t)q;
   }

@@ -11,7 +11,9 @@
 //   warp 2      allocates / frees the 512 TMEM columns;
 //   warps 4-11  epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (the
 //               tile's rows) and columns 128 ((w - 4) / 4) .. +127 (queries).
-// Work items are (128-row tiles, query tile) pairs in a static round robin:
+// Work items are (128-row tiles, query tile) pairs, pulled by the producer
+// from a device queue (an atomic counter; a static round robin without one)
+// and handed to the MMA and epilogue warps through a two-entry ring:
 // mode 1 walks row chunks x query tiles (a chunk's query tiles run side by
 // side so the chunk is read from HBM once); mode 0 walks an item list
 // (approximate leaves x the queries routed there) for the bound pass; mode 3
@@ -48,14 +50,17 @@ constexpr uint32_t kPairBlock = 1024;        // survivor pairs reserved per warp
 constexpr uint32_t kSmQ = 0;                                   // 4 x 32 KB
 constexpr uint32_t kSmA = kSmQ + kResidentKB * kQBytes;        // kAStages x 16 KB
 constexpr uint32_t kSmBar = kSmA + kAStages * kABytes;         // mbarriers
-constexpr uint32_t kNumBars = 2 * kAStages + 2 + 4 + 1;        // full/empty, q full/empty, tmem full/empty x2, done
+constexpr uint32_t kNumBars = 2 * kAStages + 2 + 4 + 1 + 4;    // full/empty, q full/empty, tmem full/empty x2, done,
+                                                               // item full/empty x2
 constexpr uint32_t kSmTmem = kSmBar + kNumBars * 8;            // TMEM base address
 constexpr uint32_t kSmAbort = kSmTmem + 4;
 constexpr uint32_t kSmThr = (kSmAbort + 4 + 15) & ~15u;        // float [256]
 constexpr uint32_t kSmQidx = kSmThr + kUN * 4;                 // uint32 [256]
 constexpr uint32_t kSmQn2 = kSmQidx + kUN * 4;                 // float [256]
 constexpr uint32_t kSmOkw = kSmQn2 + kUN * 4;                  // int [8]: epilogue warps still running
-constexpr uint32_t kSmBytes = kSmOkw + 32;
+constexpr uint32_t kSmItem = kSmOkw + 32;                      // uint32 [2]: the item ring
+constexpr uint32_t kSmBytes = kSmItem + 8;
+constexpr uint32_t kNoItem = 0xffffffffu;                      // ring entry: no more items
 constexpr size_t kDynSmem = kSmBytes + 1024;                   // + alignment slack
 
 // --- PTX wrappers -------------------------------------------------------------
@@ -159,12 +164,17 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
 }
 
 // Instruction descriptor: FP32 accumulator, BF16 A and B, both K-major,
-// N = 256 (bits 17-22: N / 8), M = 128 (bits 24-28: M / 16).
+// N (bits 17-22: N / 8; a multiple of 16 up to 256), M = 128 (bits 24-28: M / 16).
 __host__ __device__ constexpr uint32_t idesc_for(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kUM >> 4) << 24);
 }
-// the bound pass groups at most kBatchBoundQueries queries per approximate
-// leaf, so its MMAs are N = 64 wide
+// MMA width of an item: its query count rounded up to 16, at most the tile
+// (the bound pass groups at most kBatchBoundQueries queries per approximate
+// leaf; a leaf's last query tile in the pruned filter is partly filled)
+__device__ __forceinline__ int item_n(uint32_t qcnt, int qtile) {
+  const int n = (int)((qcnt + 15u) & ~15u);
+  return n < 16 ? 16 : (n > qtile ? qtile : n);
+}
 
 __device__ __forceinline__ uint32_t ordered_key(float f) {
   const uint32_t b = __float_as_uint(f);
@@ -223,6 +233,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   auto tfull_bar = [&](int b) { return qempty_bar + 8u + 8u * b; };
   auto tempty_bar = [&](int b) { return qempty_bar + 24u + 8u * b; };
   const uint32_t done_bar = qempty_bar + 40u;
+  auto ifull_bar = [&](int sl) { return done_bar + 8u + 8u * sl; };
+  auto iempty_bar = [&](int sl) { return done_bar + 24u + 8u * sl; };
+  volatile uint32_t* s_item = reinterpret_cast<volatile uint32_t*>(sm + kSmItem);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + kSmAbort);
   float* s_thr = reinterpret_cast<float*>(sm + kSmThr);
   uint32_t* s_qidx = reinterpret_cast<uint32_t*>(sm + kSmQidx);
@@ -257,6 +270,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(tempty_bar(b), kEpiThreads / 32);
     }
     mbar_init(done_bar, 1);
+    for (int sl = 0; sl < 2; ++sl) {
+      mbar_init(ifull_bar(sl), 1);
+      mbar_init(iempty_bar(sl), 1 + kEpiThreads / 32);  // the MMA lane and every epilogue warp
+    }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -273,9 +290,18 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 0) {
     // ---------------- TMA producer
     if (lane == 0) {
-      uint32_t g = 0, it_n = 0;
+      uint32_t g = 0, it_n = 0, q_issued = 0;
       bool ok = true;
-      for (uint32_t w = blockIdx.x; ok && w < total; w += gridDim.x, ++it_n) {
+      for (;; ++it_n) {
+        // the next item into the ring (its entry free once every consumer
+        // has read it), or kNoItem when the queue is empty
+        const int sl = (int)(it_n & 1);
+        ok = mbar_wait(iempty_bar(sl), ((it_n >> 1) & 1) ^ 1, abort_flag, a.err);
+        if (!ok) break;
+        const uint32_t w = a.queue ? atomicAdd(a.queue, 1u) : blockIdx.x + it_n * gridDim.x;
+        s_item[sl] = w < total ? w : kNoItem;
+        mbar_arrive(ifull_bar(sl));
+        if (w >= total) break;
         const Item it = item_of(a, w, QT, ntiles, qtile, nq);
         if (resident) {
           ok = mbar_wait(qempty_bar, (it_n & 1) ^ 1, abort_flag, a.err);
@@ -283,6 +309,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           mbar_expect_tx(qfull_bar, (uint32_t)nkb * kQBytes);
           for (int kb = 0; kb < nkb; ++kb)
             tma_load_2d(base + kSmQ + kb * kQBytes, &tmQ, kb * kUK, (int)it.qoff, qfull_bar);
+          ++q_issued;
         }
         for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t) {
           const int row0 = (int)(it.rb + (uint64_t)t * kUM);
@@ -295,12 +322,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (!resident) tma_load_2d(base + kSmQ + s * kQBytes, &tmQ, kb * kUK, (int)it.qoff, full_bar(s));
           }
         }
+        if (!ok) break;
       }
       if (!ok) {
         // drain the copies still in flight before the CTA leaves
         const uint32_t first = g > nst ? g - nst : 0;
         for (uint32_t gg = first; gg < g; ++gg) drain_wait(full_bar((int)(gg % nst)), (gg / nst) & 1);
-        if (resident && it_n > 0) drain_wait(qfull_bar, (it_n - 1) & 1);
+        if (resident && q_issued > 0) drain_wait(qfull_bar, (q_issued - 1) & 1);
       }
     }
   } else if (warp == 1) {
@@ -308,7 +336,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (lane == 0) {
       uint32_t g = 0, tcount = 0, it_n = 0;
       bool ok = true;
-      for (uint32_t w = blockIdx.x; ok && w < total; w += gridDim.x, ++it_n) {
+      for (; ok; ++it_n) {
+        const int sl = (int)(it_n & 1);
+        ok = mbar_wait(ifull_bar(sl), (it_n >> 1) & 1, abort_flag, a.err);
+        if (!ok) break;
+        const uint32_t w = s_item[sl];
+        mbar_arrive(iempty_bar(sl));
+        if (w == kNoItem) break;
         const Item it = item_of(a, w, QT, ntiles, qtile, nq);
         if (resident) {
           ok = mbar_wait(qfull_bar, it_n & 1, abort_flag, a.err);
@@ -321,7 +355,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (!ok) break;
           tc_fence_after();
           const uint32_t d = tmem + (uint32_t)b * kUN;
-          const uint32_t idesc = idesc_for(qtile);
+          const uint32_t idesc = idesc_for(item_n(it.qcnt, qtile));
           for (int kb = 0; kb < nkb; ++kb, ++g) {
             const int s = (int)(g % nst);
             ok = mbar_wait(full_bar(s), (g / nst) & 1, abort_flag, a.err);
@@ -355,16 +389,31 @@ __global__ void __launch_bounds__(kThreads, 1)
     // the certified bounds this thread's columns used (a.errstat)
     float e_sum = 0.0f, e_rel = 0.0f, e_max = 0.0f;
     uint32_t e_cnt = 0, e_rcnt = 0;
-    for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
-      const Item it = item_of(a, w, QT, ntiles, qtile, nq);
+    for (uint32_t it_n = 0;; ++it_n) {
+      // the next item from the ring (lane 0 waits, bounded)
+      const int sl = (int)(it_n & 1);
+      uint32_t w = kNoItem;
+      int got = 1;
+      if (lane == 0) {
+        got = mbar_wait(ifull_bar(sl), (it_n >> 1) & 1, abort_flag, a.err) ? 1 : 0;
+        if (got) {
+          w = s_item[sl];
+          mbar_arrive(iempty_bar(sl));
+        }
+      }
+      got = __shfl_sync(HG_FULL, got, 0);
+      w = __shfl_sync(HG_FULL, w, 0);
+      ok = ok && got;
       // item boundary: every epilogue warp is done with the previous item
-      // and all of them learn whether any gave up
+      // and all of them learn whether any gave up; all of them read the
+      // same entry, so they leave together at the end of the queue
       if (lane == 0) s_okw[ew] = ok ? 1 : 0;
       named_sync(1, kEpiThreads);
       bool all_ok = true;
 #pragma unroll
       for (int i = 0; i < kEpiThreads / 32; ++i) all_ok = all_ok && s_okw[i] != 0;
-      if (!all_ok) break;
+      if (!all_ok || w == kNoItem) break;
+      const Item it = item_of(a, w, QT, ntiles, qtile, nq);
       // column etid of the query tile
       uint32_t q = 0xffffffffu;
       float4 qm = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -414,9 +463,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         s_thr[etid] = tv;
       }
       named_sync(1, kEpiThreads);
-      // the two warp groups split the tile's columns
-      const int c_lo = half * (qtile / 2);
-      const int c_hi = min(c_lo + qtile / 2, (int)it.qcnt);
+      // the two warp groups split the item's columns (32-column granules)
+      const int half_cols = min(qtile / 2, (int)((it.qcnt + 63u) / 64u) * 32);
+      const int c_lo = half * half_cols;
+      const int c_hi = min(c_lo + half_cols, (int)it.qcnt);
       // the row's |x|^2, loaded one tile ahead
       float xn_next = 0.0f;
       auto prefetch = [&](uint32_t t) {
