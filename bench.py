@@ -492,6 +492,8 @@ def main():
         "fp64_oracle": fp64,
         "stats": {"survivors_per_query": agg["survivors"] / (nb * steps),
                   "survivor_fraction": agg["survivors"] / max(agg["bf16_pairs"], 1),
+                  "leaf_pairs_kept_fraction": (agg["leaf_pairs_kept"] / agg["leaf_pairs"]) if agg["leaf_pairs"] else None,
+                  "filter_pairs_fraction": agg["bf16_pairs"] / (float(args.n) * nb * steps),
                   "rerank_rows_per_query": agg["rows_visited"] / (nb * steps),
                   "retried_queries_per_step": agg["retried_queries"] / steps,
                   "fallback_queries_per_step": agg["fallback_queries"] / steps,

@@ -53,7 +53,8 @@ class QueryStats(ctypes.Structure):
                 ("retried_queries", ctypes.c_uint64),
                 ("bound_ms", ctypes.c_double), ("gemm_ms", ctypes.c_double), ("rerank_ms", ctypes.c_double),
                 ("fallback_ms", ctypes.c_double), ("kernel_launches", ctypes.c_uint64),
-                ("err_mean", ctypes.c_double), ("err_max", ctypes.c_double), ("err_over_bound", ctypes.c_double)]
+                ("err_mean", ctypes.c_double), ("err_max", ctypes.c_double), ("err_over_bound", ctypes.c_double),
+                ("leaf_pairs", ctypes.c_uint64), ("leaf_pairs_kept", ctypes.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

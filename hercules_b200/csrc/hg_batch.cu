@@ -553,7 +553,8 @@ __global__ void k_group_items(const LeafPlan* __restrict__ plan, int nleaves, ui
 // a run of the item list (query tiles of kBatchQueryTile x chunks of tpi
 // 128-row tiles on the global tile grid).  ctl[0] = items, ctl[1] = panel
 // rows, ctl[2] = the dense pass's query count: 0, or nq when the panel or
-// the item list would overflow (the dense pass then filters every row).
+// the item list would overflow (the dense pass then filters every row),
+// ctl[3] = the kept (leaf, query) pairs.
 // pairs = sum over leaves of kept queries x leaf rows.
 __global__ void __launch_bounds__(kGroupThreads) k_group_pruned(const uint32_t* __restrict__ leaf_cnt,
                                                                 const LeafPlan* __restrict__ plan, int nleaves,
@@ -615,6 +616,7 @@ __global__ void __launch_bounds__(kGroupThreads) k_group_pruned(const uint32_t* 
     ctl[0] = fits ? (uint32_t)ti : 0u;
     ctl[1] = fits ? (uint32_t)tq : 0u;
     ctl[2] = fits ? 0u : nq;
+    ctl[3] = (uint32_t)tq;  // kept (leaf, query) pairs
     *pairs = fits ? tp : 0ull;
   }
 }

@@ -14,6 +14,7 @@
 #include <memory>
 #include <string>
 #include <thread>
+#include <map>
 #include <vector>
 
 #include "hg_arith.cuh"
@@ -354,6 +355,10 @@ static void free_device(hg_index* ix) {
   dfree(b.items3);
   dfree(b.pctl);
   dfree(b.ppairs);
+  dfree(b.useg_start);
+  dfree(b.useg_end);
+  dfree(b.seg_uid);
+  dfree(b.segstats);
   b = hg::BatchScratch{};
 }
 
@@ -1380,13 +1385,44 @@ static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket
 
 // Buffers of the pruned filter for b.nq_cap queries; *ok = false when they
 // would not fit their limits (the batch then filters every row): the kept
-// (leaf, query) lists within 1 GiB, the query panel within 2 GiB or one
+// (leaf, query) lists within 1 GiB, the query panel within 6 GiB or one
 // copy of the batch, whichever is larger.
 static hg_status ensure_prune_scratch(hg_index* ix, bool* ok) {
   hg::BatchScratch& b = ix->bs;
   const uint64_t nl = ix->leaves.size(), nq = b.nq_cap, L = ix->L;
   *ok = nl > 0 && nl * nq * 4 <= (1ull << 30);
   if (!*ok) return HG_OK;
+  if (!b.seg_uid) {
+    // distinct (start, end) segments over the leaves, in leaf_points order
+    std::map<std::pair<int, int>, int> ids;
+    std::vector<short> us, ue;
+    std::vector<int> uid;
+    for (int l : ix->leaves) {
+      int start = 0;
+      for (short e : ix->nodes[l].points) {
+        auto it = ids.emplace(std::make_pair(start, (int)e), (int)us.size());
+        if (it.second) {
+          us.push_back((short)start);
+          ue.push_back(e);
+        }
+        uid.push_back(it.first->second);
+        start = e;
+      }
+    }
+    b.nu = (int)us.size();
+    CK(dalloc(&b.useg_start, std::max<size_t>(us.size(), 1)));
+    CK(dalloc(&b.useg_end, std::max<size_t>(ue.size(), 1)));
+    CK(dalloc(&b.seg_uid, std::max<size_t>(uid.size(), 1)));
+    if (!us.empty()) {
+      CK(cudaMemcpy(b.useg_start, us.data(), sizeof(short) * us.size(), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(b.useg_end, ue.data(), sizeof(short) * ue.size(), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(b.seg_uid, uid.data(), sizeof(int) * uid.size(), cudaMemcpyHostToDevice));
+    }
+  }
+  if ((uint64_t)b.nu * nq * sizeof(float2) > (1ull << 30)) {
+    *ok = false;
+    return HG_OK;
+  }
   if (b.prune_nq >= nq && b.leaf_q) return HG_OK;
   dfree(b.leaf_cnt);
   dfree(b.leaf_q);
@@ -1397,8 +1433,9 @@ static hg_status ensure_prune_scratch(hg_index* ix, bool* ok) {
   dfree(b.items3);
   dfree(b.pctl);
   dfree(b.ppairs);
+  dfree(b.segstats);
   b.prune_nq = 0;
-  const uint64_t panel = std::min<uint64_t>(nl * nq, std::max<uint64_t>(nq, (2ull << 30) / (2 * L)));
+  const uint64_t panel = std::min<uint64_t>(nl * nq, std::max<uint64_t>(nq, (6ull << 30) / (2 * L)));
   // items for the narrowest work item (8 tiles): chunks of every leaf x its query tiles
   const uint64_t ntiles = (ix->n + hg::kBatchTileRows - 1) / hg::kBatchTileRows;
   const uint64_t items = (ntiles / 8 + 2 * nl) * ((nq + hg::kBatchQueryTile - 1) / hg::kBatchQueryTile);
@@ -1417,6 +1454,7 @@ static hg_status ensure_prune_scratch(hg_index* ix, bool* ok) {
   CK(dalloc(&b.items3, items));
   CK(dalloc(&b.pctl, 4));
   CK(dalloc(&b.ppairs, 1));
+  CK(dalloc(&b.segstats, std::max<uint64_t>((uint64_t)b.nu * nq, 1)));
   b.panel_cap = (uint32_t)panel;
   b.items3_cap = (uint32_t)items;
   HCK(encode_bf16_map(&b.panel_map, b.panel_bf, panel, (uint32_t)L, hg::kBatchQueryTile));
@@ -1565,8 +1603,10 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
   if (prune) {
     CK(cudaMemsetAsync(b.leaf_cnt, 0, sizeof(uint32_t) * nl, st));
     CK(cudaMemsetAsync(b.ppairs, 0, sizeof(unsigned long long), st));
-    CK(hg::launch_leaf_keep(b.qin, (int)L, (int)nq, d.leaf_seg_off, d.leaf_points, d.leaf_sk, d.leaf_size, nl, b.bound,
-                            b.leaf_cnt, b.leaf_q, b.prune_nq, st));
+    CK(hg::launch_leaf_keep(b.qin, (int)L, (int)nq, b.useg_start, b.useg_end, b.nu, b.segstats, d.leaf_seg_off,
+                            d.leaf_points, b.seg_uid, d.leaf_sk, d.leaf_size, nl, b.bound, b.leaf_cnt, b.leaf_q,
+                            b.prune_nq, st));
+    ++*launches;
     CK(hg::launch_group_pruned(b.leaf_cnt, b.leaf_q, b.prune_nq, b.leaf_plan, nl, ix->tune.filter_tiles_per_item,
                                b.panel_cap, b.items3_cap, nq, b.leaf_poff, b.leaf_ioff, b.pctl, b.ppairs,
                                b.panel_list, b.items3, st));
@@ -1804,6 +1844,10 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     stats->err_mean = es[2] > 0 ? es[0] / es[2] : 0.0;
     stats->err_max = es[4];
     stats->err_over_bound = es[3] > 0 ? es[1] / es[3] : 0.0;
+    uint64_t nonempty = 0;
+    for (int l : ix->leaves) nonempty += ix->nodes[l].node_size > 0 ? 1 : 0;
+    stats->leaf_pairs = prune ? (uint64_t)nq * nonempty : 0;
+    stats->leaf_pairs_kept = prune ? pc[3] : 0;
   }
   cudaEventDestroy(fb0);
   cudaEventDestroy(fb1);

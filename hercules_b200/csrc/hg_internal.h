@@ -148,6 +148,13 @@ struct BatchScratch {
   uint32_t* pctl = nullptr;              // [4] items, panel rows, dense-pass queries
   unsigned long long* ppairs = nullptr;  // (query, row) pairs of the pruned pass
   CUtensorMap panel_map;                 // TMA descriptor of panel_bf (64 x 256 boxes)
+  // distinct leaf segments (shared by many leaves) and the queries' mean and
+  // stdev over each
+  int nu = 0;
+  short* useg_start = nullptr;
+  short* useg_end = nullptr;
+  int* seg_uid = nullptr;                // per leaf segment (leaf_points order): its distinct segment
+  float2* segstats = nullptr;            // [prune_nq][nu]
 };
 
 }  // namespace hg

@@ -278,49 +278,70 @@ __global__ void k_leaf_lb(const float* __restrict__ q, int L, int nleaves, const
   if ((threadIdx.x & 31) == 0) lb[w] = sum;
 }
 
-// Leaves each query of a batch must filter: one block per query, a warp per
-// leaf computes LB_EAPCA exactly as k_leaf_lb (the reference arithmetic of
-// calculate_node_min_distance) and keeps the leaf when
+// Mean and stdev of every query over every distinct leaf segment (leaves
+// share most of their segments: a split refines its parent's), with the
+// reference arithmetic of calculate_node_min_distance's calc_mean_stdev_SIMD:
+// one block per query, a warp per segment (warp_mean_stdev for segments of 64
+// points or more, else hg_mean_stdev on one lane).  out[q * nu + u].
+__global__ void k_query_segstats(const float* __restrict__ Q, int L, int nq, const short* __restrict__ useg_start,
+                                 const short* __restrict__ useg_end, int nu, float2* __restrict__ out) {
+  extern __shared__ float qs[];
+  const int q = blockIdx.x;
+  if (q >= nq) return;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) qs[i] = Q[(uint64_t)q * L + i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int u = threadIdx.x >> 5; u < nu; u += nw) {
+    const int start = useg_start[u], end = useg_end[u];
+    float m, sd;
+    if (end - start >= 64) {
+      warp_mean_stdev(qs, start, end, &m, &sd);
+    } else {
+      hg_mean_stdev(qs, start, end, &m, &sd);  // every lane, the same values
+    }
+    if (lane == 0) out[(uint64_t)q * nu + u] = make_float2(m, sd);
+  }
+}
+
+// Leaves each query of a batch must filter: a warp per (query, leaf) sums
+// the LB_EAPCA terms of the leaf's segments in order (the plain path's
+// k_leaf_lb arithmetic, segment statistics from k_query_segstats) and keeps
+// the leaf when
 //     LB <= B_q (1 + 2^-10) + L 2^-20,
 // B_q the query's bound (+inf keeps every leaf).  The plain path scans only
 // leaves with LB <= its running bound <= B_q, so the kept leaves include
 // every leaf it scans; the margins cover the rounding of B_q's product.
 // Kept (leaf, query) pairs go to leaf_q[leaf * stride + i], counted in
 // leaf_cnt[leaf].
-__global__ void k_leaf_keep(const float* __restrict__ Q, int L, int nq, const int* __restrict__ seg_off,
-                            const short* __restrict__ points, const float* __restrict__ sk,
+__global__ void k_leaf_keep(const float2* __restrict__ segstats, int nu, int L, int nq,
+                            const int* __restrict__ seg_off, const short* __restrict__ points,
+                            const int* __restrict__ seg_uid, const float* __restrict__ sk,
                             const uint32_t* __restrict__ leaf_size, int nleaves, const float* __restrict__ bound,
                             uint32_t* leaf_cnt, uint32_t* leaf_q, uint32_t stride) {
-  extern __shared__ float qs[];
-  const int q = blockIdx.x;
-  if (q >= nq) return;
-  for (int i = threadIdx.x; i < L; i += blockDim.x) qs[i] = Q[(uint64_t)q * L + i];
-  __syncthreads();
+  const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= (uint64_t)nq * nleaves) return;
+  const int q = (int)(gw / nleaves), w = (int)(gw % nleaves);
+  if (leaf_size[w] == 0) return;
   const float B = bound[q];
   const float lim = B < __int_as_float(0x7f800000)
                         ? __fadd_ru(__fmul_ru(B, 1.0f + 0x1p-10f), __fmul_ru((float)L, 0x1p-20f))
                         : __int_as_float(0x7f800000);
-  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int w = threadIdx.x >> 5; w < nleaves; w += nw) {
-    if (leaf_size[w] == 0) continue;
-    const int off = seg_off[w], nseg = seg_off[w + 1] - off;
-    // lane s: the term of segment s (hg_mean_stdev is warp_mean_stdev's
-    // arithmetic); the terms are then added in segment order
-    float sum = 0.0f;
-    for (int s0 = 0; s0 < nseg && sum <= lim; s0 += 32) {
-      const int s = s0 + lane;
-      float term = 0.0f;
-      if (s < nseg) {
-        const int start = s == 0 ? 0 : points[off + s - 1], end = points[off + s];
-        float m, sd;
-        hg_mean_stdev(qs, start, end, &m, &sd);
-        term = hg_eapca_term(m, sd, sk + 4 * (off + s), end - start);
-      }
-      const int n = min(32, nseg - s0);
-      for (int j = 0; j < n; ++j) sum = __fadd_rn(sum, __shfl_sync(HG_FULL, term, j));
+  const int off = seg_off[w], nseg = seg_off[w + 1] - off;
+  const float2* st = segstats + (uint64_t)q * nu;
+  float sum = 0.0f;
+  for (int s0 = 0; s0 < nseg && sum <= lim; s0 += 32) {
+    const int s = s0 + lane;
+    float term = 0.0f;
+    if (s < nseg) {
+      const int start = s == 0 ? 0 : points[off + s - 1], end = points[off + s];
+      const float2 ms = st[seg_uid[off + s]];
+      term = hg_eapca_term(ms.x, ms.y, sk + 4 * (off + s), end - start);
     }
-    if (lane == 0 && sum <= lim) leaf_q[(uint64_t)w * stride + atomicAdd(&leaf_cnt[w], 1u)] = (uint32_t)q;
+    const int n = min(32, nseg - s0);
+    for (int j = 0; j < n; ++j) sum = __fadd_rn(sum, __shfl_sync(HG_FULL, term, j));
   }
+  if (lane == 0 && sum <= lim) leaf_q[(uint64_t)w * stride + atomicAdd(&leaf_cnt[w], 1u)] = (uint32_t)q;
 }
 
 // Candidate leaves: LB_EAPCA <= current bound, not the approximate leaf, not
@@ -1015,17 +1036,21 @@ cudaError_t launch_leaf_lb(const float* q, int L, int nleaves, const int* seg_of
   return cudaGetLastError();
 }
 
-cudaError_t launch_leaf_keep(const float* Q, int L, int nq, const int* seg_off, const short* points, const float* sk,
-                             const uint32_t* leaf_size, int nleaves, const float* bound, uint32_t* leaf_cnt,
-                             uint32_t* leaf_q, uint32_t stride, cudaStream_t s) {
+cudaError_t launch_leaf_keep(const float* Q, int L, int nq, const short* useg_start, const short* useg_end, int nu,
+                             float2* segstats, const int* seg_off, const short* points, const int* seg_uid,
+                             const float* sk, const uint32_t* leaf_size, int nleaves, const float* bound,
+                             uint32_t* leaf_cnt, uint32_t* leaf_q, uint32_t stride, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_leaf_keep, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
+    cudaFuncSetAttribute(k_query_segstats, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
     attr = true;
   }
-  if (nq <= 0) return cudaSuccess;
-  k_leaf_keep<<<nq, 256, sizeof(float) * L, s>>>(Q, L, nq, seg_off, points, sk, leaf_size, nleaves, bound, leaf_cnt,
-                                                 leaf_q, stride);
+  if (nq <= 0 || nleaves <= 0) return cudaSuccess;
+  k_query_segstats<<<nq, 256, sizeof(float) * L, s>>>(Q, L, nq, useg_start, useg_end, nu, segstats);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_leaf_keep<<<blocks_for((uint64_t)nq * nleaves * 32, 256), 256, 0, s>>>(
+      segstats, nu, L, nq, seg_off, points, seg_uid, sk, leaf_size, nleaves, bound, leaf_cnt, leaf_q, stride);
   return cudaGetLastError();
 }
 

@@ -102,9 +102,10 @@ cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s)
 cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s);
 // batched path: the (leaf, query) pairs whose LB_EAPCA is within the query's
 // bound (k_leaf_keep)
-cudaError_t launch_leaf_keep(const float* Q, int L, int nq, const int* seg_off, const short* points, const float* sk,
-                             const uint32_t* leaf_size, int nleaves, const float* bound, uint32_t* leaf_cnt,
-                             uint32_t* leaf_q, uint32_t stride, cudaStream_t s);
+cudaError_t launch_leaf_keep(const float* Q, int L, int nq, const short* useg_start, const short* useg_end, int nu,
+                             float2* segstats, const int* seg_off, const short* points, const int* seg_uid,
+                             const float* sk, const uint32_t* leaf_size, int nleaves, const float* bound,
+                             uint32_t* leaf_cnt, uint32_t* leaf_q, uint32_t stride, cudaStream_t s);
 // resident blocks per SM of the distance stream for series length L
 int ed_blocks_per_sm(int L);
 // the same with id = row index (EdArgs::ids unused)

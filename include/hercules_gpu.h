@@ -89,6 +89,9 @@ typedef struct {
   double err_mean;            /* mean err */
   double err_max;             /* largest err */
   double err_over_bound;      /* mean err / B_q (B_q > 0) */
+  uint64_t leaf_pairs;        /* batched path: (query, non-empty leaf) pairs */
+  uint64_t leaf_pairs_kept;   /* of those, the pairs LB_EAPCA keeps for the filter
+                                 (LB <= the query's bound) */
 } hg_query_stats;
 
 /* Search mode. */
