@@ -1385,8 +1385,9 @@ static hg_status ensure_batch_scratch(hg_index* ix, uint32_t nq, uint32_t bucket
 
 // Buffers of the pruned filter for b.nq_cap queries; *ok = false when they
 // would not fit their limits (the batch then filters every row): the kept
-// (leaf, query) lists within 1 GiB, the query panel within 6 GiB or one
-// copy of the batch, whichever is larger.
+// (leaf, query) lists within 1 GiB, the query panel within a quarter of the
+// free device memory (1 to 16 GiB) or one copy of the batch, whichever is
+// larger.
 static hg_status ensure_prune_scratch(hg_index* ix, bool* ok) {
   hg::BatchScratch& b = ix->bs;
   const uint64_t nl = ix->leaves.size(), nq = b.nq_cap, L = ix->L;
@@ -1435,7 +1436,10 @@ static hg_status ensure_prune_scratch(hg_index* ix, bool* ok) {
   dfree(b.ppairs);
   dfree(b.segstats);
   b.prune_nq = 0;
-  const uint64_t panel = std::min<uint64_t>(nl * nq, std::max<uint64_t>(nq, (6ull << 30) / (2 * L)));
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  const uint64_t budget = std::min<uint64_t>(16ull << 30, std::max<uint64_t>(1ull << 30, free_b / 4));
+  const uint64_t panel = std::min<uint64_t>(nl * nq, std::max<uint64_t>(nq, budget / (2 * L)));
   // items for the narrowest work item (8 tiles): chunks of every leaf x its query tiles
   const uint64_t ntiles = (ix->n + hg::kBatchTileRows - 1) / hg::kBatchTileRows;
   const uint64_t items = (ntiles / 8 + 2 * nl) * ((nq + hg::kBatchQueryTile - 1) / hg::kBatchQueryTile);
