@@ -14,7 +14,11 @@ collection and the step's queries already in HBM); `e2e` is the same through
 hg_knn_batch with the queries in pinned host memory and the answers copied
 back every step.  The plain per-query path (hg_knn_device, k = 10) is timed
 beside it on the same collection (`plain`), with the leaf-scan kernel's
-HBM roofline (`leaf_scan`).
+HBM roofline (`leaf_scan`), and so is the unindexed full scan (`pscan`,
+HG_MODE_PSCAN) with the reference's multi-threaded CPU PSCAN on a bounded
+sample beside it.  `fp64_oracle` checks a timed batch's answers against an
+FP64 brute force over the whole collection; `certified_bound` reports the
+filter's error bound.
 
 The BF16 copy of the collection (12.8 GB) and the raw rows (25.6 GB) are far
 larger than L2 (126 MB); every step streams them from HBM, so no L2 flush is
@@ -309,6 +313,57 @@ def cpu_reference_run(args, index_dir, queries_host, threads, extra=(), k=10):
     return per_q, wall
 
 
+def cpu_pscan_leg(args, H, queries_host, k):
+    """The reference's PSCAN (oracle/_ref/pscan, built from code/pscan) with
+    every host core on a bounded sample: the queries over the first m rows
+    of the same collection (about 1 GB, regenerated on the host with the
+    same seed), its Query_total_time_secs scaled by n / m to the full size."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    if not os.path.exists(O.REF_PSCAN):
+        return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/pscan not built"}
+    m = int(min(args.n, max(1, (1 << 28) // args.L)))
+    d = None
+    for base in ("/dev/shm", tempfile.gettempdir()):
+        try:
+            st = os.statvfs(base)
+            if st.f_bavail * st.f_frsize > m * args.L * 4 * 1.5:
+                d = tempfile.mkdtemp(prefix="hg_bench_pscan_", dir=base)
+                break
+        except OSError:
+            continue
+    if d is None:
+        return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": "unavailable: no host space for the sample"}
+    try:
+        gen = H.generate_unit_vectors if args.data == "unit" else H.generate_walks
+        data = os.path.join(d, "data.bin")
+        gen(DATA_SEED, m, args.L).tofile(data)
+        qfile = os.path.join(d, "queries.bin")
+        np.ascontiguousarray(queries_host, np.float32).tofile(qfile)
+        nq = queries_host.shape[0]
+        cmd = [O.REF_PSCAN, "--dataset", data, "--queries", qfile, "--dataset-size", str(m),
+               "--queries-size", str(nq), "--timeseries-size", str(args.L), "--k", str(k),
+               "--num-query-threads", str(cores + 1), "--dbsize", "120000"]
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900, cwd=d)
+        if r.returncode != 0:
+            return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
+                    "sample": "unavailable: reference PSCAN failed: " + r.stderr[-200:]}
+        secs = 0.0
+        for line in r.stdout.splitlines():
+            parts = line.split("\t")
+            if len(parts) == 5 and parts[0] == "Query_total_time_secs":
+                secs += float(parts[1])
+        per_q = secs / nq * (args.n / m)
+        return {"value": round(1.0 / per_q, 4) if per_q > 0 else None, "unit": UNIT, "cores": cores,
+                "kind": "reference",
+                "sample": "%d queries (k = %d) over the first %d rows of the collection; Query_total_time_secs "
+                          "scaled by %d / %d" % (nq, k, m, args.n, m)}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def write_index_for_cpu(ix, args):
     """The index in the reference's format where the host can read it fast."""
     need = args.n * args.L * 4 * 1.3
@@ -418,9 +473,31 @@ def main():
     plain_ms = p0.elapsed_time(p1)
     plain_qps = args.plain_queries / (plain_ms / 1000.0)
 
+    # PSCAN (every row of the collection per query, HG_MODE_PSCAN): the
+    # unindexed baseline, HBM-bound
+    npq = max(1, min(4, args.plain_queries))
+    ix.knn_device(Qp.data_ptr(), 1, pk, Dp.data_ptr(), Ip.data_ptr(), stream=stream, mode=H.MODE_PSCAN)
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    sst = ix.knn_device(Qp.data_ptr(), npq, pk, Dp.data_ptr(), Ip.data_ptr(), stream=stream, mode=H.MODE_PSCAN,
+                        profile=True)
+    s1.record()
+    torch.cuda.synchronize()
+    pscan_ms = s0.elapsed_time(s1)
+    pscan_bytes = 32.0 * sst["chunks_loaded"] + 8.0 * sst["rows_completed"]
+    pscan_scan_s = (sst["scan_ms"] if sst["scan_ms"] > 0 else pscan_ms) / 1000.0
+    pscan_gbs = pscan_bytes / pscan_scan_s / 1e9
+    pscan = {"value": round(npq / (pscan_ms / 1000.0), 2), "unit": UNIT, "queries": npq, "k": pk,
+             "path": "hg_knn_device, HG_MODE_PSCAN (every row, early abandon at the running k-th distance)",
+             "scan": {"kernel": "k_ed_stream", "achieved": round(pscan_gbs, 1), "unit": "GB/s",
+                      "frac": round(pscan_gbs / measured_peaks_all()["hbm"], 4),
+                      "algorithmic_bytes_per_query": pscan_bytes / npq}}
+
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu_baseline = cpu_baseline_leg(args, ix, cpu_q, ks[:args.cpu_sample_queries])
+        pscan["cpu_baseline"] = cpu_pscan_leg(args, H, Qp[:npq].cpu().numpy(), pk)
     ix.close()
 
     # roofline of the dominant kernel, the tensor-core filter k_umma_filter:
@@ -484,6 +561,7 @@ def main():
                   "path": "hg_knn_device (one query at a time, LB_SAX on)",
                   "batched_over_plain": round(value / plain_qps, 2) if plain_qps > 0 else None},
         "cpu_baseline": cpu_baseline,
+        "pscan": pscan,
         "clocks": ck,
         "certified_bound": {"err_mean": agg["err_mean"] / steps, "err_max": agg["err_max_max"],
                             "err_over_bound_mean": agg["err_over_bound"] / steps,
