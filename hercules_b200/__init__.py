@@ -63,7 +63,7 @@ class QueryStats(ctypes.Structure):
 class KnnOpts(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("use_lb_sax", ctypes.c_int), ("profile", ctypes.c_int),
                 ("approx_blocks", ctypes.c_int), ("bucket_cap", ctypes.c_int), ("dense_filter", ctypes.c_int),
-                ("reserved", ctypes.c_int * 2)]
+                ("epsilon", ctypes.c_float), ("nprobes", ctypes.c_int)]
 
 
 class Tuning(ctypes.Structure):
@@ -255,15 +255,17 @@ class HerculesIndex:
 
     # -- queries -------------------------------------------------------------
     def knn(self, queries, k=1, mode=MODE_PLAIN, use_lb_sax=False, with_leaf_pos=False, stats=False,
-            profile=False):
-        """Exact k-NN (squared distances ascending, dataset ids)."""
+            profile=False, epsilon=0.0, nprobes=0):
+        """Exact k-NN (squared distances ascending, dataset ids); epsilon > 0
+        or nprobes > 0 give the reference's epsilon-approximate or nprobes
+        search instead."""
         q = _f32(queries, self.L)
         nq = q.shape[0]
         d = np.zeros((nq, k), dtype=np.float32)
         ids = np.zeros((nq, k), dtype=np.int64)
         pos = np.zeros((nq, k), dtype=np.uint64) if with_leaf_pos else None
         st = QueryStats()
-        opts = KnnOpts(mode, 1 if use_lb_sax else 0, 1 if profile else 0)
+        opts = KnnOpts(mode, 1 if use_lb_sax else 0, 1 if profile else 0, 0, 0, 0, float(epsilon), int(nprobes))
         _check(lib().hg_knn(self._h, _ptr(q), nq, k, ctypes.byref(opts), _ptr(d), _ptr(ids), _ptr(pos),
                             ctypes.byref(st)))
         out = [d, ids]

@@ -14,10 +14,13 @@
  * --serial, --sims, --num-queues, --num-read-threads, --flush-threshold,
  * --num-write-threads, --initial-db-size, --eapca-threshold, --sax-threshold,
  * --approx-stop-condition, --buffer-size beyond recording it) are accepted and
- * have no effect: the exact answer does not depend on them.  Modes the GPU
- * path does not serve (epsilon/delta-approximate search, --nprobes,
- * --track-bsf, --track-pruning, --max-policy, --incremental) are refused with
- * a message instead of silently running something else.
+ * have no effect: the exact answer does not depend on them.  --epsilon E
+ * (> 0) runs the reference's epsilon-approximate search and --nprobes P its
+ * nprobes search (hercules_file_loaders.c:230-243: nprobes first); --delta is
+ * accepted and, as in the reference's serial path (which passes r_delta =
+ * FLT_MAX), has no effect.  Modes the GPU path does not serve (--track-bsf,
+ * --track-pruning, --max-policy, --incremental) are refused with a message
+ * instead of silently running something else.
  *
  * Added flags: --gpu N (device, default 0), --pscan (scan every row instead
  * of the index), --no-lb-sax (skip the per-row LB_SAX filter).
@@ -113,6 +116,8 @@ static int run_queries(const opts_t *o, hg_index *ix) {
   memset(&ko, 0, sizeof ko);
   ko.mode = o->pscan ? HG_MODE_PSCAN : HG_MODE_PLAIN;
   ko.use_lb_sax = o->lb_sax;
+  ko.epsilon = o->epsilon;
+  ko.nprobes = (int)o->nprobes;
   int ok = 1;
   for (unsigned i = 0; i < o->queries_size && ok; ++i) {
     if (fread(q, sizeof(float), L, f) != L) {
@@ -231,9 +236,13 @@ int main(int argc, char **argv) {
       default: return 1;
     }
   }
-  if (o.epsilon != 0 || o.delta != 1 || o.nprobes || o.track_bsf || o.track_pruning || o.max_policy ||
-      o.incremental) {
-    fprintf(stderr, "Error in hercules: only exact search (epsilon 0, delta 1) is served on the GPU\n");
+  if (o.track_bsf || o.track_pruning || o.max_policy || o.incremental) {
+    fprintf(stderr, "Error in hercules: --track-bsf, --track-pruning, --max-policy and --incremental are not "
+                    "served on the GPU\n");
+    return 1;
+  }
+  if (o.epsilon < 0 || (o.pscan && (o.epsilon > 0 || o.nprobes))) {
+    fprintf(stderr, "Error in hercules: --epsilon must not be negative and applies to the index search only\n");
     return 1;
   }
   if (o.index_path[strlen(o.index_path) - 1] != '/') {

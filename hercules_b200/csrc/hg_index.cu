@@ -1039,6 +1039,7 @@ static hg_status ensure_scratch(hg_index* ix, int k) {
   dfree(s.err);
   dfree(s.list);
   dfree(s.counters);
+  dfree(s.actl);
   s.nparts = hg::sm_count(ix->device) * hg::ed_blocks_per_sm((int)ix->L) * hg::kEdWarps;
   CK(dalloc(&s.lb, nl));
   CK(dalloc(&s.list, ix->n));
@@ -1057,6 +1058,7 @@ static hg_status ensure_scratch(hg_index* ix, int k) {
   CK(dalloc(&s.stats, 8));
   CK(dalloc(&s.err, 1));
   CK(dalloc(&s.q, 1));
+  CK(dalloc(&s.actl, 4));
   s.kmax = hg::kMaxK;
   return HG_OK;
 }
@@ -1196,6 +1198,189 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
                                 const hg_knn_opts& o, float* d_dist, int64_t* d_id, cudaStream_t st,
                                 hg_query_stats* stats, bool host_io = false);
 
+// Best-first queue of the approximate searches: a binary min-heap on the
+// node lower bound that moves an entry past another only when strictly
+// smaller and, between equal children, takes the left one -- the order in
+// which the reference's pqueue (pqueue.c, cmp_pri in hercules_query_engine.h)
+// pops equal bounds, so both visit nodes in the same sequence.
+struct PqEntry {
+  float d;
+  int node;
+};
+static void pq_push(std::vector<PqEntry>& h, PqEntry e) {
+  h.push_back(e);
+  size_t i = h.size() - 1;
+  while (i > 0) {
+    const size_t p = (i - 1) / 2;
+    if (!(h[p].d > h[i].d)) break;
+    std::swap(h[p], h[i]);
+    i = p;
+  }
+}
+static bool pq_pop(std::vector<PqEntry>& h, PqEntry* out) {
+  if (h.empty()) return false;
+  *out = h[0];
+  h[0] = h.back();
+  h.pop_back();
+  size_t i = 0;
+  for (;;) {
+    const size_t l = 2 * i + 1, r = l + 1;
+    if (l >= h.size()) break;
+    const size_t c = (r < h.size() && h[l].d > h[r].d) ? r : l;
+    if (!(h[i].d > h[c].d)) break;
+    std::swap(h[i], h[c]);
+    i = c;
+  }
+  return true;
+}
+
+// epsilon-approximate search (exact_de_knn_search with epsilon,
+// hercules_query_engine.c:2215-2448) or nprobes search (exact_ng_knn_search,
+// :2623-2796) of one query.  The tree walk runs on the host with the
+// reference's LB_EAPCA arithmetic on the tree's own envelopes (internal
+// nodes included, as the reference prunes with them); every leaf scan is a
+// distance-stream launch over the leaf's rows followed by the merge into the
+// query's top-k on the device.
+//  - epsilon: the walk collects leaves with the k-th distance of the
+//    approximate leaf (pop stops at LB > kth/(1+eps), children pushed at
+//    LB < kth/(1+eps)); the leaves are then taken in file_pos order, each
+//    scanned only if LB <= kth/(1+eps) with the k-th distance the reference
+//    holds at that moment: the value read before the last row of the
+//    previously scanned leaf.  So each leaf is scanned as its rows but the
+//    last, then the last row, and the k-th distance between the two is kept
+//    for the next leaf's test (k_leaf_gate, k_stale_copy; no host wait).
+//  - nprobes: a leaf is scanned when popped, at most nprobes leaves with the
+//    approximate one; the walk stops at a node whose LB exceeds the
+//    approximate leaf's best distance; children are pushed at LB < the
+//    current k-th distance (read back after each leaf).
+static hg_status knn_approx_one(hg_index* ix, const float* d_q, int k, const hg_knn_opts& o, float* d_dist,
+                                int64_t* d_id, cudaStream_t st) {
+  hg::QueryScratch& s = ix->s;
+  hg::DeviceIndex& d = ix->d;
+  const int L = (int)ix->L;
+  const int sms = hg::sm_count(ix->device);
+  const int ed_blocks = sms * hg::ed_blocks_per_sm(L);
+  hg::EdArgs e{};
+  e.rows = d.rows;
+  e.ids = d.ids;
+  e.L = L;
+  e.leaf_start = d.leaf_start;
+  e.leaf_size = d.leaf_size;
+  e.q = d_q;
+  e.k = k;
+  e.bound = s.bound;
+  e.parts = s.parts;
+  e.part_count = s.part_count;
+  e.stats = s.stats;
+  e.head = s.counters + 0;
+  CK(hg::launch_query_prep(d_q, L, index_tree(ix), d.leaf_start, d.leaf_size, s.approx_leaf, s.paa, s.cand,
+                           s.cand_lb, s.cand_count, s.unit_prefix, s.bound, s.topk_count, s.counters, st));
+  e.ident_leaf = s.approx_leaf;
+  CK(hg::launch_ed_stream(e, ed_blocks, st));
+  CK(hg::launch_merge(s.parts, s.part_count, ed_blocks * hg::kEdWarps, k, s.topk, s.topk_count, s.bound, s.err, st));
+  std::vector<float> q(L);
+  int approx = -1, cnt = 0;
+  uint32_t bound_bits = 0;
+  unsigned long long best_key = ~0ull;
+  CK(cudaMemcpyAsync(q.data(), d_q, sizeof(float) * L, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&approx, s.approx_leaf, sizeof approx, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&cnt, s.topk_count, sizeof cnt, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&bound_bits, s.bound, sizeof bound_bits, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&best_key, s.topk, sizeof best_key, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  // the reference's k-th distance: FLT_MAX until k results are held
+  auto kth_of = [&](int c, uint32_t bits) {
+    float f;
+    memcpy(&f, &bits, sizeof f);
+    return c >= k ? f : FLT_MAX;
+  };
+  float kth = kth_of(cnt, bound_bits);
+  float best = FLT_MAX;
+  if (cnt > 0) {
+    const uint32_t hi = (uint32_t)(best_key >> 32);
+    memcpy(&best, &hi, sizeof best);
+  }
+  // knn_results[0].node: the approximate leaf once it produced a result
+  const int approx_node = (cnt > 0 && approx >= 0) ? ix->leaves[approx] : -1;
+  auto lb_of = [&](int node) {
+    const hg::Node& n = ix->nodes[node];
+    return hg_lb_eapca(q.data(), (int)n.points.size(), n.points.data(), n.sk.data());
+  };
+  int* flag = reinterpret_cast<int*>(s.actl + 1);
+  uint32_t* stale = s.actl + 0;
+  // one leaf: its rows but the last, the stale k-th distance, the last row
+  auto scan_leaf = [&](int node, float lb, float eps1) -> hg_status {
+    const hg::Node& n = ix->nodes[node];
+    if (n.node_size == 0) return HG_OK;
+    CK(hg::launch_leaf_gate(lb, eps1, stale, flag, s.stats + 3, st));
+    e.gate = flag;
+    e.ident_leaf = nullptr;
+    const uint64_t first = n.file_pos, count = n.node_size;
+    if (count > 1) {
+      e.ident_first = first;
+      e.ident_count = count - 1;
+      CK(hg::launch_ed_stream(e, ed_blocks, st));
+      CK(hg::launch_merge(s.parts, s.part_count, ed_blocks * hg::kEdWarps, k, s.topk, s.topk_count, s.bound,
+                          s.err, st));
+    }
+    CK(hg::launch_stale_copy(flag, s.bound, stale, st));
+    e.ident_first = first + count - 1;
+    e.ident_count = 1;
+    CK(hg::launch_ed_stream(e, 1, st));
+    CK(hg::launch_merge(s.parts, s.part_count, hg::kEdWarps, k, s.topk, s.topk_count, s.bound, s.err, st));
+    return HG_OK;
+  };
+  std::vector<PqEntry> pq;
+  pq_push(pq, PqEntry{lb_of(0), 0});  // nodes[0] is the root
+  PqEntry it;
+  if (o.nprobes > 0) {
+    int probes = 1;
+    const float never = -FLT_MAX;  // a popped leaf is always scanned
+    while (pq_pop(pq, &it) && probes < o.nprobes) {
+      if (it.d > best) break;
+      const hg::Node& n = ix->nodes[it.node];
+      if (n.is_leaf) {
+        HCK(scan_leaf(it.node, never, 1.0f));
+        ++probes;
+        CK(cudaMemcpyAsync(&cnt, s.topk_count, sizeof cnt, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&bound_bits, s.bound, sizeof bound_bits, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        kth = kth_of(cnt, bound_bits);
+      } else {
+        for (int c : {n.left, n.right}) {
+          const float lb = lb_of(c);
+          if (lb < kth && c != approx_node) pq_push(pq, PqEntry{lb, c});
+        }
+      }
+    }
+  } else {
+    const float eps1 = 1.0f + o.epsilon;
+    std::vector<PqEntry> cand;
+    while (pq_pop(pq, &it)) {
+      if (it.d > kth / eps1) break;
+      const hg::Node& n = ix->nodes[it.node];
+      if (n.is_leaf) {
+        cand.push_back(it);
+      } else {
+        for (int c : {n.left, n.right}) {
+          const float lb = lb_of(c);
+          if (lb < kth / eps1 && c != approx_node) pq_push(pq, PqEntry{lb, c});
+        }
+      }
+    }
+    std::stable_sort(cand.begin(), cand.end(), [&](const PqEntry& a, const PqEntry& b) {
+      return ix->nodes[a.node].file_pos < ix->nodes[b.node].file_pos;
+    });
+    uint32_t kth_bits;
+    memcpy(&kth_bits, &kth, sizeof kth_bits);
+    CK(cudaMemcpyAsync(stale, &kth_bits, sizeof kth_bits, cudaMemcpyHostToDevice, st));
+    for (const PqEntry& c : cand) HCK(scan_leaf(c.node, c.d, eps1));
+  }
+  CK(hg::launch_emit(s.topk, s.topk_count, k, d_dist, d_id, st));
+  CK(cudaStreamSynchronize(st));  // kth_bits and the host vectors leave scope
+  return HG_OK;
+}
+
 static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t nq, uint32_t k,
                                  const hg_knn_opts* opts, float* d_dist, int64_t* d_id, cudaStream_t st,
                                  hg_query_stats* stats) {
@@ -1217,9 +1402,16 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
   CK(cudaMemsetAsync(ix->s.stats, 0, sizeof(unsigned long long) * 8, st));
   Prof prof;
   CK(cudaEventRecord(e0, st));
-  for (uint32_t i = 0; i < nq; ++i)
-    HCK(knn_one(ix, d_queries + (uint64_t)i * ix->L, (int)k, o, d_dist ? d_dist + (uint64_t)i * k : nullptr,
-                d_id ? d_id + (uint64_t)i * k : nullptr, st, o.profile ? &prof : nullptr));
+  const bool approx = o.mode == HG_MODE_PLAIN && (o.epsilon > 0.0f || o.nprobes > 0);
+  if (o.epsilon < 0.0f || o.nprobes < 0 || !(o.epsilon == o.epsilon))
+    return set_error(HG_ERR_ARG, "hg_knn: epsilon and nprobes must not be negative");
+  for (uint32_t i = 0; i < nq; ++i) {
+    const float* qi = d_queries + (uint64_t)i * ix->L;
+    float* di = d_dist ? d_dist + (uint64_t)i * k : nullptr;
+    int64_t* ii = d_id ? d_id + (uint64_t)i * k : nullptr;
+    if (approx) HCK(knn_approx_one(ix, qi, (int)k, o, di, ii, st));
+    else HCK(knn_one(ix, qi, (int)k, o, di, ii, st, o.profile ? &prof : nullptr));
+  }
   CK(cudaEventRecord(e1, st));
   unsigned long long hs[8];
   CK(cudaMemcpyAsync(hs, ix->s.stats, sizeof hs, cudaMemcpyDeviceToHost, st));

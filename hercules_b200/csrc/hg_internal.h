@@ -73,6 +73,7 @@ struct QueryScratch {
   unsigned long long* stats = nullptr;  // see ScanArgs
   uint32_t* list = nullptr;       // LB_SAX survivors (rows), n entries
   int* err = nullptr;             // device error flag
+  uint32_t* actl = nullptr;       // approximate searches: [0] stale k-th bound bits, [1] gate flag
 };
 
 // Batched path: BF16 copy of the rows and their norms, built on the first

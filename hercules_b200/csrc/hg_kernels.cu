@@ -646,6 +646,11 @@ __global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 3 : 4) k_ed_stream(Ed
   extern __shared__ float4 qs4[];  // the query, q4_bytes(L) bytes
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int slot_lead = lane & ~(kSlot - 1), j = lane & (kSlot - 1);
+  if (a.gate && *a.gate == 0) {
+    // a gated launch that did not pass: every warp reports an empty list
+    if (lane == 0) a.part_count[blockIdx.x * W + wib] = 0;
+    return;
+  }
   unsigned long long* list = lists[wib];
   for (int i = lane; i < kWarpListCap; i += 32) list[i] = ~0ull;
   for (int i = threadIdx.x; i < (a.L >> 2); i += blockDim.x)
@@ -1051,6 +1056,25 @@ cudaError_t launch_leaf_keep(const float* Q, int L, int nq, const short* useg_st
   if (e != cudaSuccess) return e;
   k_leaf_keep<<<blocks_for((uint64_t)nq * nleaves * 32, 256), 256, 0, s>>>(
       segstats, nu, L, nq, seg_off, points, seg_uid, sk, leaf_size, nleaves, bound, leaf_cnt, leaf_q, stride);
+  return cudaGetLastError();
+}
+
+__global__ void k_leaf_gate(float lb, float eps1, const uint32_t* stale, int* flag, unsigned long long* scanned) {
+  const float kth = __uint_as_float(*stale);
+  const int pass = lb <= __fdiv_rn(kth, eps1) ? 1 : 0;
+  *flag = pass;
+  if (pass) ++*scanned;
+}
+__global__ void k_stale_copy(const int* flag, const uint32_t* bound, uint32_t* stale) {
+  if (*flag) *stale = *bound;
+}
+cudaError_t launch_leaf_gate(float lb, float eps1, const uint32_t* stale, int* flag, unsigned long long* scanned,
+                             cudaStream_t s) {
+  k_leaf_gate<<<1, 1, 0, s>>>(lb, eps1, stale, flag, scanned);
+  return cudaGetLastError();
+}
+cudaError_t launch_stale_copy(const int* flag, const uint32_t* bound, uint32_t* stale, cudaStream_t s) {
+  k_stale_copy<<<1, 1, 0, s>>>(flag, bound, stale);
   return cudaGetLastError();
 }
 

@@ -67,6 +67,7 @@ struct EdArgs {
   unsigned long long* parts;   // per-warp sorted lists (kWarpListCap stride)
   int* part_count;
   unsigned long long* stats;   // [1] chunks computed [4] rows completed [5] rows started
+  const int* gate;             // if set and *gate == 0, the launch scans nothing
 };
 
 int sm_count(int device);
@@ -106,6 +107,13 @@ cudaError_t launch_leaf_keep(const float* Q, int L, int nq, const short* useg_st
                              float2* segstats, const int* seg_off, const short* points, const int* seg_uid,
                              const float* sk, const uint32_t* leaf_size, int nleaves, const float* bound,
                              uint32_t* leaf_cnt, uint32_t* leaf_q, uint32_t stride, cudaStream_t s);
+// epsilon search: *flag = (lb <= stale / eps1), the reference's test of a
+// candidate leaf against its k-th distance of that moment; *scanned counts
+// the leaves that pass
+cudaError_t launch_leaf_gate(float lb, float eps1, const uint32_t* stale, int* flag, unsigned long long* scanned,
+                             cudaStream_t s);
+// *stale = *bound when *flag
+cudaError_t launch_stale_copy(const int* flag, const uint32_t* bound, uint32_t* stale, cudaStream_t s);
 // resident blocks per SM of the distance stream for series length L
 int ed_blocks_per_sm(int L);
 // the same with id = row index (EdArgs::ids unused)

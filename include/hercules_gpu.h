@@ -109,7 +109,12 @@ typedef struct {
                          query falls back to the plain path (0 = 65536) */
   int dense_filter;   /* HG_MODE_BATCH: 1 = filter every row against every query
                          (no LB_EAPCA leaf pruning before the filter) */
-  int reserved[2];
+  float epsilon;      /* HG_MODE_PLAIN, > 0: epsilon-approximate search of
+                         exact_de_knn_search (hercules_query_engine.c:2215-2448):
+                         leaves pruned at LB > kth / (1 + epsilon) */
+  int nprobes;        /* HG_MODE_PLAIN, > 0: exact_ng_knn_search (:2623-2796):
+                         at most nprobes leaves, best-first; takes precedence
+                         over epsilon like the reference's dispatch */
 } hg_knn_opts;
 
 /* ---- status ----------------------------------------------------------- */

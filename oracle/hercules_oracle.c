@@ -956,6 +956,108 @@ int or_exact_knn(const or_index *ix, const float *q, int k, int tie_lowest, floa
   return cur;
 }
 
+/* The approximate searches of the reference's serial query path
+ * (hercules_file_loaders.c:230-243 dispatch):
+ *  - nprobes > 0: exact_ng_knn_search (hercules_query_engine.c:2623-2796):
+ *    best-first over node LBs, a leaf scanned as soon as it is popped, at
+ *    most nprobes leaves including the approximate one; stops when a popped
+ *    node's LB exceeds the approximate search's best distance; children are
+ *    pushed when LB < the current k-th distance;
+ *  - else exact_de_knn_search with epsilon (:2215-2448): the traversal
+ *    collects leaves with the k-th distance of the approximate leaf fixed
+ *    (break when LB > kth/(1+eps), push when LB < kth/(1+eps)), then scans
+ *    them in file_pos order, each only if LB <= kth/(1+eps) with the k-th
+ *    distance of that moment.  r_delta is not used on this path.
+ * The comparisons are the reference's in both tie modes; tie_lowest only
+ * changes the top-k insert (lowest id on an exact FP32 tie). */
+int or_approx_knn(const or_index *ix, const float *q, int k, int tie_lowest, float epsilon, int nprobes,
+                  float *d_out, int64_t *row_out, uint64_t *filepos_out, or_stats *st) {
+  if (k <= 0 || !ix->root) return -1;
+  float *dist = (float *)malloc(sizeof(float) * k);
+  int64_t *id = (int64_t *)malloc(sizeof(int64_t) * k);
+  uint64_t *row = (uint64_t *)malloc(sizeof(uint64_t) * k);
+  for (int i = 0; i < k; ++i) {
+    dist[i] = FLT_MAX;
+    id[i] = -1;
+    row[i] = UINT64_MAX;
+  }
+  int cur = 0;
+  or_stats s;
+  memset(&s, 0, sizeof s);
+  float kth_var = FLT_MAX;
+  or_node *n = ix->root;
+  while (!n->is_leaf) n = route_left(n, q) ? n->left : n->right;
+  const or_node *approx = n;
+  scan_leaf(ix, n, q, k, tie_lowest, dist, id, row, &cur, &kth_var);
+  s.loaded_leaves = 1;
+  s.loaded_rows = n->node_size;
+  s.approx_leaf = (uint32_t)n->leaf_index;
+  const or_node *approx_node = (cur > 0) ? approx : NULL;
+  const float approx_best = dist[0];
+  const float eps1 = 1.0f + epsilon;
+  pq_t pq = {0, 0, 0};
+  pq_item *cand = (pq_item *)malloc(sizeof(pq_item) * (ix->num_leaves + 1));
+  int ncand = 0;
+  pq_item root = {or_lb_eapca(q, ix->root->nseg, ix->root->points, ix->root->sk), ix->root};
+  pq_push(&pq, root);
+  pq_item it;
+  if (nprobes > 0) {
+    int probes = 1;
+    while (pq_pop(&pq, &it) && probes < nprobes) {
+      if (it.d > approx_best) break;
+      if (it.n->is_leaf) {
+        s.loaded_leaves++;
+        s.loaded_rows += it.n->node_size;
+        scan_leaf(ix, it.n, q, k, tie_lowest, dist, id, row, &cur, &kth_var);
+        ++probes;
+      } else {
+        const float kth = dist[k - 1];
+        or_node *ch[2] = {it.n->left, it.n->right};
+        for (int c = 0; c < 2; ++c) {
+          const float lb = or_lb_eapca(q, ch[c]->nseg, ch[c]->points, ch[c]->sk);
+          if (lb < kth && ch[c] != approx_node) pq_push(&pq, (pq_item){lb, ch[c]});
+        }
+      }
+    }
+  } else {
+    while (pq_pop(&pq, &it)) {
+      const float kth = dist[k - 1];
+      kth_var = kth;
+      if (it.d > kth / eps1) break;
+      if (it.n->is_leaf) {
+        cand[ncand++] = it;
+      } else {
+        or_node *ch[2] = {it.n->left, it.n->right};
+        for (int c = 0; c < 2; ++c) {
+          const float lb = or_lb_eapca(q, ch[c]->nseg, ch[c]->points, ch[c]->sk);
+          if (lb < kth / eps1 && ch[c] != approx_node) pq_push(&pq, (pq_item){lb, ch[c]});
+        }
+      }
+    }
+    s.candidate_leaves = (uint32_t)ncand;
+    qsort(cand, ncand, sizeof(pq_item), cmp_cand);
+    for (int i = 0; i < ncand; ++i) {
+      if (cand[i].d <= kth_var / eps1) {
+        s.loaded_leaves++;
+        s.loaded_rows += cand[i].n->node_size;
+        scan_leaf(ix, cand[i].n, q, k, tie_lowest, dist, id, row, &cur, &kth_var);
+      }
+    }
+  }
+  free(pq.a);
+  free(cand);
+  for (int i = 0; i < k; ++i) {
+    d_out[i] = dist[i];
+    if (row_out) row_out[i] = i < cur ? (int64_t)row[i] : -1;
+    if (filepos_out) filepos_out[i] = i < cur ? leaf_pos_of_row(ix, row[i]) : 0;
+  }
+  if (st) *st = s;
+  free(dist);
+  free(id);
+  free(row);
+  return cur;
+}
+
 int or_pscan(const float *data, uint64_t n, int L, const float *q, int k, int tie_lowest,
              float *d_out, int64_t *id_out) {
   float *dist = (float *)malloc(sizeof(float) * k);

@@ -93,6 +93,10 @@ typedef struct {
 /* exact_de_knn_search, hercules_query_engine.c:2215-2448 (epsilon = 0).
  * Outputs k squared distances (ascending), the leaf-ordered row of each
  * answer and its leaf's file_pos.  tie_lowest selects the tie rule. */
+/* epsilon-approximate (nprobes == 0) or nprobes search of the reference's
+ * serial path (exact_de_knn_search with epsilon, exact_ng_knn_search). */
+int or_approx_knn(const or_index *ix, const float *q, int k, int tie_lowest, float epsilon, int nprobes,
+                  float *d_out, int64_t *row_out, uint64_t *filepos_out, or_stats *st);
 int or_exact_knn(const or_index *ix, const float *q, int k, int tie_lowest,
                  float *d_out, int64_t *row_out, uint64_t *filepos_out, or_stats *st);
 

@@ -82,6 +82,7 @@ def olib():
             "or_row_ids": (None, [_P, _P]),
             "or_rows": (_P, [_P]),
             "or_exact_knn": (i32, [_P, _P, i32, i32, _P, _P, _P, ctypes.POINTER(_Stats)]),
+            "or_approx_knn": (i32, [_P, _P, i32, i32, ctypes.c_float, i32, _P, _P, _P, ctypes.POINTER(_Stats)]),
             "or_leaf_lbs": (None, [_P, _P, _P]),
             "or_pscan": (i32, [_P, u64, i32, _P, i32, i32, _P, _P]),
         }
@@ -254,6 +255,18 @@ class OracleIndex:
         fp = np.zeros(k, np.uint64)
         st = _Stats()
         olib().or_exact_knn(self.h, _p(q), k, 1 if tie_lowest else 0, _p(d), _p(rows), _p(fp), ctypes.byref(st))
+        return d, rows, fp, {f: getattr(st, f) for f, _ in st._fields_}
+
+    def approx_knn(self, q, k=1, epsilon=0.0, nprobes=0, tie_lowest=True):
+        """exact_de_knn_search with epsilon, or exact_ng_knn_search with nprobes:
+        (squared distances, leaf-ordered rows, leaf file_pos, stats)."""
+        q = np.ascontiguousarray(q, np.float32)
+        d = np.zeros(k, np.float32)
+        rows = np.zeros(k, np.int64)
+        fp = np.zeros(k, np.uint64)
+        st = _Stats()
+        olib().or_approx_knn(self.h, _p(q), k, 1 if tie_lowest else 0, float(epsilon), int(nprobes), _p(d),
+                             _p(rows), _p(fp), ctypes.byref(st))
         return d, rows, fp, {f: getattr(st, f) for f, _ in st._fields_}
 
     def leaf_lbs(self, q):

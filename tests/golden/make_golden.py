@@ -12,7 +12,8 @@ oracle/Makefile `ref`); the GPU box only reads the committed outputs.
                                of the reference's leaves_raw.idx and
                                leaves_sims.idx and of its root.idx fields;
                                the reference CLI's answers (Query_exact_*)
-                               and per-query load counters
+                               and per-query load counters, exact and with
+                               --epsilon 0.5 / 2 and --nprobes 3 / 10
 """
 import hashlib
 import json
@@ -38,6 +39,8 @@ CONFIGS = [
 ]
 DATA_SEED = 1184
 QUERY_SEED = 14784
+APPROX_MODES = [("eps0.5", ("--epsilon", "0.5")), ("eps2", ("--epsilon", "2")),
+                ("np3", ("--nprobes", "3")), ("np10", ("--nprobes", "10"))]
 
 
 def sha(b):
@@ -154,6 +157,15 @@ def ref_config(name, n, L, leaf, nq, k):
                     "loaded_nodes": q["Query_total_loaded_nodes_count"][:, 0].tolist(),
                     "loaded_ts": q["Query_total_loaded_ts_count"][:, 0].tolist(),
                 }
+                # the approximate searches of the same serial path
+                res["approx"] = {}
+                for mode, extra in APPROX_MODES:
+                    qa = O.ref_query(binary, d, os.path.join(tmp, "q.bin"), nq, k, extra=extra)
+                    res["approx"][mode] = {
+                        "args": list(extra),
+                        "exact_distance": qa["Query_exact_distance"].tolist(),
+                        "exact_node_file_pos": qa["Query_exact_node_file_pos"].tolist(),
+                    }
                 hdr, nodes = O.parse_root_idx(d + "root.idx")
                 res["num_leaves"] = hdr[0]
                 res["num_nodes"] = len(nodes)

@@ -107,6 +107,43 @@ def test_knn_matches_oracle(built, name, k, lbsax):
     assert st["rows_visited"] > 0
 
 
+APPROX = {"eps0.5": (0.5, 0), "eps2": (2.0, 0), "np3": (0.0, 3), "np10": (0.0, 10)}
+
+
+@pytest.mark.parametrize("name", REF_CONFIGS)
+@pytest.mark.parametrize("mode", sorted(APPROX))
+def test_approximate_searches_match_oracle_and_reference(built, name, mode):
+    """epsilon-approximate and nprobes searches (host tree walk, leaf scans on
+    the GPU): bit-identical to the oracle's, the reference CLI's printed
+    answers (golden), and the same number of leaves scanned."""
+    g, X, Q, ix, oi = built[name]
+    eps, npr = APPROX[mode]
+    ids_map = oi.row_ids()
+    want = g["approx"][mode]
+    for k in (1, g["k"], 50):
+        d, ids, pos, st = ix.knn(Q, k, with_leaf_pos=True, stats=True, epsilon=eps, nprobes=npr)
+        loaded = 0
+        for j, q in enumerate(Q):
+            od, orow, ofp, ost = oi.approx_knn(q, k, epsilon=eps, nprobes=npr, tie_lowest=True)
+            assert np.array_equal(bits(d[j]), bits(od)), (mode, k, j)
+            assert np.array_equal(ids[j], ids_map[orow]), (mode, k, j)
+            loaded += ost["loaded_leaves"] - 1  # the oracle counts the approximate leaf
+            if k == g["k"]:
+                assert ["%f" % np.sqrt(v) for v in d[j]] == want["exact_distance"][j], (mode, j)
+                assert [str(int(v)) for v in pos[j]] == want["exact_node_file_pos"][j], (mode, j)
+        assert st["leaves_scanned"] == loaded, (mode, k)
+
+
+def test_approximate_search_arguments(built):
+    g, X, Q, ix, oi = built[REF_CONFIGS[0]]
+    with pytest.raises(Exception):
+        ix.knn(Q[:1], 5, epsilon=-1.0)
+    # epsilon 0 and nprobes 0 are the exact search
+    d0, i0 = ix.knn(Q[:4], 5)
+    d1, i1 = ix.knn(Q[:4], 5, epsilon=0.0, nprobes=0)
+    assert np.array_equal(bits(d0), bits(d1)) and np.array_equal(i0, i1)
+
+
 @pytest.mark.parametrize("name", REF_CONFIGS)
 def test_knn_matches_reference_cli(built, name):
     """Printed distances (sqrt, %f) and the answer leaf's file_pos of the
@@ -232,6 +269,22 @@ def test_cli_is_a_drop_in_for_the_reference_cli(hg, tmp_path, gpu_available):
         for r_ in range(g["k"]):
             assert got[("Query_exact_distance", j + 1, r_ + 1)] == g["answers"]["exact_distance"][j][r_]
             assert got[("Query_exact_node_file_pos", j + 1, r_ + 1)] == g["answers"]["exact_node_file_pos"][j][r_]
+    # the approximate searches with the reference's flags
+    for mode, want in g["approx"].items():
+        r = subprocess.run([cli, "--mode", "1", "--serial", "1", "--num-threads", "1", "--k", str(g["k"]),
+                            "--queries", qf, "--queries-size", str(g["nq"]), "--index-path", idx, "--delta", "1",
+                            *want["args"]], capture_output=True, text=True)
+        assert r.returncode == 0, (mode, r.stderr)
+        got = {}
+        for line in r.stdout.splitlines():
+            p = line.split("\t")
+            if len(p) == 5 and p[0] in ("Query_exact_distance", "Query_exact_node_file_pos"):
+                got[(p[0], int(p[3]), int(p[4]))] = p[1]
+        for j in range(g["nq"]):
+            assert [got[("Query_exact_distance", j + 1, r_ + 1)] for r_ in range(g["k"])] == \
+                want["exact_distance"][j], (mode, j)
+            assert [got[("Query_exact_node_file_pos", j + 1, r_ + 1)] for r_ in range(g["k"])] == \
+                want["exact_node_file_pos"][j], (mode, j)
 
 
 def test_device_unit_generator_matches_host(hg, gpu_available):

@@ -108,6 +108,29 @@ def test_oracle_index_and_answers_match_reference_golden(oracle_mod, hg, tmp_pat
         assert st["loaded_rows"] == int(g["answers"]["loaded_ts"][j])
 
 
+APPROX = {"eps0.5": (0.5, 0), "eps2": (2.0, 0), "np3": (0.0, 3), "np10": (0.0, 10)}
+
+
+@pytest.mark.parametrize("name", REF_CONFIGS)
+def test_oracle_approximate_searches_match_reference_golden(oracle_mod, hg, name):
+    """The oracle's epsilon and nprobes searches print the reference CLI's
+    answers (--epsilon 0.5 / 2, --nprobes 3 / 10) on the reference's index."""
+    g = json.load(open(golden_path(f"ref_{name}.json")))
+    X = hg.generate_walks(g["data_seed"], g["n"], g["L"])
+    Q = hg.generate_queries(g["query_seed"], X, np.array(g["sigma2"]))
+    oi = oracle_mod.OracleIndex.build(X, g["leaf"])
+    differs = 0
+    for mode, (eps, npr) in APPROX.items():
+        want = g["approx"][mode]
+        for j in range(g["nq"]):
+            dist, rows, fp, st = oi.approx_knn(Q[j], g["k"], epsilon=eps, nprobes=npr, tie_lowest=False)
+            assert ["%f" % np.sqrt(np.float32(v)) for v in dist] == want["exact_distance"][j], (mode, j)
+            assert [str(int(v)) for v in fp] == want["exact_node_file_pos"][j], (mode, j)
+            differs += want["exact_distance"][j] != g["answers"]["exact_distance"][j]
+    # nprobes answers are approximate: some differ from the exact ones
+    assert differs > 0
+
+
 def test_tie_rule_lowest_id_on_duplicates(oracle_mod, hg):
     """Duplicate series: the reference keeps the first one met and drops
     equal distances; the lowest-id rule keeps the smallest id instead; the
