@@ -239,20 +239,29 @@ __device__ __forceinline__ float chunk_d2_v4(const float* q, const float* x, int
 // Segment re-rank: persistent warps take segments from a counter.  A warp
 // starts from step 2's list, shares the query's running k-th distance through
 // qbound (float bits, atomicMin) and writes its compacted list as one part.
-// Within the warp, 16 two-lane slots: lane j of a slot computes chunks
-// ch + 2j and ch + 2j + 1, and both lanes add the four in order
-// (ts_euclidean_distance_SIMD's order).
+// Within the warp, 32 / kSlot slots of kSlot lanes: lane j of a slot computes
+// chunks ch + kSlot l + j (l < kLines) and every lane of the slot adds the
+// step's kSlot * kLines chunk sums in order (ts_euclidean_distance_SIMD's
+// order); one abandon test per step, as the step's lines are loaded already.
+// Short series use 2-lane slots (16 rows per warp, 128 bytes of each per
+// step); long ones 8-lane slots (4 rows, 512 bytes).
 constexpr int kRankWarps = 8;
+template <int kSlot>
+__host__ __device__ constexpr uint32_t rank_leaders() {
+  return kSlot == 2 ? 0x55555555u : (kSlot == 4 ? 0x11111111u : (kSlot == 8 ? 0x01010101u : 0x00010001u));
+}
+template <int kSlot, int kLines>
 __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_part(BatchRank a) {
   __shared__ unsigned long long lists[kRankWarps][kWarpListCap];
+  constexpr int kStep = kSlot * kLines;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int slot_lead = lane & ~1, j = lane & 1;
+  const int slot_lead = lane & ~(kSlot - 1), j = lane & (kSlot - 1);
   unsigned long long* list = lists[wib];
   const float inf = __int_as_float(0x7f800000);
   const int nlist = a.nlist_dev ? (int)*a.nlist_dev : a.nlist;
   const uint32_t total_items = a.seg_prefix[nlist];
   const int nch = a.L >> 3;
-  const uint32_t leaders = 0x55555555u;
+  const uint32_t leaders = rank_leaders<kSlot>();
   unsigned long long n_rows = 0, n_chunks = 0;
   for (;;) {
     uint32_t item = 0;
@@ -285,16 +294,19 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_part(BatchRank a) {
     uint32_t row = 0;
     int ch = 0;
     float dist = 0.0f;
+    const float4* x = nullptr;
+    const float4* qc = reinterpret_cast<const float4*>(qv) + 2 * j;
     for (;;) {
       const uint32_t need = __ballot_sync(HG_FULL, !valid) & leaders;
       if (need && next < last) {
         const int r = __popc(need & ((1u << slot_lead) - 1));
-        const uint32_t avail = min(last - next, 16u);
+        const uint32_t avail = min(last - next, (uint32_t)(32 / kSlot));
         if (((need >> slot_lead) & 1u) && (uint32_t)r < avail) {
           row = bk[next + r];
           valid = true;
           dist = 0.0f;
           ch = 0;
+          x = reinterpret_cast<const float4*>(a.rows + (uint64_t)row * a.L) + 2 * j;
           if (j == 0) ++n_rows;
         }
         next += min((uint32_t)__popc(need), avail);
@@ -302,28 +314,52 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_part(BatchRank a) {
         B = fminf(B, __uint_as_float(ld_volatile(&a.qbound[q])));
       }
       if (!__any_sync(HG_FULL, valid)) break;
-      const float* xr = a.rows + (uint64_t)row * a.L;
-      const int ca = ch + 2 * j;
-      float d0 = 0.0f, d1 = 0.0f;
-      if (valid && ca < nch) d0 = chunk_d2_v4(qv, xr, ca);
-      if (valid && ca + 1 < nch) d1 = chunk_d2_v4(qv, xr, ca + 1);
-      const float p0 = __shfl_xor_sync(HG_FULL, d0, 1), p1 = __shfl_xor_sync(HG_FULL, d1, 1);
-      // the slot's four chunk values in order
-      const float dv[4] = {j ? p0 : d0, j ? p1 : d1, j ? d0 : p0, j ? d1 : p1};
-      bool finished = false;
+      // chunk ch + kSlot l + j of the row (0 past the row's end: adding it
+      // leaves a sum unchanged)
+      float dl[kLines];
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        if (valid && ch + t < nch) {
-          dist = __fadd_rn(dist, dv[t]);
-          if (j == 0) ++n_chunks;
-          if (dist > B) valid = false;  // partial sums only grow: this row cannot enter
+      for (int l = 0; l < kLines; ++l) {
+        const bool in = valid && ch + kSlot * l + j < nch;
+        float4 x0, x1, q0, q1;
+        if (in) {
+          x0 = x[2 * kSlot * l];
+          x1 = x[2 * kSlot * l + 1];
+          q0 = qc[2 * ch + 2 * kSlot * l];
+          q1 = qc[2 * ch + 2 * kSlot * l + 1];
         }
+        const float qq[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+        const float xx[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+        const float d = hg_chunk_d2(qq, xx);
+        dl[l] = in ? d : 0.0f;
       }
+      float part[kStep];
+      float acc = dist;
+#pragma unroll
+      for (int t = 0; t < kStep; ++t) {
+        acc = __fadd_rn(acc, __shfl_sync(HG_FULL, dl[t / kSlot], slot_lead + (t % kSlot)));
+        part[t] = acc;
+      }
+      bool finished = false;
       if (valid) {
-        ch += 4;
-        if (ch >= nch) {
-          finished = true;
+        if (acc > B) {
+          // partial sums only grow: this row cannot enter; the reference
+          // reads up to the first chunk whose sum exceeds the bound
+          if (j == 0) {
+            int used = 1;
+#pragma unroll
+            for (int t = 0; t < kStep; ++t) used += part[t] <= B ? 1 : 0;
+            n_chunks += (unsigned long long)(ch + used);
+          }
           valid = false;
+        } else {
+          dist = acc;
+          ch += kStep;
+          x += 2 * kStep;
+          if (ch >= nch) {
+            finished = true;
+            valid = false;
+            if (j == 0) n_chunks += (unsigned long long)nch;
+          }
         }
       }
       const bool take = finished && j == 0;
@@ -782,7 +818,8 @@ cudaError_t launch_rerank(const BatchRank& r, int part_blocks, cudaStream_t s) {
   k_rerank_plan<<<1, 1024, 0, s>>>(r);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_rerank_part<<<part_blocks, kRankWarps * 32, 0, s>>>(r);
+  if (r.L >= 4096) k_rerank_part<8, 2><<<part_blocks, kRankWarps * 32, 0, s>>>(r);
+  else k_rerank_part<2, 2><<<part_blocks, kRankWarps * 32, 0, s>>>(r);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_rerank_merge<<<nblk(r.nlist, kRankWarps), kRankWarps * 32, 0, s>>>(r);
