@@ -118,6 +118,15 @@ __global__ void k_tile_norms(const float4* __restrict__ meta, uint64_t n, float4
 // kMaxK smallest are ranked exactly (hg_ed, reference order) and the k-th
 // distinct distance among them bounds the query's k-th neighbour distance
 // (more rows than k: a tighter bound, and k distinct distances despite ties).
+// squared distance of chunk c of x (8 floats) to the same chunk of q
+__device__ __forceinline__ float chunk_d2_v4(const float* q, const float* x, int c) {
+  const float4 x0 = reinterpret_cast<const float4*>(x)[2 * c], x1 = reinterpret_cast<const float4*>(x)[2 * c + 1];
+  const float4 q0 = reinterpret_cast<const float4*>(q)[2 * c], q1 = reinterpret_cast<const float4*>(q)[2 * c + 1];
+  const float qq[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+  const float xx[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+  return hg_chunk_d2(qq, xx);
+}
+
 constexpr int kSelThreads = 256;
 __global__ void __launch_bounds__(kSelThreads) k_bound_select(BatchRank a) {
   extern __shared__ unsigned long long ssel[];
@@ -146,14 +155,24 @@ __global__ void __launch_bounds__(kSelThreads) k_bound_select(BatchRank a) {
       __syncthreads();
     }
   const float* qv = a.Q + (uint64_t)q * a.L;
-  for (int i = tid; i < kWarpListCap; i += kSelThreads) {
+  // a warp per row: lane c computes chunk c of a 32-chunk group (one
+  // coalesced load), the chunk sums are added in chunk order
+  // (ts_euclidean_distance_SIMD's order, no abandon)
+  const int lane = tid & 31, nch = a.L >> 3;
+  for (int i = tid >> 5; i < kWarpListCap; i += kSelThreads / 32) {
     unsigned long long v = ~0ull;
-    if (i < kMaxK && i < n && buf[i] != ~0ull) {
+    if (i < kMaxK && i < n && buf[i] != ~0ull) {  // uniform over the warp
       const uint32_t row = (uint32_t)buf[i];
-      const float d = hg_ed(qv, a.rows + (uint64_t)row * a.L, a.L, __int_as_float(0x7f800000));
+      const float* xr = a.rows + (uint64_t)row * a.L;
+      float d = 0.0f;
+      for (int c0 = 0; c0 < nch; c0 += 32) {
+        const float cd = c0 + lane < nch ? chunk_d2_v4(qv, xr, c0 + lane) : 0.0f;
+        const int lim = min(32, nch - c0);
+        for (int t = 0; t < lim; ++t) d = __fadd_rn(d, __shfl_sync(HG_FULL, cd, t));
+      }
       v = ((unsigned long long)__float_as_uint(d) << 32) | (uint32_t)a.ids[row];
     }
-    list[i] = v;
+    if (lane == 0) list[i] = v;
   }
   __syncthreads();
   if (tid < 32) {
@@ -228,13 +247,6 @@ __global__ void __launch_bounds__(1024) k_rerank_plan(BatchRank a) {
 
 // Squared distance of the 8-float chunk c of q and x (ts.c:83-109 order),
 // both read as two float4.
-__device__ __forceinline__ float chunk_d2_v4(const float* q, const float* x, int c) {
-  const float4 x0 = reinterpret_cast<const float4*>(x)[2 * c], x1 = reinterpret_cast<const float4*>(x)[2 * c + 1];
-  const float4 q0 = reinterpret_cast<const float4*>(q)[2 * c], q1 = reinterpret_cast<const float4*>(q)[2 * c + 1];
-  const float qq[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-  const float xx[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-  return hg_chunk_d2(qq, xx);
-}
 
 // Segment re-rank: persistent warps take segments from a counter.  A warp
 // starts from step 2's list, shares the query's running k-th distance through
