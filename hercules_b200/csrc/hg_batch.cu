@@ -255,8 +255,9 @@ __global__ void __launch_bounds__(1024) k_rerank_plan(BatchRank a) {
 // chunks ch + kSlot l + j (l < kLines) and every lane of the slot adds the
 // step's kSlot * kLines chunk sums in order (ts_euclidean_distance_SIMD's
 // order); one abandon test per step, as the step's lines are loaded already.
-// Short series use 2-lane slots (16 rows per warp, 128 bytes of each per
-// step); long ones 8-lane slots (4 rows, 512 bytes).
+// Short series use 2-lane slots of four chunks per lane (16 rows per warp,
+// 256 bytes of each per step: rows in flight matter more than lanes per row);
+// long ones 8-lane slots of two (4 rows, 512 bytes).
 constexpr int kRankWarps = 8;
 template <int kSlot>
 __host__ __device__ constexpr uint32_t rank_leaders() {
@@ -831,7 +832,7 @@ cudaError_t launch_rerank(const BatchRank& r, int part_blocks, cudaStream_t s) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (r.L >= 4096) k_rerank_part<8, 2><<<part_blocks, kRankWarps * 32, 0, s>>>(r);
-  else k_rerank_part<2, 2><<<part_blocks, kRankWarps * 32, 0, s>>>(r);
+  else k_rerank_part<2, 4><<<part_blocks, kRankWarps * 32, 0, s>>>(r);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_rerank_merge<<<nblk(r.nlist, kRankWarps), kRankWarps * 32, 0, s>>>(r);
