@@ -38,13 +38,11 @@ static __device__ void warp_sort(unsigned long long* a, int n) {
   }
 }
 
-// Sorts list[0..cnt), dedups by distance, keeps at most k; returns the new
-// count (warp-uniform).  Entries beyond cnt must be ~0ull on entry.
-static __device__ int warp_compact(unsigned long long* list, int cnt, int k) {
+// list[0..cnt) sorted ascending by (distance, id): keeps the first entry of
+// each distance, at most k, at the front; sets list[out..cap) to ~0ull;
+// returns the count (warp-uniform).
+static __device__ int warp_dedup_sorted(unsigned long long* list, int cnt, int k, int cap) {
   const int lane = threadIdx.x & 31;
-  int n = 32;
-  while (n < cnt) n <<= 1;
-  warp_sort(list, n);
   int out = 0;
   uint32_t prev_d = 0xffffffffu;
   bool have_prev = false;
@@ -64,9 +62,18 @@ static __device__ int warp_compact(unsigned long long* list, int cnt, int k) {
     out = min(k, out + __popc(m));
     __syncwarp();
   }
-  for (int i = out + lane; i < kWarpListCap; i += 32) list[i] = ~0ull;
+  for (int i = out + lane; i < cap; i += 32) list[i] = ~0ull;
   __syncwarp();
   return out;
+}
+
+// Sorts list[0..cnt), dedups by distance, keeps at most k; returns the new
+// count (warp-uniform).  Entries beyond cnt must be ~0ull on entry.
+static __device__ int warp_compact(unsigned long long* list, int cnt, int k) {
+  int n = 32;
+  while (n < cnt) n <<= 1;
+  warp_sort(list, n);
+  return warp_dedup_sorted(list, cnt, k, kWarpListCap);
 }
 
 // Appends (key, id) candidates of the lanes in `take` to the warp's list and

@@ -1138,7 +1138,7 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
     HCK(timed_begin(prof ? &prof->ed : nullptr, st));
     CK(hg::launch_ed_stream(e, ed_blocks, st));
     HCK(timed_end(prof ? &prof->ed : nullptr, st));
-    CK(hg::launch_merge(s.parts, s.part_count, ed_blocks * hg::kEdWarps, k, s.topk, s.topk_count, s.bound, s.err,
+    CK(hg::launch_merge(s.parts, s.part_count, ed_blocks, k, s.topk, s.topk_count, s.bound, s.err,
                         st));
   } else {
     CK(hg::launch_query_prep(d_q, e.L, index_tree(ix), d.leaf_start, d.leaf_size, s.approx_leaf, s.paa, s.cand,
@@ -1155,7 +1155,7 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
     HCK(timed_begin(prof ? &prof->ed : nullptr, st));
     CK(hg::launch_ed_stream(e, a_blocks, st));
     HCK(timed_end(prof ? &prof->ed : nullptr, st));
-    CK(hg::launch_merge(s.parts, s.part_count, a_blocks * hg::kEdWarps, k, s.topk, s.topk_count, s.bound, s.err,
+    CK(hg::launch_merge(s.parts, s.part_count, a_blocks, k, s.topk, s.topk_count, s.bound, s.err,
                         st));
     CK(hg::launch_select_sort(s.lb, nl, s.bound, s.approx_leaf, d.leaf_start, d.leaf_size, s.cand, s.cand_lb,
                               s.cand_count, s.unit_prefix, st));
@@ -1187,7 +1187,7 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
     CK(hg::launch_ed_stream(e, ed_blocks, st));
     HCK(timed_end(prof ? &prof->ed : nullptr, st));
     // the merge folds the approximate leaf's top-k (in topk) into the result
-    CK(hg::launch_merge(s.parts, s.part_count, ed_blocks * hg::kEdWarps, k, s.topk, s.topk_count, s.bound, s.err,
+    CK(hg::launch_merge(s.parts, s.part_count, ed_blocks, k, s.topk, s.topk_count, s.bound, s.err,
                         st));
   }
   CK(hg::launch_emit(s.topk, s.topk_count, k, d_dist, d_id, st));
@@ -1277,7 +1277,7 @@ static hg_status knn_approx_one(hg_index* ix, const float* d_q, int k, const hg_
                            s.cand_lb, s.cand_count, s.unit_prefix, s.bound, s.topk_count, s.counters, st));
   e.ident_leaf = s.approx_leaf;
   CK(hg::launch_ed_stream(e, ed_blocks, st));
-  CK(hg::launch_merge(s.parts, s.part_count, ed_blocks * hg::kEdWarps, k, s.topk, s.topk_count, s.bound, s.err, st));
+  CK(hg::launch_merge(s.parts, s.part_count, ed_blocks, k, s.topk, s.topk_count, s.bound, s.err, st));
   std::vector<float> q(L);
   int approx = -1, cnt = 0;
   uint32_t bound_bits = 0;
@@ -1320,14 +1320,14 @@ static hg_status knn_approx_one(hg_index* ix, const float* d_q, int k, const hg_
       e.ident_first = first;
       e.ident_count = count - 1;
       CK(hg::launch_ed_stream(e, ed_blocks, st));
-      CK(hg::launch_merge(s.parts, s.part_count, ed_blocks * hg::kEdWarps, k, s.topk, s.topk_count, s.bound,
+      CK(hg::launch_merge(s.parts, s.part_count, ed_blocks, k, s.topk, s.topk_count, s.bound,
                           s.err, st));
     }
     CK(hg::launch_stale_copy(flag, s.bound, stale, st));
     e.ident_first = first + count - 1;
     e.ident_count = 1;
     CK(hg::launch_ed_stream(e, 1, st));
-    CK(hg::launch_merge(s.parts, s.part_count, hg::kEdWarps, k, s.topk, s.topk_count, s.bound, s.err, st));
+    CK(hg::launch_merge(s.parts, s.part_count, 1, k, s.topk, s.topk_count, s.bound, s.err, st));
     return HG_OK;
   };
   std::vector<PqEntry> pq;

@@ -647,8 +647,8 @@ __global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 3 : 4) k_ed_stream(Ed
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int slot_lead = lane & ~(kSlot - 1), j = lane & (kSlot - 1);
   if (a.gate && *a.gate == 0) {
-    // a gated launch that did not pass: every warp reports an empty list
-    if (lane == 0) a.part_count[blockIdx.x * W + wib] = 0;
+    // a gated launch that did not pass: the block reports an empty list
+    if (threadIdx.x == 0) a.part_count[blockIdx.x] = 0;
     return;
   }
   unsigned long long* list = lists[wib];
@@ -809,8 +809,55 @@ __global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 3 : 4) k_ed_stream(Ed
   }
   cnt = warp_compact(list, cnt, a.k);
   if (cnt == a.k && lane == 0) atomicMin(a.bound, (uint32_t)(list[a.k - 1] >> 32));
-  unsigned long long* out = a.parts + (uint64_t)gw * kWarpListCap;
-  for (int i = lane; i < cnt; i += 32) out[i] = list[i];
+  // the block's warp lists (each at most k entries) become one: the
+  // entries are packed to the front (read to registers, a barrier, written
+  // at the warp's offset), the next power of two of them sorted, the first
+  // k distinct distances kept; the merge then reads one part per block
+  __shared__ int s_cnt[W];
+  if (lane == 0) s_cnt[wib] = cnt;
+  constexpr int kPer = kWarpListCap / 32;  // entries per lane of a full list
+  unsigned long long mine[kPer];
+#pragma unroll
+  for (int r = 0; r < kPer; ++r) mine[r] = list[lane + 32 * r];
+  __syncthreads();
+  int offset = 0, packed = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    offset += w < wib ? s_cnt[w] : 0;
+    packed += s_cnt[w];
+  }
+  int nsort = 32;
+  while (nsort < packed) nsort <<= 1;
+  unsigned long long* flat = &lists[0][0];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kPer; ++r)
+    if (lane + 32 * r < cnt) flat[offset + lane + 32 * r] = mine[r];
+  for (int i = packed + (int)threadIdx.x; i < nsort; i += kEdThreads) flat[i] = ~0ull;
+  __syncthreads();
+  for (int size = 2; size <= nsort; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < nsort / 2; i += kEdThreads) {
+        const int pos = 2 * i - (i & (stride - 1));
+        const int partner = pos + stride;
+        const bool asc = (pos & size) == 0;
+        const unsigned long long x = flat[pos], y = flat[partner];
+        if ((x > y) == asc) {
+          flat[pos] = y;
+          flat[partner] = x;
+        }
+      }
+      __syncthreads();
+    }
+  if (wib == 0) {
+    const int bc = warp_dedup_sorted(flat, packed, a.k, 0);
+    unsigned long long* out = a.parts + (uint64_t)blockIdx.x * kWarpListCap;
+    for (int i = lane; i < bc; i += 32) out[i] = flat[i];
+    if (lane == 0) {
+      a.part_count[blockIdx.x] = bc;
+      if (bc == a.k) atomicMin(a.bound, (uint32_t)(flat[a.k - 1] >> 32));
+    }
+  }
   unsigned long long s_chunks = n_chunks, s_done = n_done, s_rows = n_rows;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -819,14 +866,13 @@ __global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 3 : 4) k_ed_stream(Ed
     s_rows += __shfl_xor_sync(HG_FULL, s_rows, o);
   }
   if (lane == 0) {
-    a.part_count[gw] = cnt;
     atomicAdd(&a.stats[1], s_chunks);
     atomicAdd(&a.stats[4], s_done);
     atomicAdd(&a.stats[5], s_rows);
   }
 }
 
-// Merges the per-warp lists (and the current top-k, passed as part -1) into
+// Merges the per-block lists (and the current top-k, passed as part -1) into
 // the k smallest distinct distances, lowest id per distance.  Only entries
 // <= the final bound can belong to the answer.
 constexpr int kMergeThreads = 1024;

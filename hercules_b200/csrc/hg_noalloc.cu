@@ -27,7 +27,8 @@ void hg_record_error(const char* msg);  // hg_index.cu: the text hg_last_error r
 
 namespace {
 
-// 148 blocks of 8 warps, each warp a 256-entry candidate list
+// 148 blocks of 8 warps; the scan leaves one 256-entry candidate list per
+// block (the array keeps room for one per warp)
 constexpr int kNoAllocBlocks = 148;
 constexpr int kNoAllocParts = kNoAllocBlocks * hg::kEdWarps;
 constexpr size_t kListBytes = (size_t)kNoAllocParts * hg::kWarpListCap * sizeof(unsigned long long);
@@ -109,7 +110,7 @@ extern "C" HG_API hg_status hg_pscan_noalloc(const float* d_rows, uint64_t n, ui
     a.stats = stats;
     e = hg::launch_ed_stream_row_ids(a, kNoAllocBlocks, s);
   }
-  if (e == cudaSuccess) e = hg::launch_merge(parts, part_count, kNoAllocParts, (int)k, topk, topk_count, bound, nullptr, s);
+  if (e == cudaSuccess) e = hg::launch_merge(parts, part_count, kNoAllocBlocks, (int)k, topk, topk_count, bound, nullptr, s);
   if (e == cudaSuccess) e = hg::launch_emit(topk, topk_count, (int)k, d_dist_out, d_id_out, s);
   if (e != cudaSuccess) return fail(HG_ERR_CUDA, cudaGetErrorString(e));
   return HG_OK;
