@@ -483,14 +483,10 @@ __global__ void __launch_bounds__(kFilterThreads) k_lbsax_filter(FilterArgs a) {
   // per-query table of the per-segment LB_SAX terms: dtab[j][s] is the
   // squared gap between the query's PAA value j and symbol s's region
   __shared__ float dtab[HG_PAA_SEGMENTS][HG_SAX_CARD];
-  __shared__ uint32_t wcount[W];
-  __shared__ uint32_t wbase[W];
-  __shared__ int s_stop;
   if (a.use_lbsax) {
     for (int i = threadIdx.x; i < HG_PAA_SEGMENTS * HG_SAX_CARD; i += blockDim.x)
       dtab[i >> 8][i & 255] = hg_lb_sax_lane(a.paa[i >> 8], i & 255, a.bp);
   }
-  if (threadIdx.x == 0) s_stop = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1;
@@ -510,7 +506,9 @@ __global__ void __launch_bounds__(kFilterThreads) k_lbsax_filter(FilterArgs a) {
   uint64_t lstart = 0, lend = 0;
   float clb = 0.0f;
   unsigned long long n_rows = 0, n_pruned = 0, n_leaves = 0;
-  for (uint32_t base = u0; base < u1; base += W * kFilterUnits) {
+  // each warp walks its own units (base + kFilterUnits units per step) and
+  // reserves its survivors' list slots itself: no block barrier in the loop
+  for (uint32_t base = u0 + wib * kFilterUnits; base < u1; base += W * kFilterUnits) {
     uint32_t m[kFilterUnits];
     uint64_t rr[kFilterUnits];
     bool ok[kFilterUnits];
@@ -518,7 +516,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_lbsax_filter(FilterArgs a) {
     bool stop = false;
 #pragma unroll
     for (int j = 0; j < kFilterUnits; ++j) {
-      const uint32_t unit = base + wib * kFilterUnits + j;
+      const uint32_t unit = base + j;
       ok[j] = false;
       rr[j] = 0;
       if (unit < u1 && !stop) {
@@ -563,35 +561,17 @@ __global__ void __launch_bounds__(kFilterThreads) k_lbsax_filter(FilterArgs a) {
       m[j] = __ballot_sync(HG_FULL, pass);
       cnt += __popc(m[j]);
     }
-    if (lane == 0) {
-      wcount[wib] = cnt;
-      if (stop) s_stop = 1;
-    }
-    __syncthreads();
-    if (wib == 0) {
-      const uint32_t v = lane < W ? wcount[lane] : 0u;
-      uint32_t x = v;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(HG_FULL, x, o);
-        if (lane >= o) x += y;
-      }
-      uint32_t blk = 0;
-      const uint32_t tot = __shfl_sync(HG_FULL, x, W - 1);
-      if (lane == 0 && tot) blk = atomicAdd(a.list_count, tot);
-      blk = __shfl_sync(HG_FULL, blk, 0);
-      if (lane < W) wbase[lane] = blk + x - v;
-    }
-    __syncthreads();
-    uint32_t pos = wbase[wib];
+    uint32_t pos = 0;
+    if (lane == 0 && cnt) pos = atomicAdd(a.list_count, cnt);
+    pos = __shfl_sync(HG_FULL, pos, 0);
 #pragma unroll
     for (int j = 0; j < kFilterUnits; ++j) {
       if ((m[j] >> lane) & 1u) a.list[pos + __popc(m[j] & lt)] = (uint32_t)rr[j];
       pos += __popc(m[j]);
     }
-    const int st = s_stop;
-    __syncthreads();  // s_stop and wcount are reused by the next iteration
-    if (st) break;
+    // units are in candidate order, LB non-decreasing: a unit past the bound
+    // ends this warp's walk (stop is the same on every lane)
+    if (stop) break;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
