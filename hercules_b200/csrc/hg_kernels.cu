@@ -385,11 +385,41 @@ __global__ void __launch_bounds__(kSortThreads) k_select_sort(const float* __res
     }
   }
   __syncthreads();
-  // 2. radix sort, stable, each thread owning a contiguous run of keys
+  // 2. sort by LB.  Up to kSortThreads candidates (the usual case): one
+  //    bitonic sort of (LB bits, leaf) keys; the leaves are in index order on
+  //    input, so equal LBs end in the order the stable radix sort below gives
+  //    them, which handles larger counts.
   const int per2 = (n + kSortThreads - 1) / kSortThreads;
   const int r0 = min(n, t * per2), r1 = min(n, r0 + per2);
   uint32_t *ki = keys0, *vi = vals0, *ko = keys1, *vo = vals1;
-  for (int pass = 0; pass < 8; ++pass) {
+  if (n <= kSortThreads) {
+    unsigned long long* kv = reinterpret_cast<unsigned long long*>(keys1);  // 8-byte aligned, 2 x kMaxLeavesSort words
+    int np = 2;
+    while (np < n) np <<= 1;
+    for (int i = t; i < np; i += kSortThreads)
+      kv[i] = i < n ? (((unsigned long long)keys0[i] << 32) | vals0[i]) : ~0ull;
+    __syncthreads();
+    for (int size = 2; size <= np; size <<= 1)
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int i = t; i < np / 2; i += kSortThreads) {
+          const int pos = 2 * i - (i & (stride - 1));
+          const int partner = pos + stride;
+          const bool asc = (pos & size) == 0;
+          const unsigned long long x = kv[pos], y = kv[partner];
+          if ((x > y) == asc) {
+            kv[pos] = y;
+            kv[partner] = x;
+          }
+        }
+        __syncthreads();
+      }
+    for (int i = t; i < n; i += kSortThreads) {
+      keys0[i] = (uint32_t)(kv[i] >> 32);
+      vals0[i] = (uint32_t)kv[i];
+    }
+    __syncthreads();
+  }
+  for (int pass = 0; n > kSortThreads && pass < 8; ++pass) {
     const int shift = pass * 4;
     uint32_t c[16];
 #pragma unroll
