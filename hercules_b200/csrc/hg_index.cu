@@ -2018,7 +2018,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
       if (cnt == 0 && round > 0) continue;
       gemm += tg;
       rerank += tr;
-      // round 0 with pruning: the kept pairs, plus every pair if the dense
+      // the first filter round with pruning: the kept pairs, plus every pair if the dense
       // pass ran instead
       pairs += (round == 0 && prune) ? pp + (uint64_t)pc[2] * ix->n : cnt * ix->n;
     }
