@@ -761,13 +761,9 @@ cudaError_t launch_group_queries(const int* approx, int nq, const LeafPlan* plan
                                  uint32_t* perm, uint32_t* slots, uint32_t* leaf_qoff, uint32_t* leaf_qcnt,
                                  uint32_t* item_off, uint32_t* nitems, BatchItem* items, cudaStream_t s) {
   const size_t smem = sizeof(uint32_t) * 2 * (size_t)nleaves;
-  static bool attr = false;
-  if (!attr) {
-    const cudaError_t e = cudaFuncSetAttribute(k_group_queries, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)(sizeof(uint32_t) * 2 * kMaxLeavesSort));
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static SmemLimit attr;
+  const cudaError_t ea = attr.ensure((const void*)k_group_queries, (int)(sizeof(uint32_t) * 2 * kMaxLeavesSort));
+  if (ea != cudaSuccess) return ea;
   k_group_queries<<<1, kGroupThreads, smem, s>>>(approx, nq, plan, nleaves, btpi, perm, slots, leaf_qoff, leaf_qcnt,
                                                  item_off, nitems);
   cudaError_t e = cudaGetLastError();
@@ -815,13 +811,9 @@ cudaError_t launch_bound_select(const BatchRank& r, cudaStream_t s) {
   if (!r.nq) return cudaSuccess;
   int n = 32;
   while (n < (int)r.bm_cap) n <<= 1;
-  static bool attr = false;
-  if (!attr) {
-    const cudaError_t e = cudaFuncSetAttribute(k_bound_select, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)(sizeof(unsigned long long) * kBatchMaxSlots));
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static SmemLimit attr;
+  const cudaError_t ea = attr.ensure((const void*)k_bound_select, (int)(sizeof(unsigned long long) * kBatchMaxSlots));
+  if (ea != cudaSuccess) return ea;
   k_bound_select<<<r.nq, kSelThreads, sizeof(unsigned long long) * n, s>>>(r);
   return cudaGetLastError();
 }

@@ -1454,14 +1454,17 @@ constexpr int kBatchRetries = 3;  // filter rounds after the first for overflowe
 // (128 bytes, the swizzle span) x box_rows rows, 128-byte swizzle, zero fill
 // outside the matrix.  The encoder comes from the driver through the runtime.
 static hg_status encode_bf16_map(CUtensorMap* map, const void* base, uint64_t n, uint32_t L, uint32_t box_rows) {
-  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-  if (!encode) {
+  // the driver's entry point is process-wide; a function-local static is
+  // initialised once even when several threads get here first
+  static const PFN_cuTensorMapEncodeTiled_v12000 encode = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
-    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-    if (!fn || q != cudaDriverEntryPointSuccess) return set_error(HG_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-  }
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }();
+  if (!encode) return set_error(HG_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   if (n == 0 || n >= (1ull << 31) || (L * 2) % 16 != 0)
     return set_error(HG_ERR_LIMIT, "BF16 tensor map: n must be below 2^31 and L a multiple of 8");
   const cuuint64_t dims[2] = {L, n};

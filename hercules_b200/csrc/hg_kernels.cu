@@ -1087,11 +1087,9 @@ cudaError_t launch_route_queries(const float* Q, int nq, int L, Tree t, int* lea
 cudaError_t launch_leaf_lb(const float* q, int L, int nleaves, const int* seg_off, const short* points,
                            const float* sk, float* lb_out, cudaStream_t s) {
   if (!nleaves) return cudaSuccess;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_leaf_lb, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
-    attr = true;
-  }
+  static SmemLimit attr;
+  const cudaError_t ea = attr.ensure((const void*)k_leaf_lb, 65536);
+  if (ea != cudaSuccess) return ea;
   k_leaf_lb<<<blocks_for((uint64_t)nleaves * 32, 256), 256, sizeof(float) * L, s>>>(q, L, nleaves, seg_off,
                                                                                   points, sk, lb_out);
   return cudaGetLastError();
@@ -1101,12 +1099,10 @@ cudaError_t launch_leaf_keep(const float* Q, int L, int nq, const short* useg_st
                              float2* segstats, const int* seg_off, const short* points, const int* seg_uid,
                              const float* sk, const uint32_t* leaf_size, int nleaves, const float* bound,
                              uint32_t* leaf_cnt, uint32_t* leaf_q, uint32_t stride, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_query_segstats, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
-    attr = true;
-  }
   if (nq <= 0 || nleaves <= 0) return cudaSuccess;
+  static SmemLimit attr;
+  const cudaError_t ea = attr.ensure((const void*)k_query_segstats, 65536);
+  if (ea != cudaSuccess) return ea;
   k_query_segstats<<<nq, 256, sizeof(float) * L, s>>>(Q, L, nq, useg_start, useg_end, nu, segstats);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -1139,11 +1135,9 @@ static size_t select_smem() { return sizeof(uint32_t) * 4 * kMaxLeavesSort + siz
 cudaError_t launch_select_sort(const float* lb, int nleaves, const uint32_t* bound, const int* approx_leaf,
                                const uint64_t* leaf_start, const uint32_t* leaf_size, int* cand,
                                float* cand_lb, int* cand_count, uint32_t* unit_prefix, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_select_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)select_smem());
-    attr = true;
-  }
+  static SmemLimit attr;
+  const cudaError_t ea = attr.ensure((const void*)k_select_sort, (int)select_smem());
+  if (ea != cudaSuccess) return ea;
   k_select_sort<<<1, kSortThreads, select_smem(), s>>>(lb, nleaves, bound, approx_leaf, leaf_start, leaf_size,
                                                        cand, cand_lb, cand_count, unit_prefix);
   return cudaGetLastError();
@@ -1162,13 +1156,9 @@ cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s)
 
 template <bool kRowIds, int kLines, int kSlot>
 static cudaError_t launch_ed(const EdArgs& a, int blocks, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    const cudaError_t e = cudaFuncSetAttribute(k_ed_stream<kRowIds, kLines, kSlot>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q4_bytes(16384));
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static SmemLimit attr;
+  const cudaError_t ea = attr.ensure((const void*)k_ed_stream<kRowIds, kLines, kSlot>, (int)q4_bytes(16384));
+  if (ea != cudaSuccess) return ea;
   k_ed_stream<kRowIds, kLines, kSlot><<<blocks, kEdThreads, q4_bytes(a.L), s>>>(a);
   return cudaGetLastError();
 }
@@ -1204,12 +1194,10 @@ int ed_blocks_per_sm(int L) {
 cudaError_t launch_merge(const unsigned long long* parts, const int* part_count, int nparts, int k,
                          unsigned long long* topk, int* topk_count, uint32_t* bound, int* err,
                          cudaStream_t s) {
-  static bool attr = false;
   const int smem = sizeof(unsigned long long) * kMergeCap;
-  if (!attr) {
-    cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
+  static SmemLimit attr;
+  const cudaError_t ea = attr.ensure((const void*)k_merge, smem);
+  if (ea != cudaSuccess) return ea;
   k_merge<<<1, kMergeThreads, smem, s>>>(parts, part_count, nparts, k, topk, topk_count, bound, err);
   return cudaGetLastError();
 }

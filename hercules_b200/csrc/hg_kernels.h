@@ -4,7 +4,33 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 namespace hg {
+
+// Raises one kernel's dynamic shared-memory limit on the current device
+// before its first launch there.  cudaFuncSetAttribute acts on the current
+// device only, so the "done" state is one bit per device (devices 0..63;
+// higher ones set the attribute on every launch).  Two host threads making
+// their first call at once may both set it, which is harmless: the value is
+// the same.  One instance per (kernel, limit) call site, as a function-local
+// static.
+class SmemLimit {
+ public:
+  cudaError_t ensure(const void* func, int bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+    if (bit && (done_.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && bit) done_.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+  }
+
+ private:
+  std::atomic<uint64_t> done_{0};
+};
 
 constexpr int kEdWarps = 8;  // warps per block of the distance stream
 constexpr int kEdBlocksPerSm = 4;  // resident blocks per SM of the distance stream

@@ -655,13 +655,9 @@ size_t umma_filter_smem() { return kDynSmem; }
 
 cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q_map, const BatchGemm& g, int blocks,
                                cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    const cudaError_t e =
-        cudaFuncSetAttribute(k_umma_filter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDynSmem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static SmemLimit attr;
+  const cudaError_t ea = attr.ensure((const void*)k_umma_filter, (int)kDynSmem);
+  if (ea != cudaSuccess) return ea;
   const uint64_t ntiles = (g.nrows + kUM - 1) / kUM;
   if (g.mode != 0 && g.qtile != 0 && g.qtile != 64 && g.qtile != 128 && g.qtile != 256) return cudaErrorInvalidValue;
   // counts read on the device: every CTA starts and leaves when out of items
