@@ -1,19 +1,20 @@
 // hg_noalloc.cu -- exact k-NN scan that allocates no memory.
 //
-// Some callers cannot allocate device memory: code that runs while a CUDA
-// graph is being captured elsewhere in the process, a caller inside a
+// Some callers cannot allocate device memory: a caller held to a fixed
 // memory-pool budget that must not grow, or a plugin host that forbids
-// allocation on its query threads.  hg_pscan_noalloc serves them: it scans a
-// caller-owned device matrix (the same early-abandoning distance and tie
-// rule as hg_knn's scan mode) and keeps all of its working memory in the
-// file-scope array below.
+// allocation (and the implicit synchronisation of cudaMalloc/cudaFree) on
+// its query threads.  hg_pscan_noalloc serves them: it scans a caller-owned
+// device matrix (the same early-abandoning distance and tie rule as hg_knn's
+// scan mode) and keeps all of its working memory in the file-scope array
+// below.
 //
 // That array lives on every GPU that loads this library, for as long as the
-// process runs (kNoAllocScratchBytes, about 2.4 MB).  Calls share it and it
-// keeps the previous call's contents; every call resets the counters it
-// needs before use.  Two calls whose kernels overlap on the GPU (different
-// streams, or several host threads) race on it and give wrong answers:
-// serialise them.
+// process runs (kNoAllocScratchBytes: 8 KB of counters and the top-k, plus
+// one 256-entry candidate list of 8 bytes per entry for each of the 148
+// blocks of the scan, about 0.3 MB).  Calls share it and it keeps the
+// previous call's contents; every call resets the counters it needs before
+// use.  Two calls whose kernels overlap on the GPU (different streams, or
+// several host threads) race on it and give wrong answers: serialise them.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -27,10 +28,10 @@ void hg_record_error(const char* msg);  // hg_index.cu: the text hg_last_error r
 
 namespace {
 
-// 148 blocks of 8 warps; the scan leaves one 256-entry candidate list per
-// block (the array keeps room for one per warp)
+// 148 blocks of 8 warps; the scan reduces its warps' lists to one
+// 256-entry candidate list per block, and the merge reads those 148 lists
 constexpr int kNoAllocBlocks = 148;
-constexpr int kNoAllocParts = kNoAllocBlocks * hg::kEdWarps;
+constexpr int kNoAllocParts = kNoAllocBlocks;
 constexpr size_t kListBytes = (size_t)kNoAllocParts * hg::kWarpListCap * sizeof(unsigned long long);
 constexpr size_t kHeaderBytes = 8192;  // counters, bound, top-k, per-list counts
 constexpr size_t kNoAllocScratchBytes = kHeaderBytes + kListBytes;

@@ -299,15 +299,17 @@ HG_API hg_status hg_sax_breakpoints(float *out255);
  * matrix (row-major n x L float32, 16-byte aligned; the id of a row is its
  * index), with the distance and tie rule of hg_knn; outputs k squared
  * distances and ids in device memory, ordered on `stream`.  This entry point
- * has no counterpart in the reference: it is for callers that cannot
- * allocate (a process capturing CUDA graphs, a fixed memory-pool budget, a
- * host that forbids allocation on query threads), so it allocates nothing.
- * Its working memory is one static device array of about 2.4 MB that every
- * GPU loading the library holds until exit; the first call on a device looks
- * that array up (make it before any stream capture).  Calls share the array:
- * calls whose kernels overlap on the GPU race, so serialise them.  Limits:
- * 1 <= k <= 224, L a multiple of 16 up to 16384, n < 2^32; beyond them the
- * call returns HG_ERR_LIMIT. */
+ * has no counterpart in the reference.  It is for callers that cannot
+ * allocate device memory -- code held to a fixed memory-pool budget, or a
+ * plugin host that forbids cudaMalloc/cudaFree (and the synchronisation they
+ * imply) on its query threads -- so it allocates nothing.  Its working
+ * memory is one static device array of about 0.3 MB (8 KB of counters and
+ * the top-k, plus 148 candidate lists of 256 entries) that every GPU loading
+ * the library holds until exit; the first call on a device looks that
+ * array's device address up (make that first call before any stream
+ * capture).  Calls share the array: calls whose kernels overlap on the GPU
+ * race, so serialise them.  Limits: 1 <= k <= 224, L a multiple of 16 up to
+ * 16384, n < 2^32; beyond them the call returns HG_ERR_LIMIT. */
 HG_API hg_status hg_pscan_noalloc(const float *d_rows, uint64_t n, uint32_t L, const float *d_query,
                                   uint32_t k, float *d_dist_out, int64_t *d_id_out, void *stream);
 

@@ -1,23 +1,30 @@
 """The allocation-free scan (hg_pscan_noalloc) against the scan of hg_knn.
 
-hg_pscan_noalloc exists for callers that cannot allocate device memory (a
-process capturing CUDA graphs, a fixed memory-pool budget, a host that
-forbids allocation on query threads).  It keeps its working memory in one
-static device array, so two calls in a row must not see each other's state.
-This file is collected last so that a failure here stops a `-x` run only
-after every other test has run."""
+hg_pscan_noalloc exists for callers that cannot allocate device memory (code
+held to a fixed memory-pool budget, or a plugin host that forbids
+cudaMalloc/cudaFree on its query threads).  It keeps its working memory in
+one static device array, so two calls in a row must not see each other's
+state.  This file is collected last so that a failure here stops a `-x` run
+only after every other test has run."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
-def test_pscan_noalloc_matches_pscan_on_two_calls_in_a_row(hg, gpu_available):
+# (rows, length, k, leaf size of the index whose scan mode is the comparison):
+# short series with a small k and the largest k; long series (8-lane slots,
+# the query staged in up to 64 KB of shared memory) at k = 1, 10 and 224
+SHAPES = [(30000, 256, 10, 2000), (30000, 256, 224, 2000), (4000, 4096, 10, 1000),
+          (1500, 16384, 1, 500), (1500, 16384, 224, 500)]
+
+
+@pytest.mark.parametrize("n,L,k,leaf", SHAPES)
+def test_pscan_noalloc_matches_pscan_on_two_calls_in_a_row(hg, gpu_available, n, L, k, leaf):
     import torch
-    n, L, k = 30000, 256, 10
     X = hg.generate_walks(1184, n, L)
     Q = hg.generate_queries(14784, X, np.array([0.01, 0.1, 1.0, 0.1, 0.01]))
-    ix = hg.HerculesIndex.build(X, 2000)
+    ix = hg.HerculesIndex.build(X, leaf)
     want_d, want_id = ix.pscan(Q, k)          # the existing entry point (hg_knn, scan mode)
     ix.close()
     Xd = torch.from_numpy(X).cuda()
