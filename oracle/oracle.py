@@ -28,7 +28,14 @@ REF_SO = os.path.join(REF_DIR, "libref_hercules.so")
 REF_BIN = os.path.join(REF_DIR, "hercules")
 REF_BIN_NOFMA = os.path.join(REF_DIR, "hercules_nofma")
 REF_PSCAN = os.path.join(REF_DIR, "pscan")
-REFERENCE_ROOT = "/root/reference"
+# Where the reference's sources lie: HERCULES_REF, else the conventional
+# read-only checkout path of the build container (absent on other machines,
+# where only the prebuilt _ref/ files are used).
+REFERENCE_ROOT = os.environ.get("HERCULES_REF") or "/root/reference"
+
+
+def have_ref_sources():
+    return os.path.isdir(os.path.join(REFERENCE_ROOT, "code", "hercules"))
 
 _P = ctypes.c_void_p
 
@@ -37,7 +44,7 @@ def build(ref=None):
     """Compile the restatement (and the reference when its sources exist)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     if ref is None:
-        ref = os.path.isdir(os.path.join(REFERENCE_ROOT, "code", "hercules"))
+        ref = have_ref_sources()
     if ref:
         subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + REFERENCE_ROOT], check=True)
 
@@ -71,6 +78,9 @@ def olib():
             "or_lb_eapca": (f32, [_P, i32, _P, _P]),
             "or_topk_insert": (None, [_P, _P, _P, _P, i32, f32, i64, u64, i32]),
             "or_build": (_P, [_P, u64, i32, i32]),
+            "or_build_mt": (_P, [_P, u64, i32, i32, i32, i32]),
+            "or_gen_rows": (None, [u64, u64, u64, i32, _P, i32, i32]),
+            "or_gen_queries": (None, [u64, u64, u64, i32, i32, _P, _P, _P, i32]),
             "or_write": (i32, [_P, ctypes.c_char_p, ctypes.c_double, _P]),
             "or_read": (_P, [ctypes.c_char_p]),
             "or_free": (None, [_P]),
@@ -191,6 +201,16 @@ class OracleIndex:
         return cls(h, data)
 
     @classmethod
+    def build_mt(cls, data, leaf_size, threads=0, keep_rows=True):
+        """or_build on several threads (same index).  keep_rows=False keeps
+        no leaf-ordered copy: such an index can only be written."""
+        data = np.ascontiguousarray(data, np.float32)
+        h = olib().or_build_mt(_p(data), data.shape[0], data.shape[1], leaf_size, int(threads), int(bool(keep_rows)))
+        if not h:
+            raise ValueError("or_build_mt failed")
+        return cls(h, data)
+
+    @classmethod
     def read(cls, directory):
         if not directory.endswith("/"):
             directory += "/"
@@ -274,6 +294,27 @@ class OracleIndex:
         out = np.zeros(self.num_leaves(), np.float32)
         olib().or_leaf_lbs(self.h, _p(q), _p(out))
         return out
+
+
+def gen_rows(seed, n, L, first=0, unit=False, threads=0, out=None):
+    """Rows [first, first+n) of the seeded generator (random walks, or unit
+    vectors with unit=True): the same bits as hercules_b200's generator."""
+    if out is None:
+        out = np.empty((n, L), np.float32)
+    olib().or_gen_rows(seed, first, n, L, _p(out), int(bool(unit)), int(threads))
+    return out
+
+
+def gen_queries(data_seed, seed, n, L, sigma2, unit=False):
+    """Noisy queries over a collection of n rows of stream data_seed (row
+    pick(j) plus N(0, sigma2[j]) noise, normalised); returns (queries, base
+    row ids)."""
+    s2 = np.ascontiguousarray(sigma2, np.float64)
+    nq = s2.shape[0]
+    out = np.empty((nq, L), np.float32)
+    base = np.empty(nq, np.uint64)
+    olib().or_gen_queries(data_seed, seed, n, L, nq, _p(s2), _p(out), _p(base), int(bool(unit)))
+    return out, base
 
 
 def pscan(data, q, k=1, tie_lowest=True):

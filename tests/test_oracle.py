@@ -108,6 +108,79 @@ def test_oracle_index_and_answers_match_reference_golden(oracle_mod, hg, tmp_pat
         assert st["loaded_rows"] == int(g["answers"]["loaded_ts"][j])
 
 
+def test_oracle_matches_reference_at_1M_walks_leaf_100000(oracle_mod, hg, tmp_path):
+    """The plain method's CPU-runnable configuration (1M x 256 walks, leaf
+    100,000, 100 fresh random-walk queries, k = 1 and 10): the oracle's index
+    files are the reference's and its answers and load counters are the
+    reference CLI's."""
+    import hashlib
+    import sys
+    sys.path.insert(0, os.path.dirname(golden_path("")))
+    from make_golden import root_fields_digest
+    g = json.load(open(golden_path("ref_walks1M_L256_leaf100000.json")))
+    X = hg.generate_walks(g["data_seed"], g["n"], g["L"])
+    assert hashlib.sha256(X.tobytes()).hexdigest() == g["data_sha256"]
+    Q = hg.generate_walks(g["query_seed"], g["nq"], g["L"])
+    assert hashlib.sha256(Q.tobytes()).hexdigest() == g["queries_sha256"]
+    oi = oracle_mod.OracleIndex.build(X, g["leaf"])
+    d = str(tmp_path) + "/"
+    oi.write(d, g["buffer_mb"])
+    del oi
+    assert hashlib.sha256(open(d + "leaves_raw.idx", "rb").read()).hexdigest() == g["stock"]["leaves_raw_sha256"]
+    assert hashlib.sha256(open(d + "leaves_sims.idx", "rb").read()).hexdigest() == g["stock"]["leaves_sims_sha256"]
+    assert root_fields_digest(d + "root.idx") == g["stock"]["root_fields_sha256"]
+    rd = oracle_mod.OracleIndex.read(d)
+    assert rd.num_leaves() == g["num_leaves"]
+    for k in g["ks"]:
+        want = g["answers"]["k%d" % k]
+        for j in range(g["nq"]):
+            dist, rows, fp, st = rd.knn(Q[j], k, tie_lowest=False)
+            assert ["%f" % np.sqrt(np.float32(v)) for v in dist] == want["exact_distance"][j], (k, j)
+            assert [str(int(v)) for v in fp] == want["exact_node_file_pos"][j], (k, j)
+            assert st["loaded_leaves"] == int(want["loaded_nodes"][j]), (k, j)
+            assert st["loaded_rows"] == int(want["loaded_ts"][j]), (k, j)
+
+
+@pytest.mark.parametrize("L,unit", [(256, False), (96, True), (1024, False), (16, False)])
+def test_generator_restatement_matches_library_generator(oracle_mod, hg, L, unit):
+    """oracle_gen.c gives the bits of hercules_b200's generator (its host
+    path; the device path equals the host path in the GPU tests)."""
+    n = 2000
+    want = hg.generate_unit_vectors(1184, n, L, first=77) if unit else hg.generate_walks(1184, n, L, first=77)
+    got = oracle_mod.gen_rows(1184, n, L, first=77, unit=unit)
+    assert np.array_equal(bits(got), bits(want))
+    X = hg.generate_unit_vectors(1184, n, L) if unit else hg.generate_walks(1184, n, L)
+    s2 = np.array([0.01, 0.1, 1.0, 0.3] * 6)
+    qw = (hg.generate_unit_queries if unit else hg.generate_queries)(14784, X, s2)
+    qg, base = oracle_mod.gen_queries(1184, 14784, n, L, s2, unit=unit)
+    assert np.array_equal(bits(qg), bits(qw))
+    assert base.max() < n
+
+
+@pytest.mark.parametrize("name", REF_CONFIGS + ["walks1M_L256_leaf100000"])
+def test_multithreaded_build_writes_the_reference_index(oracle_mod, tmp_path, name):
+    """or_build_mt (the benchmark's CPU-side build) writes the reference's
+    leaves_raw.idx / leaves_sims.idx byte for byte and its root.idx field by
+    field, from data made by the oracle's own generator."""
+    import hashlib
+    import sys
+    sys.path.insert(0, os.path.dirname(golden_path("")))
+    from make_golden import root_fields_digest
+    g = json.load(open(golden_path(f"ref_{name}.json")))
+    X = oracle_mod.gen_rows(g["data_seed"], g["n"], g["L"])
+    assert hashlib.sha256(X.tobytes()).hexdigest() == g["data_sha256"]
+    for keep in (False, True):
+        oi = oracle_mod.OracleIndex.build_mt(X, g["leaf"], threads=4, keep_rows=keep)
+        d = str(tmp_path / ("k%d" % keep)) + "/"
+        os.makedirs(d)
+        oi.write(d, g["buffer_mb"])
+        del oi
+        sha = lambda p: hashlib.sha256(open(p, "rb").read()).hexdigest()
+        assert sha(d + "leaves_raw.idx") == g["stock"]["leaves_raw_sha256"]
+        assert sha(d + "leaves_sims.idx") == g["stock"]["leaves_sims_sha256"]
+        assert root_fields_digest(d + "root.idx") == g["stock"]["root_fields_sha256"]
+
+
 APPROX = {"eps0.5": (0.5, 0), "eps2": (2.0, 0), "np3": (0.0, 3), "np10": (0.0, 10)}
 
 
@@ -160,7 +233,12 @@ def test_pscan_equals_exact(oracle_mod, hg):
         assert np.array_equal(i, ids[r2])
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/code/hercules"), reason="reference sources absent")
+def _ref_sources():
+    from oracle import oracle as O
+    return O.have_ref_sources()
+
+
+@pytest.mark.skipif(not _ref_sources(), reason="reference sources absent (set HERCULES_REF)")
 def test_oracle_primitives_against_reference_library(oracle_mod, hg):
     """Fresh random inputs against the reference's own functions."""
     oracle_mod.build(ref=True)
