@@ -14,6 +14,15 @@ oracle/Makefile `ref`); the GPU box only reads the committed outputs.
                                the reference CLI's answers (Query_exact_*)
                                and per-query load counters, exact and with
                                --epsilon 0.5 / 2 and --nprobes 3 / 10
+  ref_walks1M_L256_leaf100000.json
+                               the plain method's CPU-runnable configuration:
+                               1M z-normalised random walks of length 256
+                               (seed 1184), leaf size 100,000, 100 fresh
+                               random-walk queries (seed 14784) answered one
+                               at a time with k = 1 and k = 10: index digests
+                               and the reference CLI's answers and counters
+
+Usage: python tests/golden/make_golden.py [all | config1]
 """
 import hashlib
 import json
@@ -175,12 +184,57 @@ def ref_config(name, n, L, leaf, nq, k):
         shutil.rmtree(tmp)
 
 
+CONFIG1 = ("walks1M_L256_leaf100000", 1000000, 256, 100000, 100, (1, 10))
+
+
+def ref_config1(name, n, L, leaf, nq, ks):
+    """1M x 256 walks, leaf 100,000; queries are fresh random walks of the
+    query seed (the same generator, an independent seed)."""
+    tmp = tempfile.mkdtemp(prefix="golden_")
+    try:
+        X = H.generate_walks(DATA_SEED, n, L)
+        X.tofile(os.path.join(tmp, "data.bin"))
+        Q = H.generate_walks(QUERY_SEED, nq, L)
+        Q.tofile(os.path.join(tmp, "q.bin"))
+        buffer_mb = 4096.0  # holds the data and every split's copy: no flush
+        res = {"n": n, "L": L, "leaf": leaf, "nq": nq, "ks": list(ks), "data_seed": DATA_SEED,
+               "query_seed": QUERY_SEED, "queries": "fresh random walks", "data_sha256": sha(X.tobytes()),
+               "queries_sha256": sha(Q.tobytes()), "buffer_mb": buffer_mb}
+        d = os.path.join(tmp, "stock") + "/"
+        O.ref_build_index(O.REF_BIN, os.path.join(tmp, "data.bin"), n, L, leaf, d, buffer_mb=buffer_mb)
+        res["stock"] = {
+            "leaves_raw_sha256": sha(open(d + "leaves_raw.idx", "rb").read()),
+            "leaves_sims_sha256": sha(open(d + "leaves_sims.idx", "rb").read()),
+            "root_fields_sha256": root_fields_digest(d + "root.idx"),
+        }
+        hdr, nodes = O.parse_root_idx(d + "root.idx")
+        res["num_leaves"] = hdr[0]
+        res["num_nodes"] = len(nodes)
+        res["answers"] = {}
+        for k in ks:
+            q = O.ref_query(O.REF_BIN, d, os.path.join(tmp, "q.bin"), nq, k)
+            res["answers"]["k%d" % k] = {
+                "exact_distance": q["Query_exact_distance"].tolist(),
+                "exact_node_file_pos": q["Query_exact_node_file_pos"].tolist(),
+                "loaded_nodes": q["Query_total_loaded_nodes_count"][:, 0].tolist(),
+                "loaded_ts": q["Query_total_loaded_ts_count"][:, 0].tolist(),
+            }
+        with open(os.path.join(HERE, f"ref_{name}.json"), "w") as f:
+            json.dump(res, f, indent=1)
+    finally:
+        shutil.rmtree(tmp)
+
+
 def main():
     O.build(ref=True)
-    breakpoints()
-    kat_primitives()
-    for c in CONFIGS:
-        ref_config(*c)
+    which = sys.argv[1] if len(sys.argv) > 1 else "all"
+    if which == "all":
+        breakpoints()
+        kat_primitives()
+        for c in CONFIGS:
+            ref_config(*c)
+    if which in ("all", "config1"):
+        ref_config1(*CONFIG1)
 
 
 if __name__ == "__main__":
