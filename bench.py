@@ -8,25 +8,39 @@ size 100,000, built into the Hercules EAPCA index on the GPU.
 Headline workload (a step): one batch of 4,096 queries answered exactly by
 the batched path (hg_knn_batch_device): equal thirds of noisy queries (a
 random dataset series plus N(0, sigma^2) noise, sigma^2 = 0.01 / 0.1 / 1.0,
-z-normalised) plus 10% fresh random walks, k cycling 1 / 10 / 100.  `value`
-is queries per second over the timed steps (CUDA events on the stream, the
-collection and the step's queries already in HBM); `e2e` is the same through
-hg_knn_batch with the queries in pinned host memory and the answers copied
-back every step.  The plain per-query path (hg_knn_device, k = 10) is timed
-beside it on the same collection (`plain`), with the leaf-scan kernel's
-HBM roofline (`leaf_scan`), and so is the unindexed full scan (`pscan`,
-HG_MODE_PSCAN) with the reference's multi-threaded CPU PSCAN on a bounded
-sample beside it.  `fp64_oracle` checks a timed batch's answers against an
-FP64 brute force over the whole collection; `certified_bound` reports the
-filter's error bound.
+z-normalised) plus 10% fresh random walks, k in {1, 10, 100} (every
+(sigma^2, k) pair in equal shares).  `value` is queries per second over the
+timed steps (CUDA events on the stream, the collection and the step's
+queries already in HBM); `e2e` is the same through hg_knn_batch with the
+queries in pinned host memory and the answers copied back every step.
+
+Beside it, on the same collection:
+  plain      the plain per-query path (hg_knn_device) on 1,000 noisy queries
+             (sigma^2 in thirds), k = 1 and k = 10, with the leaf-scan
+             kernel's HBM roofline (`leaf_scan`);
+  pscan      the unindexed full scan (HG_MODE_PSCAN), its answers checked
+             against the plain path's, with the reference's multi-threaded
+             CPU PSCAN on a bounded sample;
+  fp64_oracle  answers of a timed batch and of both plain legs against an
+             FP64 brute force over the whole collection;
+  parity     the reference's own exact search (oracle/_ref/hercules, built
+             from the reference sources) over the index files the GPU
+             wrote, on a sample of timed queries: its printed distances and
+             answer-leaf positions against the GPU's;
+  index      SHA-256 digests of the index files the GPU wrote (the
+             `--impl reference` arm prints the same digests for the files
+             the oracle's restatement of the reference build writes).
 
 The BF16 copy of the collection (12.8 GB) and the raw rows (25.6 GB) are far
 larger than L2 (126 MB); every step streams them from HBM, so no L2 flush is
 needed between steps.
 
---impl reference runs the reference Hercules query path (oracle/_ref/hercules,
-compiled from the reference's own sources) on the host cores over the same
-index files, which the GPU build writes byte-identical to the reference's.
+--impl reference times the reference Hercules query path
+(oracle/_ref/hercules, compiled from the reference's own sources, all host
+cores) on queries drawn from the same batches.  That process loads nothing
+of hercules_b200: the collection and the queries come from the oracle's
+restatement of the generator, and the index files from the oracle's
+restatement of the reference's one-worker build.
 
 Multi-GPU (torchrun): every rank holds a full replica of the collection and
 answers its own queries; there is no data-path collective (weak scaling).
@@ -64,13 +78,14 @@ def parse():
     p.add_argument("--leaf", type=int, default=100_000)
     p.add_argument("--batch", type=int, default=4096, help="queries per batched step")
     p.add_argument("--fresh-frac", type=float, default=0.1)
-    p.add_argument("--plain-queries", type=int, default=128, help="queries through the plain path")
-    p.add_argument("--plain-k", type=int, default=10)
+    p.add_argument("--plain-queries", type=int, default=1000, help="queries through the plain path")
+    p.add_argument("--plain-ks", default="1,10", help="k of the plain legs (the last one carries the roofline)")
     p.add_argument("--data", choices=["walks", "unit"], default="walks",
                    help="z-normalised random walks, or unit-normalised Gaussian vectors")
     p.add_argument("--sigma2", default="0.01,0.1,1.0", help="noise levels of the noisy queries, in equal shares")
     p.add_argument("--ks", default="1,10,100", help="k of the batched queries, cycling")
-    p.add_argument("--cpu-sample-queries", type=int, default=3)
+    p.add_argument("--cpu-sample-queries", type=int, default=6,
+                   help="timed queries answered by the reference's serial exact search (baseline + parity)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--ref-queries-per-step", type=int, default=2)
     p.add_argument("--no-autotune", action="store_true", help="keep the default launch parameters")
@@ -220,11 +235,23 @@ def ks_of(args):
     return tuple(int(x) for x in args.ks.split(","))
 
 
+def batch_ks(args):
+    """k of each query of a batch: the noise level cycles with the query
+    index and k with the index divided by the number of levels, so every
+    (sigma^2, k) pair has an equal share."""
+    kc = np.array(ks_of(args), np.uint32)
+    return kc[(np.arange(args.batch) // len(levels_of(args))) % len(kc)]
+
+
+def fresh_count(args):
+    return int(round(args.batch * args.fresh_frac))
+
+
 def make_batches(args, torch, H, X, nbatches, device, offset):
     """nbatches batches of args.batch queries: noisy queries (sigma^2 in
-    equal thirds) followed by fresh random walks (args.fresh_frac)."""
+    equal shares) followed by fresh random walks (args.fresh_frac)."""
     nb = args.batch
-    nf = int(round(nb * args.fresh_frac))
+    nf = fresh_count(args)
     Q = torch.empty((nbatches, nb, args.L), dtype=torch.float32, device=device)
     gen = H.generate_unit_queries_device if args.data == "unit" else H.generate_queries_device
     fresh = H.generate_unit_vectors_device if args.data == "unit" else H.generate_walks_device
@@ -234,30 +261,73 @@ def make_batches(args, torch, H, X, nbatches, device, offset):
         if nf:
             fresh(FRESH_SEED + offset, nf, args.L, Q[i, nb - nf:].data_ptr(), first=(offset + i) * nf, device=device)
     torch.cuda.synchronize()
-    kc = ks_of(args)
-    ks = np.array(kc, np.uint32)[np.arange(nb) % len(kc)]
-    return Q, ks
+    return Q, batch_ks(args)
 
 
-def fp64_oracle_check(args, torch, H, Q, ks, D, I, device, nsample=32):
+def batch_on_host(args, O, i, offset=0):
+    """Batch i of make_batches computed on the host by the oracle's
+    restatement of the generator (the same bits), for the CPU-only arm."""
+    nb = args.batch
+    nf = fresh_count(args)
+    unit = args.data == "unit"
+    noisy, _ = O.gen_queries(DATA_SEED, QUERY_SEED + offset + i, args.n, args.L,
+                             sigma2_for(nb - nf, levels=levels_of(args)), unit=unit)
+    parts = [noisy]
+    if nf:
+        parts.append(O.gen_rows(FRESH_SEED + offset, nf, args.L, first=(offset + i) * nf, unit=unit))
+    return np.ascontiguousarray(np.concatenate(parts, 0)), batch_ks(args)
+
+
+def config_of(args):
+    """The workload, identical in both arms' JSON lines."""
+    what = "z-normalised random walks" if args.data == "walks" else "unit-normalised Gaussian vectors"
+    return {"workload": "batched exact k-NN, %d x %d float32 %s, leaf %d, %d queries/step, k in {%s}, "
+                        "sigma2 in equal shares %s + %d%% fresh %s"
+                        % (args.n, args.L, what, args.leaf, args.batch, ",".join(map(str, ks_of(args))),
+                           "/".join(map(str, levels_of(args))), int(round(100 * args.fresh_frac)),
+                           "walks" if args.data == "walks" else "vectors"),
+            "n": args.n, "L": args.L, "leaf_size": args.leaf, "queries_per_step": args.batch,
+            "k": list(ks_of(args)), "data": args.data,
+            "l2": "inputs (%.1f GB f32 + %.1f GB bf16) larger than L2; no flush needed"
+                  % (args.n * args.L * 4 / 1e9, args.n * args.L * 2 / 1e9),
+            "parallelism": "replica per GPU" if int(os.environ.get("WORLD_SIZE", "1")) > 1 else "single GPU"}
+
+
+def fp64_oracle_check(args, torch, H, groups, device):
     """FP64 brute force over the whole collection (regenerated chunk by chunk
-    from the same seed) for the first nsample queries of a timed batch:
-    recall of the returned ids against the FP64 k nearest, and the relative
-    error of the returned FP32 distances against the FP64 distances of the
-    same rows."""
-    s = min(nsample, Q.shape[0])
+    from the same seed) for groups of answered queries, each
+    (name, Q [s, L] device, ks [s], D [s, >=kmax], I [s, >=kmax]): recall of
+    the returned ids against the FP64 k nearest, and the relative error of
+    the returned FP32 distances against the FP64 distances of the same rows.
+    One pass over the collection serves every group."""
     n, L = args.n, args.L
-    q = Q[:s].double()
-    kq = torch.as_tensor(ks[:s].astype(np.int64), device=q.device)
-    kmax = int(kq.max())
-    ours = I[:s, :kmax]
-    ours_d = D[:s, :kmax].double()
+    names, qs, kss, ours_i, ours_d = [], [], [], [], []
+    width = max(int(np.max(ks)) for _, _, ks, _, _ in groups)
+    for name, Q, ks, D, I in groups:
+        s = Q.shape[0]
+        kq = np.broadcast_to(np.asarray(ks, np.int64), (s,))
+        kmax = int(kq.max())
+        names.append((name, s))
+        qs.append(Q.double())
+        kss.append(kq)
+        pad_i = torch.full((s, width), -1, dtype=torch.int64, device=device)
+        pad_d = torch.full((s, width), float("nan"), dtype=torch.float64, device=device)
+        pad_i[:, :kmax] = I[:, :kmax]
+        pad_d[:, :kmax] = D[:, :kmax].double()
+        ours_i.append(pad_i)
+        ours_d.append(pad_d)
+    q = torch.cat(qs, 0)
+    ks_all = np.concatenate(kss)
+    ours = torch.cat(ours_i, 0)
+    ours_dd = torch.cat(ours_d, 0)
+    s = q.shape[0]
+    kmax = int(ks_all.max())
     gen = H.generate_unit_vectors_device if args.data == "unit" else H.generate_walks_device
     chunk = max(1, min(n, (1 << 28) // L))
     buf = torch.empty((chunk, L), dtype=torch.float32, device=device)
     best_d = torch.full((s, kmax), float("inf"), dtype=torch.float64, device=device)
     best_i = torch.full((s, kmax), -1, dtype=torch.int64, device=device)
-    d64_ours = torch.full((s, kmax), float("nan"), dtype=torch.float64, device=device)
+    d64_ours = torch.full((s, width), float("nan"), dtype=torch.float64, device=device)
     qn = (q * q).sum(1)
     for first in range(0, n, chunk):
         m = min(chunk, n - first)
@@ -274,24 +344,33 @@ def fp64_oracle_check(args, torch, H, Q, ks, D, I, device, nsample=32):
             rr, cc = inside.nonzero(as_tuple=True)
             d64_ours[rr, cc] = d[rr, ours[rr, cc] - first]
     torch.cuda.synchronize()
-    hits, total, max_rel = 0, 0, 0.0
-    for j in range(s):
-        k = int(kq[j])
-        a = set(ours[j, :k].tolist())
-        b = set(best_i[j, :k].tolist())
-        hits += len(a & b)
-        total += k
-        d64 = d64_ours[j, :k]
-        rel = ((ours_d[j, :k] - d64).abs() / d64.clamp_min(1e-30)).max()
-        max_rel = max(max_rel, float(rel))
-    return {"queries": s, "pairs": total, "recall_vs_fp64_topk": round(hits / max(total, 1), 6),
-            "max_rel_err_vs_fp64": max_rel,
-            "how": "FP64 brute force over all %d rows, regenerated from the data seed in chunks" % n}
+    out = {"how": "FP64 brute force over all %d rows, regenerated from the data seed in chunks" % n}
+    row = 0
+    for name, cnt in names:
+        hits, total, max_rel = 0, 0, 0.0
+        for j in range(row, row + cnt):
+            k = int(ks_all[j])
+            a = set(ours[j, :k].tolist())
+            b = set(best_i[j, :k].tolist())
+            hits += len(a & b)
+            total += k
+            d64 = d64_ours[j, :k]
+            rel = ((ours_dd[j, :k] - d64).abs() / d64.clamp_min(1e-30)).max()
+            max_rel = max(max_rel, float(rel))
+        out[name] = {"queries": cnt, "pairs": total, "recall_vs_fp64_topk": round(hits / max(total, 1), 6),
+                     "max_rel_err_vs_fp64": max_rel}
+        row += cnt
+    return out
+
+
+_TSV_ANSWER = ("Query_exact_distance", "Query_exact_node_file_pos")
 
 
 def cpu_reference_run(args, index_dir, queries_host, threads, extra=(), k=10):
-    """Runs the reference CLI over the written index; per-query seconds from
-    its own Query_total_time_secs lines."""
+    """Runs the reference CLI over the written index.  Returns per-query
+    seconds from its own Query_total_time_secs lines, the wall time, and its
+    printed answers {query number: {"dist": [...], "pos": [...]}} (the %f
+    square-root distances and answer-leaf file positions, by rank)."""
     from oracle import oracle as O
     binary = O.REF_BIN
     qfile = os.path.join(index_dir, "bench_queries.bin")
@@ -304,13 +383,41 @@ def cpu_reference_run(args, index_dir, queries_host, threads, extra=(), k=10):
     wall = time.perf_counter() - t0
     if r.returncode != 0:
         raise RuntimeError("reference query failed: " + r.stderr[-500:])
-    per_q = {}
+    per_q, ans = {}, {}
     for line in r.stdout.splitlines():
         parts = line.split("\t")
-        if len(parts) == 5 and parts[0] == "Query_total_time_secs":
+        if len(parts) != 5:
+            continue
+        if parts[0] == "Query_total_time_secs":
             per_q.setdefault(int(parts[3]), 0.0)
             per_q[int(parts[3])] += float(parts[1])
-    return per_q, wall
+        elif parts[0] in _TSV_ANSWER:
+            a = ans.setdefault(int(parts[3]), {"dist": {}, "pos": {}})
+            a["dist" if parts[0] == _TSV_ANSWER[0] else "pos"][int(parts[4])] = parts[1]
+    answers = {qn: {"dist": [a["dist"][r] for r in sorted(a["dist"])], "pos": [a["pos"][r] for r in sorted(a["pos"])]}
+               for qn, a in ans.items()}
+    return per_q, wall, answers
+
+
+def file_digest(path, chunk=1 << 26):
+    """SHA-256 of the concatenated SHA-256 digests of the file's 64 MiB
+    chunks, hashed on every host core."""
+    import hashlib
+    from concurrent.futures import ThreadPoolExecutor
+    size = os.path.getsize(path)
+
+    def one(off):
+        with open(path, "rb") as f:
+            f.seek(off)
+            return hashlib.sha256(f.read(chunk)).digest()
+
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        parts = list(ex.map(one, range(0, max(size, 1), chunk)))
+    return hashlib.sha256(b"".join(parts)).hexdigest()
+
+
+def index_digests(d):
+    return {f: file_digest(os.path.join(d, f)) for f in ("root.idx", "leaves_raw.idx", "leaves_sims.idx")}
 
 
 def cpu_pscan_leg(args, H, queries_host, k):
@@ -366,17 +473,10 @@ def cpu_pscan_leg(args, H, queries_host, k):
 
 def write_index_for_cpu(ix, args):
     """The index in the reference's format where the host can read it fast."""
-    need = args.n * args.L * 4 * 1.3
-    for base in ("/dev/shm", tempfile.gettempdir()):
-        try:
-            st = os.statvfs(base)
-            if st.f_bavail * st.f_frsize > need:
-                d = tempfile.mkdtemp(prefix="hg_bench_idx_", dir=base) + "/"
-                ix.write(d, buffer_mb=64.0)
-                return d
-        except OSError:
-            continue
-    return None
+    d = host_index_dir(args.n * args.L * 4 * 1.3, "hg_bench_idx_")
+    if d is not None:
+        ix.write(d, buffer_mb=64.0)
+    return d
 
 
 def main():
@@ -400,7 +500,6 @@ def main():
     t0 = time.perf_counter()
     ix = H.HerculesIndex.build_device(X.data_ptr(), args.n, args.L, args.leaf, device=device)
     build_s = time.perf_counter() - t0
-    cpu_q = Qb[0, :args.cpu_sample_queries].cpu().numpy() if (rank == 0 and world == 1) else None
     del X
     torch.cuda.empty_cache()
     kmax = int(ks.max())
@@ -438,6 +537,7 @@ def main():
     ms = max_over_ranks(e0.elapsed_time(e1), world, device=torch.device("cuda", device))
     total_q = nb * steps * world
     value = total_q / (ms / 1000.0)
+    last = warm + steps - 1  # D / I hold the answers of this batch
 
     # end to end through the host API: pinned host queries in, answers out
     Qh = torch.empty(tuple(Qe.shape), dtype=torch.float32, pin_memory=True)
@@ -454,33 +554,43 @@ def main():
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, device=torch.device("cuda", device))
     e2e_value = total_q / e2e_s
 
-    # answers of the last timed batch against an FP64 brute force
-    fp64 = fp64_oracle_check(args, torch, H, Qb[warm + steps - 1], ks, D, I, device)
-
-    # the plain per-query path on the same collection, every scan launch timed
-    pk = args.plain_k
-    Dp = torch.empty((args.plain_queries, pk), dtype=torch.float32, device=device)
-    Ip = torch.empty((args.plain_queries, pk), dtype=torch.int64, device=device)
-    ix.knn_device(Qp.data_ptr(), min(8, args.plain_queries), pk, Dp.data_ptr(), Ip.data_ptr(), stream=stream,
-                  use_lb_sax=True)
-    torch.cuda.synchronize()
-    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    p0.record()
-    pst = ix.knn_device(Qp.data_ptr(), args.plain_queries, pk, Dp.data_ptr(), Ip.data_ptr(), stream=stream,
-                        use_lb_sax=True, profile=True)
-    p1.record()
-    torch.cuda.synchronize()
-    plain_ms = p0.elapsed_time(p1)
-    plain_qps = args.plain_queries / (plain_ms / 1000.0)
+    # the plain per-query path on 1,000 noisy queries, one leg per k; the
+    # last leg times every scan launch (roofline of the leaf scan)
+    plain_ks = [int(x) for x in args.plain_ks.split(",")]
+    npl = args.plain_queries
+    plain, plain_ans = {}, {}
+    for j, pk in enumerate(plain_ks):
+        Dp = torch.empty((npl, pk), dtype=torch.float32, device=device)
+        Ip = torch.empty((npl, pk), dtype=torch.int64, device=device)
+        ix.knn_device(Qp.data_ptr(), min(8, npl), pk, Dp.data_ptr(), Ip.data_ptr(), stream=stream, use_lb_sax=True)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        prof = j == len(plain_ks) - 1
+        p0.record()
+        pst = ix.knn_device(Qp.data_ptr(), npl, pk, Dp.data_ptr(), Ip.data_ptr(), stream=stream, use_lb_sax=True,
+                            profile=prof)
+        p1.record()
+        torch.cuda.synchronize()
+        qps = npl / (p0.elapsed_time(p1) / 1000.0)
+        plain["k%d" % pk] = {"value": round(qps, 2), "unit": UNIT, "queries": npl, "k": pk,
+                             "profiled": prof, "leaves_scanned_per_query": pst["leaves_scanned"] / npl,
+                             "rows_visited_per_query": pst["rows_visited"] / npl}
+        plain_ans[pk] = (Dp, Ip)
+        if prof:
+            plain_st = pst
+    pk = plain_ks[-1]
+    plain_qps = plain["k%d" % pk]["value"]
 
     # PSCAN (every row of the collection per query, HG_MODE_PSCAN): the
-    # unindexed baseline, HBM-bound
-    npq = max(1, min(4, args.plain_queries))
-    ix.knn_device(Qp.data_ptr(), 1, pk, Dp.data_ptr(), Ip.data_ptr(), stream=stream, mode=H.MODE_PSCAN)
+    # unindexed baseline, HBM-bound; its answers must equal the plain path's
+    npq = max(1, min(4, npl))
+    Ds = torch.empty((npq, pk), dtype=torch.float32, device=device)
+    Is = torch.empty((npq, pk), dtype=torch.int64, device=device)
+    ix.knn_device(Qp.data_ptr(), 1, pk, Ds.data_ptr(), Is.data_ptr(), stream=stream, mode=H.MODE_PSCAN)
     torch.cuda.synchronize()
     s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s0.record()
-    sst = ix.knn_device(Qp.data_ptr(), npq, pk, Dp.data_ptr(), Ip.data_ptr(), stream=stream, mode=H.MODE_PSCAN,
+    sst = ix.knn_device(Qp.data_ptr(), npq, pk, Ds.data_ptr(), Is.data_ptr(), stream=stream, mode=H.MODE_PSCAN,
                         profile=True)
     s1.record()
     torch.cuda.synchronize()
@@ -488,26 +598,41 @@ def main():
     pscan_bytes = 32.0 * sst["chunks_loaded"] + 8.0 * sst["rows_completed"]
     pscan_scan_s = (sst["scan_ms"] if sst["scan_ms"] > 0 else pscan_ms) / 1000.0
     pscan_gbs = pscan_bytes / pscan_scan_s / 1e9
+    Dpk, Ipk = plain_ans[pk]
+    pscan_same = bool(torch.equal(Ds.view(torch.int32), Dpk[:npq].contiguous().view(torch.int32))
+                      and torch.equal(Is, Ipk[:npq]))
     pscan = {"value": round(npq / (pscan_ms / 1000.0), 2), "unit": UNIT, "queries": npq, "k": pk,
              "path": "hg_knn_device, HG_MODE_PSCAN (every row, early abandon at the running k-th distance)",
+             "answers_equal_plain_path": pscan_same,
              "scan": {"kernel": "k_ed_stream", "achieved": round(pscan_gbs, 1), "unit": "GB/s",
                       "frac": round(pscan_gbs / measured_peaks_all()["hbm"], 4),
                       "algorithmic_bytes_per_query": pscan_bytes / npq}}
 
-    cpu_baseline = None
+    # answers of the last timed batch and of both plain legs against FP64
+    ns = 32
+    groups = [("batched", Qb[last, :ns], ks[:ns], D[:ns], I[:ns])]
+    for pk_, (Dp, Ip) in plain_ans.items():
+        groups.append(("plain_k%d" % pk_, Qp[:ns], np.full(ns, pk_), Dp[:ns], Ip[:ns]))
+    fp64 = fp64_oracle_check(args, torch, H, groups, device)
+
+    cpu_baseline, parity, index = None, None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu_baseline = cpu_baseline_leg(args, ix, cpu_q, ks[:args.cpu_sample_queries])
+        sample = sample_positions(args, args.cpu_sample_queries)
+        cpu_q = Qb[last, sample].cpu().numpy()
+        cpu_k = ks[sample]
+        cpu_d = D[sample].cpu().numpy()
+        cpu_i = I[sample].cpu().numpy()
+        cpu_baseline, parity, index = cpu_baseline_leg(args, ix, cpu_q, cpu_k, cpu_d, cpu_i)
         pscan["cpu_baseline"] = cpu_pscan_leg(args, H, Qp[:npq].cpu().numpy(), pk)
     ix.close()
 
     # roofline of the dominant kernel, the tensor-core filter k_umma_filter:
     # algorithmic FLOPs = 2 L per (query, row) pair it evaluated, over its
-    # summed launch time (CUDA events around every launch)
+    # summed launch time (%globaltimer stamps around every filter phase)
     peaks = measured_peaks_all()
     gemm_s = agg["gemm_ms"] / 1000.0
     flops = 2.0 * args.L * agg["bf16_pairs"]
     achieved_tf = flops / gemm_s / 1e12 if gemm_s > 0 else 0.0
-    filt_launches = steps  # one full filter pass per step, plus retry rounds on a few queries
     tr = profile_json("k_umma_filter_traffic.json")
     traffic = None
     if tr and tr.get("dram_bytes_per_row_pass"):
@@ -521,6 +646,7 @@ def main():
     # leaf scan of the plain path: k_ed_stream's algorithmic bytes = 32 B per
     # 8-float chunk computed + 4 B list entry per row started + 8 B id per
     # finished row, over its summed launch time
+    pst = plain_st
     launches = int(pst["scan_launches"])
     alg_bytes = 32.0 * pst["chunks_loaded"] + 4.0 * pst["rows_visited"] + 8.0 * pst["rows_completed"]
     scan_s = pst["scan_ms"] / 1000.0
@@ -533,34 +659,38 @@ def main():
                  "unit": "GB/s", "frac": round(ed_gbs / peaks["hbm"], 4), "peak_source": peaks["source"],
                  "traffic": ed_traffic, "algorithmic_bytes_per_launch": alg_bytes / max(launches, 1),
                  "avg_launch_ms": pst["scan_ms"] / max(launches, 1), "launches": launches}
+    # the LB_SAX filter of the plain path: 16 B word per row considered + 4 B
+    # per survivor written, over its summed launch time
+    flt_s = pst["filter_ms"] / 1000.0
+    flt_bytes = 16.0 * pst["rows_considered"] + 4.0 * (pst["rows_considered"] - pst["rows_lbsax_pruned"])
+    flt_gbs = flt_bytes / flt_s / 1e9 if flt_s > 0 else 0.0
+    lbsax = {"bound": "hbm", "kernel": "k_lbsax_filter", "achieved": round(flt_gbs, 1), "peak": peaks["hbm"],
+             "unit": "GB/s", "frac": round(flt_gbs / peaks["hbm"], 4),
+             "launches": int(pst["filter_launches"]),
+             "avg_launch_ms": pst["filter_ms"] / max(int(pst["filter_launches"]), 1),
+             "share_of_plain_device_time": round(pst["filter_ms"] / max(pst["device_ms"], 1e-9), 4)}
+    plain.update({"value": plain_qps, "unit": UNIT, "k": pk,
+                  "batched_over_plain": round(value / plain_qps, 2) if plain_qps > 0 else None,
+                  "path": "hg_knn_device (one query at a time, LB_SAX on); value = the k = %d leg" % pk})
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warm,
         "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "bf16 filter (fp32 accumulate) + f32 exact re-rank",
         "data": "synthetic (seeded z-normalised random walks; noisy and fresh queries)",
-        "config": {"workload": "batched exact k-NN, %d x %d float32 %s, leaf %d, %d queries/step, k cycling %s, "
-                               "sigma2 in equal shares %s + %d%% fresh %s"
-                               % (args.n, args.L, "z-normalised random walks" if args.data == "walks" else
-                                  "unit-normalised Gaussian vectors", args.leaf, nb, "/".join(map(str, ks_of(args))),
-                                  "/".join(map(str, levels_of(args))), int(round(100 * args.fresh_frac)),
-                                  "walks" if args.data == "walks" else "vectors"),
-                   "n": args.n, "L": args.L, "leaf_size": args.leaf, "queries_per_step": nb, "k": list(ks_of(args)),
-                   "data": args.data,
-                   "l2": "inputs (%.1f GB f32 + %.1f GB bf16) larger than L2; no flush needed"
-              % (args.n * args.L * 4 / 1e9, args.n * args.L * 2 / 1e9),
-                   "parallelism": "replica per GPU" if world > 1 else "single GPU",
-                   "tuning": {k: tuning[k] for k in ("filter_tiles_per_item", "bound_tiles_per_item",
-                                                     "rerank_blocks_per_sm", "approx_blocks_per_sm")},
-                   "tuned": not args.no_autotune},
+        "config": config_of(args),
+        "tuning": dict({k: tuning[k] for k in ("filter_tiles_per_item", "bound_tiles_per_item",
+                                                "rerank_blocks_per_sm", "approx_blocks_per_sm")},
+                       tuned=not args.no_autotune),
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": nb * args.L * 4,
                 "d2h_bytes_per_step": nb * kmax * (4 + 8)},
         "gpu_launches": int(agg["kernel_launches"]),
         "roofline": roofline,
         "leaf_scan": leaf_scan,
-        "plain": {"value": round(plain_qps, 2), "unit": UNIT, "queries": args.plain_queries, "k": pk,
-                  "path": "hg_knn_device (one query at a time, LB_SAX on)",
-                  "batched_over_plain": round(value / plain_qps, 2) if plain_qps > 0 else None},
+        "lbsax_filter": lbsax,
+        "plain": plain,
         "cpu_baseline": cpu_baseline,
+        "parity": parity,
+        "index": index,
         "pscan": pscan,
         "clocks": ck,
         "certified_bound": {"err_mean": agg["err_mean"] / steps, "err_max": agg["err_max_max"],
@@ -587,42 +717,94 @@ def main():
         dist.destroy_process_group()
 
 
-def cpu_baseline_leg(args, ix, cpu_q, cpu_k):
+def sample_positions(args, m):
+    """m query positions of a batch spread over it: every k and every noise
+    level appears (k cycling with the sample index, the level shifted by one
+    per round of k), the last one a fresh walk when the batch has some."""
+    nb, nlev, nk = args.batch, len(levels_of(args)), len(ks_of(args))
+    nf = fresh_count(args)
+    out = []
+    for t in range(m):
+        want_k = t % nk
+        fresh = nf > 0 and t == m - 1
+        lo, hi = (nb - nf, nb) if fresh else (t * (nb - nf) // max(m - 1, 1), nb - nf)
+        want_s = None if fresh else (t // nk + t) % nlev
+        for j in range(lo, hi):
+            if (j // nlev) % nk == want_k and (want_s is None or j % nlev == want_s):
+                out.append(j)
+                break
+    return np.array(out, np.int64)
+
+
+def cpu_baseline_leg(args, ix, cpu_q, cpu_k, gpu_d, gpu_i):
     """The reference's serial exact search (oracle/_ref/hercules, built from
     the reference sources) on a few of the timed queries, each with its own
-    k, over the same index."""
+    k, over the index files the GPU wrote.  Returns (baseline, parity,
+    index digests): parity compares the reference's printed answers
+    (Query_exact_distance = %f of the square root, Query_exact_node_file_pos)
+    with the GPU's batched answers for the same queries and with the plain
+    path's answer-leaf positions."""
     from oracle import oracle as O
     d = None
+    na = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference"}
     try:
         if not os.path.exists(O.REF_BIN):
-            return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
-                    "sample": "unavailable: oracle/_ref/hercules not built"}
+            return dict(na, sample="unavailable: oracle/_ref/hercules not built"), None, None
         d = write_index_for_cpu(ix, args)
         if d is None:
-            return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
-                    "sample": "unavailable: no host space for the index files"}
+            return dict(na, sample="unavailable: no host space for the index files"), None, None
+        index = dict(index_digests(d), built_by="GPU (hg_index_build on the device, written by hg_index_write)",
+                     digest="SHA-256 over the SHA-256 of each 64 MiB chunk")
         secs, nq, wall = 0.0, 0, 0.0
-        for q, k in zip(cpu_q, cpu_k):
-            per_q, w = cpu_reference_run(args, d, q[None, :], threads=1, k=int(k))
+        checked, mismatches = 0, []
+        for j, (q, k) in enumerate(zip(cpu_q, cpu_k)):
+            k = int(k)
+            per_q, w, ans = cpu_reference_run(args, d, q[None, :], threads=1, k=k)
             secs += sum(per_q.values())
             nq += len(per_q)
             wall += w
-        return {"value": round(nq / secs, 4) if secs > 0 else None, "unit": UNIT, "cores": 1,
-                "kind": "reference",
-                "sample": "%d of the timed queries (k = %s), reference exact_de_knn_search (--num-threads 1) over "
-                          "the same %dx%d index; per-query time from its Query_total_time_secs; wall %.1f s"
-                          % (nq, ",".join(str(int(k)) for k in cpu_k), args.n, args.L, wall)}
+            _, _, pos = ix.knn(q[None, :], k, with_leaf_pos=True)
+            want_d = ["%f" % np.sqrt(v) for v in gpu_d[j, :k]]
+            want_p = [str(int(v)) for v in pos[0]]
+            got = ans.get(1, {"dist": [], "pos": []})
+            checked += 1
+            if got["dist"] != want_d or got["pos"] != want_p:
+                mismatches.append({"query": j, "k": k, "reference": got, "gpu": {"dist": want_d, "pos": want_p}})
+        baseline = dict(na, value=round(nq / secs, 4) if secs > 0 else None,
+                        sample="%d of the timed queries (k = %s), reference exact_de_knn_search (--num-threads 1) "
+                               "over the same %dx%d index files; per-query time from its Query_total_time_secs; "
+                               "wall %.1f s" % (nq, ",".join(str(int(k)) for k in cpu_k), args.n, args.L, wall))
+        parity = {"ref_queries": checked, "k": [int(k) for k in cpu_k], "match": not mismatches,
+                  "what": "reference CLI's printed distances and answer-leaf file positions == the GPU batched "
+                          "path's distances (%f of the square root) and the plain path's answer leaves",
+                  "mismatches": mismatches[:3]}
+        return baseline, parity, index
     except Exception as e:  # the baseline is reported, never fatal
-        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": "failed: %s" % e}
+        return dict(na, sample="failed: %s" % e), {"match": None, "error": str(e)}, None
     finally:
         if d:
             shutil.rmtree(d, ignore_errors=True)
 
 
+def host_index_dir(need_bytes, prefix):
+    for base in ("/dev/shm", tempfile.gettempdir()):
+        try:
+            st = os.statvfs(base)
+            if st.f_bavail * st.f_frsize > need_bytes:
+                return tempfile.mkdtemp(prefix=prefix, dir=base) + "/"
+        except OSError:
+            continue
+    return None
+
+
 def run_reference(args, rank, world, local):
     """--impl reference: the reference's multi-threaded query path on the
-    host cores over the same index files, on queries of the batched
-    workload (each with its own k)."""
+    host cores, on queries of the timed batches (each with its own k).  This
+    process maps nothing of hercules_b200: the collection and the queries
+    come from the oracle's restatement of the generator (the same bits as
+    the GPU's), the index files from the oracle's restatement of the
+    reference's one-worker build (byte-identical to the reference's own
+    build, as the tests check), written on every host core."""
     if rank != 0:
         return
     from oracle import oracle as O
@@ -630,57 +812,57 @@ def run_reference(args, rank, world, local):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/hercules was not built from the "
                                                                "reference sources"}))
         return
-    import torch
-    import hercules_b200 as H
-    from hercules_b200 import build as B
-    B.build()
-    torch.cuda.set_device(local)
+    threads = os.cpu_count() or 1
     nps = args.ref_queries_per_step
-    X = build_collection(args, torch, H, local)
-    Qb, ks = make_batches(args, torch, H, X, 1, local, offset=0)
-    ix = H.HerculesIndex.build_device(X.data_ptr(), args.n, args.L, args.leaf, device=local)
-    del X
-    torch.cuda.empty_cache()
-    d = write_index_for_cpu(ix, args)
-    ix.close()
+    t0 = time.perf_counter()
+    d = host_index_dir(args.n * args.L * 4 * 1.05 + (1 << 30), "hg_ref_idx_")
     if d is None:
         print(json.dumps({"impl": "reference", "unavailable": "no host space for the %d x %d index files"
                                                                % (args.n, args.L)}))
         return
     try:
-        threads = os.cpu_count() or 1
+        X = O.gen_rows(DATA_SEED, args.n, args.L, unit=args.data == "unit")
+        oi = O.OracleIndex.build_mt(X, args.leaf, keep_rows=False)
+        oi.write(d, 64.0)
+        del oi, X
+        setup_s = time.perf_counter() - t0
+        index = dict(index_digests(d), built_by="oracle restatement of the reference's one-worker build "
+                                                "(or_build_mt), on the host", digest="SHA-256 over the SHA-256 "
+                                                                                     "of each 64 MiB chunk")
         # --sax-threshold above 1 keeps the reference on its serial refine
         # branch: its threaded refine worker never advances and hangs
         # (hercules_query_engine.c:1987-2026)
         extra = ("--sims", "--eapca-threshold", "0.25", "--sax-threshold", "1.1")
-        total = (args.steps + args.warmup) * nps
-        # spread the sample over the batch so the noise levels, fresh walks
-        # and k values appear in the batch's proportions
-        pick = np.linspace(0, args.batch - 1, total).astype(np.int64)
-        Qh = Qb[0].cpu().numpy()
-        times, wall = [], 0.0
-        for j in pick:
-            per_q, w = cpu_reference_run(args, d, Qh[j][None, :], threads=threads, extra=extra, k=int(ks[j]))
-            times.append(sum(per_q.values()))
-            wall += w
-        timed = times[args.warmup * nps:]
+        times, wall, ks_used = [], 0.0, []
+        for step in range(args.warmup + args.steps):
+            Qh, ks = batch_on_host(args, O, step)
+            # nps positions of this step's batch, rotating so that the
+            # steps together cover every (sigma^2, k) pair and the fresh walks
+            pos = [(step * 131 + t * args.batch // nps) % args.batch for t in range(nps)]
+            for j in pos:
+                per_q, w, _ = cpu_reference_run(args, d, Qh[j][None, :], threads=threads, extra=extra, k=int(ks[j]))
+                times.append((step, sum(per_q.values())))
+                wall += w
+                if step >= args.warmup:
+                    ks_used.append(int(ks[j]))
+        timed = [t for st, t in times if st >= args.warmup]
         secs = sum(timed)
         value = len(timed) / secs if secs > 0 else None
+        sample = ("%d queries per step from that step's batch of the workload (k used: %s); reference "
+                  "--num-threads %d --sims --eapca-threshold 0.25 --sax-threshold 1.1 over index files built by "
+                  "the oracle on the host; per-query time from its Query_total_time_secs; wall %.1f s, "
+                  "setup %.1f s" % (nps, ",".join(map(str, sorted(set(ks_used)))), threads, wall, setup_s))
         line = {"impl": "reference", "metric": METRIC, "value": round(value, 4) if value else None, "unit": UNIT,
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1000.0 * secs / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded z-normalised random walks)",
-                "config": {"workload": "batched exact k-NN workload, %d x %d float32, leaf %d, k cycling 1/10/100, "
-                                       "queries answered one at a time by the reference" % (args.n, args.L, args.leaf),
-                           "queries_per_step": nps},
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded z-normalised random walks; "
+                                                             "noisy and fresh queries)",
+                "config": config_of(args),
                 "cpu_baseline": {"value": round(value, 4) if value else None, "unit": UNIT, "cores": threads,
-                                 "kind": "reference",
-                                 "sample": "%d queries per step spread over a batch of the workload; reference "
-                                           "--num-threads %d --sims --eapca-threshold 0.25 --sax-threshold 1.1 "
-                                           "over the index files (built on the GPU, byte-identical to the "
-                                           "reference's); wall %.1f s" % (nps, threads, wall)},
+                                 "kind": "reference", "sample": sample},
                 "e2e": {"value": round(value, 4) if value else None, "unit": UNIT, "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
+                        "d2h_bytes_per_step": 0},
+                "index": index}
         print(json.dumps(line), flush=True)
     finally:
         shutil.rmtree(d, ignore_errors=True)

@@ -16,6 +16,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
 /* ---------------------------------------------------------------------- */
 /* primitives                                                              */
 /* ---------------------------------------------------------------------- */
@@ -237,9 +241,10 @@ struct or_index {
   int num_nodes;
   int num_leaves;
   or_node **leaves; /* DFS (left first) order */
-  float *rows;      /* leaf-ordered rows */
+  float *rows;      /* leaf-ordered rows (NULL after or_build_mt without rows) */
   int64_t *ids;     /* dataset id per leaf-ordered row */
   int owns_rows;
+  int threads;      /* or_build_mt: worker threads (0 = the sequential build) */
 };
 
 /* calc_hs_split_points, hercules_node_split.c:371-396 (min_length = 1) */
@@ -371,8 +376,9 @@ static int cmp_short(const void *a, const void *b) {
   return x < y ? -1 : (x > y ? 1 : 0);
 }
 
-/* hercules_index_split_node, hercules_node_split.c:1043-1345 */
-static void split_node(or_index *ix, or_node *n) {
+/* hercules_index_split_node, hercules_node_split.c:1043-1345: the split
+ * decision from the node's sketches and the two children, left empty. */
+static void split_decide(or_index *ix, or_node *n) {
   float max_diff = -FLT_MAX;
   int hs_split_point = -1;
   short from = 0, to = 0;
@@ -435,6 +441,11 @@ static void split_node(or_index *ix, or_node *n) {
   n->left = l;
   n->right = r;
   ix->num_nodes += 2;
+}
+
+static void split_node(or_index *ix, or_node *n) {
+  split_decide(ix, n);
+  or_node *l = n->left, *r = n->right;
   /* redistribution in insertion order, :1294-1333 */
   for (unsigned m = 0; m < n->node_size; ++m) {
     uint32_t id = n->members[m];
@@ -531,18 +542,177 @@ or_index *or_build(const float *data, uint64_t n, int L, int leaf_size) {
   return ix;
 }
 
+/* ---- the same build on several threads ----------------------------------
+ * A node's sketches are the element-wise max / min of (mean, stdev) over the
+ * series appended to it, and max / min do not depend on order; the
+ * sequential build updates them per insert, this one computes them over the
+ * member list when they are needed (at the node's split and, for the final
+ * leaves, at the end), in parallel.  Routing, which depends on the tree at
+ * the time of each insert, is done for a window of series at a time against
+ * the current tree; a series whose cached leaf split before its turn is
+ * routed on from that node.  The insertion order, the split decisions and
+ * the redistribution order are those of or_build, so the tree, the leaf
+ * order and every float are identical (tests check the index files). */
+
+static void sketch_members(const or_index *ix, or_node *n, int threads) {
+  const int nseg = n->nseg, nhs = n->nhs;
+  init_sketch(n->sk, nseg);
+  init_sketch(n->hs_sk, nhs);
+  if (!n->node_size) return;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(threads)
+#endif
+  {
+    float *sk = (float *)malloc(sizeof(float) * 4 * (nseg + nhs));
+    init_sketch(sk, nseg + nhs);
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+    for (int64_t m = 0; m < (int64_t)n->node_size; ++m) {
+      const float *x = ix->data + (uint64_t)n->members[m] * ix->L;
+      for (int i = 0; i < nseg; ++i) sketch_update(sk + 4 * i, x, seg_start(n->points, i), n->points[i]);
+      for (int i = 0; i < nhs; ++i)
+        sketch_update(sk + 4 * (nseg + i), x, seg_start(n->hs_points, i), n->hs_points[i]);
+    }
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+    {
+      for (int i = 0; i < nseg; ++i) {
+        float *p = n->sk + 4 * i;
+        const float *c = sk + 4 * i;
+        p[0] = fmaxf(p[0], c[0]);
+        p[1] = fminf(p[1], c[1]);
+        p[2] = fmaxf(p[2], c[2]);
+        p[3] = fminf(p[3], c[3]);
+      }
+      for (int i = 0; i < nhs; ++i) {
+        float *p = n->hs_sk + 4 * i;
+        const float *c = sk + 4 * (nseg + i);
+        p[0] = fmaxf(p[0], c[0]);
+        p[1] = fminf(p[1], c[1]);
+        p[2] = fmaxf(p[2], c[2]);
+        p[3] = fminf(p[3], c[3]);
+      }
+    }
+    free(sk);
+  }
+  (void)threads;
+}
+
+static void append_only(or_node *n, uint32_t id) {
+  ++n->node_size;
+  append_member(n, id);
+}
+
+static void split_node_mt(or_index *ix, or_node *n, unsigned char *flags) {
+  sketch_members(ix, n, ix->threads);
+  split_decide(ix, n);
+  or_node *l = n->left, *r = n->right;
+  const unsigned cnt = n->node_size;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(ix->threads)
+#endif
+  for (int64_t m = 0; m < (int64_t)cnt; ++m)
+    flags[m] = (unsigned char)route_left(n, ix->data + (uint64_t)n->members[m] * ix->L);
+  for (unsigned m = 0; m < cnt; ++m) append_only(flags[m] ? l : r, n->members[m]);
+  free(n->members);
+  n->members = NULL;
+  n->cap = 0;
+  n->is_leaf = 0;
+}
+
+or_index *or_build_mt(const float *data, uint64_t n, int L, int leaf_size, int threads, int keep_rows) {
+  if (L <= 0 || L % 16 != 0 || leaf_size <= 0) return NULL;
+#ifdef _OPENMP
+  if (threads <= 0) threads = omp_get_max_threads();
+#else
+  threads = 1;
+#endif
+  or_index *ix = (or_index *)calloc(1, sizeof(or_index));
+  ix->L = L;
+  ix->leaf_size = leaf_size;
+  ix->n = n;
+  ix->data = data;
+  ix->threads = threads;
+  short pt = (short)L;
+  ix->root = new_leaf(&pt, 1);
+  make_filename(ix->root, NULL);
+  ix->num_nodes = 1;
+  const uint64_t W = (uint64_t)1 << 18;
+  or_node **route = (or_node **)malloc(sizeof(or_node *) * W);
+  unsigned char *flags = (unsigned char *)malloc((size_t)leaf_size + 1);
+  for (uint64_t i0 = 0; i0 < n; i0 += W) {
+    const uint64_t w = n - i0 < W ? n - i0 : W;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static, 256) num_threads(threads)
+#endif
+    for (int64_t j = 0; j < (int64_t)w; ++j) {
+      const float *x = data + (i0 + (uint64_t)j) * L;
+      or_node *nd = ix->root;
+      while (!nd->is_leaf) nd = route_left(nd, x) ? nd->left : nd->right;
+      route[j] = nd;
+    }
+    for (uint64_t j = 0; j < w; ++j) {
+      const uint32_t id = (uint32_t)(i0 + j);
+      const float *x = data + (uint64_t)id * L;
+      or_node *nd = route[j];
+      while (!nd->is_leaf) nd = route_left(nd, x) ? nd->left : nd->right;
+      append_only(nd, id);
+      if (nd->node_size >= (unsigned)leaf_size) split_node_mt(ix, nd, flags);
+    }
+  }
+  free(route);
+  free(flags);
+  /* sketches of the final leaves, then the leaf order and the ancestor merge */
+  int cnt = 0;
+  collect_leaves(ix, ix->root, &cnt);
+  ix->num_leaves = cnt;
+  ix->leaves = (or_node **)malloc(sizeof(or_node *) * (cnt > 0 ? cnt : 1));
+  cnt = 0;
+  collect_leaves(ix, ix->root, &cnt);
+  for (int i = 0; i < cnt; ++i) sketch_members(ix, ix->leaves[i], threads);
+  ix->ids = (int64_t *)malloc(sizeof(int64_t) * (n ? n : 1));
+  uint64_t pos = 0;
+  for (int i = 0; i < cnt; ++i) {
+    or_node *lf = ix->leaves[i];
+    lf->file_pos = pos;
+    for (unsigned m = 0; m < lf->node_size; ++m) ix->ids[pos + m] = lf->members[m];
+    pos += lf->node_size;
+    merge_ancestors(lf);
+  }
+  if (keep_rows) {
+    ix->rows = (float *)malloc(sizeof(float) * L * (n ? n : 1));
+    ix->owns_rows = 1;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static, 1024) num_threads(threads)
+#endif
+    for (int64_t r = 0; r < (int64_t)n; ++r)
+      memcpy(ix->rows + (uint64_t)r * L, data + (uint64_t)ix->ids[r] * L, sizeof(float) * L);
+    ix->data = NULL;
+  }
+  /* without rows, ix->data stays the caller's matrix until or_write */
+  return ix;
+}
+
 /* ---------------------------------------------------------------------- */
 /* on-disk format                                                          */
 /* ---------------------------------------------------------------------- */
 
+/* Leaf-ordered row r: the resident copy, or the caller's matrix after
+ * or_build_mt without rows. */
+static const float *leaf_row(const or_index *ix, uint64_t r) {
+  return ix->rows ? ix->rows + r * ix->L : ix->data + (uint64_t)ix->ids[r] * ix->L;
+}
+
 static void write_node(or_index *ix, or_node *n, FILE *f, FILE *raw, FILE *sims, const float *bp,
-                       uint64_t *leaves_written) {
+                       uint64_t *leaves_written, const unsigned char *words) {
   unsigned char is_leaf = (unsigned char)n->is_leaf;
   fwrite(&is_leaf, 1, 1, f);
   fwrite(&n->level, 4, 1, f);
   if (!n->is_leaf) {
-    write_node(ix, n->left, f, raw, sims, bp, leaves_written);
-    write_node(ix, n->right, f, raw, sims, bp, leaves_written);
+    write_node(ix, n->left, f, raw, sims, bp, leaves_written, words);
+    write_node(ix, n->right, f, raw, sims, bp, leaves_written, words);
     fwrite(&n->node_size, 4, 1, f);
     short split_segment = -1;
     fwrite(&split_segment, 2, 1, f);
@@ -582,11 +752,15 @@ static void write_node(or_index *ix, or_node *n, FILE *f, FILE *raw, FILE *sims,
     }
     fwrite(&n->file_pos, 8, 1, f);
     for (unsigned m = 0; m < n->node_size; ++m) {
-      const float *x = ix->rows + (n->file_pos + m) * ix->L;
+      const float *x = leaf_row(ix, n->file_pos + m);
       fwrite(x, 4, ix->L, raw);
-      unsigned char w[OR_PAA_SEGMENTS];
-      or_sax(x, w, ix->L, bp);
-      fwrite(w, 1, OR_PAA_SEGMENTS, sims);
+      if (words) {
+        fwrite(words + (n->file_pos + m) * OR_PAA_SEGMENTS, 1, OR_PAA_SEGMENTS, sims);
+      } else {
+        unsigned char w[OR_PAA_SEGMENTS];
+        or_sax(x, w, ix->L, bp);
+        fwrite(w, 1, OR_PAA_SEGMENTS, sims);
+      }
     }
     ++(*leaves_written);
   }
@@ -620,7 +794,21 @@ int or_write(or_index *ix, const char *dir, double buffer_mb, const float *bp255
   fwrite(&leaf, 4, 1, f);
   fwrite(&serial, 4, 1, f);
   fwrite(&sims_flag, 4, 1, f);
-  write_node(ix, ix->root, f, raw, sims, bp255, &leaves);
+  /* the multi-threaded build: iSAX words of every row in parallel first,
+   * and large stdio buffers for the two data files */
+  unsigned char *words = NULL;
+  if (ix->threads > 0) {
+    setvbuf(raw, NULL, _IOFBF, (size_t)1 << 24);
+    setvbuf(sims, NULL, _IOFBF, (size_t)1 << 22);
+    words = (unsigned char *)malloc((size_t)OR_PAA_SEGMENTS * (ix->n ? ix->n : 1));
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static, 1024) num_threads(ix->threads)
+#endif
+    for (int64_t r = 0; r < (int64_t)ix->n; ++r)
+      or_sax(leaf_row(ix, (uint64_t)r), words + (uint64_t)r * OR_PAA_SEGMENTS, ix->L, bp255);
+  }
+  write_node(ix, ix->root, f, raw, sims, bp255, &leaves, words);
+  free(words);
   fseek(f, 0, SEEK_SET);
   fwrite(&leaves, 8, 1, f);
   fclose(f);

@@ -61,6 +61,11 @@ typedef struct or_index or_index;
  * hercules_node_split.c:1043-1345).  data is row-major n x L. */
 or_index *or_build(const float *data, uint64_t n, int L, int leaf_size);
 
+/* or_build on `threads` threads (0 = every core): the same tree, leaf order
+ * and floats.  keep_rows = 0 keeps no leaf-ordered copy of the rows: data
+ * must then stay valid until or_write, which reads the rows from it. */
+or_index *or_build_mt(const float *data, uint64_t n, int L, int leaf_size, int threads, int keep_rows);
+
 /* hercules_index_write_sequential (hercules_index.c:1611-1692, 1967-2077,
  * hercules_file_buffer.c:539-583).  dir must end with '/'. */
 int or_write(or_index *ix, const char *dir, double buffer_mb, const float *bp255);
@@ -78,6 +83,13 @@ uint64_t or_num_rows(const or_index *ix);
 /* leaf i in DFS order: file_pos and size */
 void or_leaf_info(const or_index *ix, int i, uint64_t *file_pos, uint32_t *size,
                   int *nseg, short *points /* >= nseg */, float *sk /* >= 4*nseg */);
+/* seeded synthetic data (oracle_gen.c): rows [first, first+n) of stream
+ * seed -- random walks (unit = 0) or unit vectors (unit = 1) -- and noisy
+ * queries whose base rows are regenerated from data_seed */
+void or_gen_rows(uint64_t seed, uint64_t first, uint64_t n, int L, float *out, int unit, int threads);
+void or_gen_queries(uint64_t data_seed, uint64_t seed, uint64_t n, int L, int nq, const double *sigma2, float *out,
+                    uint64_t *base_ids, int unit);
+
 /* dataset id of leaf-ordered row r (valid after or_build) */
 void or_row_ids(const or_index *ix, int64_t *ids_out);
 /* leaf-ordered raw rows (valid after or_build or or_read) */
