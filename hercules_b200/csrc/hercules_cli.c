@@ -91,6 +91,37 @@ static int build_index(const opts_t *o, hg_index **ix) {
   return 1;
 }
 
+/* The query file must hold --queries-skip + --queries-size series of the
+ * index's length (root.idx header: timeseries_size at byte 16).  Checked
+ * before the index is loaded, so a bad request fails fast with the
+ * reference's messages and no device work. */
+static int check_query_file(const opts_t *o) {
+  char path[4096];
+  snprintf(path, sizeof path, "%sroot.idx", o->index_path ? o->index_path : "");
+  FILE *r = fopen(path, "rb");
+  if (!r) return 1; /* hg_index_read reports it */
+  unsigned char hdr[20];
+  const size_t got = fread(hdr, 1, sizeof hdr, r);
+  fclose(r);
+  if (got != sizeof hdr) return 1;
+  uint32_t L;
+  memcpy(&L, hdr + 16, 4);
+  if (L == 0) return 1;
+  FILE *f = fopen(o->queries, "rb");
+  if (!f) {
+    fprintf(stderr, "File %s not found!\n", o->queries);
+    return 0;
+  }
+  fseeko(f, 0, SEEK_END);
+  const unsigned long long total = (unsigned long long)ftello(f) / (sizeof(float) * L);
+  fclose(f);
+  if (total < (unsigned long long)o->queries_size + o->queries_skip) {
+    fprintf(stderr, "File %s has only %llu records!\n", o->queries, total);
+    return 0;
+  }
+  return 1;
+}
+
 static int run_queries(const opts_t *o, hg_index *ix) {
   hg_index_info info;
   hg_index_info_get(ix, &info);
@@ -257,6 +288,7 @@ int main(int argc, char **argv) {
   }
   if (ok && (o.mode == 1 || o.mode == 2)) {
     if (!o.queries) { fprintf(stderr, "Error in hercules: --queries is required\n"); return 1; }
+    if (!ix && !check_query_file(&o)) return 1;
     if (!ix) {
       double t0 = now_s();
       ok = check(hg_index_read(o.index_path, o.gpu, &ix), "read");

@@ -26,7 +26,6 @@
 using hg::Node;
 
 // Launch geometry of the leaf scan.
-constexpr int kFilterBlocksPerSm = 8;  // k_lbsax_filter
 
 // ---------------------------------------------------------------------------
 // errors
@@ -301,6 +300,7 @@ static void free_device(hg_index* ix) {
   dfree(s.topk_count);
   dfree(s.topk_row);
   dfree(s.paa);
+  dfree(s.sax_tab);
   dfree(s.stats);
   dfree(s.err);
   dfree(s.list);
@@ -927,6 +927,53 @@ static hg_status write_impl(hg_index* ix, const char* dir, double buffer_mb) {
   return ok ? HG_OK : set_error(HG_ERR_IO, "hg_index_write: short write");
 }
 
+// The device half of hg_index_read: rows from the open leaves_raw.idx
+// (closed here), ids, breakpoints, iSAX words and the tables.
+static hg_status read_device_part(hg_index* ix, FILE* raw, const char* dir) {
+  hg::DeviceIndex& d = ix->d;
+  // leaves_raw.idx is the HBM image: copy it in pieces
+  const uint64_t piece = std::max<uint64_t>(1, (64u << 20) / (sizeof(float) * ix->L));
+  std::vector<float> h_rm(piece * ix->L);
+  cudaError_t e = dalloc(&d.rows, (size_t)ix->n * ix->L);
+  for (uint64_t r0 = 0; r0 < ix->n && e == cudaSuccess; r0 += piece) {
+    const uint64_t cnt = std::min(piece, ix->n - r0);
+    if (fread(h_rm.data(), sizeof(float) * ix->L, cnt, raw) != cnt) {
+      fclose(raw);
+      free_device(ix);
+      return set_error(HG_ERR_IO, "hg_index_read: leaves_raw.idx is shorter than the leaves");
+    }
+    e = cudaMemcpy(d.rows + r0 * ix->L, h_rm.data(), sizeof(float) * cnt * ix->L, cudaMemcpyHostToDevice);
+  }
+  fclose(raw);
+  if (e != cudaSuccess) {
+    free_device(ix);
+    return cuda_fail(e, "hg_index_read");
+  }
+  // dataset ids: leaves_ids.idx when present, else the row number
+  ix->ids.resize(ix->n);
+  FILE* idf = fopen(join(dir, "leaves_ids.idx").c_str(), "rb");
+  ix->has_ids = false;
+  if (idf) {
+    std::vector<uint64_t> ids64(ix->n);
+    if (fread(ids64.data(), 8, ix->n, idf) == ix->n) {
+      for (uint64_t i = 0; i < ix->n; ++i) ix->ids[i] = (int64_t)ids64[i];
+      ix->has_ids = true;
+    }
+    fclose(idf);
+  }
+  if (!ix->has_ids)
+    for (uint64_t i = 0; i < ix->n; ++i) ix->ids[i] = (int64_t)i;
+  CK(dalloc(&d.ids, ix->n));
+  CK(cudaMemcpy(d.ids, ix->ids.data(), sizeof(int64_t) * ix->n, cudaMemcpyHostToDevice));
+  CK(dalloc(&d.bp, 256));
+  CK(cudaMemcpy(d.bp, kHgBreakpoints, sizeof(float) * 255, cudaMemcpyHostToDevice));
+  CK(dalloc(&d.sax, (size_t)ix->n * 16));
+  CK(hg::launch_sax_rows(d.rows, ix->L, ix->n, d.bp, d.sax, ix->stream));
+  CK(cudaStreamSynchronize(ix->stream));
+  HCK(upload_tables(ix));
+  return HG_OK;
+}
+
 static hg_status read_impl(const char* dir, int device, hg_index** out) {
   if (!dir || !out) return set_error(HG_ERR_ARG, "hg_index_read: null argument");
   FILE* f = fopen(join(dir, "root.idx").c_str(), "rb");
@@ -965,51 +1012,28 @@ static hg_status read_impl(const char* dir, int device, hg_index** out) {
   (void)nleaves_hdr;
   ix->n = pos;
   ix->device = device;
-  CK(cudaSetDevice(device));
-  CK(cudaStreamCreateWithFlags(&ix->stream, cudaStreamNonBlocking));
-  hg::DeviceIndex& d = ix->d;
+  // the data file must hold every leaf's rows: checked before any device work
   FILE* raw = fopen(join(dir, "leaves_raw.idx").c_str(), "rb");
   if (!raw) return set_error(HG_ERR_IO, "hg_index_read: cannot open leaves_raw.idx");
-  // leaves_raw.idx is the HBM image: copy it in pieces
-  const uint64_t piece = std::max<uint64_t>(1, (64u << 20) / (sizeof(float) * ix->L));
-  std::vector<float> h_rm(piece * ix->L);
-  cudaError_t e = dalloc(&d.rows, (size_t)ix->n * ix->L);
-  for (uint64_t r0 = 0; r0 < ix->n && e == cudaSuccess; r0 += piece) {
-    const uint64_t cnt = std::min(piece, ix->n - r0);
-    if (fread(h_rm.data(), sizeof(float) * ix->L, cnt, raw) != cnt) {
+  if (fseeko(raw, 0, SEEK_END) != 0 || (uint64_t)ftello(raw) < ix->n * ix->L * sizeof(float) ||
+      fseeko(raw, 0, SEEK_SET) != 0) {
+    fclose(raw);
+    return set_error(HG_ERR_IO, "hg_index_read: leaves_raw.idx is shorter than the leaves");
+  }
+  {
+    const cudaError_t e0 = cudaSetDevice(device);
+    cudaError_t e1 = e0 == cudaSuccess ? cudaStreamCreateWithFlags(&ix->stream, cudaStreamNonBlocking) : e0;
+    if (e1 != cudaSuccess) {
       fclose(raw);
-      free_device(ix.get());
-      return set_error(HG_ERR_IO, "hg_index_read: leaves_raw.idx is shorter than the leaves");
+      ix->stream = nullptr;
+      return cuda_fail(e1, "hg_index_read");
     }
-    e = cudaMemcpy(d.rows + r0 * ix->L, h_rm.data(), sizeof(float) * cnt * ix->L, cudaMemcpyHostToDevice);
   }
-  fclose(raw);
-  if (e != cudaSuccess) {
-    free_device(ix.get());
-    return cuda_fail(e, "hg_index_read");
+  const hg_status st = read_device_part(ix.get(), raw, dir);
+  if (st != HG_OK) {
+    hg_index_destroy(ix.release());
+    return st;
   }
-  // dataset ids: leaves_ids.idx when present, else the row number
-  ix->ids.resize(ix->n);
-  FILE* idf = fopen(join(dir, "leaves_ids.idx").c_str(), "rb");
-  ix->has_ids = false;
-  if (idf) {
-    std::vector<uint64_t> ids64(ix->n);
-    if (fread(ids64.data(), 8, ix->n, idf) == ix->n) {
-      for (uint64_t i = 0; i < ix->n; ++i) ix->ids[i] = (int64_t)ids64[i];
-      ix->has_ids = true;
-    }
-    fclose(idf);
-  }
-  if (!ix->has_ids)
-    for (uint64_t i = 0; i < ix->n; ++i) ix->ids[i] = (int64_t)i;
-  CK(dalloc(&d.ids, ix->n));
-  CK(cudaMemcpy(d.ids, ix->ids.data(), sizeof(int64_t) * ix->n, cudaMemcpyHostToDevice));
-  CK(dalloc(&d.bp, 256));
-  CK(cudaMemcpy(d.bp, kHgBreakpoints, sizeof(float) * 255, cudaMemcpyHostToDevice));
-  CK(dalloc(&d.sax, (size_t)ix->n * 16));
-  CK(hg::launch_sax_rows(d.rows, ix->L, ix->n, d.bp, d.sax, ix->stream));
-  CK(cudaStreamSynchronize(ix->stream));
-  HCK(upload_tables(ix.get()));
   *out = ix.release();
   return HG_OK;
 }
@@ -1035,6 +1059,7 @@ static hg_status ensure_scratch(hg_index* ix, int k) {
   dfree(s.topk);
   dfree(s.topk_count);
   dfree(s.paa);
+  dfree(s.sax_tab);
   dfree(s.stats);
   dfree(s.err);
   dfree(s.list);
@@ -1055,6 +1080,7 @@ static hg_status ensure_scratch(hg_index* ix, int k) {
   CK(dalloc(&s.topk, hg::kMaxK));
   CK(dalloc(&s.topk_count, 1));
   CK(dalloc(&s.paa, 16));
+  CK(dalloc(&s.sax_tab, HG_PAA_SEGMENTS * HG_SAX_CARD));
   CK(dalloc(&s.stats, 8));
   CK(dalloc(&s.err, 1));
   CK(dalloc(&s.q, 1));
@@ -1143,7 +1169,8 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
   } else {
     CK(hg::launch_query_prep(d_q, e.L, index_tree(ix), d.leaf_start, d.leaf_size, s.approx_leaf, s.paa, s.cand,
                              s.cand_lb, s.cand_count, s.unit_prefix, s.bound, s.topk_count, s.counters, st));
-    CK(hg::launch_leaf_lb(d_q, e.L, nl, d.leaf_seg_off, d.leaf_points, d.leaf_sk, s.lb, st));
+    CK(hg::launch_leaf_lb(d_q, e.L, nl, d.leaf_seg_off, d.leaf_points, d.leaf_sk, s.lb, st, s.paa, d.bp,
+                          o.use_lb_sax ? s.sax_tab : nullptr));
     // the approximate leaf, with an unbounded k-th distance at the start
         // two blocks per SM: the bound starts at +inf, so more warps would finish
     // more rows of this leaf before it tightens; fewer leave HBM idle
@@ -1171,13 +1198,14 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
     f.cand_count = s.cand_count;
     f.unit_prefix = s.unit_prefix;
     f.paa = s.paa;
+    f.sax_tab = s.sax_tab;
     f.use_lbsax = o.use_lb_sax ? 1 : 0;
     f.bound = s.bound;
     f.list = s.list;
     f.list_count = s.counters + 2;
     f.stats = s.stats;
     HCK(timed_begin(prof ? &prof->filter : nullptr, st));
-    CK(hg::launch_lbsax_filter(f, sms * kFilterBlocksPerSm, st));
+    CK(hg::launch_lbsax_filter(f, sms, st));
     HCK(timed_end(prof ? &prof->filter : nullptr, st));
     e.list = s.list;
     e.list_count = s.counters + 2;
