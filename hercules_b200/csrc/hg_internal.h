@@ -70,6 +70,7 @@ struct QueryScratch {
   int* topk_count = nullptr;
   uint64_t* topk_row = nullptr;   // kmax leaf-ordered rows of the answers
   float* paa = nullptr;           // 16
+  float* sax_tab = nullptr;       // 16 x 256 LB_SAX terms of the current query
   unsigned long long* stats = nullptr;  // see ScanArgs
   uint32_t* list = nullptr;       // LB_SAX survivors (rows), n entries
   int* err = nullptr;             // device error flag

@@ -258,9 +258,19 @@ __global__ void k_route_queries(const float* __restrict__ Q, int nq, int L, Tree
 }
 
 // LB_EAPCA of the query against every leaf, one warp per leaf.
+// LB_EAPCA of every leaf (a warp per leaf).  With sax_tab set, the
+// threads also write the query's LB_SAX term table for the filter:
+// sax_tab[t * 256 + s] = hg_lb_sax_lane(paa[t], s) (reference arithmetic,
+// sax.c:310-479), 4,096 entries, computed once per query.
 __global__ void k_leaf_lb(const float* __restrict__ q, int L, int nleaves, const int* __restrict__ seg_off,
-                          const short* __restrict__ points, const float* __restrict__ sk, float* __restrict__ lb) {
+                          const short* __restrict__ points, const float* __restrict__ sk, float* __restrict__ lb,
+                          const float* __restrict__ paa, const float* __restrict__ bp, float* __restrict__ sax_tab) {
   extern __shared__ float qs[];
+  if (sax_tab) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < HG_PAA_SEGMENTS * HG_SAX_CARD;
+         i += gridDim.x * blockDim.x)
+      sax_tab[i] = hg_lb_sax_lane(paa[i >> 8], i & 255, bp);
+  }
   for (int i = threadIdx.x; i < L; i += blockDim.x) qs[i] = q[i];
   __syncthreads();
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -500,25 +510,53 @@ __global__ void k_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_pre
 
 // Stage 1.  Work: the candidate leaves in ascending LB_EAPCA order, cut into
 // 32-row units (32-aligned rows; a unit's rows outside its leaf are skipped).
-// Block b owns a contiguous range of units and its 8 warps take 4 units each
-// per iteration (1024 rows, 16 KiB of iSAX words in flight per block); the
-// block stops at the first leaf whose LB exceeds the bound.  Each row's
-// LB_SAX comes from its 16-byte iSAX word (minidist_paa_to_isax_raw_SIMD,
-// sax.c:310-479); survivors are appended with one atomicAdd per block
-// iteration.
-constexpr int kFilterThreads = 256;
-constexpr int kFilterUnits = 4;
-__global__ void __launch_bounds__(kFilterThreads) k_lbsax_filter(FilterArgs a) {
+// One persistent block per SM owns a contiguous range of units; each warp
+// takes kFilterUnits units per step (one 16-byte iSAX word per lane and
+// unit in flight), and a warp stops at the first leaf whose LB exceeds the
+// bound.  Survivors are appended with one atomicAdd per warp and step.
+//
+// The per-row test is a certified lower bound of the reference's LB_SAX
+// (minidist_paa_to_isax_raw_SIMD, sax.c:310-479).  The query's 16 x 256
+// table of per-segment terms (k_leaf_lb, reference arithmetic) is turned,
+// per block, into 8-bit terms q = floor(term * 254 / T) (rounded down at
+// every step, at most 255) against the pruning threshold
+// T = (B (1 + 2^-10) + 1e-6) / (L / 16); a row is pruned when its 16 terms
+// add up to at least 255, which implies (L / 16) * (sum of the terms) >=
+// (255 / 254) (B (1 + 2^-10) + 1e-6): the reference's float LB_SAX exceeds
+// the bound with room to spare for its rounding, so every row this test
+// prunes is one the exact float test prunes too (never a true neighbour).
+// The 8-bit table is laid out lane-private -- word ((t * 256 + s) / 4) * 32
+// + lane holds the terms of symbols s..s+3 of segment t for that lane -- so
+// the 16 data-dependent lookups of a row never conflict on a bank.
+constexpr int kFilterThreads = 768;
+constexpr int kFilterUnits = 8;
+constexpr int kSaxTabWords = HG_PAA_SEGMENTS * HG_SAX_CARD / 4 * 32;  // 128 KB
+size_t lbsax_filter_smem() { return sizeof(uint32_t) * kSaxTabWords; }
+
+__device__ __forceinline__ uint32_t sax_qterm(float term, float scale) {
+  const float p = __fmul_rd(term, scale);
+  return p >= 255.0f ? 255u : (uint32_t)p;
+}
+
+__global__ void __launch_bounds__(kFilterThreads, 1) k_lbsax_filter(FilterArgs a) {
   constexpr int W = kFilterThreads / 32;
-  // per-query table of the per-segment LB_SAX terms: dtab[j][s] is the
-  // squared gap between the query's PAA value j and symbol s's region
-  __shared__ float dtab[HG_PAA_SEGMENTS][HG_SAX_CARD];
+  extern __shared__ uint32_t qtab[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const float B = __int_as_float((int)ld_volatile(a.bound));
   if (a.use_lbsax) {
-    for (int i = threadIdx.x; i < HG_PAA_SEGMENTS * HG_SAX_CARD; i += blockDim.x)
-      dtab[i >> 8][i & 255] = hg_lb_sax_lane(a.paa[i >> 8], i & 255, a.bp);
+    const float Bs = __fadd_rn(__fmul_rn(B, 1.0009765625f), 1e-6f);
+    const float T = __fdiv_ru(Bs, (float)(a.L / HG_PAA_SEGMENTS));
+    const float scale = __fdiv_rd(254.0f, T);  // 0 when the bound is +inf: nothing is pruned
+    for (int g = threadIdx.x; g < kSaxTabWords / 32; g += blockDim.x) {
+      const float4 v = reinterpret_cast<const float4*>(a.sax_tab)[g];
+      const uint32_t packed = sax_qterm(v.x, scale) | (sax_qterm(v.y, scale) << 8) |
+                              (sax_qterm(v.z, scale) << 16) | (sax_qterm(v.w, scale) << 24);
+#pragma unroll 8
+      for (int r = 0; r < 32; ++r) qtab[g * 32 + ((r + lane) & 31)] = packed;
+    }
   }
   __syncthreads();
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t* tl = qtab + lane;
   const uint32_t lt = (1u << lane) - 1;
   const int ncand = *a.cand_count;
   const uint32_t total = a.unit_prefix[ncand];
@@ -526,64 +564,60 @@ __global__ void __launch_bounds__(kFilterThreads) k_lbsax_filter(FilterArgs a) {
   const uint32_t u0 = blockIdx.x * per_block;
   const uint32_t u1 = min(total, u0 + per_block);
   if (u0 >= u1) return;
-  const float B = __int_as_float((int)ld_volatile(a.bound));
-  // LB_SAX is a lower bound of the exact distance; the margin covers the
-  // float rounding of both sides so that no true neighbour is dropped.
-  const float Bs = __fadd_rn(__fmul_rn(B, 1.0009765625f), 1e-6f);
-  const float ratio = (float)(a.L / HG_PAA_SEGMENTS);
   int c = unit_candidate(a.unit_prefix, ncand, 0, u0);
+  uint32_t next_c = c + 1 < ncand ? a.unit_prefix[c + 1] : 0xffffffffu;  // first unit of candidate c + 1
   int cur = -1;
-  uint64_t lstart = 0, lend = 0;
+  uint32_t lstart = 0, lend = 0, first_unit = 0;
   float clb = 0.0f;
   unsigned long long n_rows = 0, n_pruned = 0, n_leaves = 0;
-  // each warp walks its own units (base + kFilterUnits units per step) and
-  // reserves its survivors' list slots itself: no block barrier in the loop
   for (uint32_t base = u0 + wib * kFilterUnits; base < u1; base += W * kFilterUnits) {
-    uint32_t m[kFilterUnits];
-    uint64_t rr[kFilterUnits];
-    bool ok[kFilterUnits];
+    uint32_t rr[kFilterUnits];
     uint4 w[kFilterUnits];
+    uint32_t okm = 0;
     bool stop = false;
 #pragma unroll
     for (int j = 0; j < kFilterUnits; ++j) {
       const uint32_t unit = base + j;
-      ok[j] = false;
       rr[j] = 0;
       if (unit < u1 && !stop) {
-        while (c + 1 < ncand && a.unit_prefix[c + 1] <= unit) ++c;
+        while (unit >= next_c) {
+          ++c;
+          next_c = c + 1 < ncand ? a.unit_prefix[c + 1] : 0xffffffffu;
+        }
         if (c != cur) {
           cur = c;
           const int leaf = a.cand[c];
-          lstart = a.leaf_start[leaf];
+          lstart = (uint32_t)a.leaf_start[leaf];
           lend = lstart + a.leaf_size[leaf];
           clb = a.cand_lb[c];
+          first_unit = a.unit_prefix[c];
         }
         if (clb > B) {
           stop = true;  // every later unit belongs to a leaf with a larger LB
         } else {
-          const uint32_t tile_in = unit - a.unit_prefix[c];
+          const uint32_t tile_in = unit - first_unit;
           if (tile_in == 0 && lane == 0) ++n_leaves;
           rr[j] = (((lstart >> 5) + tile_in) << 5) + lane;
-          ok[j] = rr[j] >= lstart && rr[j] < lend;
+          if (rr[j] >= lstart && rr[j] < lend) okm |= 1u << j;
         }
       }
-      if (a.use_lbsax && ok[j]) w[j] = reinterpret_cast<const uint4*>(a.sax)[rr[j]];
+      if (a.use_lbsax && ((okm >> j) & 1u)) w[j] = __ldcs(reinterpret_cast<const uint4*>(a.sax) + rr[j]);
     }
+    uint32_t m[kFilterUnits];
     uint32_t cnt = 0;
 #pragma unroll
     for (int j = 0; j < kFilterUnits; ++j) {
-      bool pass = ok[j];
+      bool pass = (okm >> j) & 1u;
       if (pass) ++n_rows;
       if (pass && a.use_lbsax) {
         const uint32_t ws[4] = {w[j].x, w[j].y, w[j].z, w[j].w};
-        float d[16];
+        uint32_t sum = 0;
 #pragma unroll
-        for (int t = 0; t < 16; ++t) d[t] = dtab[t][(ws[t >> 2] >> ((t & 3) * 8)) & 255];
-        float s8[8];
-#pragma unroll
-        for (int t = 0; t < 8; ++t) s8[t] = __fadd_rn(d[t], d[t + 8]);
-        const float lbs = __fmul_rn(hg_hsum8(s8[0], s8[1], s8[2], s8[3], s8[4], s8[5], s8[6], s8[7]), ratio);
-        if (lbs > Bs) {
+        for (int t = 0; t < 16; ++t) {
+          const uint32_t sym = (ws[t >> 2] >> ((t & 3) * 8)) & 255u;
+          sum += __byte_perm(tl[t * 2048 + (sym >> 2) * 32], 0u, 0x4440u | (sym & 3u));
+        }
+        if (sum >= 255u) {
           pass = false;
           ++n_pruned;
         }
@@ -596,7 +630,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_lbsax_filter(FilterArgs a) {
     pos = __shfl_sync(HG_FULL, pos, 0);
 #pragma unroll
     for (int j = 0; j < kFilterUnits; ++j) {
-      if ((m[j] >> lane) & 1u) a.list[pos + __popc(m[j] & lt)] = (uint32_t)rr[j];
+      if ((m[j] >> lane) & 1u) a.list[pos + __popc(m[j] & lt)] = rr[j];
       pos += __popc(m[j]);
     }
     // units are in candidate order, LB non-decreasing: a unit past the bound
@@ -1085,13 +1119,15 @@ cudaError_t launch_route_queries(const float* Q, int nq, int L, Tree t, int* lea
 }
 
 cudaError_t launch_leaf_lb(const float* q, int L, int nleaves, const int* seg_off, const short* points,
-                           const float* sk, float* lb_out, cudaStream_t s) {
+                           const float* sk, float* lb_out, cudaStream_t s, const float* paa, const float* bp,
+                           float* sax_tab) {
   if (!nleaves) return cudaSuccess;
   static SmemLimit attr;
   const cudaError_t ea = attr.ensure((const void*)k_leaf_lb, 65536);
   if (ea != cudaSuccess) return ea;
-  k_leaf_lb<<<blocks_for((uint64_t)nleaves * 32, 256), 256, sizeof(float) * L, s>>>(q, L, nleaves, seg_off,
-                                                                                  points, sk, lb_out);
+  unsigned grid = blocks_for((uint64_t)nleaves * 32, 256);
+  if (sax_tab && grid < HG_PAA_SEGMENTS) grid = HG_PAA_SEGMENTS;  // 16 x 256 threads: one per table entry
+  k_leaf_lb<<<grid, 256, sizeof(float) * L, s>>>(q, L, nleaves, seg_off, points, sk, lb_out, paa, bp, sax_tab);
   return cudaGetLastError();
 }
 
@@ -1150,7 +1186,10 @@ cudaError_t launch_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_pr
 }
 
 cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s) {
-  k_lbsax_filter<<<blocks, kFilterThreads, 0, s>>>(a);
+  static SmemLimit attr;
+  const cudaError_t ea = attr.ensure((const void*)k_lbsax_filter, (int)lbsax_filter_smem());
+  if (ea != cudaSuccess) return ea;
+  k_lbsax_filter<<<blocks, kFilterThreads, lbsax_filter_smem(), s>>>(a);
   return cudaGetLastError();
 }
 

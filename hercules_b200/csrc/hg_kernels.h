@@ -67,6 +67,7 @@ struct FilterArgs {
   const int* cand_count;
   const uint32_t* unit_prefix;  // exclusive prefix of 32-row units per candidate
   const float* paa;
+  const float* sax_tab;  // the query's 16 x 256 LB_SAX terms (k_leaf_lb), 16-byte aligned
   int use_lbsax;
   const uint32_t* bound;
   uint32_t* list;        // surviving rows
@@ -119,13 +120,15 @@ cudaError_t launch_query_prep(const float* q, int L, Tree t, const uint64_t* lea
                               int* topk_count, uint32_t* counters, cudaStream_t s);
 cudaError_t launch_route_queries(const float* Q, int nq, int L, Tree t, int* leaf_out, cudaStream_t s);
 cudaError_t launch_leaf_lb(const float* q, int L, int nleaves, const int* seg_off, const short* points,
-                           const float* sk, float* lb_out, cudaStream_t s);
+                           const float* sk, float* lb_out, cudaStream_t s, const float* paa = nullptr,
+                           const float* bp = nullptr, float* sax_tab = nullptr);
 cudaError_t launch_select_sort(const float* lb, int nleaves, const uint32_t* bound, const int* approx_leaf,
                                const uint64_t* leaf_start, const uint32_t* leaf_size, int* cand,
                                float* cand_lb, int* cand_count, uint32_t* unit_prefix, cudaStream_t s);
 cudaError_t launch_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
                               int* topk_count, uint32_t* counters, cudaStream_t s);
-cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s);
+cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s);  // blocks: one per SM
+size_t lbsax_filter_smem();
 cudaError_t launch_ed_stream(const EdArgs& a, int blocks, cudaStream_t s);
 // batched path: the (leaf, query) pairs whose LB_EAPCA is within the query's
 // bound (k_leaf_keep)
