@@ -42,8 +42,12 @@ of hercules_b200: the collection and the queries come from the oracle's
 restatement of the generator, and the index files from the oracle's
 restatement of the reference's one-worker build.
 
-Multi-GPU (torchrun): every rank holds a full replica of the collection and
-answers its own queries; there is no data-path collective (weak scaling).
+Multi-GPU (torchrun, N > 1): by default the collection is split into N
+row-range shards, each rank builds and searches its own, and every batch's
+per-shard answers are all-gathered over NCCL and merged on the device inside
+the timed region (strong scaling: the total work is fixed).  --multi replica
+gives every rank a full copy and its own queries instead (weak scaling, no
+data-path collective).
 """
 import argparse
 import json
@@ -89,6 +93,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--ref-queries-per-step", type=int, default=2)
     p.add_argument("--no-autotune", action="store_true", help="keep the default launch parameters")
+    p.add_argument("--multi", choices=["shard", "replica"], default="shard",
+                   help="N > 1: row-range shards of one collection (all-gather + merge per batch) or full replicas")
     return p.parse_args()
 
 
@@ -290,7 +296,16 @@ def config_of(args):
             "k": list(ks_of(args)), "data": args.data,
             "l2": "inputs (%.1f GB f32 + %.1f GB bf16) larger than L2; no flush needed"
                   % (args.n * args.L * 4 / 1e9, args.n * args.L * 2 / 1e9),
-            "parallelism": "replica per GPU" if int(os.environ.get("WORLD_SIZE", "1")) > 1 else "single GPU"}
+            "parallelism": parallelism_of(args)}
+
+
+def parallelism_of(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world == 1:
+        return "single GPU"
+    if args.multi == "replica":
+        return "replica per GPU (each rank its own queries)"
+    return "%d row-range shards; every rank answers the whole batch, NCCL all-gather of the k nearest + merge" % world
 
 
 def fp64_oracle_check(args, torch, H, groups, device):
@@ -484,6 +499,8 @@ def main():
     rank, world, local = dist_setup(args)
     if args.impl == "reference":
         return run_reference(args, rank, world, local)
+    if world > 1 and args.multi == "shard":
+        return run_sharded(args, rank, world, local)
     import torch
     import hercules_b200 as H
     from hercules_b200 import build as B
@@ -717,6 +734,152 @@ def main():
         dist.destroy_process_group()
 
 
+def make_batches_seeded(args, torch, H, nbatches, device, offset):
+    """make_batches without the collection on the device: each noisy query's
+    base row is regenerated from the data seed (the same bits)."""
+    nb = args.batch
+    nf = fresh_count(args)
+    unit = args.data == "unit"
+    Q = torch.empty((nbatches, nb, args.L), dtype=torch.float32, device=device)
+    fresh = H.generate_unit_vectors_device if unit else H.generate_walks_device
+    for i in range(nbatches):
+        H.generate_queries_seeded_device(DATA_SEED, QUERY_SEED + offset + i, args.n, args.L,
+                                         sigma2_for(nb - nf, levels=levels_of(args)), Q[i].data_ptr(), unit=unit,
+                                         device=device)
+        if nf:
+            fresh(FRESH_SEED + offset, nf, args.L, Q[i, nb - nf:].data_ptr(), first=(offset + i) * nf, device=device)
+    torch.cuda.synchronize()
+    return Q, batch_ks(args)
+
+
+def run_sharded(args, rank, world, local):
+    """N > 1: rank r holds rows shard_range(n, N, r) of the collection as its
+    own index and answers every query of each batch on it; one NCCL
+    all-gather of the k (distance, id) pairs per query and a merge on the
+    device give the answers of the whole collection (hercules_b200.shard).
+    The timed region holds the batched search, the collective and the merge;
+    the total work is fixed as N grows (strong scaling)."""
+    import torch
+    import hercules_b200 as H
+    from hercules_b200 import build as B
+    from hercules_b200.shard import shard_range, sharded_batch_answers
+    B.build()
+    torch.cuda.set_device(local)
+    device = local
+    dev = torch.device("cuda", device)
+    steps, warm, nb = args.steps, args.warmup, args.batch
+    t_setup = time.perf_counter()
+    first, count = shard_range(args.n, world, rank)
+    X = torch.empty((count, args.L), dtype=torch.float32, device=device)
+    gen = H.generate_unit_vectors_device if args.data == "unit" else H.generate_walks_device
+    gen(DATA_SEED, count, args.L, X.data_ptr(), first=first, device=device)
+    torch.cuda.synchronize()
+    ix = H.HerculesIndex.build_device(X.data_ptr(), count, args.L, args.leaf, device=device)
+    del X
+    torch.cuda.empty_cache()
+    Qb, ks = make_batches_seeded(args, torch, H, steps + warm, device, offset=0)
+    kmax = int(ks.max())
+    D = torch.empty((nb, kmax), dtype=torch.float32, device=device)
+    I = torch.empty((nb, kmax), dtype=torch.int64, device=device)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def step(qptr):
+        st = ix.knn_batch_device(qptr, nb, ks, kmax, D.data_ptr(), I.data_ptr(), stream=stream)
+        md, mi = sharded_batch_answers(D, I, first, ks, kmax)
+        return st, md, mi
+
+    step(Qb[0].data_ptr())  # the first call also builds the BF16 copy of the shard
+    torch.cuda.synchronize()
+    tuning = ix.tuning() if args.no_autotune else ix.autotune_device(Qb[0].data_ptr(), nb, ks, kmax, stream=stream)
+    for i in range(1, warm):
+        step(Qb[i].data_ptr())
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(device)
+    clocks.start()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    agg = {}
+    for i in range(warm, warm + steps):
+        st, md, mi = step(Qb[i].data_ptr())
+        for kk, v in st.items():
+            agg[kk] = agg.get(kk, 0) + v
+    e1.record()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), world, device=dev)
+    value = nb * steps / (ms / 1000.0)
+    last_d, last_i = md, mi
+
+    # end to end: pinned host queries in, merged answers back to pinned host
+    # memory, every step
+    Qe, _ = make_batches_seeded(args, torch, H, steps + warm, device, offset=5000)
+    Qh = torch.empty(tuple(Qe.shape), dtype=torch.float32, pin_memory=True)
+    Qh.copy_(Qe.cpu())
+    del Qe
+    Qd = torch.empty((nb, args.L), dtype=torch.float32, device=device)
+    Dh = torch.empty((nb, kmax), dtype=torch.float32, pin_memory=True)
+    Ih = torch.empty((nb, kmax), dtype=torch.int64, pin_memory=True)
+
+    def e2e_step(i):
+        Qd.copy_(Qh[i], non_blocking=True)
+        _, md2, mi2 = step(Qd.data_ptr())
+        Dh.copy_(md2, non_blocking=True)
+        Ih.copy_(mi2, non_blocking=True)
+        torch.cuda.synchronize()
+
+    for i in range(warm):
+        e2e_step(i)
+    barrier(world)
+    t0 = time.perf_counter()
+    for i in range(warm, warm + steps):
+        e2e_step(i)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, device=dev)
+    e2e_value = nb * steps / e2e_s
+
+    fp64 = None
+    if rank == 0:
+        ns = 32
+        fp64 = fp64_oracle_check(args, torch, H, [("sharded_batched", Qb[warm + steps - 1, :ns], ks[:ns],
+                                                   last_d[:ns], last_i[:ns])], device)
+    barrier(world)
+    ix.close()
+    peaks = measured_peaks_all()
+    gemm_s = agg["gemm_ms"] / 1000.0
+    flops = 2.0 * args.L * agg["bf16_pairs"]
+    achieved_tf = flops / gemm_s / 1e12 if gemm_s > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warm,
+        "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "bf16 filter (fp32 accumulate) + f32 exact re-rank",
+        "data": "synthetic (seeded z-normalised random walks; noisy and fresh queries)",
+        "config": config_of(args),
+        "tuning": dict({k: tuning[k] for k in ("filter_tiles_per_item", "bound_tiles_per_item",
+                                                "rerank_blocks_per_sm", "approx_blocks_per_sm")},
+                       tuned=not args.no_autotune),
+        "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": nb * args.L * 4,
+                "d2h_bytes_per_step": nb * kmax * (4 + 8)},
+        "gpu_launches": int(agg["kernel_launches"]),
+        "roofline": {"bound": "tensor", "kernel": "k_umma_filter (rank 0's shard)", "achieved": round(achieved_tf, 1),
+                     "peak": peaks["bf16_sustained"], "unit": "TFLOP/s",
+                     "frac": round(achieved_tf / peaks["bf16_sustained"], 4),
+                     "peak_source": peaks["source"] + " sustained bf16", "traffic": None},
+        "shard": {"rows_rank0": count, "collective": "torch.distributed all_gather (NCCL) of [batch, kmax] "
+                                                     "distances and ids, merge_topk_torch on the device"},
+        "clocks": ck,
+        "fp64_oracle": fp64,
+        "stats": {"filter_ms_per_step_rank0": agg["gemm_ms"] / steps,
+                  "rerank_ms_per_step_rank0": agg["rerank_ms"] / steps,
+                  "bound_ms_per_step_rank0": agg["bound_ms"] / steps,
+                  "setup_s": round(time.perf_counter() - t_setup, 2)},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    import torch.distributed as dist
+    dist.destroy_process_group()
+
+
 def sample_positions(args, m):
     """m query positions of a batch spread over it: every k and every noise
     level appears (k cycling with the sample index, the level shifted by one
@@ -854,7 +1017,8 @@ def run_reference(args, rank, world, local):
                   "setup %.1f s" % (nps, ",".join(map(str, sorted(set(ks_used)))), threads, wall, setup_s))
         line = {"impl": "reference", "metric": METRIC, "value": round(value, 4) if value else None, "unit": UNIT,
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": 1000.0 * secs / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+                "ms_per_step": 1000.0 * secs / max(args.steps, 1), "higher_is_better": True,
+                "scaling": "strong" if world > 1 and args.multi == "shard" else "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded z-normalised random walks; "
                                                              "noisy and fresh queries)",
                 "config": config_of(args),

@@ -117,6 +117,9 @@ _SIGS = [
                                                 _P, ctypes.c_int, ctypes.c_int]),
     ("hg_generate_unit_queries", ctypes.c_int, [ctypes.c_uint64, _P, ctypes.c_uint64, ctypes.c_uint32,
                                                 ctypes.c_uint32, _P, _P, _P, ctypes.c_int, ctypes.c_int]),
+    ("hg_generate_queries_seeded", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
+                                                  ctypes.c_uint32, _P, ctypes.c_int, _P, _P, ctypes.c_int,
+                                                  ctypes.c_int]),
     ("hg_sax_breakpoints", ctypes.c_int, [_P]),
     ("hg_pscan_noalloc", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint32, _P, ctypes.c_uint32, _P, _P, _P]),
 ]
@@ -412,6 +415,24 @@ def generate_unit_queries_device(seed, data_ptr, n, L, sigma2, out_ptr, device=0
     s2 = np.ascontiguousarray(sigma2, dtype=np.float64)
     _check(lib().hg_generate_unit_queries(seed, ctypes.c_void_p(data_ptr), n, L, s2.shape[0], _ptr(s2),
                                           ctypes.c_void_p(out_ptr), None, 1, device))
+
+
+def generate_queries_seeded(data_seed, seed, n, L, sigma2, unit=False, return_base=False):
+    """Noisy queries over the seeded collection of data_seed (n rows), base
+    rows regenerated on the host: the bits of generate_queries /
+    generate_unit_queries given that collection."""
+    s2 = np.ascontiguousarray(sigma2, dtype=np.float64)
+    out = np.zeros((s2.shape[0], L), dtype=np.float32)
+    base = np.zeros(s2.shape[0], dtype=np.uint64)
+    _check(lib().hg_generate_queries_seeded(data_seed, seed, n, L, s2.shape[0], _ptr(s2), int(bool(unit)),
+                                            _ptr(out), _ptr(base), 0, 0))
+    return (out, base) if return_base else out
+
+
+def generate_queries_seeded_device(data_seed, seed, n, L, sigma2, out_ptr, unit=False, device=0):
+    s2 = np.ascontiguousarray(sigma2, dtype=np.float64)
+    _check(lib().hg_generate_queries_seeded(data_seed, seed, n, L, s2.shape[0], _ptr(s2), int(bool(unit)),
+                                            ctypes.c_void_p(out_ptr), None, 1, device))
 
 
 def sax_breakpoints():

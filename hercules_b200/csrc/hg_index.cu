@@ -2498,17 +2498,20 @@ static hg_status generate_rows(uint64_t seed, uint64_t first, uint64_t n, uint32
   return HG_OK;
 }
 
+// data == nullptr: each base row is regenerated from data_seed (the rows
+// of hg_generate_walks / hg_generate_unit_vectors with that seed).
 static hg_status generate_queries(uint64_t seed, const float* data, uint64_t n, uint32_t L, uint32_t nq,
                                   const double* sigma2, float* out, uint64_t* base_ids, int on_device, int device,
-                                  int unit) {
-  if (!data || !out || !sigma2 || n == 0 || L == 0 || L % 4 != 0)
+                                  int unit, uint64_t data_seed = 0) {
+  if (!out || !sigma2 || n == 0 || L == 0 || L % 4 != 0)
     return set_error(HG_ERR_ARG, "hg_generate_queries: bad argument");
   if (on_device) {
     CK(cudaSetDevice(device));
     double* d_s = nullptr;
     CK(dalloc(&d_s, nq));
     cudaError_t e = cudaMemcpy(d_s, sigma2, sizeof(double) * nq, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = hg::launch_generate_queries(seed, data, n, (int)L, (int)nq, d_s, out, base_ids, 0, unit);
+    if (e == cudaSuccess)
+      e = hg::launch_generate_queries(seed, data, n, (int)L, (int)nq, d_s, out, base_ids, 0, unit, data_seed);
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     cudaFree(d_s);
     return e == cudaSuccess ? HG_OK : cuda_fail(e, "hg_generate_queries");
@@ -2516,9 +2519,22 @@ static hg_status generate_queries(uint64_t seed, const float* data, uint64_t n, 
   parallel_for(nq, [=](uint64_t j) {
     const uint64_t b = hg::pick_row(seed, j, n);
     if (base_ids) base_ids[j] = b;
-    hg::noisy_query(seed, j, data + b * L, (int)L, sigma2[j], out + j * L, unit);
+    float* o = out + j * L;
+    const float* base = data ? data + b * L : o;
+    if (!data) {
+      if (unit) hg::gaussian_unit(data_seed, b, (int)L, o);
+      else hg::random_walk(data_seed, b, (int)L, o);
+    }
+    hg::noisy_query(seed, j, base, (int)L, sigma2[j], o, unit);
   });
   return HG_OK;
+}
+
+hg_status hg_generate_queries_seeded(uint64_t data_seed, uint64_t seed, uint64_t n, uint32_t L, uint32_t nq,
+                                     const double* sigma2, int unit, float* out, uint64_t* base_ids, int on_device,
+                                     int device) {
+  return generate_queries(seed, nullptr, n, L, nq, sigma2, out, base_ids, on_device, device, unit ? 1 : 0,
+                          data_seed);
 }
 
 hg_status hg_generate_walks(uint64_t seed, uint64_t first, uint64_t n, uint32_t L, float* out, int on_device,

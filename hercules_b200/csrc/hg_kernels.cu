@@ -1042,13 +1042,24 @@ __global__ void k_generate_walks(uint64_t seed, uint64_t first, uint64_t n, int 
   else random_walk(seed, first + i, L, out + i * (uint64_t)L);
 }
 
+// data == nullptr: the base row is regenerated from data_seed into the
+// query's own output row (the collection need not be resident), then the
+// noise is added in place.
 __global__ void k_generate_queries(uint64_t seed, const float* data, uint64_t n, int L, int nq,
-                                   const double* sigma2, float* out, uint64_t* base_ids, int unit) {
+                                   const double* sigma2, float* out, uint64_t* base_ids, int unit,
+                                   uint64_t data_seed) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nq) return;
   const uint64_t b = pick_row(seed, (uint64_t)j, n);
   if (base_ids) base_ids[j] = b;
-  noisy_query(seed, (uint64_t)j, data + b * (uint64_t)L, L, sigma2[j], out + (uint64_t)j * L, unit);
+  float* o = out + (uint64_t)j * L;
+  const float* base = data + b * (uint64_t)L;
+  if (!data) {
+    if (unit) gaussian_unit(data_seed, b, L, o);
+    else random_walk(data_seed, b, L, o);
+    base = o;
+  }
+  noisy_query(seed, (uint64_t)j, base, L, sigma2[j], o, unit);
 }
 
 // ---------------------------------------------------------------------------
@@ -1255,9 +1266,11 @@ cudaError_t launch_generate_walks(uint64_t seed, uint64_t first, uint64_t n, int
 }
 
 cudaError_t launch_generate_queries(uint64_t seed, const float* data, uint64_t n, int L, int nq,
-                                    const double* sigma2, float* out, uint64_t* base_ids, cudaStream_t s, int unit) {
+                                    const double* sigma2, float* out, uint64_t* base_ids, cudaStream_t s, int unit,
+                                    uint64_t data_seed) {
   if (!nq) return cudaSuccess;
-  k_generate_queries<<<blocks_for(nq, 64), 64, 0, s>>>(seed, data, n, L, nq, sigma2, out, base_ids, unit);
+  k_generate_queries<<<blocks_for(nq, 64), 64, 0, s>>>(seed, data, n, L, nq, sigma2, out, base_ids, unit,
+                                                       data_seed);
   return cudaGetLastError();
 }
 

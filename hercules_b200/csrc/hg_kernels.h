@@ -159,6 +159,6 @@ cudaError_t launch_generate_walks(uint64_t seed, uint64_t first, uint64_t n, int
                                   cudaStream_t s, int unit = 0);
 cudaError_t launch_generate_queries(uint64_t seed, const float* data, uint64_t n, int L, int nq,
                                     const double* sigma2, float* out, uint64_t* base_ids, cudaStream_t s,
-                                    int unit = 0);
+                                    int unit = 0, uint64_t data_seed = 0);  // data == nullptr: rows from data_seed
 
 }  // namespace hg

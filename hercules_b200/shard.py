@@ -80,3 +80,18 @@ def allgather_knn(dist, ids, k, group=None):
     dist_.all_gather(dl, dist.contiguous(), group=group)
     dist_.all_gather(il, ids.contiguous(), group=group)
     return merge_topk_torch(torch.cat(dl, 1), torch.cat(il, 1), k)
+
+
+def sharded_batch_answers(dist, ids, first, ks, kmax, group=None):
+    """One batch answered on a row-range shard -> the answers of the whole
+    collection, on every rank.  dist, ids: this shard's [nq, kmax] answers
+    with ids local to the shard (row i of the shard is global row first + i;
+    -1 marks an empty entry); ks: each query's k.  The ids are made global,
+    every rank's lists are all-gathered and merged, and each query's entries
+    past its own k are cleared (+inf / -1), as a single index returns them."""
+    import torch
+    gi = torch.where(ids >= 0, ids + int(first), torch.full_like(ids, -1))
+    md, mi = allgather_knn(dist, gi, kmax, group=group)
+    kq = torch.as_tensor(np.asarray(ks, np.int64), device=dist.device)
+    beyond = torch.arange(kmax, device=dist.device)[None, :] >= kq[:, None]
+    return md.masked_fill(beyond, float("inf")), mi.masked_fill(beyond, -1)

@@ -290,6 +290,17 @@ HG_API hg_status hg_generate_unit_queries(uint64_t seed, const float *data, uint
                                           const double *sigma2, float *out, uint64_t *base_ids, int on_device,
                                           int device);
 
+/* Noisy queries over a seeded collection that need not be resident: query j
+ * = row pick(j) of the stream data_seed (a random walk, or with unit = 1 a
+ * unit vector), regenerated, plus N(0, sigma2[j]) noise, then normalised as
+ * hg_generate_queries / hg_generate_unit_queries do -- the same bits as
+ * those entry points given the collection of data_seed.  For row-range
+ * shards, where no process holds every row.  out (nq x L) is host or device
+ * memory (on_device). */
+HG_API hg_status hg_generate_queries_seeded(uint64_t data_seed, uint64_t seed, uint64_t n, uint32_t L, uint32_t nq,
+                                            const double *sigma2, int unit, float *out, uint64_t *base_ids,
+                                            int on_device, int device);
+
 /* The 255 iSAX breakpoints of cardinality 256 used by this library. */
 HG_API hg_status hg_sax_breakpoints(float *out255);
 

@@ -55,6 +55,24 @@ def test_device_generator_matches_host(hg, gpu_available):
     assert np.array_equal(qd.cpu().numpy().view(np.uint32), qh.view(np.uint32))
 
 
+@pytest.mark.parametrize("unit", [False, True])
+def test_seeded_query_generator_matches_generator_over_the_collection(hg, gpu_available, unit):
+    """hg_generate_queries_seeded (base rows regenerated from the data seed,
+    for row-range shards) gives the bits of the generator given the whole
+    collection, on the device and on the host."""
+    import torch
+    n, L = 4000, 96
+    X = hg.generate_unit_vectors(1184, n, L) if unit else hg.generate_walks(1184, n, L)
+    s2 = np.array([0.01, 0.1, 1.0] * 11)
+    want = (hg.generate_unit_queries if unit else hg.generate_queries)(77, X, s2)
+    t = torch.empty((len(s2), L), dtype=torch.float32, device="cuda")
+    hg.generate_queries_seeded_device(1184, 77, n, L, s2, t.data_ptr(), unit=unit)
+    torch.cuda.synchronize()
+    assert np.array_equal(t.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    host = hg.generate_queries_seeded(1184, 77, n, L, s2, unit=unit)
+    assert np.array_equal(host.view(np.uint32), want.view(np.uint32))
+
+
 @pytest.mark.parametrize("name", REF_CONFIGS)
 def test_build_reproduces_reference_index_files(built, tmp_path, name):
     sys.path.insert(0, os.path.dirname(golden_path("")))

@@ -117,3 +117,56 @@ def test_two_gloo_ranks_allgather_and_merge(oracle_mod, hg):
         for j, q in enumerate(Q):
             wd, wi = oracle_mod.pscan(X, q, 10)
             assert np.array_equal(bits(md[j]), bits(wd)) and np.array_equal(mi[j], wi)
+
+
+def _rank_batch(rank, world, port, out):
+    """bench.py's sharded step on the host: shard answers with per-query k
+    (local ids, entries past k empty), then sharded_batch_answers."""
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    import hercules_b200 as H
+    from hercules_b200.shard import shard_range, sharded_batch_answers
+    from oracle import oracle as O
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    X = H.generate_walks(1184, 2500, 64)
+    Q = H.generate_queries(14784, X, np.array([0.01, 0.1, 1.0] * 3))
+    ks = np.array([1, 10, 25] * 3, np.uint32)
+    kmax = int(ks.max())
+    s, c = shard_range(X.shape[0], world, rank)
+    D = np.full((len(Q), kmax), np.inf, np.float32)
+    I = np.full((len(Q), kmax), -1, np.int64)
+    for j, q in enumerate(Q):
+        k = int(ks[j])
+        D[j, :k], I[j, :k] = O.pscan(X[s:s + c], q, k)  # shard-local ids
+    md, mi = sharded_batch_answers(torch.from_numpy(D), torch.from_numpy(I), s, ks, kmax)
+    out.put((rank, md.numpy(), mi.numpy()))
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_sharded_batch_equals_one_index(oracle_mod, hg, world):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_batch, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted((out.get(timeout=120) for _ in procs), key=lambda r: r[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    X = hg.generate_walks(1184, 2500, 64)
+    Q = hg.generate_queries(14784, X, np.array([0.01, 0.1, 1.0] * 3))
+    ks = [1, 10, 25] * 3
+    for _, md, mi in res:
+        for j, q in enumerate(Q):
+            k = ks[j]
+            wd, wi = oracle_mod.pscan(X, q, k)
+            assert np.array_equal(bits(md[j, :k]), bits(wd)) and np.array_equal(mi[j, :k], wi)
+            assert np.all(np.isinf(md[j, k:])) and np.all(mi[j, k:] == -1)
