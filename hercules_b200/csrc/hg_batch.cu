@@ -501,10 +501,13 @@ __global__ void __launch_bounds__(kGroupThreads) k_group_queries(const int* __re
                                                                  const LeafPlan* __restrict__ plan, int nleaves,
                                                                  uint32_t btpi, uint32_t* perm, uint32_t* slots,
                                                                  uint32_t* leaf_qoff, uint32_t* leaf_qcnt,
-                                                                 uint32_t* item_off, uint32_t* nitems) {
+                                                                 uint32_t* item_off, uint32_t* nitems,
+                                                                 uint32_t* gcnt) {
+  // per-leaf counters in shared memory, or in gcnt (2 x nleaves words of
+  // global memory) above kMaxLeavesSort leaves
   extern __shared__ uint32_t gsh[];
-  uint32_t* cnt = gsh;            // [nleaves]
-  uint32_t* cur = gsh + nleaves;  // [nleaves]
+  uint32_t* cnt = gcnt ? gcnt : gsh;   // [nleaves]
+  uint32_t* cur = cnt + nleaves;       // [nleaves]
   __shared__ uint32_t wsum[2][32];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   for (int i = tid; i < nleaves; i += kGroupThreads) cnt[i] = cur[i] = 0;
@@ -759,13 +762,16 @@ cudaError_t launch_scatter_pairs(const unsigned long long* pairs, const uint32_t
 
 cudaError_t launch_group_queries(const int* approx, int nq, const LeafPlan* plan, int nleaves, uint32_t btpi,
                                  uint32_t* perm, uint32_t* slots, uint32_t* leaf_qoff, uint32_t* leaf_qcnt,
-                                 uint32_t* item_off, uint32_t* nitems, BatchItem* items, cudaStream_t s) {
-  const size_t smem = sizeof(uint32_t) * 2 * (size_t)nleaves;
+                                 uint32_t* item_off, uint32_t* nitems, BatchItem* items, cudaStream_t s,
+                                 uint32_t* gcnt) {
+  const bool global_cnt = nleaves > kMaxLeavesSort;
+  if (global_cnt && !gcnt) return cudaErrorInvalidValue;
+  const size_t smem = global_cnt ? 0 : sizeof(uint32_t) * 2 * (size_t)nleaves;
   static SmemLimit attr;
   const cudaError_t ea = attr.ensure((const void*)k_group_queries, (int)(sizeof(uint32_t) * 2 * kMaxLeavesSort));
   if (ea != cudaSuccess) return ea;
   k_group_queries<<<1, kGroupThreads, smem, s>>>(approx, nq, plan, nleaves, btpi, perm, slots, leaf_qoff, leaf_qcnt,
-                                                 item_off, nitems);
+                                                 item_off, nitems, global_cnt ? gcnt : nullptr);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_group_items<<<nblk((uint64_t)nleaves * 32, 256), 256, 0, s>>>(plan, nleaves, btpi, leaf_qoff, leaf_qcnt,

@@ -109,7 +109,8 @@ cudaError_t launch_rows_to_bf16(const float* rows, const uint32_t* idx, uint64_t
                                 cudaStream_t s, const uint32_t* n_dev = nullptr);
 cudaError_t launch_group_queries(const int* approx, int nq, const LeafPlan* plan, int nleaves, uint32_t btpi,
                                  uint32_t* perm, uint32_t* slots, uint32_t* leaf_qoff, uint32_t* leaf_qcnt,
-                                 uint32_t* item_off, uint32_t* nitems, BatchItem* items, cudaStream_t s);
+                                 uint32_t* item_off, uint32_t* nitems, BatchItem* items, cudaStream_t s,
+                                 uint32_t* gcnt = nullptr);  // 2 x nleaves words above kMaxLeavesSort leaves
 // the pruned filter's query panel list and work items from the kept
 // (leaf, query) pairs (k_group_pruned, k_emit_pruned)
 cudaError_t launch_group_pruned(const uint32_t* leaf_cnt, const uint32_t* leaf_q, uint32_t stride,

@@ -301,6 +301,7 @@ static void free_device(hg_index* ix) {
   dfree(s.topk_row);
   dfree(s.paa);
   dfree(s.sax_tab);
+  dfree(s.sort_keys);
   dfree(s.stats);
   dfree(s.err);
   dfree(s.list);
@@ -339,6 +340,7 @@ static void free_device(hg_index* ix) {
   dfree(b.out_dist);
   dfree(b.out_id);
   dfree(b.leaf_plan);
+  dfree(b.group_cnt);
   dfree(b.leaf_qoff);
   dfree(b.leaf_qcnt);
   dfree(b.item_off);
@@ -1060,6 +1062,7 @@ static hg_status ensure_scratch(hg_index* ix, int k) {
   dfree(s.topk_count);
   dfree(s.paa);
   dfree(s.sax_tab);
+  dfree(s.sort_keys);
   dfree(s.stats);
   dfree(s.err);
   dfree(s.list);
@@ -1081,6 +1084,7 @@ static hg_status ensure_scratch(hg_index* ix, int k) {
   CK(dalloc(&s.topk_count, 1));
   CK(dalloc(&s.paa, 16));
   CK(dalloc(&s.sax_tab, HG_PAA_SEGMENTS * HG_SAX_CARD));
+  if (nl > hg::kMaxLeavesSort) CK(dalloc(&s.sort_keys, 4 * (size_t)nl));
   CK(dalloc(&s.stats, 8));
   CK(dalloc(&s.err, 1));
   CK(dalloc(&s.q, 1));
@@ -1136,7 +1140,7 @@ static double drain(ProfEvents& p) {
 //   candidate leaves sorted by LB -> LB_SAX filter -> exact distances of the
 //   survivors -> merge.
 static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opts& o, float* d_dist,
-                         int64_t* d_id, cudaStream_t st, Prof* prof) {
+                         int64_t* d_id, cudaStream_t st, Prof* prof, bool has_floor = false, float floor = 0.0f) {
   hg::QueryScratch& s = ix->s;
   hg::DeviceIndex& d = ix->d;
   const int nl = (int)ix->leaves.size();
@@ -1154,6 +1158,8 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
   e.parts = s.parts;
   e.part_count = s.part_count;
   e.stats = s.stats;
+  e.has_floor = has_floor ? 1 : 0;
+  e.floor = floor;
   if (o.mode == HG_MODE_PSCAN) {
     CK(hg::launch_pscan_prep(ix->n, s.cand_count, s.unit_prefix, s.bound, s.topk_count, s.counters, st));
     e.list = nullptr;
@@ -1185,7 +1191,7 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
     CK(hg::launch_merge(s.parts, s.part_count, a_blocks, k, s.topk, s.topk_count, s.bound, s.err,
                         st));
     CK(hg::launch_select_sort(s.lb, nl, s.bound, s.approx_leaf, d.leaf_start, d.leaf_size, s.cand, s.cand_lb,
-                              s.cand_count, s.unit_prefix, st));
+                              s.cand_count, s.unit_prefix, st, s.sort_keys));
     hg::FilterArgs f{};
     f.sax = d.sax;
     f.bp = d.bp;
@@ -1409,20 +1415,66 @@ static hg_status knn_approx_one(hg_index* ix, const float* d_q, int k, const hg_
   return HG_OK;
 }
 
+// k above kMaxK: rounds of at most kMaxK answers.  Round r returns the next
+// smallest distinct distances strictly above the last distance of round
+// r - 1 (the distance stream admits only rows above that floor; pruning by
+// LB_EAPCA / LB_SAX against the round's own k-th bound is unchanged), so
+// the rounds together are the k smallest distinct distances, each with its
+// lowest id -- the answer of one search with that k.  A round that comes
+// back short means the collection has no more distances: the remaining
+// entries are +inf / -1.  The host reads each round's last distance back.
+static hg_status knn_rounds(hg_index* ix, const float* d_q, uint32_t k, const hg_knn_opts& o, float* d_dist,
+                            int64_t* d_id, cudaStream_t st, Prof* prof, uint64_t* launches) {
+  hg::QueryScratch& s = ix->s;
+  uint32_t done = 0;
+  bool has_floor = false;
+  float floor = 0.0f;
+  while (done < k) {
+    const int kr = (int)std::min<uint32_t>((uint32_t)hg::kMaxK, k - done);
+    HCK(knn_one(ix, d_q, kr, o, d_dist ? d_dist + done : nullptr, d_id ? d_id + done : nullptr, st, prof, has_floor,
+                floor));
+    *launches += o.mode == HG_MODE_PSCAN ? 4 : 9;
+    int cnt = 0;
+    unsigned long long last = 0;
+    CK(cudaMemcpyAsync(&cnt, s.topk_count, sizeof cnt, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last, s.topk + (kr - 1), sizeof last, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    done += (uint32_t)kr;
+    if (cnt < kr) {
+      if (done < k) {
+        // nothing above this round's distances: the rest is empty
+        CK(cudaMemsetAsync(s.topk_count, 0, sizeof(int), st));
+        CK(hg::launch_emit(s.topk, s.topk_count, (int)(k - done), d_dist ? d_dist + done : nullptr,
+                           d_id ? d_id + done : nullptr, st));
+        ++*launches;
+      }
+      break;
+    }
+    has_floor = true;
+    const uint32_t bits = (uint32_t)(last >> 32);
+    memcpy(&floor, &bits, sizeof floor);
+  }
+  return HG_OK;
+}
+
 static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t nq, uint32_t k,
                                  const hg_knn_opts* opts, float* d_dist, int64_t* d_id, cudaStream_t st,
                                  hg_query_stats* stats) {
   if (!ix || (!d_queries && nq)) return set_error(HG_ERR_ARG, "hg_knn: null argument");
   if (k == 0) return set_error(HG_ERR_ARG, "hg_knn: k must be positive");
-  if ((int)k > hg::kMaxK) return set_error(HG_ERR_LIMIT, "hg_knn: k above 224");
   if (ix->L > 16384) return set_error(HG_ERR_LIMIT, "hg_knn: series longer than 16384");
-  if (ix->leaves.size() > (size_t)hg::kMaxLeavesSort)
-    return set_error(HG_ERR_LIMIT, "hg_knn: more than 8192 leaves");
   hg_knn_opts o{};
   if (opts) o = *opts;
   if (o.mode == HG_MODE_BATCH) return knn_batch_impl(ix, d_queries, nq, nullptr, k, o, d_dist, d_id, st, stats);
+  const bool approx = o.mode == HG_MODE_PLAIN && (o.epsilon > 0.0f || o.nprobes > 0);
+  if (o.epsilon < 0.0f || o.nprobes < 0 || !(o.epsilon == o.epsilon))
+    return set_error(HG_ERR_ARG, "hg_knn: epsilon and nprobes must not be negative");
+  // k above kMaxK is answered in rounds (exact); the approximate searches
+  // depend on the k-th distance at every step, so they keep the limit
+  if (approx && (int)k > hg::kMaxK)
+    return set_error(HG_ERR_LIMIT, "hg_knn: k above 224 with epsilon or nprobes");
   CK(cudaSetDevice(ix->device));
-  HCK(ensure_scratch(ix, (int)k));
+  HCK(ensure_scratch(ix, std::min((int)k, hg::kMaxK)));
   if (!st) st = ix->stream;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
@@ -1430,15 +1482,21 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
   CK(cudaMemsetAsync(ix->s.stats, 0, sizeof(unsigned long long) * 8, st));
   Prof prof;
   CK(cudaEventRecord(e0, st));
-  const bool approx = o.mode == HG_MODE_PLAIN && (o.epsilon > 0.0f || o.nprobes > 0);
-  if (o.epsilon < 0.0f || o.nprobes < 0 || !(o.epsilon == o.epsilon))
-    return set_error(HG_ERR_ARG, "hg_knn: epsilon and nprobes must not be negative");
+  uint64_t launches = 0;
   for (uint32_t i = 0; i < nq; ++i) {
     const float* qi = d_queries + (uint64_t)i * ix->L;
     float* di = d_dist ? d_dist + (uint64_t)i * k : nullptr;
     int64_t* ii = d_id ? d_id + (uint64_t)i * k : nullptr;
-    if (approx) HCK(knn_approx_one(ix, qi, (int)k, o, di, ii, st));
-    else HCK(knn_one(ix, qi, (int)k, o, di, ii, st, o.profile ? &prof : nullptr));
+    if (approx) {
+      HCK(knn_approx_one(ix, qi, (int)k, o, di, ii, st));
+    } else if ((int)k <= hg::kMaxK) {
+      HCK(knn_one(ix, qi, (int)k, o, di, ii, st, o.profile ? &prof : nullptr));
+      launches += o.mode == HG_MODE_PSCAN ? 4 : 9;
+    } else {
+      uint64_t l = 0;
+      HCK(knn_rounds(ix, qi, k, o, di, ii, st, o.profile ? &prof : nullptr, &l));
+      launches += l;
+    }
   }
   CK(cudaEventRecord(e1, st));
   unsigned long long hs[8];
@@ -1465,7 +1523,7 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
     stats->scan_ms = scan_ms;
     stats->filter_launches = filter_launches;
     stats->filter_ms = filter_ms;
-    stats->kernel_launches = (uint64_t)nq * (o.mode == HG_MODE_PSCAN ? 4 : 9);
+    stats->kernel_launches = launches;
   }
   return HG_OK;
 }
@@ -1730,6 +1788,7 @@ static hg_status ensure_leaf_plan(hg_index* ix, uint64_t want, cudaStream_t st) 
   }
   if (!b.leaf_plan) {
     CK(dalloc(&b.leaf_plan, nl));
+    if (nl > hg::kMaxLeavesSort) CK(dalloc(&b.group_cnt, 2 * (size_t)nl));
     CK(dalloc(&b.leaf_qoff, nl + 1));
     CK(dalloc(&b.leaf_qcnt, nl + 1));
     CK(dalloc(&b.item_off, nl + 1));
@@ -1765,7 +1824,7 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
   // 1. approximate leaves, grouping
   CK(hg::launch_route_queries(b.qin, (int)nq, (int)L, index_tree(ix), b.approx, st));
   CK(hg::launch_group_queries(b.approx, (int)nq, b.leaf_plan, nl, ix->tune.bound_tiles_per_item, b.qperm, b.slots,
-                              b.leaf_qoff, b.leaf_qcnt, b.item_off, b.ctrl + 0, b.items, st));
+                              b.leaf_qoff, b.leaf_qcnt, b.item_off, b.ctrl + 0, b.items, st, b.group_cnt));
   CK(hg::launch_rows_to_bf16(b.qin, b.qperm, nq, (int)L, b.qbf, b.qmeta, st));
   // 2. bound pass
   hg::BatchGemm g{};
@@ -1896,6 +1955,76 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
   return HG_OK;
 }
 
+// A batch whose kmax is above kMaxK (the batched filter ranks at most
+// kMaxK rows per query for its bound): every query through the plain path,
+// in rounds above kMaxK, into the nq x kmax layout of the batched entry
+// points (entries past a query's own k are +inf / -1).
+static hg_status knn_batch_plain(hg_index* ix, const float* Q, uint32_t nq, const std::vector<uint32_t>& kq,
+                                 uint32_t kmax, const hg_knn_opts& o, float* dist, int64_t* id, cudaStream_t st,
+                                 hg_query_stats* stats, bool host_io) {
+  CK(cudaSetDevice(ix->device));
+  if (!st) st = ix->stream;
+  const uint32_t L = ix->L;
+  float* dq = const_cast<float*>(Q);
+  float* dd = dist;
+  int64_t* di = id;
+  if (host_io) {
+    CK(dalloc(&dq, (size_t)nq * L));
+    cudaError_t e = dalloc(&dd, (size_t)nq * kmax);
+    if (e == cudaSuccess) e = dalloc(&di, (size_t)nq * kmax);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dq, Q, sizeof(float) * nq * L, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+      dfree(dq);
+      dfree(dd);
+      dfree(di);
+      return cuda_fail(e, "hg_knn_batch");
+    }
+  }
+  hg_knn_opts po{};
+  po.mode = HG_MODE_PLAIN;
+  po.use_lb_sax = o.use_lb_sax;
+  hg_status status = HG_OK;
+  hg_query_stats acc{};
+  for (uint32_t i = 0; i < nq && status == HG_OK; ++i) {
+    hg_query_stats one{};
+    status = knn_device_impl(ix, dq + (uint64_t)i * L, 1, kq[i], &po, dd + (uint64_t)i * kmax,
+                             di + (uint64_t)i * kmax, st, &one);
+    if (status == HG_OK && kq[i] < kmax) {
+      cudaError_t e = cudaMemsetAsync(ix->s.topk_count, 0, sizeof(int), st);
+      if (e == cudaSuccess)
+        e = hg::launch_emit(ix->s.topk, ix->s.topk_count, (int)(kmax - kq[i]), dd + (uint64_t)i * kmax + kq[i],
+                            di + (uint64_t)i * kmax + kq[i], st);
+      if (e != cudaSuccess) status = cuda_fail(e, "hg_knn_batch");
+    }
+    acc.leaves_scanned += one.leaves_scanned;
+    acc.rows_visited += one.rows_visited;
+    acc.rows_lbsax_pruned += one.rows_lbsax_pruned;
+    acc.chunks_loaded += one.chunks_loaded;
+    acc.rows_completed += one.rows_completed;
+    acc.rows_considered += one.rows_considered;
+    acc.device_ms += one.device_ms;
+    acc.fallback_ms += one.device_ms;
+    acc.kernel_launches += one.kernel_launches + (kq[i] < kmax ? 1 : 0);
+  }
+  if (host_io) {
+    if (status == HG_OK) {
+      cudaError_t e = cudaMemcpyAsync(dist, dd, sizeof(float) * nq * kmax, cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(id, di, sizeof(int64_t) * nq * kmax, cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) status = cuda_fail(e, "hg_knn_batch");
+    }
+    dfree(dq);
+    dfree(dd);
+    dfree(di);
+  }
+  if (status == HG_OK && stats) {
+    *stats = acc;
+    stats->queries = nq;
+    stats->fallback_queries = nq;
+  }
+  return status;
+}
+
 // Batched exact k-NN; ks is a host array (or null).  Queries and answers are
 // device buffers, or host buffers with host_io (copied straight into and out
 // of the handle's fixed buffers: no allocation per call).
@@ -1904,11 +2033,19 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
                                 hg_query_stats* stats, bool host_io) {
   if (!ix || (!d_Q && nq)) return set_error(HG_ERR_ARG, "hg_knn_batch: null argument");
   if (kmax == 0) return set_error(HG_ERR_ARG, "hg_knn_batch: k must be positive");
-  if ((int)kmax > hg::kMaxK) return set_error(HG_ERR_LIMIT, "hg_knn_batch: k above 224");
   if (ix->L > 16384) return set_error(HG_ERR_LIMIT, "hg_knn_batch: series longer than 16384");
-  if (ix->leaves.size() > (size_t)hg::kMaxLeavesSort)
-    return set_error(HG_ERR_LIMIT, "hg_knn_batch: more than 8192 leaves");
   if (nq > (1u << 24)) return set_error(HG_ERR_LIMIT, "hg_knn_batch: more than 2^24 queries");
+  if ((int)kmax > hg::kMaxK) {
+    std::vector<uint32_t> kq(nq, kmax);
+    if (ks)
+      for (uint32_t i = 0; i < nq; ++i) {
+        if (ks[i] == 0 || ks[i] > kmax) return set_error(HG_ERR_ARG, "hg_knn_batch: ks[i] outside 1..kmax");
+        kq[i] = ks[i];
+      }
+    if (stats) memset(stats, 0, sizeof *stats);
+    if (nq == 0) return HG_OK;
+    return knn_batch_plain(ix, d_Q, nq, kq, kmax, o, d_dist, d_id, st, stats, host_io);
+  }
   if (!host_io && ((uintptr_t)d_Q & 15) != 0)
     return set_error(HG_ERR_ARG, "hg_knn_batch: queries must be 16-byte aligned");
   std::vector<uint32_t> kq(nq, kmax);

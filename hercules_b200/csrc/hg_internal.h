@@ -71,6 +71,7 @@ struct QueryScratch {
   uint64_t* topk_row = nullptr;   // kmax leaf-ordered rows of the answers
   float* paa = nullptr;           // 16
   float* sax_tab = nullptr;       // 16 x 256 LB_SAX terms of the current query
+  uint32_t* sort_keys = nullptr;  // 4 x leaves: candidate sort above kMaxLeavesSort leaves
   unsigned long long* stats = nullptr;  // see ScanArgs
   uint32_t* list = nullptr;       // LB_SAX survivors (rows), n entries
   int* err = nullptr;             // device error flag
@@ -123,6 +124,7 @@ struct BatchScratch {
   uint32_t out_kmax = 0;
   // bound-pass plan per leaf, for the `want` slots it was made for
   LeafPlan* leaf_plan = nullptr;
+  uint32_t* group_cnt = nullptr;  // 2 x leaves: query grouping above kMaxLeavesSort leaves
   uint32_t* leaf_qoff = nullptr;
   uint32_t* leaf_qcnt = nullptr;
   uint32_t* item_off = nullptr;

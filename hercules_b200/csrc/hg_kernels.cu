@@ -363,13 +363,17 @@ __global__ void __launch_bounds__(kSortThreads) k_select_sort(const float* __res
                                                               const uint64_t* __restrict__ leaf_start,
                                                               const uint32_t* __restrict__ leaf_size, int* cand,
                                                               float* cand_lb, int* cand_count,
-                                                              uint32_t* unit_prefix) {
+                                                              uint32_t* unit_prefix, uint32_t* gkeys) {
+  // keys and values (two buffers each) live in shared memory up to
+  // kMaxLeavesSort leaves, else in gkeys (4 x nleaves words of global memory)
   extern __shared__ uint32_t sm[];
-  uint32_t* keys0 = sm;
-  uint32_t* vals0 = keys0 + kMaxLeavesSort;
-  uint32_t* keys1 = vals0 + kMaxLeavesSort;
-  uint32_t* vals1 = keys1 + kMaxLeavesSort;
-  uint16_t* cnt = reinterpret_cast<uint16_t*>(vals1 + kMaxLeavesSort);  // 16 x kSortThreads
+  uint32_t* cnt = sm;  // 16 x kSortThreads digit counts
+  uint32_t* kbase = gkeys ? gkeys : sm + 16 * kSortThreads;
+  const int cap = gkeys ? nleaves : kMaxLeavesSort;
+  uint32_t* keys0 = kbase;
+  uint32_t* vals0 = keys0 + cap;
+  uint32_t* keys1 = vals0 + cap;
+  uint32_t* vals1 = keys1 + cap;
   __shared__ uint32_t tmp[kSortThreads / 32 + 1];
   __shared__ uint32_t total;
   const int t = threadIdx.x;
@@ -403,7 +407,7 @@ __global__ void __launch_bounds__(kSortThreads) k_select_sort(const float* __res
   const int r0 = min(n, t * per2), r1 = min(n, r0 + per2);
   uint32_t *ki = keys0, *vi = vals0, *ko = keys1, *vo = vals1;
   if (n <= kSortThreads) {
-    unsigned long long* kv = reinterpret_cast<unsigned long long*>(keys1);  // 8-byte aligned, 2 x kMaxLeavesSort words
+    unsigned long long* kv = reinterpret_cast<unsigned long long*>(keys1);  // 8-byte aligned, 2 x cap words (n <= 1024)
     int np = 2;
     while (np < n) np <<= 1;
     for (int i = t; i < np; i += kSortThreads)
@@ -438,7 +442,7 @@ __global__ void __launch_bounds__(kSortThreads) k_select_sort(const float* __res
     // flattened digit-major counts: index d * kSortThreads + t; scan them in
     // that order (thread t owns the 16 entries t*16 .. t*16+15 of the flat array)
 #pragma unroll
-    for (int d = 0; d < 16; ++d) cnt[d * kSortThreads + t] = (uint16_t)c[d];
+    for (int d = 0; d < 16; ++d) cnt[d * kSortThreads + t] = c[d];
     __syncthreads();
     uint32_t s = 0;
     uint32_t loc[16];
@@ -449,7 +453,7 @@ __global__ void __launch_bounds__(kSortThreads) k_select_sort(const float* __res
     }
     const uint32_t base = block_exclusive_scan<kSortThreads>(s, tmp, nullptr);
 #pragma unroll
-    for (int j = 0; j < 16; ++j) cnt[t * 16 + j] = (uint16_t)(base + loc[j]);
+    for (int j = 0; j < 16; ++j) cnt[t * 16 + j] = base + loc[j];
     __syncthreads();
     uint32_t off[16];
 #pragma unroll
@@ -739,6 +743,7 @@ __global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 3 : 4) k_ed_stream(Ed
   int cnt = 0;
   float T = __int_as_float(0x7f800000);
   float B = __int_as_float((int)ld_volatile(a.bound));
+  const float F = a.has_floor ? a.floor : -1.0f;  // distances are >= 0
   bool valid = false;  // slot-uniform
   uint32_t row = 0;
   int ch = 0;  // a multiple of kStep: the query offsets below stay inside one 32-chunk group
@@ -846,7 +851,7 @@ __global__ void __launch_bounds__(kEdThreads, kLines > 2 ? 3 : 4) k_ed_stream(Ed
         }
       }
     }
-    const bool take = finished && j == 0 && dist <= B && dist <= T;
+    const bool take = finished && j == 0 && dist <= B && dist <= T && dist > F;
     warp_list_add(list, cnt, T, a.k, a.bound, take, dist,
                   take ? (kRowIds ? row : (uint32_t)a.ids[row]) : 0u);
     B = fminf(fminf(B, T), __int_as_float((int)bnext));
@@ -1177,16 +1182,22 @@ cudaError_t launch_stale_copy(const int* flag, const uint32_t* bound, uint32_t* 
   return cudaGetLastError();
 }
 
-static size_t select_smem() { return sizeof(uint32_t) * 4 * kMaxLeavesSort + sizeof(uint16_t) * 16 * kSortThreads; }
+static size_t select_smem(bool global_keys) {
+  return sizeof(uint32_t) * 16 * kSortThreads + (global_keys ? 0 : sizeof(uint32_t) * 4 * kMaxLeavesSort);
+}
 
 cudaError_t launch_select_sort(const float* lb, int nleaves, const uint32_t* bound, const int* approx_leaf,
                                const uint64_t* leaf_start, const uint32_t* leaf_size, int* cand,
-                               float* cand_lb, int* cand_count, uint32_t* unit_prefix, cudaStream_t s) {
+                               float* cand_lb, int* cand_count, uint32_t* unit_prefix, cudaStream_t s,
+                               uint32_t* gkeys) {
+  const bool global_keys = nleaves > kMaxLeavesSort;
+  if (global_keys && !gkeys) return cudaErrorInvalidValue;
   static SmemLimit attr;
-  const cudaError_t ea = attr.ensure((const void*)k_select_sort, (int)select_smem());
+  const cudaError_t ea = attr.ensure((const void*)k_select_sort, (int)select_smem(false));
   if (ea != cudaSuccess) return ea;
-  k_select_sort<<<1, kSortThreads, select_smem(), s>>>(lb, nleaves, bound, approx_leaf, leaf_start, leaf_size,
-                                                       cand, cand_lb, cand_count, unit_prefix);
+  k_select_sort<<<1, kSortThreads, select_smem(global_keys), s>>>(lb, nleaves, bound, approx_leaf, leaf_start,
+                                                                  leaf_size, cand, cand_lb, cand_count, unit_prefix,
+                                                                  global_keys ? gkeys : nullptr);
   return cudaGetLastError();
 }
 

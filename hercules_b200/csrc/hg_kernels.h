@@ -36,7 +36,7 @@ constexpr int kEdWarps = 8;  // warps per block of the distance stream
 constexpr int kEdBlocksPerSm = 4;  // resident blocks per SM of the distance stream
 constexpr int kWarpListCap = 256;  // per-warp candidate buffer (k <= kWarpListCap - 32)
 constexpr int kMaxK = kWarpListCap - 32;
-constexpr int kMaxLeavesSort = 8192;  // single-CTA radix sort capacity
+constexpr int kMaxLeavesSort = 8192;  // leaves whose sort / grouping arrays fit in shared memory
 constexpr int kMergeCap = 8192;       // single-CTA bitonic merge capacity
 
 // A routing node of the EAPCA tree: an internal node's split policy
@@ -95,6 +95,8 @@ struct EdArgs {
   int* part_count;
   unsigned long long* stats;   // [1] chunks computed [4] rows completed [5] rows started
   const int* gate;             // if set and *gate == 0, the launch scans nothing
+  int has_floor;               // 1: only rows at distance > floor enter the lists (the
+  float floor;                 //   answers of k above kMaxK come in rounds above it)
 };
 
 int sm_count(int device);
@@ -122,9 +124,11 @@ cudaError_t launch_route_queries(const float* Q, int nq, int L, Tree t, int* lea
 cudaError_t launch_leaf_lb(const float* q, int L, int nleaves, const int* seg_off, const short* points,
                            const float* sk, float* lb_out, cudaStream_t s, const float* paa = nullptr,
                            const float* bp = nullptr, float* sax_tab = nullptr);
+// gkeys: 4 x nleaves words of global scratch, needed above kMaxLeavesSort leaves
 cudaError_t launch_select_sort(const float* lb, int nleaves, const uint32_t* bound, const int* approx_leaf,
                                const uint64_t* leaf_start, const uint32_t* leaf_size, int* cand,
-                               float* cand_lb, int* cand_count, uint32_t* unit_prefix, cudaStream_t s);
+                               float* cand_lb, int* cand_count, uint32_t* unit_prefix, cudaStream_t s,
+                               uint32_t* gkeys = nullptr);
 cudaError_t launch_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
                               int* topk_count, uint32_t* counters, cudaStream_t s);
 cudaError_t launch_lbsax_filter(const FilterArgs& a, int blocks, cudaStream_t s);  // blocks: one per SM
