@@ -104,6 +104,7 @@ _SIGS = [
     ("hg_knn_batch_device", ctypes.c_int, [_P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, ctypes.POINTER(KnnOpts),
                                            _P, _P, _P, ctypes.POINTER(QueryStats)]),
     ("hg_bf16_dots", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint32, _P, ctypes.c_uint32, _P, _P]),
+    ("hg_filter_wait_check", ctypes.c_int, [ctypes.c_uint32, ctypes.c_int, _P]),
     ("hg_tuning_get", ctypes.c_int, [_P, ctypes.POINTER(Tuning)]),
     ("hg_tuning_set", ctypes.c_int, [_P, ctypes.POINTER(Tuning)]),
     ("hg_autotune", ctypes.c_int, [_P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, _P, ctypes.POINTER(Tuning)]),
@@ -361,6 +362,12 @@ def bf16_dots_device(rows_ptr, n, L, q_ptr, nq, out_ptr, stream=0):
 
 
 # -- data --------------------------------------------------------------------
+
+def filter_wait_check(wait_us, withhold, stream=0):
+    """hg_filter_wait_check: the status code (HG_OK, or HG_ERR_TIMEOUT when a
+    withheld copy makes the filter kernel's shortened wait run out)."""
+    return lib().hg_filter_wait_check(wait_us, int(bool(withhold)), ctypes.c_void_p(stream))
+
 
 def generate_walks(seed, n, L, first=0):
     """Host-side z-normalised random walks (same bits as the GPU generator)."""

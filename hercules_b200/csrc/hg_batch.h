@@ -69,6 +69,8 @@ struct BatchGemm {
   // mode 2 (diagnostics): raw dot products q~.x~, [query position][dots_ld]
   float* dots;
   uint64_t dots_ld;
+  uint64_t wait_ns;         // each bounded wait gives up after this (0: 2 s)
+  int withhold_first_copy;  // diagnostics: the first operand copy is never issued
 };
 
 struct BatchRank {

@@ -2418,8 +2418,8 @@ hg_status hg_knn_batch(hg_index* ix, const float* queries, uint32_t nq, const ui
   return knn_batch_impl(ix, queries, nq, ks, kmax, o, dist_out, id_out, nullptr, stats, true);
 }
 
-hg_status hg_bf16_dots(const float* d_rows, uint64_t n, uint32_t L, const float* d_queries, uint32_t nq,
-                       float* d_dots, void* stream) {
+static hg_status bf16_dots_impl(const float* d_rows, uint64_t n, uint32_t L, const float* d_queries, uint32_t nq,
+                                float* d_dots, void* stream, uint64_t wait_ns, int withhold) {
   if (!d_rows || !d_queries || !d_dots) return set_error(HG_ERR_ARG, "hg_bf16_dots: null argument");
   if (n == 0 || nq == 0) return HG_OK;
   if (L == 0 || L % 16 != 0 || L > 16384) return set_error(HG_ERR_ARG, "hg_bf16_dots: L must be a multiple of 16");
@@ -2482,6 +2482,8 @@ hg_status hg_bf16_dots(const float* d_rows, uint64_t n, uint32_t L, const float*
   g.err = err;
   g.dots = d_dots;
   g.dots_ld = n;
+  g.wait_ns = wait_ns;
+  g.withhold_first_copy = withhold;
   e = hg::launch_umma_filter(xmap, qmap, g, hg::sm_count(dev), st);
   int herr = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof herr, cudaMemcpyDeviceToHost, st);
@@ -2490,6 +2492,32 @@ hg_status hg_bf16_dots(const float* d_rows, uint64_t n, uint32_t L, const float*
   if (e != cudaSuccess) return cuda_fail(e, "hg_bf16_dots");
   if (herr) return set_error(HG_ERR_TIMEOUT, "hg_bf16_dots: a tensor-core wait timed out");
   return HG_OK;
+}
+
+hg_status hg_bf16_dots(const float* d_rows, uint64_t n, uint32_t L, const float* d_queries, uint32_t nq,
+                       float* d_dots, void* stream) {
+  return bf16_dots_impl(d_rows, n, L, d_queries, nq, d_dots, stream, 0, 0);
+}
+
+hg_status hg_filter_wait_check(uint32_t wait_us, int withhold, void* stream) {
+  if (wait_us == 0 || wait_us > 2000000u) return set_error(HG_ERR_ARG, "hg_filter_wait_check: wait_us outside 1..2e6");
+  cudaStream_t st = (cudaStream_t)stream;
+  constexpr uint64_t n = 512;
+  constexpr uint32_t L = 64, nq = 64;
+  float* rows = nullptr;
+  float* qs = nullptr;
+  float* dots = nullptr;
+  cudaError_t e = dalloc(&rows, n * L);
+  if (e == cudaSuccess) e = dalloc(&qs, (size_t)nq * L);
+  if (e == cudaSuccess) e = dalloc(&dots, n * nq);
+  if (e == cudaSuccess) e = hg::launch_generate_walks(1, 0, n, (int)L, rows, st, 0);
+  if (e == cudaSuccess) e = hg::launch_generate_walks(2, 0, nq, (int)L, qs, st, 0);
+  hg_status hs = e == cudaSuccess ? HG_OK : cuda_fail(e, "hg_filter_wait_check");
+  if (hs == HG_OK) hs = bf16_dots_impl(rows, n, L, qs, nq, dots, stream, (uint64_t)wait_us * 1000ull, withhold ? 1 : 0);
+  dfree(rows);
+  dfree(qs);
+  dfree(dots);
+  return hs;
 }
 
 hg_status hg_tuning_get(const hg_index* ix, hg_tuning* out) {

@@ -19,8 +19,8 @@
 // (approximate leaves x the queries routed there) for the bound pass; mode 3
 // walks an item list (leaves x the queries that LB_EAPCA keeps for them) with
 // mode 1's screening epilogue; mode 2 writes the raw dot products
-// (diagnostics).  Every mbarrier wait gives up after kWaitNs of
-// global time: the CTA then raises *err, drains its copies and MMAs, frees
+// (diagnostics).  Every mbarrier wait gives up after kWaitNs (or the
+// launch's wait_ns) of global time: the CTA then raises *err, drains its copies and MMAs, frees
 // TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -93,15 +93,16 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 }
 
 // Bounded wait for the phase of `parity`; false when this CTA aborted or
-// the wait ran past kWaitNs (then the CTA aborts and *err is raised).
-__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err) {
+// the wait ran past wait_ns (then the CTA aborts and *err is raised).
+__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                       uint64_t wait_ns) {
   if (mbar_try(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   for (uint32_t i = 1;; ++i) {
     if (mbar_try(bar, parity)) return true;
     if ((i & 63) == 0) {
       if (*abort_flag) return false;
-      if (global_ns() - t0 > kWaitNs) {
+      if (global_ns() - t0 > wait_ns) {
         *abort_flag = 1;
         atomicExch(err, kErrTimeout);
         return false;
@@ -112,9 +113,9 @@ __device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile i
 
 // Wait for a phase that is known to complete on its own (copies and MMAs
 // already issued), bounded, ignoring the abort flag.
-__device__ __noinline__ void drain_wait(uint32_t bar, uint32_t parity) {
+__device__ __noinline__ void drain_wait(uint32_t bar, uint32_t parity, uint64_t wait_ns) {
   const uint64_t t0 = global_ns();
-  while (!mbar_try(bar, parity) && global_ns() - t0 < kWaitNs) {
+  while (!mbar_try(bar, parity) && global_ns() - t0 < wait_ns) {
   }
 }
 
@@ -249,6 +250,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   float* s_qn2 = reinterpret_cast<float*>(sm + kSmQn2);
   volatile int* s_okw = reinterpret_cast<volatile int*>(sm + kSmOkw);
 
+  const uint64_t wns = a.wait_ns ? a.wait_ns : kWaitNs;  // every bounded wait gives up after this
   const int nkb = (a.L + kUK - 1) / kUK;
   const bool resident = nkb <= kResidentKB;
   const uint32_t nst = resident ? kAStages : kResidentKB;  // streamed: one query slot per stage
@@ -303,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         // the next item into the ring (its entry free once every consumer
         // has read it), or kNoItem when the queue is empty
         const int sl = (int)(it_n & 1);
-        ok = mbar_wait(iempty_bar(sl), ((it_n >> 1) & 1) ^ 1, abort_flag, a.err);
+        ok = mbar_wait(iempty_bar(sl), ((it_n >> 1) & 1) ^ 1, abort_flag, a.err, wns);
         if (!ok) break;
         const uint32_t w = a.queue ? atomicAdd(a.queue, 1u) : blockIdx.x + it_n * gridDim.x;
         s_item[sl] = w < total ? w : kNoItem;
@@ -311,7 +313,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (w >= total) break;
         const Item it = item_of(a, w, QT, ntiles, qtile, nq);
         if (resident) {
-          ok = mbar_wait(qempty_bar, (it_n & 1) ^ 1, abort_flag, a.err);
+          ok = mbar_wait(qempty_bar, (it_n & 1) ^ 1, abort_flag, a.err, wns);
           if (!ok) break;
           mbar_expect_tx(qfull_bar, (uint32_t)nkb * kQBytes);
           for (int kb = 0; kb < nkb; ++kb)
@@ -322,8 +324,11 @@ __global__ void __launch_bounds__(kThreads, 1)
           const int row0 = (int)(it.rb + (uint64_t)t * kUM);
           for (int kb = 0; kb < nkb; ++kb, ++g) {
             const int s = (int)(g % nst);
-            ok = mbar_wait(empty_bar(s), ((g / nst) & 1) ^ 1, abort_flag, a.err);
+            ok = mbar_wait(empty_bar(s), ((g / nst) & 1) ^ 1, abort_flag, a.err, wns);
             if (!ok) break;
+            // diagnostics: the first stage's copy withheld, so its barrier
+            // phase never completes and the MMA warp's bounded wait runs out
+            if (a.withhold_first_copy && g == 0) continue;
             mbar_expect_tx(full_bar(s), resident ? kABytes : kABytes + kQBytes);
             tma_load_2d(base + kSmA + s * kABytes, &tmA, kb * kUK, row0, full_bar(s));
             if (!resident) tma_load_2d(base + kSmQ + s * kQBytes, &tmQ, kb * kUK, (int)it.qoff, full_bar(s));
@@ -331,11 +336,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         if (!ok) break;
       }
-      if (!ok) {
-        // drain the copies still in flight before the CTA leaves
+      if (!ok || a.withhold_first_copy) {
+        // drain the copies still in flight before the CTA leaves (bounded:
+        // a withheld copy's phase never completes)
         const uint32_t first = g > nst ? g - nst : 0;
-        for (uint32_t gg = first; gg < g; ++gg) drain_wait(full_bar((int)(gg % nst)), (gg / nst) & 1);
-        if (resident && q_issued > 0) drain_wait(qfull_bar, (q_issued - 1) & 1);
+        for (uint32_t gg = first; gg < g; ++gg) drain_wait(full_bar((int)(gg % nst)), (gg / nst) & 1, wns);
+        if (resident && q_issued > 0) drain_wait(qfull_bar, (q_issued - 1) & 1, wns);
       }
     }
   } else if (warp == 1) {
@@ -345,27 +351,27 @@ __global__ void __launch_bounds__(kThreads, 1)
       bool ok = true;
       for (; ok; ++it_n) {
         const int sl = (int)(it_n & 1);
-        ok = mbar_wait(ifull_bar(sl), (it_n >> 1) & 1, abort_flag, a.err);
+        ok = mbar_wait(ifull_bar(sl), (it_n >> 1) & 1, abort_flag, a.err, wns);
         if (!ok) break;
         const uint32_t w = s_item[sl];
         mbar_arrive(iempty_bar(sl));
         if (w == kNoItem) break;
         const Item it = item_of(a, w, QT, ntiles, qtile, nq);
         if (resident) {
-          ok = mbar_wait(qfull_bar, it_n & 1, abort_flag, a.err);
+          ok = mbar_wait(qfull_bar, it_n & 1, abort_flag, a.err, wns);
           if (!ok) break;
           tc_fence_after();
         }
         for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t, ++tcount) {
           const int b = (int)(tcount & 1);
-          ok = mbar_wait(tempty_bar(b), ((tcount >> 1) & 1) ^ 1, abort_flag, a.err);
+          ok = mbar_wait(tempty_bar(b), ((tcount >> 1) & 1) ^ 1, abort_flag, a.err, wns);
           if (!ok) break;
           tc_fence_after();
           const uint32_t d = tmem + (uint32_t)b * kUN;
           const uint32_t idesc = idesc_for(item_n(it.qcnt, qtile));
           for (int kb = 0; kb < nkb; ++kb, ++g) {
             const int s = (int)(g % nst);
-            ok = mbar_wait(full_bar(s), (g / nst) & 1, abort_flag, a.err);
+            ok = mbar_wait(full_bar(s), (g / nst) & 1, abort_flag, a.err, wns);
             if (!ok) break;
             tc_fence_after();
             const uint32_t sa = base + kSmA + s * kABytes;
@@ -381,7 +387,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       // every MMA issued has completed before TMEM is freed
       tc_commit(done_bar);
-      drain_wait(done_bar, 0);
+      drain_wait(done_bar, 0, wns);
     }
   } else if (warp >= 4) {
     // ---------------- epilogue
@@ -402,7 +408,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t w = kNoItem;
       int got = 1;
       if (lane == 0) {
-        got = mbar_wait(ifull_bar(sl), (it_n >> 1) & 1, abort_flag, a.err) ? 1 : 0;
+        got = mbar_wait(ifull_bar(sl), (it_n >> 1) & 1, abort_flag, a.err, wns) ? 1 : 0;
         if (got) {
           w = s_item[sl];
           mbar_arrive(iempty_bar(sl));
@@ -491,7 +497,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const float h_row = row_ok ? 0.5f * xn2 : inf;
         // each warp waits for the accumulator itself (lane 0, result shared)
         int go = 0;
-        if (lane == 0) go = mbar_wait(tfull_bar(b), (tcount >> 1) & 1, abort_flag, a.err) ? 1 : 0;
+        if (lane == 0) go = mbar_wait(tfull_bar(b), (tcount >> 1) & 1, abort_flag, a.err, wns) ? 1 : 0;
         go = __shfl_sync(HG_FULL, go, 0);
         if (!go) {
           ok = false;

@@ -226,6 +226,17 @@ HG_API hg_status hg_knn_batch_device(hg_index *ix, const float *d_queries, uint3
 HG_API hg_status hg_bf16_dots(const float *d_rows, uint64_t n, uint32_t L, const float *d_queries, uint32_t nq,
                               float *d_dots, void *stream);
 
+/* Diagnostics (no counterpart in the reference): the failure path of the
+ * tensor-core filter kernel.  Runs it once on a small internal problem (512
+ * rows x 64 queries of length 64, on the current device, ordered on
+ * `stream`) with every bounded wait shortened to wait_us microseconds
+ * (1..2,000,000).  withhold = 1 withholds the first operand copy, so a
+ * barrier phase never completes and the MMA warp's wait runs out: the kernel
+ * then drains its copies and MMAs, frees its tensor memory, returns, and the
+ * call reports HG_ERR_TIMEOUT with the device still usable.  withhold = 0
+ * returns HG_OK.  Allocates its own temporaries. */
+HG_API hg_status hg_filter_wait_check(uint32_t wait_us, int withhold, void *stream);
+
 /* Launch parameters of the query kernels that depend on the data and the
  * GPU (no counterpart in the reference: its parallel search takes thread
  * counts and thresholds on the command line instead).  0 in a field means
