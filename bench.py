@@ -686,6 +686,16 @@ def main():
              "launches": int(pst["filter_launches"]),
              "avg_launch_ms": pst["filter_ms"] / max(int(pst["filter_launches"]), 1),
              "share_of_plain_device_time": round(pst["filter_ms"] / max(pst["device_ms"], 1e-9), 4)}
+    # the exact re-rank of the batched path: 32 B per chunk it computed + 4 B
+    # per survivor row it read from the buckets, over its phase time (plan,
+    # segments and merge, %globaltimer stamps)
+    rr_bytes = 32.0 * agg["chunks_loaded"] + 4.0 * agg["rows_visited"]
+    rr_s = agg["rerank_ms"] / 1000.0
+    rr_gbs = rr_bytes / rr_s / 1e9 if rr_s > 0 else 0.0
+    rerank = {"bound": "hbm", "kernels": "k_rerank_plan + k_rerank_part + k_rerank_merge",
+              "achieved": round(rr_gbs, 1), "peak": peaks["hbm"], "unit": "GB/s",
+              "frac": round(rr_gbs / peaks["hbm"], 4), "bytes_per_step": rr_bytes / steps,
+              "ms_per_step": agg["rerank_ms"] / steps}
     plain.update({"value": plain_qps, "unit": UNIT, "k": pk,
                   "batched_over_plain": round(value / plain_qps, 2) if plain_qps > 0 else None,
                   "path": "hg_knn_device (one query at a time, LB_SAX on); value = the k = %d leg" % pk})
@@ -704,6 +714,7 @@ def main():
         "roofline": roofline,
         "leaf_scan": leaf_scan,
         "lbsax_filter": lbsax,
+        "rerank": rerank,
         "plain": plain,
         "cpu_baseline": cpu_baseline,
         "parity": parity,
