@@ -63,7 +63,7 @@ class QueryStats(ctypes.Structure):
 class KnnOpts(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("use_lb_sax", ctypes.c_int), ("profile", ctypes.c_int),
                 ("approx_blocks", ctypes.c_int), ("bucket_cap", ctypes.c_int), ("dense_filter", ctypes.c_int),
-                ("epsilon", ctypes.c_float), ("nprobes", ctypes.c_int)]
+                ("epsilon", ctypes.c_float), ("nprobes", ctypes.c_int), ("approx_leaves", ctypes.c_int)]
 
 
 class Tuning(ctypes.Structure):
@@ -259,17 +259,19 @@ class HerculesIndex:
 
     # -- queries -------------------------------------------------------------
     def knn(self, queries, k=1, mode=MODE_PLAIN, use_lb_sax=False, with_leaf_pos=False, stats=False,
-            profile=False, epsilon=0.0, nprobes=0):
+            profile=False, epsilon=0.0, nprobes=0, approx_leaves=0):
         """Exact k-NN (squared distances ascending, dataset ids); epsilon > 0
         or nprobes > 0 give the reference's epsilon-approximate or nprobes
-        search instead."""
+        search instead; approx_leaves > 1 seeds the exact search with that
+        many leaves best-first (the answers are the same)."""
         q = _f32(queries, self.L)
         nq = q.shape[0]
         d = np.zeros((nq, k), dtype=np.float32)
         ids = np.zeros((nq, k), dtype=np.int64)
         pos = np.zeros((nq, k), dtype=np.uint64) if with_leaf_pos else None
         st = QueryStats()
-        opts = KnnOpts(mode, 1 if use_lb_sax else 0, 1 if profile else 0, 0, 0, 0, float(epsilon), int(nprobes))
+        opts = KnnOpts(mode, 1 if use_lb_sax else 0, 1 if profile else 0, 0, 0, 0, float(epsilon), int(nprobes),
+                       int(approx_leaves))
         _check(lib().hg_knn(self._h, _ptr(q), nq, k, ctypes.byref(opts), _ptr(d), _ptr(ids), _ptr(pos),
                             ctypes.byref(st)))
         out = [d, ids]
@@ -283,10 +285,10 @@ class HerculesIndex:
         return self.knn(queries, k, mode=MODE_PSCAN, stats=stats)
 
     def knn_device(self, q_ptr, nq, k, dist_ptr, id_ptr, stream=0, mode=MODE_PLAIN, use_lb_sax=False,
-                   profile=False):
+                   profile=False, approx_leaves=0):
         """Device-resident variant; pointers are raw device addresses."""
         st = QueryStats()
-        opts = KnnOpts(mode, 1 if use_lb_sax else 0, 1 if profile else 0)
+        opts = KnnOpts(mode, 1 if use_lb_sax else 0, 1 if profile else 0, 0, 0, 0, 0.0, 0, int(approx_leaves))
         _check(lib().hg_knn_device(self._h, ctypes.c_void_p(q_ptr), nq, k, ctypes.byref(opts),
                                    ctypes.c_void_p(dist_ptr), ctypes.c_void_p(id_ptr), ctypes.c_void_p(stream),
                                    ctypes.byref(st)))

@@ -13,8 +13,11 @@
  * Flags that choose among the reference's CPU strategies (--num-threads,
  * --serial, --sims, --num-queues, --num-read-threads, --flush-threshold,
  * --num-write-threads, --initial-db-size, --eapca-threshold, --sax-threshold,
- * --approx-stop-condition, --buffer-size beyond recording it) are accepted and
- * have no effect: the exact answer does not depend on them.  --epsilon E
+ * --buffer-size beyond recording it) are accepted and have no effect: the
+ * exact answer does not depend on them.  --approx-stop-condition N, given
+ * explicitly, seeds the exact search with N leaves best-first (the greedy
+ * seeding of the reference's parallel path; the answers are the same).
+ * --epsilon E
  * (> 0) runs the reference's epsilon-approximate search and --nprobes P its
  * nprobes search (hercules_file_loaders.c:230-243: nprobes first); --delta is
  * accepted and, as in the reference's serial path (which passes r_delta =
@@ -61,6 +64,7 @@ typedef struct {
   int mode, gpu, pscan, lb_sax;
   float epsilon, delta;
   unsigned nprobes;
+  int approx_leaves; /* --approx-stop-condition: greedy seeding with L_max leaves */
   int track_bsf, track_pruning, max_policy, incremental;
 } opts_t;
 
@@ -149,6 +153,7 @@ static int run_queries(const opts_t *o, hg_index *ix) {
   ko.use_lb_sax = o->lb_sax;
   ko.epsilon = o->epsilon;
   ko.nprobes = (int)o->nprobes;
+  ko.approx_leaves = o->approx_leaves;
   int ok = 1;
   for (unsigned i = 0; i < o->queries_size && ok; ++i) {
     if (fread(q, sizeof(float), L, f) != L) {
@@ -260,7 +265,8 @@ int main(int argc, char **argv) {
       case 1001: o.gpu = atoi(optarg); break;
       case 1002: o.pscan = 1; break;
       case 1003: o.lb_sax = 0; break;
-      case 'j': case 'n': case 'r': case 's': case 'A': case 'B': case 'C': case 'D': case 'S':
+      case 'D': o.approx_leaves = (int)atof(optarg); break; /* the reference's L_max, read as a leaf count */
+      case 'j': case 'n': case 'r': case 's': case 'A': case 'B': case 'C': case 'S':
       case 'F': case 'G': case 'H': case 'I': case 'J':
         break; /* CPU strategy knobs of the reference: no effect on the exact answer */
       case '?': usage(); return 0;

@@ -1192,6 +1192,10 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
                         st));
     CK(hg::launch_select_sort(s.lb, nl, s.bound, s.approx_leaf, d.leaf_start, d.leaf_size, s.cand, s.cand_lb,
                               s.cand_count, s.unit_prefix, st, s.sort_keys));
+    // greedy seeding (the paper's L_max): the next approx_leaves - 1
+    // candidates in LB order, scanned before the rest so that the bound the
+    // rest is filtered against is tighter; the merge folds them in
+    const int seed = (o.mode == HG_MODE_PLAIN && o.approx_leaves > 1) ? o.approx_leaves - 1 : 0;
     hg::FilterArgs f{};
     f.sax = d.sax;
     f.bp = d.bp;
@@ -1208,8 +1212,26 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
     f.use_lbsax = o.use_lb_sax ? 1 : 0;
     f.bound = s.bound;
     f.list = s.list;
-    f.list_count = s.counters + 2;
     f.stats = s.stats;
+    if (seed > 0) {
+      f.cand_lo = 0;
+      f.cand_hi = seed;
+      f.list_count = s.counters + 4;
+      HCK(timed_begin(prof ? &prof->filter : nullptr, st));
+      CK(hg::launch_lbsax_filter(f, sms, st));
+      HCK(timed_end(prof ? &prof->filter : nullptr, st));
+      e.list = s.list;
+      e.list_count = s.counters + 4;
+      e.ident_leaf = nullptr;
+      e.head = s.counters + 5;
+      HCK(timed_begin(prof ? &prof->ed : nullptr, st));
+      CK(hg::launch_ed_stream(e, ed_blocks, st));
+      HCK(timed_end(prof ? &prof->ed : nullptr, st));
+      CK(hg::launch_merge(s.parts, s.part_count, ed_blocks, k, s.topk, s.topk_count, s.bound, s.err, st));
+      f.cand_lo = seed;
+      f.cand_hi = 0;
+    }
+    f.list_count = s.counters + 2;
     HCK(timed_begin(prof ? &prof->filter : nullptr, st));
     CK(hg::launch_lbsax_filter(f, sms, st));
     HCK(timed_end(prof ? &prof->filter : nullptr, st));
@@ -1433,7 +1455,7 @@ static hg_status knn_rounds(hg_index* ix, const float* d_q, uint32_t k, const hg
     const int kr = (int)std::min<uint32_t>((uint32_t)hg::kMaxK, k - done);
     HCK(knn_one(ix, d_q, kr, o, d_dist ? d_dist + done : nullptr, d_id ? d_id + done : nullptr, st, prof, has_floor,
                 floor));
-    *launches += o.mode == HG_MODE_PSCAN ? 4 : 9;
+    *launches += o.mode == HG_MODE_PSCAN ? 4 : (o.approx_leaves > 1 ? 12 : 9);
     int cnt = 0;
     unsigned long long last = 0;
     CK(cudaMemcpyAsync(&cnt, s.topk_count, sizeof cnt, cudaMemcpyDeviceToHost, st));
@@ -1491,7 +1513,7 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
       HCK(knn_approx_one(ix, qi, (int)k, o, di, ii, st));
     } else if ((int)k <= hg::kMaxK) {
       HCK(knn_one(ix, qi, (int)k, o, di, ii, st, o.profile ? &prof : nullptr));
-      launches += o.mode == HG_MODE_PSCAN ? 4 : 9;
+      launches += o.mode == HG_MODE_PSCAN ? 4 : (o.approx_leaves > 1 ? 12 : 9);
     } else {
       uint64_t l = 0;
       HCK(knn_rounds(ix, qi, k, o, di, ii, st, o.profile ? &prof : nullptr, &l));

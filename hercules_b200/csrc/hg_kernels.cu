@@ -230,7 +230,7 @@ __global__ void k_query_prep(const float* __restrict__ q, int L, Tree t, const u
                              float* cand_lb, int* cand_count, uint32_t* unit_prefix, uint32_t* bound,
                              int* topk_count, uint32_t* counters) {
   const int lane = threadIdx.x & 31;
-  if (lane < 4) counters[lane] = 0;
+  if (lane < 6) counters[lane] = 0;
   const int leaf = warp_route(q, t);
   if (lane < HG_PAA_SEGMENTS) {
     const int per = L / HG_PAA_SEGMENTS;
@@ -257,7 +257,6 @@ __global__ void k_route_queries(const float* __restrict__ Q, int nq, int L, Tree
   if ((threadIdx.x & 31) == 0) leaf_out[w] = leaf;
 }
 
-// LB_EAPCA of the query against every leaf, one warp per leaf.
 // LB_EAPCA of every leaf (a warp per leaf).  With sax_tab set, the
 // threads also write the query's LB_SAX term table for the filter:
 // sax_tab[t * 256 + s] = hg_lb_sax_lane(paa[t], s) (reference arithmetic,
@@ -562,13 +561,18 @@ __global__ void __launch_bounds__(kFilterThreads, 1) k_lbsax_filter(FilterArgs a
   __syncthreads();
   const uint32_t* tl = qtab + lane;
   const uint32_t lt = (1u << lane) - 1;
+  // candidates [clo, chi) of the sorted list (all of them by default)
   const int ncand = *a.cand_count;
-  const uint32_t total = a.unit_prefix[ncand];
+  const int clo = min(a.cand_lo, ncand);
+  const int chi = a.cand_hi > 0 ? min(a.cand_hi, ncand) : ncand;
+  if (clo >= chi) return;
+  const uint32_t ubase = a.unit_prefix[clo];
+  const uint32_t total = a.unit_prefix[chi] - ubase;
   const uint32_t per_block = (total + gridDim.x - 1) / gridDim.x;
-  const uint32_t u0 = blockIdx.x * per_block;
-  const uint32_t u1 = min(total, u0 + per_block);
+  const uint32_t u0 = ubase + blockIdx.x * per_block;
+  const uint32_t u1 = min(ubase + total, u0 + per_block);
   if (u0 >= u1) return;
-  int c = unit_candidate(a.unit_prefix, ncand, 0, u0);
+  int c = unit_candidate(a.unit_prefix, ncand, clo, u0);
   uint32_t next_c = c + 1 < ncand ? a.unit_prefix[c + 1] : 0xffffffffu;  // first unit of candidate c + 1
   int cur = -1;
   uint32_t lstart = 0, lend = 0, first_unit = 0;

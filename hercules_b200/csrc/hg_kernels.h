@@ -69,6 +69,7 @@ struct FilterArgs {
   const float* paa;
   const float* sax_tab;  // the query's 16 x 256 LB_SAX terms (k_leaf_lb), 16-byte aligned
   int use_lbsax;
+  int cand_lo, cand_hi;  // candidates [cand_lo, cand_hi) of the sorted list; cand_hi <= 0: to the end
   const uint32_t* bound;
   uint32_t* list;        // surviving rows
   uint32_t* list_count;  // must be 0 before the launch

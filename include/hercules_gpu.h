@@ -115,6 +115,16 @@ typedef struct {
   int nprobes;        /* HG_MODE_PLAIN, > 0: exact_ng_knn_search (:2623-2796):
                          at most nprobes leaves, best-first; takes precedence
                          over epsilon like the reference's dispatch */
+  int approx_leaves;  /* HG_MODE_PLAIN exact search, > 1: greedy seeding with
+                         L_max = approx_leaves leaves (the paper's L_max;
+                         approximate_greedy_knn_search, :70-174, with
+                         --approx-stop-condition): after the routed leaf, the
+                         approx_leaves - 1 other leaves of smallest LB_EAPCA
+                         are scanned first, best-first, so the k-th distance
+                         the remaining candidates are filtered against is
+                         tighter.  0 or 1: the routed leaf only, as the
+                         reference's serial exact search.  The answers do not
+                         depend on it. */
 } hg_knn_opts;
 
 /* ---- status ----------------------------------------------------------- */
