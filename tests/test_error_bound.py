@@ -61,3 +61,24 @@ def test_bf16_rounding_matches_torch():
     a = np.random.default_rng(3).standard_normal(10000).astype(np.float32) * 7
     t = torch.from_numpy(a).to(torch.bfloat16).to(torch.float32).numpy()
     assert np.array_equal(bf16(a).view(np.uint32), t.view(np.uint32))
+
+
+def test_threshold_split_stays_inside_its_margin():
+    """The screening filter subtracts each query's threshold t inside the
+    tensor-core accumulation as two BF16 numbers t_hi = bf16(t) and
+    t_lo = bf16(t - t_hi).  Their sum misses t by at most 2^-16 |t| (BF16
+    keeps 8 significant bits: half an ulp is 2^-8 relative, twice); the
+    kernel lowers t first by c_acc |t| + 2^-14 (|t| + |q~| |x~|), which
+    covers that split error and the rounding of the larger partial sums."""
+    rng = np.random.default_rng(11)
+    t = np.concatenate([rng.normal(size=20000) * 10.0 ** rng.integers(-3, 5, size=20000),
+                        np.array([0.0, 1.0, -1.0, 127.99, 8191.5])]).astype(np.float32)
+    th = bf16(t)
+    tl = (t - th).astype(np.float32)  # exact in FP32
+    assert np.array_equal(tl.astype(np.float64), t.astype(np.float64) - th.astype(np.float64))
+    split_err = np.abs(t.astype(np.float64) - th.astype(np.float64) - bf16(tl).astype(np.float64))
+    assert np.all(split_err <= 2.0 ** -16 * np.abs(t.astype(np.float64)))
+    for L in (96, 256, 1024, 16384):
+        c_acc = L * 2.0 ** -20
+        margin = c_acc * np.abs(t) + 2.0 ** -14 * np.abs(t)
+        assert np.all(margin >= split_err)
