@@ -626,10 +626,11 @@ def main():
                       "algorithmic_bytes_per_query": pscan_bytes / npq}}
 
     # answers of the last timed batch and of both plain legs against FP64
-    ns = 32
+    ns = min(32, nb)
     groups = [("batched", Qb[last, :ns], ks[:ns], D[:ns], I[:ns])]
+    npk = min(32, npl)
     for pk_, (Dp, Ip) in plain_ans.items():
-        groups.append(("plain_k%d" % pk_, Qp[:ns], np.full(ns, pk_), Dp[:ns], Ip[:ns]))
+        groups.append(("plain_k%d" % pk_, Qp[:npk], np.full(npk, pk_), Dp[:npk], Ip[:npk]))
     fp64 = fp64_oracle_check(args, torch, H, groups, device)
 
     cpu_baseline, parity, index = None, None, None

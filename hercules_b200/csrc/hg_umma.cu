@@ -49,13 +49,19 @@ constexpr uint32_t kPairBlock = 1024;        // survivor pairs reserved per warp
 // shared memory map (offsets from a 1024-byte aligned base)
 constexpr uint32_t kSmQ = 0;                                   // 4 x 32 KB
 constexpr uint32_t kSmA = kSmQ + kResidentKB * kQBytes;        // kAStages x 16 KB
-constexpr uint32_t kSmBar = kSmA + kAStages * kABytes;         // mbarriers
-constexpr uint32_t kNumBars = 2 * kAStages + 2 + 4 + 1 + 4;    // full/empty, q full/empty, tmem full/empty x2, done,
-                                                               // item full/empty x2
+// The screening modes fold each query's threshold into the accumulator with
+// one more K = 16 MMA per tile: A_ext (128 rows x 16, every element 1) times
+// B_ext (the item's queries x 16: -t_hi, -t_lo, then zeros), both K-major in
+// the 32-byte swizzle layout (rows of 32 bytes, 8-row groups 256 bytes apart)
+constexpr uint32_t kExtRow = 32;                               // bytes per row of a K = 16 BF16 slab
+constexpr uint32_t kSmAext = kSmA + kAStages * kABytes;        // 128 x 32 B
+constexpr uint32_t kSmBext = kSmAext + kUM * kExtRow;          // 256 x 32 B
+constexpr uint32_t kSmBar = kSmBext + kUN * kExtRow;           // mbarriers
+constexpr uint32_t kNumBars = 2 * kAStages + 2 + 4 + 1 + 4 + 2;  // full/empty, q full/empty, tmem full/empty x2,
+                                                                 // done, item full/empty x2, B_ext full/empty
 constexpr uint32_t kSmTmem = kSmBar + kNumBars * 8;            // TMEM base address
 constexpr uint32_t kSmAbort = kSmTmem + 4;
-constexpr uint32_t kSmThr = (kSmAbort + 4 + 15) & ~15u;        // float [256]
-constexpr uint32_t kSmQidx = kSmThr + kUN * 4;                 // uint32 [256]
+constexpr uint32_t kSmQidx = (kSmAbort + 4 + 15) & ~15u;       // uint32 [256]
 constexpr uint32_t kSmQn2 = kSmQidx + kUN * 4;                 // float [256]
 constexpr uint32_t kSmOkw = kSmQn2 + kUN * 4;                  // int [8]: epilogue warps still running
 constexpr uint32_t kSmItem = kSmOkw + 32;                      // uint32 [2]: the item ring
@@ -164,6 +170,19 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
          ((uint64_t)2 << 61);
 }
 
+// The same for a K = 16 slab in the 32-byte swizzle layout: rows of 32
+// bytes, 8-row groups 256 bytes apart (stride byte offset 16 x 16 B),
+// layout type 6.
+__device__ __forceinline__ uint64_t sw32_desc(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)16 << 32) | ((uint64_t)1 << 46) |
+         ((uint64_t)6 << 61);
+}
+
+// BF16 bits of a float, round to nearest even (finite or infinite inputs)
+__device__ __forceinline__ uint32_t bf16_bits(float f) {
+  return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f));
+}
+
 // Instruction descriptor: FP32 accumulator, BF16 A and B, both K-major,
 // N (bits 17-22: N / 8; a multiple of 16 up to 256), M = 128 (bits 24-28: M / 16).
 __host__ __device__ constexpr uint32_t idesc_for(int n) {
@@ -243,9 +262,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t done_bar = qempty_bar + 40u;
   auto ifull_bar = [&](int sl) { return done_bar + 8u + 8u * sl; };
   auto iempty_bar = [&](int sl) { return done_bar + 24u + 8u * sl; };
+  const uint32_t bfull_bar = done_bar + 40u;   // B_ext written for the item (epilogue -> MMA)
+  const uint32_t bempty_bar = done_bar + 48u;  // the item's MMAs have read B_ext (MMA -> epilogue)
   volatile uint32_t* s_item = reinterpret_cast<volatile uint32_t*>(sm + kSmItem);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + kSmAbort);
-  float* s_thr = reinterpret_cast<float*>(sm + kSmThr);
   uint32_t* s_qidx = reinterpret_cast<uint32_t*>(sm + kSmQidx);
   float* s_qn2 = reinterpret_cast<float*>(sm + kSmQn2);
   volatile int* s_okw = reinterpret_cast<volatile int*>(sm + kSmOkw);
@@ -279,12 +299,24 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(tempty_bar(b), kEpiThreads / 32);
     }
     mbar_init(done_bar, 1);
+    mbar_init(bfull_bar, 1);
+    mbar_init(bempty_bar, 1);
     for (int sl = 0; sl < 2; ++sl) {
       mbar_init(ifull_bar(sl), 1);
       mbar_init(iempty_bar(sl), 1 + kEpiThreads / 32);  // the MMA lane and every epilogue warp
     }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (screen) {
+    // A_ext: every element 1 (BF16 0x3F80); B_ext: zero until an item's
+    // thresholds are written.  Generic-proxy writes, made visible to the
+    // tensor cores (async proxy) before the barrier below.
+    uint32_t* ae = reinterpret_cast<uint32_t*>(sm + kSmAext);
+    uint32_t* be = reinterpret_cast<uint32_t*>(sm + kSmBext);
+    for (int i = tid; i < (int)(kUM * kExtRow / 4); i += kThreads) ae[i] = 0x3F803F80u;
+    for (int i = tid; i < (int)(kUN * kExtRow / 4); i += kThreads) be[i] = 0u;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 2) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(base + kSmTmem)
@@ -362,6 +394,12 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (!ok) break;
           tc_fence_after();
         }
+        if (screen) {
+          // the item's thresholds in B_ext (written by the epilogue warps)
+          ok = mbar_wait(bfull_bar, it_n & 1, abort_flag, a.err, wns);
+          if (!ok) break;
+          tc_fence_after();
+        }
         for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t, ++tcount) {
           const int b = (int)(tcount & 1);
           ok = mbar_wait(tempty_bar(b), ((tcount >> 1) & 1) ^ 1, abort_flag, a.err, wns);
@@ -369,6 +407,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           tc_fence_after();
           const uint32_t d = tmem + (uint32_t)b * kUN;
           const uint32_t idesc = idesc_for(item_n(it.qcnt, qtile));
+          // screening: the accumulator starts as -(t_hi + t_lo) of its column
+          if (screen) tc_mma(d, sw32_desc(base + kSmAext), sw32_desc(base + kSmBext), idesc, 0u);
           for (int kb = 0; kb < nkb; ++kb, ++g) {
             const int s = (int)(g % nst);
             ok = mbar_wait(full_bar(s), (g / nst) & 1, abort_flag, a.err, wns);
@@ -378,12 +418,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t sq = base + kSmQ + (resident ? kb : s) * kQBytes;
 #pragma unroll
             for (int k16 = 0; k16 < kUK / 16; ++k16)
-              tc_mma(d, sw128_desc(sa + k16 * 32), sw128_desc(sq + k16 * 32), idesc, (kb | k16) != 0);
+              tc_mma(d, sw128_desc(sa + k16 * 32), sw128_desc(sq + k16 * 32), idesc, (screen || kb || k16) ? 1u : 0u);
             tc_commit(empty_bar(s));
           }
           if (ok) tc_commit(tfull_bar(b));
         }
         if (ok && resident) tc_commit(qempty_bar);
+        if (ok && screen) tc_commit(bempty_bar);  // B_ext free once the item's MMAs are done
       }
       // every MMA issued has completed before TMEM is freed
       tc_commit(done_bar);
@@ -441,6 +482,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       s_qidx[etid] = q;
       s_qn2[etid] = qm.x;
+      float tv = inf;
       if (screen) {
         // norm maxima over the item's rows (its 128-row tiles), then the
         // column's threshold: keep (row, q) when acc - t_q >= |x|^2 / 2 with
@@ -458,7 +500,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           tm.y = fmaxf(tm.y, __shfl_xor_sync(HG_FULL, tm.y, o));
           tm.z = fmaxf(tm.z, __shfl_xor_sync(HG_FULL, tm.z, o));
         }
-        float tv = inf;  // no bound (or no query): acc - inf = -inf never survives
+        tv = inf;  // no bound (or no query): acc - inf = -inf never survives
         if (qb >= 0.0f) {
           const float err = 2.000002f * (qm.y * tm.z + qm.z * tm.y + qm.z * tm.z + a.c_acc * qm.y * tm.y) +
                             a.c_sq * (qm.x + tm.x + qb) + 1e-5f;
@@ -473,9 +515,37 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
           }
         }
-        s_thr[etid] = tv;
+        // the tensor cores subtract tv as the BF16 pair t_hi + t_lo inside
+        // the accumulation: lower it by the split's rounding (2^-16 |tv|)
+        // and by the accumulation's rounding of the larger partial sums
+        // (c_acc |tv|), with room to spare (2^-14 (|tv| + |q~| |x~|)), so
+        // the test keeps at least every pair the exact test keeps
+        if (tv < inf) tv -= a.c_acc * fabsf(tv) + 6.103515625e-05f * (fabsf(tv) + qm.y * tm.y);
+      }
+      if (screen) {
+        // B_ext may be rewritten once the previous item's MMAs have read it
+        if (ew == 0 && it_n > 0) {
+          int okb = 1;
+          if (lane == 0) okb = mbar_wait(bempty_bar, (it_n - 1) & 1, abort_flag, a.err, wns) ? 1 : 0;
+          okb = __shfl_sync(HG_FULL, okb, 0);
+          ok = ok && okb;
+        }
+        named_sync(1, kEpiThreads);
+        // row etid of B_ext: -t_hi, -t_lo in K positions 0 and 1 (the rest
+        // stays zero); the 32-byte swizzle puts a row's logical 16-byte
+        // chunk 0 at chunk (row >> 2) & 1 (address bit 4 ^= bit 7)
+        float th = tv, tl = 0.0f;
+        if (tv < inf) {
+          th = __bfloat162float(__float2bfloat16_rn(tv));
+          tl = tv - th;  // exact: th is within a factor 2 of tv
+        }
+        const uint32_t row = (uint32_t)etid;
+        *reinterpret_cast<uint32_t*>(sm + kSmBext + row * kExtRow + (((row >> 2) & 1u) << 4)) =
+            bf16_bits(-th) | (bf16_bits(-tl) << 16);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       }
       named_sync(1, kEpiThreads);
+      if (screen && etid == 0) mbar_arrive(bfull_bar);
       // the two warp groups split the item's columns (32-column granules)
       const int half_cols = min(qtile / 2, (int)((it.qcnt + 63u) / 64u) * 32);
       const int c_lo = half * half_cols;
@@ -521,24 +591,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int hh = 0; hh < 2; ++hh) {
               const int cb = c0 + 32 * hh;
               if (cb >= c_hi) break;  // uniform over the warp
-              // v_j = acc_j - t_j in place (packed FP32 adds), screen by the max
-              float* v = reinterpret_cast<float*>(r[hh]);
+              // the accumulators already hold acc_j - t_j: screen by their
+              // maximum; columns past the item's queries never survive
+              const float* v = reinterpret_cast<const float*>(r[hh]);
               float m = -inf;
 #pragma unroll
-              for (int j = 0; j < 32; j += 4) {
-                const float4 t4 = *reinterpret_cast<const float4*>(s_thr + cb + j);
-                const float2 d0 = __fadd2_rn(make_float2(v[j], v[j + 1]), make_float2(-t4.x, -t4.y));
-                const float2 d1 = __fadd2_rn(make_float2(v[j + 2], v[j + 3]), make_float2(-t4.z, -t4.w));
-                v[j] = d0.x;
-                v[j + 1] = d0.y;
-                v[j + 2] = d1.x;
-                v[j + 3] = d1.y;
-                m = fmax3(fmax3(m, d0.x, d0.y), d1.x, d1.y);
-              }
+              for (int j = 0; j < 32; j += 2) m = fmax3(m, v[j], v[j + 1]);
               if (m >= h_row) {
+                const int nv = c_hi - cb;
                 uint32_t mask = 0;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) mask |= (v[j] >= h_row) ? (1u << j) : 0u;
+                for (int j = 0; j < 32; ++j) mask |= (j < nv && v[j] >= h_row) ? (1u << j) : 0u;
                 masks[2 * i2 + hh] = mask;
               }
             }
