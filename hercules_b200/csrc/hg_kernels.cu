@@ -559,7 +559,8 @@ __global__ void __launch_bounds__(kFilterThreads, 1) k_lbsax_filter(FilterArgs a
     }
   }
   __syncthreads();
-  const uint32_t* tl = qtab + lane;
+  const unsigned char* tb = reinterpret_cast<const unsigned char*>(qtab);
+  const uint32_t lane2 = (uint32_t)(4 * lane) * 0x00010001u;  // 4 lane in both 16-bit halves
   const uint32_t lt = (1u << lane) - 1;
   // candidates [clo, chi) of the sorted list (all of them by default)
   const int ncand = *a.cand_count;
@@ -618,12 +619,21 @@ __global__ void __launch_bounds__(kFilterThreads, 1) k_lbsax_filter(FilterArgs a
       bool pass = (okm >> j) & 1u;
       if (pass) ++n_rows;
       if (pass && a.use_lbsax) {
+        // byte (t, s) of this lane's table sits at t * 8192 + f(s) + 4 lane
+        // with f(s) = (s & 0xFC) * 32 + (s & 3) = (s & 0xFC) * 31 + s; the
+        // four symbols of a word get their offsets two at a time, in the
+        // 16-bit halves of one register (no carry: f(s) + 4 lane < 8192)
         const uint32_t ws[4] = {w[j].x, w[j].y, w[j].z, w[j].w};
         uint32_t sum = 0;
 #pragma unroll
-        for (int t = 0; t < 16; ++t) {
-          const uint32_t sym = (ws[t >> 2] >> ((t & 3) * 8)) & 255u;
-          sum += __byte_perm(tl[t * 2048 + (sym >> 2) * 32], 0u, 0x4440u | (sym & 3u));
+        for (int i = 0; i < 4; ++i) {
+          const uint32_t e = ws[i] & 0x00FF00FFu;         // symbols of segments 4i and 4i + 2
+          const uint32_t o = (ws[i] >> 8) & 0x00FF00FFu;  // 4i + 1 and 4i + 3
+          const uint32_t fe = (e & 0x00FC00FCu) * 31u + e + lane2;
+          const uint32_t fo = (o & 0x00FC00FCu) * 31u + o + lane2;
+          const int t0 = 4 * i;
+          sum += (uint32_t)tb[t0 * 8192 + (fe & 0xFFFFu)] + (uint32_t)tb[(t0 + 1) * 8192 + (fo & 0xFFFFu)] +
+                 (uint32_t)tb[(t0 + 2) * 8192 + (fe >> 16)] + (uint32_t)tb[(t0 + 3) * 8192 + (fo >> 16)];
         }
         if (sum >= 255u) {
           pass = false;
