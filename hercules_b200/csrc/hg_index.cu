@@ -689,7 +689,8 @@ static hg_status finalize_build(hg_index* ix, const float* X, cudaStream_t st) {
   CK(cudaMemcpyAsync(d.ids, ix->ids.data(), sizeof(int64_t) * ix->n, cudaMemcpyHostToDevice, st));
   CK(dalloc(&d.bp, 256));
   CK(cudaMemcpyAsync(d.bp, kHgBreakpoints, sizeof(float) * 255, cudaMemcpyHostToDevice, st));
-  CK(dalloc(&d.sax, (size_t)ix->n * 16));
+  // padded to whole 32-row units: the LB_SAX filter bulk-copies whole units
+  CK(dalloc(&d.sax, (size_t)((ix->n + 31) & ~31ull) * 16));
   CK(hg::launch_sax_rows(d.rows, ix->L, ix->n, d.bp, d.sax, st));
   CK(cudaStreamSynchronize(st));
   for (size_t i = 0; i < ix->leaves.size(); ++i) {
@@ -969,7 +970,8 @@ static hg_status read_device_part(hg_index* ix, FILE* raw, const char* dir) {
   CK(cudaMemcpy(d.ids, ix->ids.data(), sizeof(int64_t) * ix->n, cudaMemcpyHostToDevice));
   CK(dalloc(&d.bp, 256));
   CK(cudaMemcpy(d.bp, kHgBreakpoints, sizeof(float) * 255, cudaMemcpyHostToDevice));
-  CK(dalloc(&d.sax, (size_t)ix->n * 16));
+  // padded to whole 32-row units: the LB_SAX filter bulk-copies whole units
+  CK(dalloc(&d.sax, (size_t)((ix->n + 31) & ~31ull) * 16));
   CK(hg::launch_sax_rows(d.rows, ix->L, ix->n, d.bp, d.sax, ix->stream));
   CK(cudaStreamSynchronize(ix->stream));
   HCK(upload_tables(ix));
@@ -1213,6 +1215,7 @@ static hg_status knn_one(hg_index* ix, const float* d_q, int k, const hg_knn_opt
     f.bound = s.bound;
     f.list = s.list;
     f.stats = s.stats;
+    f.err = s.err;
     if (seed > 0) {
       f.cand_lo = 0;
       f.cand_hi = seed;
@@ -1502,6 +1505,7 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   CK(cudaMemsetAsync(ix->s.stats, 0, sizeof(unsigned long long) * 8, st));
+  CK(cudaMemsetAsync(ix->s.err, 0, sizeof(int), st));
   Prof prof;
   CK(cudaEventRecord(e0, st));
   uint64_t launches = 0;
@@ -1522,12 +1526,15 @@ static hg_status knn_device_impl(hg_index* ix, const float* d_queries, uint32_t 
   }
   CK(cudaEventRecord(e1, st));
   unsigned long long hs[8];
+  int ferr = 0;
   CK(cudaMemcpyAsync(hs, ix->s.stats, sizeof hs, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&ferr, ix->s.err, sizeof ferr, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (ferr) return set_error(HG_ERR_TIMEOUT, "hg_knn: an LB_SAX filter wait timed out");
   const size_t ed_launches = prof.ed.size(), filter_launches = prof.filter.size();
   const double scan_ms = drain(prof.ed);
   const double filter_ms = drain(prof.filter);
@@ -2174,6 +2181,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     hg_knn_opts po{};
     po.mode = HG_MODE_PLAIN;
     po.use_lb_sax = 1;
+    CK(cudaMemsetAsync(ix->s.err, 0, sizeof(int), st));
     for (uint32_t q = 0; q < nq && fs == HG_OK; ++q) {
       if (ok[q] == 1) continue;
       ++fallbacks;
@@ -2189,7 +2197,13 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     if (ce == cudaSuccess && d_id) ce = cudaMemcpyAsync(d_id, b.out_id, sizeof(int64_t) * nq * kmax, kind, st);
     if (ce != cudaSuccess) fs = cuda_fail(ce, "hg_knn_batch");
   }
+  int ferr = 0;
+  if (fallbacks && fs == HG_OK) {
+    const cudaError_t ce = cudaMemcpyAsync(&ferr, ix->s.err, sizeof ferr, cudaMemcpyDeviceToHost, st);
+    if (ce != cudaSuccess) fs = cuda_fail(ce, "hg_knn_batch");
+  }
   cudaStreamSynchronize(st);
+  if (fs == HG_OK && ferr) fs = set_error(HG_ERR_TIMEOUT, "hg_knn_batch: an LB_SAX filter wait timed out");
   if (fs != HG_OK) {
     cudaEventDestroy(fb0);
     cudaEventDestroy(fb1);

@@ -513,10 +513,15 @@ __global__ void k_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_pre
 
 // Stage 1.  Work: the candidate leaves in ascending LB_EAPCA order, cut into
 // 32-row units (32-aligned rows; a unit's rows outside its leaf are skipped).
-// One persistent block per SM owns a contiguous range of units; each warp
-// takes kFilterUnits units per step (one 16-byte iSAX word per lane and
-// unit in flight), and a warp stops at the first leaf whose LB exceeds the
-// bound.  Survivors are appended with one atomicAdd per warp and step.
+// One persistent block per SM owns a contiguous range of units, ending at the
+// first leaf whose LB exceeds the bound.  Its producer lane bulk-copies the
+// units' iSAX words (a leaf's units are contiguous in memory: one
+// cp.async.bulk per leaf run, 512 bytes per unit) into kFiltStages stages of
+// shared memory, each guarded by a full and an empty mbarrier; 16 consumer
+// warps take 3 units of every stage each (lane = row), test the rows from
+// shared memory and append the survivors with one atomicAdd per warp and
+// stage.  Every wait is bounded: on timeout the block raises *err, the
+// producer drains the copies it issued, and the call reports HG_ERR_TIMEOUT.
 //
 // The per-row test is a certified lower bound of the reference's LB_SAX
 // (minidist_paa_to_isax_raw_SIMD, sax.c:310-479).  The query's 16 x 256
@@ -531,21 +536,98 @@ __global__ void k_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_pre
 // The 8-bit table is laid out lane-private -- word ((t * 256 + s) / 4) * 32
 // + lane holds the terms of symbols s..s+3 of segment t for that lane -- so
 // the 16 data-dependent lookups of a row never conflict on a bank.
-constexpr int kFilterThreads = 768;
-constexpr int kFilterUnits = 8;
+constexpr int kFiltConsumers = 16;                          // consumer warps
+constexpr int kFilterThreads = 32 * (kFiltConsumers + 1);   // + the producer warp
+constexpr int kUnitsPerWarp = 3;                            // units of a stage per consumer warp
+constexpr int kStageUnits = kFiltConsumers * kUnitsPerWarp; // 48 units: 24 KB
+constexpr int kFiltStages = 4;
+constexpr uint32_t kUnitBytes = 32 * 16;
+constexpr uint32_t kStageBytes = kStageUnits * kUnitBytes;
 constexpr int kSaxTabWords = HG_PAA_SEGMENTS * HG_SAX_CARD / 4 * 32;  // 128 KB
-size_t lbsax_filter_smem() { return sizeof(uint32_t) * kSaxTabWords; }
+constexpr uint32_t kFiltSmStage = kSaxTabWords * 4;                     // stages after the table
+constexpr uint32_t kFiltSmBar = kFiltSmStage + kFiltStages * kStageBytes;  // 2 x kFiltStages mbarriers
+constexpr uint32_t kFiltSmMeta = kFiltSmBar + 2 * kFiltStages * 8;        // end unit, abort flag
+constexpr uint64_t kFiltWaitNs = 2000000000ull;                           // 2 s per wait
+size_t lbsax_filter_smem() { return kFiltSmMeta + 16; }
 
 __device__ __forceinline__ uint32_t sax_qterm(float term, float scale) {
   const float p = __fmul_rd(term, scale);
   return p >= 255.0f ? 255u : (uint32_t)p;
 }
 
+__device__ __forceinline__ bool fl_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t fl_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait for the phase of `parity`: false when the block aborted or
+// the wait ran out (then the block aborts and *err is raised).
+__device__ __noinline__ bool fl_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err) {
+  if (fl_try(bar, parity)) return true;
+  const uint64_t t0 = fl_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (fl_try(bar, parity)) return true;
+    if ((i & 63) == 0) {
+      if (*abort_flag) return false;
+      if (fl_ns() - t0 > kFiltWaitNs) {
+        *abort_flag = 1;
+        if (err) atomicExch(err, 1);
+        return false;
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kFilterThreads, 1) k_lbsax_filter(FilterArgs a) {
-  constexpr int W = kFilterThreads / 32;
-  extern __shared__ uint32_t qtab[];
+  extern __shared__ __align__(16) unsigned char fsm[];
+  uint32_t* qtab = reinterpret_cast<uint32_t*>(fsm);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(fsm);
+  auto full_bar = [&](int st) { return sbase + kFiltSmBar + 8u * st; };
+  auto empty_bar = [&](int st) { return sbase + kFiltSmBar + 8u * (kFiltStages + st); };
+  volatile uint32_t* s_uend = reinterpret_cast<volatile uint32_t*>(fsm + kFiltSmMeta);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(fsm + kFiltSmMeta + 4);
   const float B = __int_as_float((int)ld_volatile(a.bound));
+  // candidates [clo, chi) of the sorted list (all of them by default); this
+  // block's contiguous range of their units
+  const int ncand = *a.cand_count;
+  const int clo = min(a.cand_lo, ncand);
+  const int chi = a.cand_hi > 0 ? min(a.cand_hi, ncand) : ncand;
+  const uint32_t ubase = clo < chi ? a.unit_prefix[clo] : 0u;
+  const uint32_t total = clo < chi ? a.unit_prefix[chi] - ubase : 0u;
+  const uint32_t per_block = (total + gridDim.x - 1) / gridDim.x;
+  const uint32_t u0 = ubase + blockIdx.x * per_block;
+  const uint32_t u1 = min(ubase + total, u0 + per_block);
+  if (threadIdx.x == 0) {
+    // the range ends at the first leaf whose LB exceeds the bound (LBs
+    // ascend along the list, so every later unit is past it too)
+    uint32_t ue = u0;
+    if (u0 < u1) {
+      int c = unit_candidate(a.unit_prefix, ncand, clo, u0);
+      ue = u1;
+      for (; c < chi && a.unit_prefix[c] < u1; ++c)
+        if (a.cand_lb[c] > B) {
+          ue = max(u0, a.unit_prefix[c]);
+          break;
+        }
+    }
+    *s_uend = ue;
+    *abort_flag = 0;
+    for (int st = 0; st < kFiltStages; ++st) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(full_bar(st)), "r"(1) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty_bar(st)), "r"(kFiltConsumers) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
   if (a.use_lbsax) {
     const float Bs = __fadd_rn(__fmul_rn(B, 1.0009765625f), 1e-6f);
     const float T = __fdiv_ru(Bs, (float)(a.L / HG_PAA_SEGMENTS));
@@ -559,36 +641,70 @@ __global__ void __launch_bounds__(kFilterThreads, 1) k_lbsax_filter(FilterArgs a
     }
   }
   __syncthreads();
-  const unsigned char* tb = reinterpret_cast<const unsigned char*>(qtab);
-  const uint32_t lane2 = (uint32_t)(4 * lane) * 0x00010001u;  // 4 lane in both 16-bit halves
-  const uint32_t lt = (1u << lane) - 1;
-  // candidates [clo, chi) of the sorted list (all of them by default)
-  const int ncand = *a.cand_count;
-  const int clo = min(a.cand_lo, ncand);
-  const int chi = a.cand_hi > 0 ? min(a.cand_hi, ncand) : ncand;
-  if (clo >= chi) return;
-  const uint32_t ubase = a.unit_prefix[clo];
-  const uint32_t total = a.unit_prefix[chi] - ubase;
-  const uint32_t per_block = (total + gridDim.x - 1) / gridDim.x;
-  const uint32_t u0 = ubase + blockIdx.x * per_block;
-  const uint32_t u1 = min(ubase + total, u0 + per_block);
-  if (u0 >= u1) return;
-  int c = unit_candidate(a.unit_prefix, ncand, clo, u0);
-  uint32_t next_c = c + 1 < ncand ? a.unit_prefix[c + 1] : 0xffffffffu;  // first unit of candidate c + 1
-  int cur = -1;
-  uint32_t lstart = 0, lend = 0, first_unit = 0;
-  float clb = 0.0f;
-  unsigned long long n_rows = 0, n_pruned = 0, n_leaves = 0;
-  for (uint32_t base = u0 + wib * kFilterUnits; base < u1; base += W * kFilterUnits) {
-    uint32_t rr[kFilterUnits];
-    uint4 w[kFilterUnits];
-    uint32_t okm = 0;
-    bool stop = false;
+  const uint32_t uend = *s_uend;
+  const uint32_t nstages = (uend - u0 + kStageUnits - 1) / kStageUnits;  // 0 when u0 == uend
+  if (wib == kFiltConsumers) {
+    // ---------------- producer: bulk copies of whole units, leaf by leaf
+    if (lane == 0 && nstages) {
+      int c = unit_candidate(a.unit_prefix, ncand, clo, u0);
+      uint32_t k = 0;
+      bool ok = true;
+      for (; k < nstages; ++k) {
+        const int st = (int)(k % kFiltStages);
+        ok = fl_wait(empty_bar(st), ((k / kFiltStages) & 1) ^ 1, abort_flag, a.err);
+        if (!ok) break;
+        const uint32_t us = u0 + k * kStageUnits, ue = min(uend, us + kStageUnits);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full_bar(st)),
+                     "r"((ue - us) * kUnitBytes)
+                     : "memory");
+        for (uint32_t u = us; u < ue;) {
+          while (c + 1 < ncand && a.unit_prefix[c + 1] <= u) ++c;
+          const uint32_t run_end = min(ue, c + 1 < ncand ? a.unit_prefix[c + 1] : ue);
+          const uint64_t first_row = ((a.leaf_start[a.cand[c]] >> 5) + (u - a.unit_prefix[c])) << 5;
+          const unsigned char* src = a.sax + first_row * 16;
+          const uint32_t dst = sbase + kFiltSmStage + (uint32_t)st * kStageBytes + (u - us) * kUnitBytes;
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+              "l"(reinterpret_cast<uint64_t>(src)), "r"((run_end - u) * kUnitBytes), "r"(full_bar(st))
+              : "memory");
+          u = run_end;
+        }
+      }
+      // leaving early: the copies in flight land before the block exits
+      if (!ok) {
+        const uint32_t first = k > (uint32_t)kFiltStages ? k - kFiltStages : 0u;
+        for (uint32_t kk = first; kk < k; ++kk) {
+          const uint64_t t0 = fl_ns();
+          while (!fl_try(full_bar((int)(kk % kFiltStages)), (kk / kFiltStages) & 1) && fl_ns() - t0 < kFiltWaitNs) {
+          }
+        }
+      }
+    }
+  } else {
+    // ---------------- consumers: lane = row of a unit
+    const unsigned char* tb = fsm;
+    const uint32_t lane2 = (uint32_t)(4 * lane) * 0x00010001u;  // 4 lane in both 16-bit halves
+    const uint32_t lt = (1u << lane) - 1;
+    int c = nstages ? unit_candidate(a.unit_prefix, ncand, clo, u0 + wib * kUnitsPerWarp) : 0;
+    uint32_t next_c = c + 1 < ncand ? a.unit_prefix[c + 1] : 0xffffffffu;
+    int cur = -1;
+    uint32_t lstart = 0, lend = 0, first_unit = 0;
+    uint32_t n_rows = 0, n_pass = 0, n_leaves = 0;  // lane 0's counts
+    for (uint32_t k = 0; k < nstages; ++k) {
+      const int st = (int)(k % kFiltStages);
+      int got = 1;
+      if (lane == 0) got = fl_wait(full_bar(st), (k / kFiltStages) & 1, abort_flag, a.err) ? 1 : 0;
+      if (!__shfl_sync(HG_FULL, got, 0)) break;
+      const uint32_t us = u0 + k * kStageUnits, ue = min(uend, us + kStageUnits);
+      const uint4* stage = reinterpret_cast<const uint4*>(fsm + kFiltSmStage + st * kStageBytes);
+      uint32_t m[kUnitsPerWarp], rr[kUnitsPerWarp];
+      uint32_t cnt = 0;
 #pragma unroll
-    for (int j = 0; j < kFilterUnits; ++j) {
-      const uint32_t unit = base + j;
-      rr[j] = 0;
-      if (unit < u1 && !stop) {
+      for (int i = 0; i < kUnitsPerWarp; ++i) {
+        const uint32_t slot = (uint32_t)(wib * kUnitsPerWarp + i), unit = us + slot;
+        m[i] = 0;
+        rr[i] = 0;
+        if (unit >= ue) continue;  // uniform over the warp
         while (unit >= next_c) {
           ++c;
           next_c = c + 1 < ncand ? a.unit_prefix[c + 1] : 0xffffffffu;
@@ -598,73 +714,55 @@ __global__ void __launch_bounds__(kFilterThreads, 1) k_lbsax_filter(FilterArgs a
           const int leaf = a.cand[c];
           lstart = (uint32_t)a.leaf_start[leaf];
           lend = lstart + a.leaf_size[leaf];
-          clb = a.cand_lb[c];
           first_unit = a.unit_prefix[c];
         }
-        if (clb > B) {
-          stop = true;  // every later unit belongs to a leaf with a larger LB
-        } else {
-          const uint32_t tile_in = unit - first_unit;
-          if (tile_in == 0 && lane == 0) ++n_leaves;
-          rr[j] = (((lstart >> 5) + tile_in) << 5) + lane;
-          if (rr[j] >= lstart && rr[j] < lend) okm |= 1u << j;
+        const uint32_t tile_in = unit - first_unit;
+        n_leaves += tile_in == 0 ? 1u : 0u;
+        rr[i] = (((lstart >> 5) + tile_in) << 5) + lane;
+        bool pass = rr[i] >= lstart && rr[i] < lend;
+        n_rows += (uint32_t)__popc(__ballot_sync(HG_FULL, pass));
+        if (pass && a.use_lbsax) {
+          // byte (t, s) of this lane's table sits at t * 8192 + f(s) + 4 lane
+          // with f(s) = (s & 0xFC) * 32 + (s & 3) = (s & 0xFC) * 31 + s; the
+          // four symbols of a word get their offsets two at a time, in the
+          // 16-bit halves of one register (no carry: f(s) + 4 lane < 8192)
+          const uint4 w = stage[slot * 32 + lane];
+          const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+          uint32_t sum = 0;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const uint32_t e = ws[q] & 0x00FF00FFu;         // symbols of segments 4q and 4q + 2
+            const uint32_t o = (ws[q] >> 8) & 0x00FF00FFu;  // 4q + 1 and 4q + 3
+            const uint32_t fe = (e & 0x00FC00FCu) * 31u + e + lane2;
+            const uint32_t fo = (o & 0x00FC00FCu) * 31u + o + lane2;
+            const int t0 = 4 * q;
+            sum += (uint32_t)tb[t0 * 8192 + (fe & 0xFFFFu)] + (uint32_t)tb[(t0 + 1) * 8192 + (fo & 0xFFFFu)] +
+                   (uint32_t)tb[(t0 + 2) * 8192 + (fe >> 16)] + (uint32_t)tb[(t0 + 3) * 8192 + (fo >> 16)];
+          }
+          pass = sum < 255u;
         }
+        m[i] = __ballot_sync(HG_FULL, pass);
+        cnt += (uint32_t)__popc(m[i]);
       }
-      if (a.use_lbsax && ((okm >> j) & 1u)) w[j] = __ldcs(reinterpret_cast<const uint4*>(a.sax) + rr[j]);
-    }
-    uint32_t m[kFilterUnits];
-    uint32_t cnt = 0;
+      // the stage's words are read: hand it back to the producer
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(empty_bar(st)) : "memory");
+      n_pass += cnt;
+      uint32_t pos = 0;
+      if (lane == 0 && cnt) pos = atomicAdd(a.list_count, cnt);
+      pos = __shfl_sync(HG_FULL, pos, 0);
 #pragma unroll
-    for (int j = 0; j < kFilterUnits; ++j) {
-      bool pass = (okm >> j) & 1u;
-      if (pass) ++n_rows;
-      if (pass && a.use_lbsax) {
-        // byte (t, s) of this lane's table sits at t * 8192 + f(s) + 4 lane
-        // with f(s) = (s & 0xFC) * 32 + (s & 3) = (s & 0xFC) * 31 + s; the
-        // four symbols of a word get their offsets two at a time, in the
-        // 16-bit halves of one register (no carry: f(s) + 4 lane < 8192)
-        const uint32_t ws[4] = {w[j].x, w[j].y, w[j].z, w[j].w};
-        uint32_t sum = 0;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const uint32_t e = ws[i] & 0x00FF00FFu;         // symbols of segments 4i and 4i + 2
-          const uint32_t o = (ws[i] >> 8) & 0x00FF00FFu;  // 4i + 1 and 4i + 3
-          const uint32_t fe = (e & 0x00FC00FCu) * 31u + e + lane2;
-          const uint32_t fo = (o & 0x00FC00FCu) * 31u + o + lane2;
-          const int t0 = 4 * i;
-          sum += (uint32_t)tb[t0 * 8192 + (fe & 0xFFFFu)] + (uint32_t)tb[(t0 + 1) * 8192 + (fo & 0xFFFFu)] +
-                 (uint32_t)tb[(t0 + 2) * 8192 + (fe >> 16)] + (uint32_t)tb[(t0 + 3) * 8192 + (fo >> 16)];
-        }
-        if (sum >= 255u) {
-          pass = false;
-          ++n_pruned;
-        }
+      for (int i = 0; i < kUnitsPerWarp; ++i) {
+        if ((m[i] >> lane) & 1u) a.list[pos + __popc(m[i] & lt)] = rr[i];
+        pos += __popc(m[i]);
       }
-      m[j] = __ballot_sync(HG_FULL, pass);
-      cnt += __popc(m[j]);
     }
-    uint32_t pos = 0;
-    if (lane == 0 && cnt) pos = atomicAdd(a.list_count, cnt);
-    pos = __shfl_sync(HG_FULL, pos, 0);
-#pragma unroll
-    for (int j = 0; j < kFilterUnits; ++j) {
-      if ((m[j] >> lane) & 1u) a.list[pos + __popc(m[j] & lt)] = rr[j];
-      pos += __popc(m[j]);
+    // rows considered, pruned (considered minus survivors) and leaves visited
+    if (lane == 0) {
+      atomicAdd(&a.stats[0], (unsigned long long)n_rows);
+      atomicAdd(&a.stats[2], (unsigned long long)(n_rows - n_pass));
+      atomicAdd(&a.stats[3], (unsigned long long)n_leaves);
     }
-    // units are in candidate order, LB non-decreasing: a unit past the bound
-    // ends this warp's walk (stop is the same on every lane)
-    if (stop) break;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    n_rows += __shfl_xor_sync(HG_FULL, n_rows, o);
-    n_pruned += __shfl_xor_sync(HG_FULL, n_pruned, o);
-    n_leaves += __shfl_xor_sync(HG_FULL, n_leaves, o);
-  }
-  if (lane == 0) {
-    atomicAdd(&a.stats[0], n_rows);
-    atomicAdd(&a.stats[2], n_pruned);
-    atomicAdd(&a.stats[3], n_leaves);
   }
 }
 

@@ -74,6 +74,7 @@ struct FilterArgs {
   uint32_t* list;        // surviving rows
   uint32_t* list_count;  // must be 0 before the launch
   unsigned long long* stats;  // [0] rows considered [2] rows pruned by LB_SAX [3] leaves visited
+  int* err;                   // set to 1 when a bounded wait ran out (may be NULL)
 };
 
 // Stage 2: early-abandoning distances over a row list (or a row range).
