@@ -706,7 +706,7 @@ def main():
         "dtype": "bf16 filter (fp32 accumulate) + f32 exact re-rank",
         "data": "synthetic (seeded z-normalised random walks; noisy and fresh queries)",
         "config": config_of(args),
-        "tuning": dict({k: tuning[k] for k in ("filter_tiles_per_item", "bound_tiles_per_item",
+        "tuning": dict({k: tuning[k] for k in ("filter_cta_pair", "filter_tiles_per_item", "bound_tiles_per_item",
                                                 "rerank_blocks_per_sm", "approx_blocks_per_sm")},
                        tuned=not args.no_autotune),
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": nb * args.L * 4,
@@ -867,7 +867,7 @@ def run_sharded(args, rank, world, local):
         "dtype": "bf16 filter (fp32 accumulate) + f32 exact re-rank",
         "data": "synthetic (seeded z-normalised random walks; noisy and fresh queries)",
         "config": config_of(args),
-        "tuning": dict({k: tuning[k] for k in ("filter_tiles_per_item", "bound_tiles_per_item",
+        "tuning": dict({k: tuning[k] for k in ("filter_cta_pair", "filter_tiles_per_item", "bound_tiles_per_item",
                                                 "rerank_blocks_per_sm", "approx_blocks_per_sm")},
                        tuned=not args.no_autotune),
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": nb * args.L * 4,

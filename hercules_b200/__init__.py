@@ -69,7 +69,7 @@ class KnnOpts(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("filter_tiles_per_item", ctypes.c_uint32), ("bound_tiles_per_item", ctypes.c_uint32),
                 ("rerank_blocks_per_sm", ctypes.c_uint32), ("approx_blocks_per_sm", ctypes.c_uint32),
-                ("batch_ms", ctypes.c_double), ("plain_ms", ctypes.c_double)]
+                ("filter_cta_pair", ctypes.c_uint32), ("batch_ms", ctypes.c_double), ("plain_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -105,6 +105,7 @@ _SIGS = [
                                            _P, _P, _P, ctypes.POINTER(QueryStats)]),
     ("hg_bf16_dots", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint32, _P, ctypes.c_uint32, _P, _P]),
     ("hg_filter_wait_check", ctypes.c_int, [ctypes.c_uint32, ctypes.c_int, _P]),
+    ("hg_filter_pair_wait_check", ctypes.c_int, [ctypes.c_uint32, ctypes.c_int, _P]),
     ("hg_tuning_get", ctypes.c_int, [_P, ctypes.POINTER(Tuning)]),
     ("hg_tuning_set", ctypes.c_int, [_P, ctypes.POINTER(Tuning)]),
     ("hg_autotune", ctypes.c_int, [_P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, _P, ctypes.POINTER(Tuning)]),
@@ -369,6 +370,11 @@ def filter_wait_check(wait_us, withhold, stream=0):
     """hg_filter_wait_check: the status code (HG_OK, or HG_ERR_TIMEOUT when a
     withheld copy makes the filter kernel's shortened wait run out)."""
     return lib().hg_filter_wait_check(wait_us, int(bool(withhold)), ctypes.c_void_p(stream))
+
+
+def filter_pair_wait_check(wait_us, withhold, stream=0):
+    """hg_filter_pair_wait_check: the same for the CTA-pair filter kernel."""
+    return lib().hg_filter_pair_wait_check(wait_us, int(bool(withhold)), ctypes.c_void_p(stream))
 
 
 def generate_walks(seed, n, L, first=0):

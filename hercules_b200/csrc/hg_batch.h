@@ -127,6 +127,12 @@ cudaError_t launch_stamp(unsigned long long* slot, cudaStream_t s);  // global-t
 cudaError_t launch_tile_norms(const float4* meta, uint64_t n, float4* tile_meta, cudaStream_t s);
 cudaError_t launch_bound_select(const BatchRank& r, cudaStream_t s);
 size_t umma_filter_smem();
+// modes 1 and 3 on CTA pairs (cta_group::2, L <= 256): q_half_map has boxes
+// of 128 queries (half of the query tile per CTA); blocks is rounded down to
+// an even count
+size_t umma_pair_smem();
+cudaError_t launch_umma_pair(const CUtensorMap& rows_map, const CUtensorMap& q_half_map, const BatchGemm& g,
+                             int blocks, cudaStream_t s);
 cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q_map, const BatchGemm& g, int blocks,
                                cudaStream_t s);
 cudaError_t launch_rerank(const BatchRank& r, int part_blocks, cudaStream_t s);

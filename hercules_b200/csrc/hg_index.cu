@@ -1772,6 +1772,7 @@ static hg_status ensure_prune_scratch(hg_index* ix, bool* ok) {
   b.panel_cap = (uint32_t)panel;
   b.items3_cap = (uint32_t)items;
   HCK(encode_bf16_map(&b.panel_map, b.panel_bf, panel, (uint32_t)L, hg::kBatchQueryTile));
+  HCK(encode_bf16_map(&b.panel_map_half, b.panel_bf, panel, (uint32_t)L, hg::kBatchQueryTile / 2));
   b.prune_nq = (uint32_t)nq;
   ++b.gen;  // a captured pipeline holds the old addresses
   return HG_OK;
@@ -1838,7 +1839,7 @@ static hg_status ensure_leaf_plan(hg_index* ix, uint64_t want, cudaStream_t st) 
 // the device (an empty round costs a few microseconds), the count of queries
 // left unverified.  Events gev[0..] mark the phases.
 static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_t bucket_cap, const CUtensorMap& qmap,
-                               bool prune, cudaStream_t st, uint64_t* launches) {
+                               const CUtensorMap& qmap_half, bool prune, cudaStream_t st, uint64_t* launches) {
   hg::BatchScratch& b = ix->bs;
   const uint32_t L = ix->L;
   const int sms = hg::sm_count(ix->device);
@@ -1930,7 +1931,14 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
   }
   CK(stamp(1));
   // 3-5. certified filter, exact re-rank, verification; queries whose bucket
-  // overflowed are retried with the bound their first survivors gave
+  // overflowed are retried with the bound their first survivors gave.  The
+  // screening passes run on CTA pairs (cta_group::2) where the query tile
+  // stays resident (L <= 256) unless the tuning asks for one CTA per tile.
+  const bool pair = ix->tune.filter_cta_pair != 2 && L <= 256;  // four resident 64-column K blocks
+  auto screen = [&](const CUtensorMap& full_map, const CUtensorMap& half_map) {
+    return pair ? hg::launch_umma_pair(ix->bd.rows_map, half_map, g, sms, st)
+                : hg::launch_umma_filter(ix->bd.rows_map, full_map, g, sms, st);
+  };
   uint32_t* lists[2] = {b.qlist, b.qlist2};
   for (int round = 0; round <= kBatchRetries; ++round) {
     const uint32_t* list_in = round == 0 ? nullptr : lists[(round - 1) & 1];
@@ -1955,7 +1963,7 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
       g.nq_dev = nullptr;
       g.qtile = hg::kBatchQueryTile;
       g.queue = b.queues + 1;
-      CK(hg::launch_umma_filter(ix->bd.rows_map, b.panel_map, g, sms, st));
+      CK(screen(b.panel_map, b.panel_map_half));
       ++*launches;
     }
     g.mode = 1;
@@ -1963,7 +1971,7 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
     g.nq_dev = round == 0 ? (prune ? b.pctl + 2 : nullptr) : n_dev;
     g.qtile = round == 0 ? hg::kBatchQueryTile : 0;
     g.queue = b.queues + 2 + round;
-    CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
+    CK(screen(qmap, qmap_half));
     CK(stamp(3 + 3 * round));
     CK(hg::launch_scatter_pairs(b.pairs, b.heads + 1, b.pairs_cap, list_in, (int)nq, n_dev, b.bucket, b.bucket_cnt,
                                 bucket_cap, st));
@@ -2121,13 +2129,14 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   CK(cudaMemcpyAsync(b.qin, d_Q, sizeof(float) * nq * L,
                      host_io ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
   CK(cudaMemcpyAsync(b.kq, kq.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
-  CUtensorMap qmap;
+  CUtensorMap qmap, qmap_half;
   HCK(encode_bf16_map(&qmap, b.qbf, nq, L, hg::kBatchQueryTile));
+  HCK(encode_bf16_map(&qmap_half, b.qbf, nq, L, hg::kBatchQueryTile / 2));
   // the pipeline, captured once per shape in a CUDA graph and replayed
   bool prune = false;
   if (!o.dense_filter) HCK(ensure_prune_scratch(ix, &prune));
   const uint64_t key[8] = {nq, kmax, bucket_cap, b.gen, ix->tune.filter_tiles_per_item, ix->tune.bound_tiles_per_item,
-                           ix->tune.rerank_blocks_per_sm, prune ? 2u : 1u};
+                           ix->tune.rerank_blocks_per_sm, (prune ? 2u : 1u) | (ix->tune.filter_cta_pair << 4)};
   uint64_t launches = 0;
   if (!b.graph || memcmp(key, b.graph_key, sizeof key) != 0) {
     if (b.graph) {
@@ -2136,7 +2145,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     }
     cudaGraph_t graph = nullptr;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-    const hg_status s = enqueue_batch(ix, nq, kmax, bucket_cap, qmap, prune, st, &launches);
+    const hg_status s = enqueue_batch(ix, nq, kmax, bucket_cap, qmap, qmap_half, prune, st, &launches);
     const cudaError_t ce = cudaStreamEndCapture(st, &graph);
     if (s != HG_OK) {
       if (graph) cudaGraphDestroy(graph);
@@ -2556,6 +2565,119 @@ hg_status hg_filter_wait_check(uint32_t wait_us, int withhold, void* stream) {
   return hs;
 }
 
+// The CTA-pair filter (k_umma_pair, mode 1) once over n rows x nq queries
+// with every bound +inf (no survivors), each bounded wait shortened to
+// wait_ns; withhold = 1 leaves out the odd CTA's first row copy, so the
+// leader's barrier phase never completes.
+static hg_status pair_wait_impl(const float* d_rows, uint64_t n, uint32_t L, const float* d_queries, uint32_t nq,
+                                cudaStream_t st, uint64_t wait_ns, int withhold) {
+  uint16_t* xbf = nullptr;
+  uint16_t* qbf = nullptr;
+  float4* xmeta = nullptr;
+  float4* qmeta = nullptr;
+  float4* tmeta = nullptr;
+  uint32_t* perm = nullptr;
+  float* bound = nullptr;
+  unsigned long long* pairs = nullptr;
+  uint32_t* cnt = nullptr;
+  int* err = nullptr;
+  auto release = [&]() {
+    dfree(xbf);
+    dfree(qbf);
+    dfree(xmeta);
+    dfree(qmeta);
+    dfree(tmeta);
+    dfree(perm);
+    dfree(bound);
+    dfree(pairs);
+    dfree(cnt);
+    dfree(err);
+  };
+  constexpr uint32_t kPairsCap = 4096;
+  std::vector<uint32_t> ident(nq);
+  std::vector<float> inf(nq, INFINITY);
+  for (uint32_t i = 0; i < nq; ++i) ident[i] = i;
+  cudaError_t e = dalloc(&xbf, n * L);
+  if (e == cudaSuccess) e = dalloc(&qbf, (size_t)nq * L);
+  if (e == cudaSuccess) e = dalloc(&xmeta, n);
+  if (e == cudaSuccess) e = dalloc(&qmeta, nq);
+  if (e == cudaSuccess) e = dalloc(&tmeta, (n + 127) / 128);
+  if (e == cudaSuccess) e = dalloc(&perm, nq);
+  if (e == cudaSuccess) e = dalloc(&bound, nq);
+  if (e == cudaSuccess) e = dalloc(&pairs, kPairsCap);
+  if (e == cudaSuccess) e = dalloc(&cnt, 1);
+  if (e == cudaSuccess) e = dalloc(&err, 1);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(perm, ident.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(bound, inf.data(), sizeof(float) * nq, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(uint32_t), st);
+  if (e == cudaSuccess) e = hg::launch_rows_to_bf16(d_rows, nullptr, n, (int)L, xbf, xmeta, st);
+  if (e == cudaSuccess) e = hg::launch_rows_to_bf16(d_queries, nullptr, nq, (int)L, qbf, qmeta, st);
+  if (e == cudaSuccess) e = hg::launch_tile_norms(xmeta, n, tmeta, st);
+  if (e != cudaSuccess) {
+    release();
+    return cuda_fail(e, "hg_filter_pair_wait_check");
+  }
+  CUtensorMap xmap, qmap;
+  hg_status hs = encode_bf16_map(&xmap, xbf, n, L, 128);
+  if (hs == HG_OK) hs = encode_bf16_map(&qmap, qbf, nq, L, hg::kBatchQueryTile / 2);
+  if (hs != HG_OK) {
+    release();
+    return hs;
+  }
+  hg::BatchGemm g{};
+  g.L = (int)L;
+  g.nrows = n;
+  g.xmeta = xmeta;
+  g.tile_meta = tmeta;
+  g.qmeta = qmeta;
+  g.qperm = perm;
+  g.nq = (int)nq;
+  g.mode = 1;
+  g.qtile = hg::kBatchQueryTile;
+  g.tiles_per_item = 8;
+  filter_coefficients(L, &g.c_acc, &g.c_sq);
+  g.bound = bound;
+  g.pairs = pairs;
+  g.pairs_cnt = cnt;
+  g.pairs_cap = kPairsCap;
+  g.err = err;
+  g.wait_ns = wait_ns;
+  g.withhold_first_copy = withhold;
+  int dev = 0;
+  e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = hg::launch_umma_pair(xmap, qmap, g, hg::sm_count(dev), st);
+  int herr = 0;
+  uint32_t hcnt = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof herr, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hcnt, cnt, sizeof hcnt, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  release();
+  if (e != cudaSuccess) return cuda_fail(e, "hg_filter_pair_wait_check");
+  if (herr) return set_error(HG_ERR_TIMEOUT, "hg_filter_pair_wait_check: a tensor-core wait timed out");
+  if (hcnt != 0) return set_error(HG_ERR_CUDA, "hg_filter_pair_wait_check: survivors without a bound");
+  return HG_OK;
+}
+
+hg_status hg_filter_pair_wait_check(uint32_t wait_us, int withhold, void* stream) {
+  if (wait_us == 0 || wait_us > 2000000u)
+    return set_error(HG_ERR_ARG, "hg_filter_pair_wait_check: wait_us outside 1..2e6");
+  cudaStream_t st = (cudaStream_t)stream;
+  constexpr uint64_t n = 1024;
+  constexpr uint32_t L = 64, nq = 64;
+  float* rows = nullptr;
+  float* qs = nullptr;
+  cudaError_t e = dalloc(&rows, n * L);
+  if (e == cudaSuccess) e = dalloc(&qs, (size_t)nq * L);
+  if (e == cudaSuccess) e = hg::launch_generate_walks(1, 0, n, (int)L, rows, st, 0);
+  if (e == cudaSuccess) e = hg::launch_generate_walks(2, 0, nq, (int)L, qs, st, 0);
+  hg_status hs = e == cudaSuccess ? HG_OK : cuda_fail(e, "hg_filter_pair_wait_check");
+  if (hs == HG_OK) hs = pair_wait_impl(rows, n, L, qs, nq, st, (uint64_t)wait_us * 1000ull, withhold ? 1 : 0);
+  dfree(rows);
+  dfree(qs);
+  return hs;
+}
+
 hg_status hg_tuning_get(const hg_index* ix, hg_tuning* out) {
   if (!ix || !out) return set_error(HG_ERR_ARG, "hg_tuning_get: null argument");
   *out = ix->tune;
@@ -2566,12 +2688,13 @@ hg_status hg_tuning_set(hg_index* ix, const hg_tuning* t) {
   if (!ix || !t) return set_error(HG_ERR_ARG, "hg_tuning_set: null argument");
   auto bad = [](uint32_t v, uint32_t lo, uint32_t hi) { return v != 0 && (v < lo || v > hi); };
   if (bad(t->filter_tiles_per_item, 8, 128) || bad(t->bound_tiles_per_item, 2, 64) ||
-      bad(t->rerank_blocks_per_sm, 1, 16) || bad(t->approx_blocks_per_sm, 1, 4))
+      bad(t->rerank_blocks_per_sm, 1, 16) || bad(t->approx_blocks_per_sm, 1, 4) || bad(t->filter_cta_pair, 1, 2))
     return set_error(HG_ERR_ARG, "hg_tuning_set: a parameter outside its range");
   if (t->filter_tiles_per_item) ix->tune.filter_tiles_per_item = t->filter_tiles_per_item;
   if (t->bound_tiles_per_item) ix->tune.bound_tiles_per_item = t->bound_tiles_per_item;
   if (t->rerank_blocks_per_sm) ix->tune.rerank_blocks_per_sm = t->rerank_blocks_per_sm;
   if (t->approx_blocks_per_sm) ix->tune.approx_blocks_per_sm = t->approx_blocks_per_sm;
+  if (t->filter_cta_pair) ix->tune.filter_cta_pair = t->filter_cta_pair;
   return HG_OK;
 }
 
@@ -2615,7 +2738,8 @@ hg_status hg_autotune(hg_index* ix, const float* d_queries, uint32_t nq, const u
     bool plain;
   };
   hg_tuning& t = ix->tune;
-  std::vector<Param> params = {{&t.filter_tiles_per_item, {16, 32, 64}, false},
+  std::vector<Param> params = {{&t.filter_cta_pair, {2, 1}, false},
+                               {&t.filter_tiles_per_item, {16, 32, 64}, false},
                                {&t.bound_tiles_per_item, {4, 8, 16}, false},
                                {&t.rerank_blocks_per_sm, {4, 8, 16}, false},
                                {&t.approx_blocks_per_sm, {1, 2, 4}, true}};

@@ -152,6 +152,7 @@ struct BatchScratch {
   uint32_t* pctl = nullptr;              // [4] items, panel rows, dense-pass queries
   unsigned long long* ppairs = nullptr;  // (query, row) pairs of the pruned pass
   CUtensorMap panel_map;                 // TMA descriptor of panel_bf (64 x 256 boxes)
+  CUtensorMap panel_map_half;            // the same with 64 x 128 boxes (the CTA-pair filter)
   // distinct leaf segments (shared by many leaves) and the queries' mean and
   // stdev over each
   int nu = 0;
@@ -179,5 +180,5 @@ struct hg_index {
   hg::BatchScratch bs;
   cudaStream_t stream = nullptr;
   int max_seg = 0;
-  hg_tuning tune = {32, 8, 8, 2, 0.0, 0.0};  // launch parameters (hg_autotune)
+  hg_tuning tune = {32, 8, 8, 2, 2, 0.0, 0.0};  // launch parameters (hg_autotune)
 };

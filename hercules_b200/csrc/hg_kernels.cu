@@ -517,7 +517,7 @@ __global__ void k_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_pre
 // first leaf whose LB exceeds the bound.  Its producer lane bulk-copies the
 // units' iSAX words (a leaf's units are contiguous in memory: one
 // cp.async.bulk per leaf run, 512 bytes per unit) into kFiltStages stages of
-// shared memory, each guarded by a full and an empty mbarrier; 16 consumer
+// shared memory, each guarded by a full and an empty mbarrier; 20 consumer
 // warps take 3 units of every stage each (lane = row), test the rows from
 // shared memory and append the survivors with one atomicAdd per warp and
 // stage.  Every wait is bounded: on timeout the block raises *err, the
@@ -536,11 +536,11 @@ __global__ void k_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_pre
 // The 8-bit table is laid out lane-private -- word ((t * 256 + s) / 4) * 32
 // + lane holds the terms of symbols s..s+3 of segment t for that lane -- so
 // the 16 data-dependent lookups of a row never conflict on a bank.
-constexpr int kFiltConsumers = 16;                          // consumer warps
+constexpr int kFiltConsumers = 20;                          // consumer warps
 constexpr int kFilterThreads = 32 * (kFiltConsumers + 1);   // + the producer warp
 constexpr int kUnitsPerWarp = 3;                            // units of a stage per consumer warp
-constexpr int kStageUnits = kFiltConsumers * kUnitsPerWarp; // 48 units: 24 KB
-constexpr int kFiltStages = 4;
+constexpr int kStageUnits = kFiltConsumers * kUnitsPerWarp; // 60 units: 30 KB
+constexpr int kFiltStages = 3;
 constexpr uint32_t kUnitBytes = 32 * 16;
 constexpr uint32_t kStageBytes = kStageUnits * kUnitBytes;
 constexpr int kSaxTabWords = HG_PAA_SEGMENTS * HG_SAX_CARD / 4 * 32;  // 128 KB
@@ -571,8 +571,7 @@ __device__ __forceinline__ uint64_t fl_ns() {
 }
 // Bounded wait for the phase of `parity`: false when the block aborted or
 // the wait ran out (then the block aborts and *err is raised).
-__device__ __noinline__ bool fl_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err) {
-  if (fl_try(bar, parity)) return true;
+__device__ __noinline__ bool fl_wait_slow(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err) {
   const uint64_t t0 = fl_ns();
   for (uint32_t i = 1;; ++i) {
     if (fl_try(bar, parity)) return true;
@@ -585,6 +584,11 @@ __device__ __noinline__ bool fl_wait(uint32_t bar, uint32_t parity, volatile int
       }
     }
   }
+}
+
+// the first test inline, the polling loop out of line
+__device__ __forceinline__ bool fl_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err) {
+  return fl_try(bar, parity) || fl_wait_slow(bar, parity, abort_flag, err);
 }
 
 __global__ void __launch_bounds__(kFilterThreads, 1) k_lbsax_filter(FilterArgs a) {

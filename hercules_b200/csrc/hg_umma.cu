@@ -100,9 +100,8 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 
 // Bounded wait for the phase of `parity`; false when this CTA aborted or
 // the wait ran past wait_ns (then the CTA aborts and *err is raised).
-__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err,
-                                       uint64_t wait_ns) {
-  if (mbar_try(bar, parity)) return true;
+__device__ __noinline__ bool mbar_wait_slow(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                            uint64_t wait_ns) {
   const uint64_t t0 = global_ns();
   for (uint32_t i = 1;; ++i) {
     if (mbar_try(bar, parity)) return true;
@@ -115,6 +114,12 @@ __device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile i
       }
     }
   }
+}
+
+// the first test inline, the polling loop out of line
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                         uint64_t wait_ns) {
+  return mbar_try(bar, parity) || mbar_wait_slow(bar, parity, abort_flag, err, wait_ns);
 }
 
 // Wait for a phase that is known to complete on its own (copies and MMAs
@@ -246,6 +251,10 @@ __device__ __forceinline__ Item item_of(const BatchGemm& a, uint32_t w, uint32_t
 
 }  // namespace
 
+// kScreen: modes 1 and 3 (else 0 and 2); kResident: L <= 256, the query tile
+// stays in shared memory (else it is streamed with the row tiles).  The
+// launcher picks the instance, so the per-stage loops carry no mode tests.
+template <bool kScreen, bool kResident>
 __global__ void __launch_bounds__(kThreads, 1)
     k_umma_filter(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmQ, BatchGemm a) {
   extern __shared__ unsigned char umma_raw[];
@@ -272,14 +281,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   const uint64_t wns = a.wait_ns ? a.wait_ns : kWaitNs;  // every bounded wait gives up after this
   const int nkb = (a.L + kUK - 1) / kUK;
-  const bool resident = nkb <= kResidentKB;
-  const uint32_t nst = resident ? kAStages : kResidentKB;  // streamed: one query slot per stage
+  constexpr bool resident = kResident;
+  constexpr uint32_t nst = resident ? kAStages : kResidentKB;  // streamed: one query slot per stage
   // query count (read on the device for rounds planned there) and queries
   // per tile (MMA N): 64 in the bound pass, else the launch's choice or, for
   // 0, the narrowest of 64 / 128 / 256 that holds the queries
   const int nq = a.nq_dev ? (int)min((uint32_t)a.nq, *a.nq_dev) : a.nq;
   const bool listed = a.mode == 0 || a.mode == 3;  // items from a.items
-  const bool screen = a.mode == 1 || a.mode == 3;  // threshold epilogue, survivor pairs
+  constexpr bool screen = kScreen;  // threshold epilogue, survivor pairs
   const int qtile = a.mode == 0 ? kBatchBoundQueries
                                 : (a.qtile ? a.qtile : (nq <= 64 ? 64 : (nq <= 128 ? 128 : kUN)));
   const uint32_t QT = (uint32_t)((nq + qtile - 1) / qtile);
@@ -332,6 +341,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     // ---------------- TMA producer
     if (lane == 0) {
       uint32_t g = 0, it_n = 0, q_issued = 0;
+      uint32_t s_cur = 0, ph = 0;  // stage g % nst and the parity of g / nst
       bool ok = true;
       for (;; ++it_n) {
         // the next item into the ring (its entry free once every consumer
@@ -355,8 +365,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t) {
           const int row0 = (int)(it.rb + (uint64_t)t * kUM);
           for (int kb = 0; kb < nkb; ++kb, ++g) {
-            const int s = (int)(g % nst);
-            ok = mbar_wait(empty_bar(s), ((g / nst) & 1) ^ 1, abort_flag, a.err, wns);
+            const int s = (int)s_cur;
+            const uint32_t par = ph;
+            if (++s_cur == nst) {
+              s_cur = 0;
+              ph ^= 1u;
+            }
+            ok = mbar_wait(empty_bar(s), par ^ 1, abort_flag, a.err, wns);
             if (!ok) break;
             // diagnostics: the first stage's copy withheld, so its barrier
             // phase never completes and the MMA warp's bounded wait runs out
@@ -380,6 +395,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     // ---------------- MMA issuer
     if (lane == 0) {
       uint32_t g = 0, tcount = 0, it_n = 0;
+      uint32_t s_cur = 0, ph = 0;  // stage g % nst and the parity of g / nst
+      const uint64_t dae = sw32_desc(base + kSmAext), dbe = sw32_desc(base + kSmBext);
       bool ok = true;
       for (; ok; ++it_n) {
         const int sl = (int)(it_n & 1);
@@ -400,25 +417,31 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (!ok) break;
           tc_fence_after();
         }
+        const uint32_t idesc = idesc_for(item_n(it.qcnt, qtile));
         for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t, ++tcount) {
           const int b = (int)(tcount & 1);
           ok = mbar_wait(tempty_bar(b), ((tcount >> 1) & 1) ^ 1, abort_flag, a.err, wns);
           if (!ok) break;
           tc_fence_after();
           const uint32_t d = tmem + (uint32_t)b * kUN;
-          const uint32_t idesc = idesc_for(item_n(it.qcnt, qtile));
           // screening: the accumulator starts as -(t_hi + t_lo) of its column
-          if (screen) tc_mma(d, sw32_desc(base + kSmAext), sw32_desc(base + kSmBext), idesc, 0u);
+          if (screen) tc_mma(d, dae, dbe, idesc, 0u);
           for (int kb = 0; kb < nkb; ++kb, ++g) {
-            const int s = (int)(g % nst);
-            ok = mbar_wait(full_bar(s), (g / nst) & 1, abort_flag, a.err, wns);
+            const int s = (int)s_cur;
+            const uint32_t par = ph;
+            if (++s_cur == nst) {
+              s_cur = 0;
+              ph ^= 1u;
+            }
+            ok = mbar_wait(full_bar(s), par, abort_flag, a.err, wns);
             if (!ok) break;
             tc_fence_after();
-            const uint32_t sa = base + kSmA + s * kABytes;
-            const uint32_t sq = base + kSmQ + (resident ? kb : s) * kQBytes;
+            // K step k16 is 32 bytes on: 2 in the descriptors' address field
+            const uint64_t da = sw128_desc(base + kSmA + s * kABytes);
+            const uint64_t dq = sw128_desc(base + kSmQ + (resident ? kb : s) * kQBytes);
 #pragma unroll
             for (int k16 = 0; k16 < kUK / 16; ++k16)
-              tc_mma(d, sw128_desc(sa + k16 * 32), sw128_desc(sq + k16 * 32), idesc, (screen || kb || k16) ? 1u : 0u);
+              tc_mma(d, da + 2 * k16, dq + 2 * k16, idesc, (screen || kb || k16) ? 1u : 0u);
             tc_commit(empty_bar(s));
           }
           if (ok) tc_commit(tfull_bar(b));
@@ -727,13 +750,610 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// The screening passes (modes 1 and 3) on CTA pairs: tcgen05.mma with
+// cta_group::2, M = 256 rows (128 in each CTA of a 2-CTA cluster) x N
+// queries (N / 2 of the query tile in each CTA).  Each CTA keeps only half
+// of the query tile resident (64 KB instead of 128 KB), so nine 16 KB row
+// stages fit beside it instead of five, and each SM's tensor core reads half
+// of the query tile from shared memory per MMA.  Same roles as
+// k_umma_filter; the even CTA of the pair (the leader) fetches the work
+// items and hands them to its peer, waits for both CTAs' copies (each CTA's
+// TMA signals the leader's mbarrier), issues the MMAs, and its commits
+// arrive on the barriers of both CTAs (multicast).  Each CTA's epilogue
+// reads its own 128 TMEM lanes (its rows) and hands the accumulator back to
+// the leader.  Every wait is bounded; a CTA that gives up raises the abort
+// flag of both CTAs.  Rows are walked in 256-row pair tiles: the item's
+// 128-row tiles t_lo + 2j (even CTA) and t_lo + 2j + 1 (odd CTA).
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kPStages = 9;                              // row stages of 16 KB
+constexpr uint32_t kPQBytes = (kUN / 2) * kUK * 2;       // 16 KB: half a query K block
+constexpr uint32_t kPSmQ = 0;                            // 4 x 16 KB
+constexpr uint32_t kPSmA = kPSmQ + kResidentKB * kPQBytes;
+constexpr uint32_t kPSmAext = kPSmA + kPStages * kABytes;   // 128 x 32 B of ones
+constexpr uint32_t kPSmBext = kPSmAext + kUM * kExtRow;     // this CTA's N / 2 thresholds
+constexpr uint32_t kPSmBar = kPSmBext + (kUN / 2) * kExtRow;
+constexpr uint32_t kPNumBars = 2 * kPStages + 2 + 4 + 1 + 4 + 2;
+constexpr uint32_t kPSmTmem = kPSmBar + kPNumBars * 8;
+constexpr uint32_t kPSmAbort = kPSmTmem + 4;
+constexpr uint32_t kPSmQidx = (kPSmAbort + 4 + 15) & ~15u;
+constexpr uint32_t kPSmOkw = kPSmQidx + kUN * 4;
+constexpr uint32_t kPSmItem = kPSmOkw + 32;
+constexpr uint32_t kPSmBytes = kPSmItem + 8;
+constexpr size_t kPDynSmem = kPSmBytes + 1024;
+constexpr uint32_t kPEpiArrivals = 2 * kEpiThreads / 32;  // epilogue warps of both CTAs
+static_assert(kPDynSmem <= 232448, "pair kernel shared memory");
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// shared::cluster address of the same offset in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t mapa(uint32_t addr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_cluster(uint32_t caddr, uint32_t v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(caddr), "r"(v) : "memory");
+}
+// arrive on a barrier of either CTA (shared::cluster address), release at cluster scope
+__device__ __forceinline__ void mbar_arrive_cl(uint32_t caddr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(caddr) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_cl(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait (acquire at cluster scope); on timeout both CTAs' abort flags
+// are raised and *err is set.
+__device__ __noinline__ bool mbar_wait_cl_slow(uint32_t bar, uint32_t parity, volatile int* abort_flag,
+                                               uint32_t peer_abort, int* err, uint64_t wait_ns) {
+  const uint64_t t0 = global_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try_cl(bar, parity)) return true;
+    if ((i & 63) == 0) {
+      if (*abort_flag) return false;
+      if (global_ns() - t0 > wait_ns) {
+        *abort_flag = 1;
+        st_cluster(peer_abort, 1u);
+        atomicExch(err, kErrTimeout);
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ bool mbar_wait_cl(uint32_t bar, uint32_t parity, volatile int* abort_flag,
+                                             uint32_t peer_abort, int* err, uint64_t wait_ns) {
+  return mbar_try_cl(bar, parity) || mbar_wait_cl_slow(bar, parity, abort_flag, peer_abort, err, wait_ns);
+}
+__device__ __noinline__ void drain_wait_cl(uint32_t bar, uint32_t parity, uint64_t wait_ns) {
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_cl(bar, parity) && global_ns() - t0 < wait_ns) {
+  }
+}
+// a CTA-pair TMA load into this CTA's shared memory, completing on the
+// mbarrier at `mbar` (shared::cluster address, the leader's)
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
+}
+__device__ __forceinline__ void tc_mma_pair(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// arrive on the barrier at this offset in both CTAs once the MMAs issued so far complete
+__device__ __forceinline__ void tc_commit_pair_both(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(bar),
+      "h"((uint16_t)3)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit_pair_own(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+__host__ __device__ constexpr uint32_t idesc_pair(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(2 * kUM >> 4) << 24);
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_umma_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmQ, BatchGemm a) {
+  extern __shared__ unsigned char umma_raw[];
+  unsigned char* sm = umma_raw + ((1024 - (s2u(umma_raw) & 1023)) & 1023);
+  const uint32_t base = s2u(sm);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t rank = cluster_rank(), peer = rank ^ 1u;
+  const bool leader = rank == 0;
+  const uint32_t bar0 = base + kPSmBar;
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (kPStages + s); };
+  const uint32_t qfull_bar = bar0 + 8u * (2 * kPStages);
+  const uint32_t qempty_bar = qfull_bar + 8;
+  auto tfull_bar = [&](int b) { return qempty_bar + 8u + 8u * b; };
+  auto tempty_bar = [&](int b) { return qempty_bar + 24u + 8u * b; };
+  const uint32_t done_bar = qempty_bar + 40u;
+  auto ifull_bar = [&](int sl) { return done_bar + 8u + 8u * sl; };
+  auto iempty_bar = [&](int sl) { return done_bar + 24u + 8u * sl; };
+  const uint32_t bfull_bar = done_bar + 40u;   // both halves of B_ext written (leader's)
+  const uint32_t bempty_bar = done_bar + 48u;  // the item's MMAs have read B_ext (both CTAs)
+  volatile uint32_t* s_item = reinterpret_cast<volatile uint32_t*>(sm + kPSmItem);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + kPSmAbort);
+  const uint32_t peer_abort = mapa(base + kPSmAbort, peer);
+  uint32_t* s_qidx = reinterpret_cast<uint32_t*>(sm + kPSmQidx);
+  volatile int* s_okw = reinterpret_cast<volatile int*>(sm + kPSmOkw);
+
+  const uint64_t wns = a.wait_ns ? a.wait_ns : kWaitNs;
+  const int nkb = (a.L + kUK - 1) / kUK;  // <= kResidentKB (checked by the launcher)
+  const int nq = a.nq_dev ? (int)min((uint32_t)a.nq, *a.nq_dev) : a.nq;
+  const bool listed = a.mode == 3;
+  const int qtile = a.qtile ? a.qtile : (nq <= 64 ? 64 : (nq <= 128 ? 128 : kUN));
+  const uint32_t QT = (uint32_t)((nq + qtile - 1) / qtile);
+  const uint64_t ntiles = (a.nrows + kUM - 1) / kUM;
+  const uint32_t nchunks = (uint32_t)((ntiles + a.tiles_per_item - 1) / a.tiles_per_item);
+  const uint32_t total = listed ? (a.nitems_dev ? min(a.nitems, *a.nitems_dev) : a.nitems) : nchunks * QT;
+  auto wait = [&](uint32_t bar, uint32_t parity) {
+    return mbar_wait_cl(bar, parity, abort_flag, peer_abort, a.err, wns);
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < kPStages; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(qfull_bar, 1);
+    mbar_init(qempty_bar, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(tfull_bar(b), 1);
+      mbar_init(tempty_bar(b), kPEpiArrivals);
+    }
+    mbar_init(done_bar, 1);
+    mbar_init(bfull_bar, 2);  // the epilogue of each CTA
+    mbar_init(bempty_bar, 1);
+    for (int sl = 0; sl < 2; ++sl) {
+      mbar_init(ifull_bar(sl), 1);
+      // the leader's MMA lane and, of both CTAs, the epilogue warps; the
+      // peer's producer lane
+      mbar_init(iempty_bar(sl), 1 + kPEpiArrivals + 1);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  {
+    uint32_t* ae = reinterpret_cast<uint32_t*>(sm + kPSmAext);
+    uint32_t* be = reinterpret_cast<uint32_t*>(sm + kPSmBext);
+    for (int i = tid; i < (int)(kUM * kExtRow / 4); i += kThreads) ae[i] = 0x3F803F80u;
+    for (int i = tid; i < (int)((kUN / 2) * kExtRow / 4); i += kThreads) be[i] = 0u;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(base + kPSmTmem)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  // both CTAs' barriers are initialised before any remote arrival or copy
+  cluster_sync_all();
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kPSmTmem);
+
+  // the item's 128-row tiles [t_lo, t_hi) are walked as pair tiles of 256 rows
+  auto pair_tiles = [](const Item& it) { return it.t_hi > it.t_lo ? (it.t_hi - it.t_lo + 1) / 2 : 0u; };
+
+  if (warp == 0) {
+    // ---------------- TMA producer of this CTA's half
+    if (lane == 0) {
+      uint32_t g = 0, q_issued = 0;
+      uint32_t s_cur = 0, ph = 0;  // stage g % kPStages and the parity of g / kPStages
+      bool ok = true;
+      const uint32_t lq = mapa(qfull_bar, 0);
+      for (uint32_t it_n = 0;; ++it_n) {
+        const int sl = (int)(it_n & 1);
+        uint32_t w;
+        if (leader) {
+          ok = wait(iempty_bar(sl), ((it_n >> 1) & 1) ^ 1);
+          if (!ok) break;
+          const uint32_t v = a.queue ? atomicAdd(a.queue, 1u) : (blockIdx.x >> 1) + it_n * (gridDim.x >> 1);
+          w = v < total ? v : kNoItem;
+          s_item[sl] = w;
+          st_cluster(mapa(base + kPSmItem + 4u * sl, 1), w);
+          mbar_arrive(ifull_bar(sl));
+          mbar_arrive_cl(mapa(ifull_bar(sl), 1));
+        } else {
+          ok = wait(ifull_bar(sl), (it_n >> 1) & 1);
+          if (!ok) break;
+          w = s_item[sl];
+          mbar_arrive_cl(mapa(iempty_bar(sl), 0));
+        }
+        if (w == kNoItem) break;
+        const Item it = item_of(a, w, QT, ntiles, qtile, nq);
+        const int n = item_n(it.qcnt, qtile);
+        ok = wait(qempty_bar, (it_n & 1) ^ 1);
+        if (!ok) break;
+        if (leader) mbar_expect_tx(qfull_bar, 2u * (uint32_t)nkb * kPQBytes);
+        for (int kb = 0; kb < nkb; ++kb)
+          tma_load_2d_pair(base + kPSmQ + kb * kPQBytes, &tmQ, kb * kUK, (int)(it.qoff + rank * (uint32_t)(n / 2)), lq);
+        ++q_issued;
+        const uint32_t np = pair_tiles(it);
+        for (uint32_t j = 0; ok && j < np; ++j) {
+          const int row0 = (int)(it.rb + (uint64_t)(it.t_lo + 2 * j + rank) * kUM);
+          for (int kb = 0; kb < nkb; ++kb, ++g) {
+            const int s = (int)s_cur;
+            const uint32_t par = ph;
+            if (++s_cur == kPStages) {
+              s_cur = 0;
+              ph ^= 1u;
+            }
+            ok = wait(empty_bar(s), par ^ 1);
+            if (!ok) break;
+            if (a.withhold_first_copy && g == 0 && !leader) continue;
+            if (leader) mbar_expect_tx(full_bar(s), 2u * kABytes);
+            tma_load_2d_pair(base + kPSmA + s * kABytes, &tmA, kb * kUK, row0, mapa(full_bar(s), 0));
+          }
+        }
+        if (!ok) break;
+      }
+      if (leader && (!ok || a.withhold_first_copy)) {
+        // the copies of both CTAs complete on the leader's barriers: wait
+        // (bounded) for the stages issued before the CTAs leave
+        const uint32_t first = g > kPStages ? g - kPStages : 0;
+        for (uint32_t gg = first; gg < g; ++gg) drain_wait_cl(full_bar((int)(gg % kPStages)), (gg / kPStages) & 1, wns);
+        if (q_issued > 0) drain_wait_cl(qfull_bar, (q_issued - 1) & 1, wns);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer (the leader's lane 0)
+    if (leader && lane == 0) {
+      uint32_t g = 0, tcount = 0;
+      uint32_t s_cur = 0, ph = 0;
+      const uint64_t dae = sw32_desc(base + kPSmAext), dbe = sw32_desc(base + kPSmBext);
+      bool ok = true;
+      for (uint32_t it_n = 0; ok; ++it_n) {
+        const int sl = (int)(it_n & 1);
+        ok = wait(ifull_bar(sl), (it_n >> 1) & 1);
+        if (!ok) break;
+        const uint32_t w = s_item[sl];
+        mbar_arrive(iempty_bar(sl));
+        if (w == kNoItem) break;
+        const Item it = item_of(a, w, QT, ntiles, qtile, nq);
+        ok = wait(qfull_bar, it_n & 1);
+        if (!ok) break;
+        tc_fence_after();
+        ok = wait(bfull_bar, it_n & 1);
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t idesc = idesc_pair(item_n(it.qcnt, qtile));
+        const uint32_t np = pair_tiles(it);
+        for (uint32_t j = 0; ok && j < np; ++j, ++tcount) {
+          const int b = (int)(tcount & 1);
+          ok = wait(tempty_bar(b), ((tcount >> 1) & 1) ^ 1);
+          if (!ok) break;
+          tc_fence_after();
+          const uint32_t d = tmem + (uint32_t)b * kUN;
+          // the accumulator starts as -(t_hi + t_lo) of its column
+          tc_mma_pair(d, dae, dbe, idesc, 0u);
+          for (int kb = 0; kb < nkb; ++kb, ++g) {
+            const int s = (int)s_cur;
+            const uint32_t par = ph;
+            if (++s_cur == kPStages) {
+              s_cur = 0;
+              ph ^= 1u;
+            }
+            ok = wait(full_bar(s), par);
+            if (!ok) break;
+            tc_fence_after();
+            const uint64_t da = sw128_desc(base + kPSmA + s * kABytes);
+            const uint64_t dq = sw128_desc(base + kPSmQ + kb * kPQBytes);
+#pragma unroll
+            for (int k16 = 0; k16 < kUK / 16; ++k16) tc_mma_pair(d, da + 2 * k16, dq + 2 * k16, idesc, 1u);
+            tc_commit_pair_both(empty_bar(s));
+          }
+          if (ok) tc_commit_pair_both(tfull_bar(b));
+        }
+        if (ok) {
+          tc_commit_pair_both(qempty_bar);
+          tc_commit_pair_both(bempty_bar);
+        }
+      }
+      // every MMA issued has completed before either CTA frees its TMEM
+      tc_commit_pair_own(done_bar);
+      drain_wait_cl(done_bar, 0, wns);
+    }
+  } else if (warp >= 4) {
+    // ---------------- epilogue of this CTA's 128 rows
+    const int etid = tid - 128;
+    const int ew = warp - 4;
+    const int quarter = warp & 3;
+    const int half = ew >> 2;
+    const float inf = __int_as_float(0x7f800000);
+    const uint32_t l_bfull = mapa(bfull_bar, 0);
+    uint32_t tcount = 0;
+    uint32_t pcur = 0, pend = 0;
+    bool ok = true;
+    float e_sum = 0.0f, e_rel = 0.0f, e_max = 0.0f;
+    uint32_t e_cnt = 0, e_rcnt = 0;
+    for (uint32_t it_n = 0;; ++it_n) {
+      const int sl = (int)(it_n & 1);
+      uint32_t w = kNoItem;
+      int got = 1;
+      if (lane == 0) {
+        got = wait(ifull_bar(sl), (it_n >> 1) & 1) ? 1 : 0;
+        if (got) {
+          w = s_item[sl];
+          if (leader) mbar_arrive(iempty_bar(sl));
+          else mbar_arrive_cl(mapa(iempty_bar(sl), 0));
+        }
+      }
+      got = __shfl_sync(HG_FULL, got, 0);
+      w = __shfl_sync(HG_FULL, w, 0);
+      ok = ok && got;
+      if (lane == 0) s_okw[ew] = ok ? 1 : 0;
+      named_sync(1, kEpiThreads);
+      bool all_ok = true;
+#pragma unroll
+      for (int i = 0; i < kEpiThreads / 32; ++i) all_ok = all_ok && s_okw[i] != 0;
+      if (!all_ok || w == kNoItem) break;
+      const Item it = item_of(a, w, QT, ntiles, qtile, nq);
+      const int n = item_n(it.qcnt, qtile);
+      // column etid of the item's query tile
+      uint32_t q = 0xffffffffu;
+      float4 qm = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      float qb = -1.0f;
+      if ((uint32_t)etid < it.qcnt) {
+        q = a.qperm[it.qoff + etid];
+        qm = a.qmeta[q];
+        const float b = a.bound[q];
+        qb = b < inf ? b : -1.0f;
+      }
+      s_qidx[etid] = q;
+      // this CTA holds columns [rank n / 2, rank n / 2 + n / 2) of B_ext
+      const int col0 = (int)rank * (n / 2);
+      const bool mine = etid >= col0 && etid < col0 + n / 2;
+      float4 tm = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      for (uint32_t t = it.t_lo + lane; t < it.t_hi; t += 32) {
+        const float4 v = a.tile_meta[(it.rb + (uint64_t)t * kUM) / kUM];
+        tm.x = fmaxf(tm.x, v.x);
+        tm.y = fmaxf(tm.y, v.y);
+        tm.z = fmaxf(tm.z, v.z);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        tm.x = fmaxf(tm.x, __shfl_xor_sync(HG_FULL, tm.x, o));
+        tm.y = fmaxf(tm.y, __shfl_xor_sync(HG_FULL, tm.y, o));
+        tm.z = fmaxf(tm.z, __shfl_xor_sync(HG_FULL, tm.z, o));
+      }
+      float tv = inf;
+      if (qb >= 0.0f) {
+        const float err = 2.000002f * (qm.y * tm.z + qm.z * tm.y + qm.z * tm.z + a.c_acc * qm.y * tm.y) +
+                          a.c_sq * (qm.x + tm.x + qb) + 1e-5f;
+        tv = 0.5f * (qm.x - qb - err);
+        if (a.errstat && mine) {
+          e_sum += err;
+          e_max = fmaxf(e_max, err);
+          ++e_cnt;
+          if (qb > 0.0f) {
+            e_rel += err / qb;
+            ++e_rcnt;
+          }
+        }
+      }
+      // the split's and the accumulation's rounding, with room to spare (as
+      // in k_umma_filter)
+      if (tv < inf) tv -= a.c_acc * fabsf(tv) + 6.103515625e-05f * (fabsf(tv) + qm.y * tm.y);
+      // B_ext may be rewritten once the previous item's MMAs have read it
+      if (ew == 0 && it_n > 0) {
+        int okb = 1;
+        if (lane == 0) okb = wait(bempty_bar, (it_n - 1) & 1) ? 1 : 0;
+        okb = __shfl_sync(HG_FULL, okb, 0);
+        ok = ok && okb;
+      }
+      named_sync(1, kEpiThreads);
+      if (mine) {
+        float th = tv, tl = 0.0f;
+        if (tv < inf) {
+          th = __bfloat162float(__float2bfloat16_rn(tv));
+          tl = tv - th;
+        }
+        const uint32_t row = (uint32_t)(etid - col0);
+        *reinterpret_cast<uint32_t*>(sm + kPSmBext + row * kExtRow + (((row >> 2) & 1u) << 4)) =
+            bf16_bits(-th) | (bf16_bits(-tl) << 16);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      }
+      named_sync(1, kEpiThreads);
+      if (etid == 0) mbar_arrive_cl(l_bfull);
+      const int half_cols = min(qtile / 2, (int)((it.qcnt + 63u) / 64u) * 32);
+      const int c_lo = half * half_cols;
+      const int c_hi = min(c_lo + half_cols, (int)it.qcnt);
+      const uint32_t np = pair_tiles(it);
+      auto row_of = [&](uint32_t j) {
+        return it.rb + (uint64_t)(it.t_lo + 2 * j + rank) * kUM + quarter * 32 + lane;
+      };
+      auto valid = [&](uint32_t j, uint64_t rw) {
+        return it.t_lo + 2 * j + rank < it.t_hi && rw >= it.vb && rw < it.re && rw < a.nrows;
+      };
+      float xn_next = 0.0f;
+      auto prefetch = [&](uint32_t j) {
+        if (j >= np) return;
+        const uint64_t rw = row_of(j);
+        xn_next = valid(j, rw) ? a.xmeta[rw].x : 0.0f;
+      };
+      prefetch(0);
+      for (uint32_t j = 0; ok && j < np; ++j, ++tcount) {
+        const int b = (int)(tcount & 1);
+        const uint64_t row = row_of(j);
+        const bool row_ok = valid(j, row);
+        const float xn2 = xn_next;
+        prefetch(j + 1);
+        const float h_row = row_ok ? 0.5f * xn2 : inf;
+        int go = 0;
+        if (lane == 0) go = wait(tfull_bar(b), (tcount >> 1) & 1) ? 1 : 0;
+        go = __shfl_sync(HG_FULL, go, 0);
+        if (!go) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)b * kUN;
+        uint32_t masks[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int i2 = 0; i2 < 2; ++i2) {
+          const int c0 = c_lo + 64 * i2;
+          if (c0 >= c_hi) break;
+          uint32_t r[2][32];
+          tc_ld32(tbase + (uint32_t)c0, r[0]);
+          tc_ld32(tbase + (uint32_t)(c0 + 32), r[1]);
+          tc_wait_ld();
+#pragma unroll
+          for (int hh = 0; hh < 2; ++hh) {
+            const int cb = c0 + 32 * hh;
+            if (cb >= c_hi) break;
+            const float* v = reinterpret_cast<const float*>(r[hh]);
+            float m = -inf;
+#pragma unroll
+            for (int jj = 0; jj < 32; jj += 2) m = fmax3(m, v[jj], v[jj + 1]);
+            if (m >= h_row) {
+              const int nv = c_hi - cb;
+              uint32_t mask = 0;
+#pragma unroll
+              for (int jj = 0; jj < 32; ++jj) mask |= (jj < nv && v[jj] >= h_row) ? (1u << jj) : 0u;
+              masks[2 * i2 + hh] = mask;
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) {
+          if (leader) mbar_arrive(tempty_bar(b));
+          else mbar_arrive_cl(mapa(tempty_bar(b), 0));
+        }
+#pragma unroll
+        for (int ci = 0; ci < 4; ++ci) {
+          uint32_t mask = masks[ci];
+          while (__any_sync(HG_FULL, mask != 0)) {
+            const bool has = mask != 0;
+            unsigned long long e = 0;
+            if (has) {
+              const int jj = __ffs(mask) - 1;
+              mask &= mask - 1;
+              e = ((unsigned long long)s_qidx[c_lo + 32 * ci + jj] << 32) | (uint32_t)row;
+            }
+            const uint32_t bal = __ballot_sync(HG_FULL, has);
+            const uint32_t cnt = (uint32_t)__popc(bal);
+            if (pcur + cnt > pend) {
+              for (uint32_t i = pcur + lane; i < pend; i += 32) a.pairs[i] = ~0ull;
+              uint32_t nb = 0;
+              if (lane == 0) nb = atomicAdd(a.pairs_cnt, (uint32_t)kPairBlock);
+              nb = __shfl_sync(HG_FULL, nb, 0);
+              pcur = nb;
+              pend = nb + kPairBlock < a.pairs_cap ? nb + kPairBlock : (nb < a.pairs_cap ? a.pairs_cap : nb);
+            }
+            const uint32_t slot = pcur + (uint32_t)__popc(bal & ((1u << lane) - 1));
+            if (has && slot < pend) a.pairs[slot] = e;
+            pcur += cnt;
+          }
+        }
+      }
+    }
+    for (uint32_t i = pcur + lane; i < pend; i += 32) a.pairs[i] = ~0ull;
+    if (a.errstat) {
+      double ds = e_sum, dr = e_rel;
+      uint32_t c = e_cnt, rc = e_rcnt;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        ds += __shfl_xor_sync(HG_FULL, ds, o);
+        dr += __shfl_xor_sync(HG_FULL, dr, o);
+        c += __shfl_xor_sync(HG_FULL, c, o);
+        rc += __shfl_xor_sync(HG_FULL, rc, o);
+        e_max = fmaxf(e_max, __shfl_xor_sync(HG_FULL, e_max, o));
+      }
+      if (lane == 0 && c) {
+        atomicAdd(&a.errstat[0], ds);
+        atomicAdd(&a.errstat[1], dr);
+        atomicAdd(&a.errstat[2], (double)c);
+        atomicAdd(&a.errstat[3], (double)rc);
+        atomicMax(reinterpret_cast<unsigned long long*>(&a.errstat[4]),
+                  (unsigned long long)__double_as_longlong((double)e_max));
+      }
+    }
+  }
+  // no CTA of the pair leaves (or frees TMEM) while the other may still
+  // signal its barriers or the MMAs may still write its TMEM
+  tc_fence_before();
+  cluster_sync_all();
+  if (warp == 2) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+  }
+}
+
+size_t umma_pair_smem() { return kPDynSmem; }
+
+cudaError_t launch_umma_pair(const CUtensorMap& rows_map, const CUtensorMap& q_half_map, const BatchGemm& g,
+                             int blocks, cudaStream_t s) {
+  if (g.mode != 1 && g.mode != 3) return cudaErrorInvalidValue;
+  if ((g.L + kUK - 1) / kUK > kResidentKB) return cudaErrorInvalidValue;
+  if (g.qtile != 0 && g.qtile != 64 && g.qtile != 128 && g.qtile != 256) return cudaErrorInvalidValue;
+  static SmemLimit attr;
+  const cudaError_t ea = attr.ensure((const void*)k_umma_pair, (int)kPDynSmem);
+  if (ea != cudaSuccess) return ea;
+  int grid = blocks & ~1;
+  if (!(g.mode == 3 ? g.nitems_dev : g.nq_dev)) {
+    const uint64_t ntiles = (g.nrows + kUM - 1) / kUM;
+    const int qtile = g.qtile ? g.qtile : (g.nq <= 64 ? 64 : (g.nq <= 128 ? 128 : kUN));
+    const uint32_t QT = (uint32_t)((g.nq + qtile - 1) / qtile);
+    const uint64_t total = g.mode == 3 ? g.nitems : ((ntiles + g.tiles_per_item - 1) / g.tiles_per_item) * (uint64_t)QT;
+    if (total == 0) return cudaSuccess;
+    if (2 * total < (uint64_t)grid) grid = (int)(2 * total);
+  }
+  if (grid < 2) return cudaErrorInvalidValue;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid, 1, 1);
+  cfg.blockDim = dim3(kThreads, 1, 1);
+  cfg.dynamicSmemBytes = kPDynSmem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr2[1];
+  attr2[0].id = cudaLaunchAttributeClusterDimension;
+  attr2[0].val.clusterDim.x = 2;
+  attr2[0].val.clusterDim.y = 1;
+  attr2[0].val.clusterDim.z = 1;
+  cfg.attrs = attr2;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_umma_pair, rows_map, q_half_map, g);
+}
+
 size_t umma_filter_smem() { return kDynSmem; }
+
+template <bool kScreen, bool kResident>
+static cudaError_t launch_filter_instance(const CUtensorMap& rows_map, const CUtensorMap& q_map, const BatchGemm& g,
+                                          int grid, cudaStream_t s) {
+  static SmemLimit attr;
+  const cudaError_t ea = attr.ensure((const void*)k_umma_filter<kScreen, kResident>, (int)kDynSmem);
+  if (ea != cudaSuccess) return ea;
+  k_umma_filter<kScreen, kResident><<<grid, kThreads, kDynSmem, s>>>(rows_map, q_map, g);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q_map, const BatchGemm& g, int blocks,
                                cudaStream_t s) {
-  static SmemLimit attr;
-  const cudaError_t ea = attr.ensure((const void*)k_umma_filter, (int)kDynSmem);
-  if (ea != cudaSuccess) return ea;
   const uint64_t ntiles = (g.nrows + kUM - 1) / kUM;
   if (g.mode != 0 && g.qtile != 0 && g.qtile != 64 && g.qtile != 128 && g.qtile != 256) return cudaErrorInvalidValue;
   // counts read on the device: every CTA starts and leaves when out of items
@@ -747,8 +1367,14 @@ cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q
     if (total == 0) return cudaSuccess;
     grid = (int)(total < (uint64_t)blocks ? total : (uint64_t)blocks);
   }
-  k_umma_filter<<<grid, kThreads, kDynSmem, s>>>(rows_map, q_map, g);
-  return cudaGetLastError();
+  const bool screen = g.mode == 1 || g.mode == 3;
+  const bool resident = (g.L + kUK - 1) / kUK <= kResidentKB;
+  if (screen) {
+    return resident ? launch_filter_instance<true, true>(rows_map, q_map, g, grid, s)
+                    : launch_filter_instance<true, false>(rows_map, q_map, g, grid, s);
+  }
+  return resident ? launch_filter_instance<false, true>(rows_map, q_map, g, grid, s)
+                  : launch_filter_instance<false, false>(rows_map, q_map, g, grid, s);
 }
 
 }  // namespace hg

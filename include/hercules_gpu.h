@@ -247,6 +247,14 @@ HG_API hg_status hg_bf16_dots(const float *d_rows, uint64_t n, uint32_t L, const
  * returns HG_OK.  Allocates its own temporaries. */
 HG_API hg_status hg_filter_wait_check(uint32_t wait_us, int withhold, void *stream);
 
+/* The same for the CTA-pair filter kernel (the screening pass on 2-CTA
+ * clusters, cta_group::2): one pass over 1,024 rows x 64 queries of length 64
+ * with no bounds.  withhold = 1 withholds the odd CTA's first row copy, so
+ * the leader CTA's barrier phase never completes; both CTAs of every pair
+ * then give up, the leader drains its copies and MMAs, both free their
+ * tensor memory, and the call reports HG_ERR_TIMEOUT. */
+HG_API hg_status hg_filter_pair_wait_check(uint32_t wait_us, int withhold, void *stream);
+
 /* Launch parameters of the query kernels that depend on the data and the
  * GPU (no counterpart in the reference: its parallel search takes thread
  * counts and thresholds on the command line instead).  0 in a field means
@@ -256,6 +264,9 @@ typedef struct {
   uint32_t bound_tiles_per_item;   /* batched bound pass: tiles per work item (2..64) */
   uint32_t rerank_blocks_per_sm;   /* batched re-rank: blocks of 8 warps per SM (1..16) */
   uint32_t approx_blocks_per_sm;   /* plain path: blocks per SM of the approximate-leaf scan (1..4) */
+  uint32_t filter_cta_pair;        /* batched filter (L <= 256): 1 = CTA pairs (cta_group::2 MMAs of
+                                      256 rows, half of the query tile per CTA), 2 = one CTA per 128 rows
+                                      (the default) */
   double batch_ms;                 /* hg_autotune: device time of one batch with the chosen values */
   double plain_ms;                 /* hg_autotune: device time of the plain-path sample */
 } hg_tuning;
