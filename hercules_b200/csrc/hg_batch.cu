@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_part(BatchRank a) {
         }
       }
       const bool take = finished && j == 0;
-      warp_list_add(list, cnt, T, k, &a.qbound[q], take, dist, take ? (uint32_t)a.ids[row] : 0u);
+      warp_list_add<true>(list, cnt, T, k, &a.qbound[q], take, dist, take ? (uint32_t)a.ids[row] : 0u);
       B = fminf(B, T);
     }
     cnt = warp_compact(list, cnt, k);
@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_merge(BatchRank a) {
       const float d = __uint_as_float((uint32_t)(v >> 32));
       const bool take = base + lane < pc && d <= Tq && d <= T;
       if (!__any_sync(HG_FULL, take)) break;  // sorted: nothing further qualifies
-      warp_list_add(list, cnt, T, k, nullptr, take, d, (uint32_t)v);
+      warp_list_add<true>(list, cnt, T, k, nullptr, take, d, (uint32_t)v);
     }
   }
   cnt = warp_compact(list, cnt, k);
@@ -611,7 +611,8 @@ __global__ void k_group_items(const LeafPlan* __restrict__ plan, int nleaves, ui
 __global__ void __launch_bounds__(kGroupThreads) k_group_pruned(const uint32_t* __restrict__ leaf_cnt,
                                                                 const LeafPlan* __restrict__ plan, int nleaves,
                                                                 uint32_t tpi, uint32_t panel_cap, uint32_t items_cap,
-                                                                uint32_t nq, uint32_t* leaf_poff, uint32_t* leaf_ioff,
+                                                                uint32_t nq, const uint32_t* nq_dev,
+                                                                uint32_t* leaf_poff, uint32_t* leaf_ioff,
                                                                 uint32_t* ctl, unsigned long long* pairs) {
   __shared__ unsigned long long wsum[3][32];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -667,7 +668,7 @@ __global__ void __launch_bounds__(kGroupThreads) k_group_pruned(const uint32_t* 
     const bool fits = tq <= panel_cap && ti <= items_cap;
     ctl[0] = fits ? (uint32_t)ti : 0u;
     ctl[1] = fits ? (uint32_t)tq : 0u;
-    ctl[2] = fits ? 0u : nq;
+    ctl[2] = fits ? 0u : (nq_dev ? *nq_dev : nq);
     ctl[3] = (uint32_t)tq;  // kept (leaf, query) pairs
     *pairs = fits ? tp : 0ull;
   }
@@ -783,9 +784,9 @@ cudaError_t launch_group_pruned(const uint32_t* leaf_cnt, const uint32_t* leaf_q
                                 const LeafPlan* plan, int nleaves, uint32_t tpi, uint32_t panel_cap,
                                 uint32_t items_cap, uint32_t nq, uint32_t* leaf_poff, uint32_t* leaf_ioff,
                                 uint32_t* ctl, unsigned long long* pairs, uint32_t* panel_list, BatchItem* items,
-                                cudaStream_t s) {
-  k_group_pruned<<<1, kGroupThreads, 0, s>>>(leaf_cnt, plan, nleaves, tpi, panel_cap, items_cap, nq, leaf_poff,
-                                             leaf_ioff, ctl, pairs);
+                                cudaStream_t s, const uint32_t* nq_dev) {
+  k_group_pruned<<<1, kGroupThreads, 0, s>>>(leaf_cnt, plan, nleaves, tpi, panel_cap, items_cap, nq, nq_dev,
+                                             leaf_poff, leaf_ioff, ctl, pairs);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || nleaves == 0) return e;
   k_emit_pruned<<<nleaves, 256, 0, s>>>(leaf_cnt, leaf_q, stride, leaf_poff, leaf_ioff, plan, tpi, ctl, panel_list,

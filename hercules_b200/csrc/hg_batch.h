@@ -114,12 +114,13 @@ cudaError_t launch_group_queries(const int* approx, int nq, const LeafPlan* plan
                                  uint32_t* item_off, uint32_t* nitems, BatchItem* items, cudaStream_t s,
                                  uint32_t* gcnt = nullptr);  // 2 x nleaves words above kMaxLeavesSort leaves
 // the pruned filter's query panel list and work items from the kept
-// (leaf, query) pairs (k_group_pruned, k_emit_pruned)
+// (leaf, query) pairs (k_group_pruned, k_emit_pruned); ctl[2] = the query
+// count (*nq_dev if set, else nq) when the panel or the items do not fit
 cudaError_t launch_group_pruned(const uint32_t* leaf_cnt, const uint32_t* leaf_q, uint32_t stride,
                                 const LeafPlan* plan, int nleaves, uint32_t tpi, uint32_t panel_cap,
                                 uint32_t items_cap, uint32_t nq, uint32_t* leaf_poff, uint32_t* leaf_ioff,
                                 uint32_t* ctl, unsigned long long* pairs, uint32_t* panel_list, BatchItem* items,
-                                cudaStream_t s);
+                                cudaStream_t s, const uint32_t* nq_dev = nullptr);
 cudaError_t launch_collect_retry(const int* ok, const uint32_t* list, uint32_t n, const uint32_t* n_dev,
                                  uint32_t* out, uint32_t* out_n, cudaStream_t s);
 cudaError_t launch_count_unverified(const int* ok, uint32_t nq, uint32_t* out, cudaStream_t s);
@@ -133,6 +134,8 @@ size_t umma_filter_smem();
 size_t umma_pair_smem();
 cudaError_t launch_umma_pair(const CUtensorMap& rows_map, const CUtensorMap& q_half_map, const BatchGemm& g,
                              int blocks, cudaStream_t s);
+// q_map: boxes of 256 queries, except for the bound pass (mode 0) with L <= 256:
+// boxes of kBatchBoundQueries
 cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q_map, const BatchGemm& g, int blocks,
                                cudaStream_t s);
 cudaError_t launch_rerank(const BatchRank& r, int part_blocks, cudaStream_t s);

@@ -79,6 +79,9 @@ static __device__ int warp_compact(unsigned long long* list, int cnt, int k) {
 // Appends (key, id) candidates of the lanes in `take` to the warp's list and
 // compacts it once it holds k entries; returns the warp's k-th distance T
 // (+inf until k distinct distances are held) and lowers the global bound.
+// kLazy: compact only when the list may not hold another 32 entries (fewer
+// sorts; T and the global bound are lowered at each compaction only).
+template <bool kLazy = false>
 __device__ __forceinline__ void warp_list_add(unsigned long long* list, int& cnt, float& T, int k, uint32_t* bound,
                                               bool take, float dist, uint32_t id) {
   const int lane = threadIdx.x & 31;
@@ -90,7 +93,7 @@ __device__ __forceinline__ void warp_list_add(unsigned long long* list, int& cnt
   }
   cnt += __popc(m);
   __syncwarp();
-  if (cnt >= k) {
+  if (kLazy ? cnt > kWarpListCap - 32 : cnt >= k) {
     cnt = warp_compact(list, cnt, k);
     if (cnt == k) {
       const float nt = __uint_as_float((uint32_t)(list[k - 1] >> 32));

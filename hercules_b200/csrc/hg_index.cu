@@ -1766,8 +1766,8 @@ static hg_status ensure_prune_scratch(hg_index* ix, bool* ok) {
   CK(dalloc(&p, panel * L));
   b.panel_bf = p;
   CK(dalloc(&b.items3, items));
-  CK(dalloc(&b.pctl, 4));
-  CK(dalloc(&b.ppairs, 1));
+  CK(dalloc(&b.pctl, 8));    // [0, 4): the first round's panel controls, [4, 8): a retry round's
+  CK(dalloc(&b.ppairs, 2));
   CK(dalloc(&b.segstats, std::max<uint64_t>((uint64_t)b.nu * nq, 1)));
   b.panel_cap = (uint32_t)panel;
   b.items3_cap = (uint32_t)items;
@@ -1839,7 +1839,8 @@ static hg_status ensure_leaf_plan(hg_index* ix, uint64_t want, cudaStream_t st) 
 // the device (an empty round costs a few microseconds), the count of queries
 // left unverified.  Events gev[0..] mark the phases.
 static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_t bucket_cap, const CUtensorMap& qmap,
-                               const CUtensorMap& qmap_half, bool prune, cudaStream_t st, uint64_t* launches) {
+                               const CUtensorMap& qmap_half, const CUtensorMap& qmap_bound, bool prune, cudaStream_t st,
+                               uint64_t* launches) {
   hg::BatchScratch& b = ix->bs;
   const uint32_t L = ix->L;
   const int sms = hg::sm_count(ix->device);
@@ -1849,7 +1850,7 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
   CK(cudaMemsetAsync(b.ctrl, 0, sizeof(uint32_t) * 16, st));
   CK(cudaMemsetAsync(b.heads, 0, sizeof(uint32_t) * 4, st));
   CK(cudaMemsetAsync(b.stats, 0, sizeof(unsigned long long) * 8, st));
-  CK(cudaMemsetAsync(b.queues, 0, sizeof(uint32_t) * 8, st));
+  CK(cudaMemsetAsync(b.queues, 0, sizeof(uint32_t) * 12, st));
   CK(cudaMemsetAsync(b.bm, 0xff, sizeof(unsigned long long) * nq * b.plan_bm_cap, st));
   // 1. approximate leaves, grouping
   CK(hg::launch_route_queries(b.qin, (int)nq, (int)L, index_tree(ix), b.approx, st));
@@ -1880,7 +1881,7 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
   g.pairs_cap = b.pairs_cap;
   g.err = reinterpret_cast<int*>(b.heads + 3);
   g.queue = b.queues + 0;
-  CK(hg::launch_umma_filter(ix->bd.rows_map, qmap, g, sms, st));
+  CK(hg::launch_umma_filter(ix->bd.rows_map, L <= 256 ? qmap_bound : qmap, g, sms, st));
   hg::BatchRank r{};
   r.rows = ix->d.rows;
   r.ids = ix->d.ids;
@@ -1947,28 +1948,42 @@ static hg_status enqueue_batch(hg_index* ix, uint32_t nq, uint32_t kmax, uint32_
       CK(hg::launch_rows_to_bf16(b.qin, list_in, nq, (int)L, b.qbf, b.qmeta, st, n_dev));
       ++*launches;
     }
+    // a retry round prunes leaves again for its queries, against the bounds
+    // the previous round lowered (a subset of the leaves kept before)
+    uint32_t* ctl = round == 0 ? b.pctl : b.pctl + 4;
+    if (round > 0 && prune) {
+      CK(cudaMemsetAsync(b.leaf_cnt, 0, sizeof(uint32_t) * nl, st));
+      CK(hg::launch_leaf_keep_list(b.segstats, b.nu, (int)L, (int)nq, d.leaf_seg_off, d.leaf_points, b.seg_uid,
+                                   d.leaf_sk, d.leaf_size, nl, b.bound, b.leaf_cnt, b.leaf_q, b.prune_nq, list_in,
+                                   n_dev, st));
+      CK(hg::launch_group_pruned(b.leaf_cnt, b.leaf_q, b.prune_nq, b.leaf_plan, nl, ix->tune.filter_tiles_per_item,
+                                 b.panel_cap, b.items3_cap, nq, b.leaf_poff, b.leaf_ioff, ctl, b.ppairs + 1,
+                                 b.panel_list, b.items3, st, n_dev));
+      CK(hg::launch_rows_to_bf16(b.qin, b.panel_list, b.panel_cap, (int)L, b.panel_bf, b.qmeta, st, ctl + 1));
+      *launches += 4;
+    }
     g.errstat = round == 0 ? b.errstat : nullptr;
     if (round == 0) CK(cudaMemsetAsync(b.errstat, 0, 5 * sizeof(double), st));
     CK(cudaMemsetAsync(b.bucket_cnt, 0, sizeof(uint32_t) * nq, st));
     CK(cudaMemsetAsync(b.heads + 1, 0, sizeof(uint32_t), st));
     CK(stamp(2 + 3 * round));
-    if (round == 0 && prune) {
+    if (prune) {
       // the kept (leaf, query) pairs; the dense pass below runs only when
-      // the panel overflowed (its query count is then nq, else 0)
+      // the panel overflowed (its query count is then the round's, else 0)
       g.mode = 3;
       g.items = b.items3;
       g.nitems = b.items3_cap;
-      g.nitems_dev = b.pctl + 0;
+      g.nitems_dev = ctl + 0;
       g.qperm = b.panel_list;
       g.nq_dev = nullptr;
       g.qtile = hg::kBatchQueryTile;
-      g.queue = b.queues + 1;
+      g.queue = round == 0 ? b.queues + 1 : b.queues + 5 + round;
       CK(screen(b.panel_map, b.panel_map_half));
       ++*launches;
     }
     g.mode = 1;
     g.qperm = round == 0 ? b.qperm : list_in;
-    g.nq_dev = round == 0 ? (prune ? b.pctl + 2 : nullptr) : n_dev;
+    g.nq_dev = prune ? ctl + 2 : n_dev;
     g.qtile = round == 0 ? hg::kBatchQueryTile : 0;
     g.queue = b.queues + 2 + round;
     CK(screen(qmap, qmap_half));
@@ -2111,7 +2126,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     CK(dalloc(&b.ctrl, 16));
     CK(dalloc(&b.stamps, 16));
     CK(dalloc(&b.errstat, 5));
-    CK(dalloc(&b.queues, 8));
+    CK(dalloc(&b.queues, 12));
   }
   if (!b.qlist2 || !b.qin || b.out_kmax < kmax) {
     dfree(b.qlist2);
@@ -2129,9 +2144,10 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
   CK(cudaMemcpyAsync(b.qin, d_Q, sizeof(float) * nq * L,
                      host_io ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
   CK(cudaMemcpyAsync(b.kq, kq.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
-  CUtensorMap qmap, qmap_half;
+  CUtensorMap qmap, qmap_half, qmap_bound;
   HCK(encode_bf16_map(&qmap, b.qbf, nq, L, hg::kBatchQueryTile));
   HCK(encode_bf16_map(&qmap_half, b.qbf, nq, L, hg::kBatchQueryTile / 2));
+  HCK(encode_bf16_map(&qmap_bound, b.qbf, nq, L, hg::kBatchBoundQueries));
   // the pipeline, captured once per shape in a CUDA graph and replayed
   bool prune = false;
   if (!o.dense_filter) HCK(ensure_prune_scratch(ix, &prune));
@@ -2145,7 +2161,7 @@ static hg_status knn_batch_impl(hg_index* ix, const float* d_Q, uint32_t nq, con
     }
     cudaGraph_t graph = nullptr;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-    const hg_status s = enqueue_batch(ix, nq, kmax, bucket_cap, qmap, qmap_half, prune, st, &launches);
+    const hg_status s = enqueue_batch(ix, nq, kmax, bucket_cap, qmap, qmap_half, qmap_bound, prune, st, &launches);
     const cudaError_t ce = cudaStreamEndCapture(st, &graph);
     if (s != HG_OK) {
       if (graph) cudaGraphDestroy(graph);

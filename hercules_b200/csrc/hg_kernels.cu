@@ -322,16 +322,21 @@ __global__ void k_query_segstats(const float* __restrict__ Q, int L, int nq, con
 // every leaf it scans; the margins cover the rounding of B_q's product.
 // Kept (leaf, query) pairs go to leaf_q[leaf * stride + i], counted in
 // leaf_cnt[leaf].
+// qlist (optional): the queries are qlist[0 .. *nq_dev) instead of 0 .. nq.
+// A warp per (query, leaf) pair, grid-stride.
 __global__ void k_leaf_keep(const float2* __restrict__ segstats, int nu, int L, int nq,
                             const int* __restrict__ seg_off, const short* __restrict__ points,
                             const int* __restrict__ seg_uid, const float* __restrict__ sk,
                             const uint32_t* __restrict__ leaf_size, int nleaves, const float* __restrict__ bound,
-                            uint32_t* leaf_cnt, uint32_t* leaf_q, uint32_t stride) {
-  const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+                            uint32_t* leaf_cnt, uint32_t* leaf_q, uint32_t stride, const uint32_t* qlist,
+                            const uint32_t* nq_dev) {
   const int lane = threadIdx.x & 31;
-  if (gw >= (uint64_t)nq * nleaves) return;
-  const int q = (int)(gw / nleaves), w = (int)(gw % nleaves);
-  if (leaf_size[w] == 0) return;
+  const uint64_t n = (uint64_t)(nq_dev ? min((uint32_t)nq, *nq_dev) : (uint32_t)nq) * nleaves;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gw < n; gw += nw) {
+  const int qi = (int)(gw / nleaves), w = (int)(gw % nleaves);
+  const int q = qlist ? (int)qlist[qi] : qi;
+  if (leaf_size[w] == 0) continue;
   const float B = bound[q];
   const float lim = B < __int_as_float(0x7f800000)
                         ? __fadd_ru(__fmul_ru(B, 1.0f + 0x1p-10f), __fmul_ru((float)L, 0x1p-20f))
@@ -351,6 +356,7 @@ __global__ void k_leaf_keep(const float2* __restrict__ segstats, int nu, int L, 
     for (int j = 0; j < n; ++j) sum = __fadd_rn(sum, __shfl_sync(HG_FULL, term, j));
   }
   if (lane == 0 && sum <= lim) leaf_q[(uint64_t)w * stride + atomicAdd(&leaf_cnt[w], 1u)] = (uint32_t)q;
+  }
 }
 
 // Candidate leaves: LB_EAPCA <= current bound, not the approximate leaf, not
@@ -1274,8 +1280,24 @@ cudaError_t launch_leaf_keep(const float* Q, int L, int nq, const short* useg_st
   k_query_segstats<<<nq, 256, sizeof(float) * L, s>>>(Q, L, nq, useg_start, useg_end, nu, segstats);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_leaf_keep<<<blocks_for((uint64_t)nq * nleaves * 32, 256), 256, 0, s>>>(
-      segstats, nu, L, nq, seg_off, points, seg_uid, sk, leaf_size, nleaves, bound, leaf_cnt, leaf_q, stride);
+  return launch_leaf_keep_list(segstats, nu, L, nq, seg_off, points, seg_uid, sk, leaf_size, nleaves, bound,
+                               leaf_cnt, leaf_q, stride, nullptr, nullptr, s);
+}
+
+cudaError_t launch_leaf_keep_list(const float2* segstats, int nu, int L, int nq, const int* seg_off,
+                                  const short* points, const int* seg_uid, const float* sk, const uint32_t* leaf_size,
+                                  int nleaves, const float* bound, uint32_t* leaf_cnt, uint32_t* leaf_q,
+                                  uint32_t stride, const uint32_t* qlist, const uint32_t* nq_dev, cudaStream_t s) {
+  if (nq <= 0 || nleaves <= 0) return cudaSuccess;
+  // grid-stride over the (query, leaf) pairs: at most 64 blocks of 8 warps per SM
+  int dev = 0;
+  const cudaError_t ed = cudaGetDevice(&dev);
+  if (ed != cudaSuccess) return ed;
+  const uint64_t want = blocks_for((uint64_t)nq * nleaves * 32, 256);
+  const uint64_t cap = 64ull * (uint64_t)sm_count(dev);
+  k_leaf_keep<<<(unsigned)(want < cap ? want : cap), 256, 0, s>>>(
+      segstats, nu, L, nq, seg_off, points, seg_uid, sk, leaf_size, nleaves, bound, leaf_cnt, leaf_q, stride, qlist,
+      nq_dev);
   return cudaGetLastError();
 }
 

@@ -142,6 +142,12 @@ cudaError_t launch_leaf_keep(const float* Q, int L, int nq, const short* useg_st
                              float2* segstats, const int* seg_off, const short* points, const int* seg_uid,
                              const float* sk, const uint32_t* leaf_size, int nleaves, const float* bound,
                              uint32_t* leaf_cnt, uint32_t* leaf_q, uint32_t stride, cudaStream_t s);
+// the same over the queries qlist[0 .. *nq_dev) (nq: their most), with the
+// segment statistics already computed
+cudaError_t launch_leaf_keep_list(const float2* segstats, int nu, int L, int nq, const int* seg_off,
+                                  const short* points, const int* seg_uid, const float* sk, const uint32_t* leaf_size,
+                                  int nleaves, const float* bound, uint32_t* leaf_cnt, uint32_t* leaf_q,
+                                  uint32_t stride, const uint32_t* qlist, const uint32_t* nq_dev, cudaStream_t s);
 // epsilon search: *flag = (lb <= stale / eps1), the reference's test of a
 // candidate leaf against its k-th distance of that moment; *scanned counts
 // the leaves that pass

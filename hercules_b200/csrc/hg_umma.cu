@@ -46,28 +46,40 @@ constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s per wait
 constexpr int kErrTimeout = 1;
 constexpr uint32_t kPairBlock = 1024;        // survivor pairs reserved per warp at a time
 
-// shared memory map (offsets from a 1024-byte aligned base)
-constexpr uint32_t kSmQ = 0;                                   // 4 x 32 KB
-constexpr uint32_t kSmA = kSmQ + kResidentKB * kQBytes;        // kAStages x 16 KB
 // The screening modes fold each query's threshold into the accumulator with
 // one more K = 16 MMA per tile: A_ext (128 rows x 16, every element 1) times
 // B_ext (the item's queries x 16: -t_hi, -t_lo, then zeros), both K-major in
 // the 32-byte swizzle layout (rows of 32 bytes, 8-row groups 256 bytes apart)
 constexpr uint32_t kExtRow = 32;                               // bytes per row of a K = 16 BF16 slab
-constexpr uint32_t kSmAext = kSmA + kAStages * kABytes;        // 128 x 32 B
-constexpr uint32_t kSmBext = kSmAext + kUM * kExtRow;          // 256 x 32 B
-constexpr uint32_t kSmBar = kSmBext + kUN * kExtRow;           // mbarriers
-constexpr uint32_t kNumBars = 2 * kAStages + 2 + 4 + 1 + 4 + 2;  // full/empty, q full/empty, tmem full/empty x2,
-                                                                 // done, item full/empty x2, B_ext full/empty
-constexpr uint32_t kSmTmem = kSmBar + kNumBars * 8;            // TMEM base address
-constexpr uint32_t kSmAbort = kSmTmem + 4;
-constexpr uint32_t kSmQidx = (kSmAbort + 4 + 15) & ~15u;       // uint32 [256]
-constexpr uint32_t kSmQn2 = kSmQidx + kUN * 4;                 // float [256]
-constexpr uint32_t kSmOkw = kSmQn2 + kUN * 4;                  // int [8]: epilogue warps still running
-constexpr uint32_t kSmItem = kSmOkw + 32;                      // uint32 [2]: the item ring
-constexpr uint32_t kSmBytes = kSmItem + 8;
 constexpr uint32_t kNoItem = 0xffffffffu;                      // ring entry: no more items
-constexpr size_t kDynSmem = kSmBytes + 1024;                   // + alignment slack
+
+// Shared memory map (offsets from a 1024-byte aligned base): the query tile
+// (4 K blocks; 256 queries, or 64 in the bound pass with L <= 256, which then
+// keeps eleven row stages instead of five), the row stages (128 rows x 64 K),
+// A_ext (128 x 32 B), B_ext (256 x 32 B), the mbarriers (full / empty per
+// stage, query tile full / empty, TMEM full / empty x2, done, item ring
+// full / empty x2, B_ext full / empty), the TMEM base address, the abort
+// flag, the tile's query indices and norms, the epilogue warps' flags and the
+// item ring.
+template <bool kBound>
+struct FilterLayout {
+  static constexpr uint32_t kQBlk = kBound ? (uint32_t)kBatchBoundQueries * kUK * 2 : kQBytes;  // per K block
+  static constexpr int kStages = kBound ? 11 : kAStages;
+  static constexpr uint32_t kQ = 0;
+  static constexpr uint32_t kA = kQ + kResidentKB * kQBlk;
+  static constexpr uint32_t kAext = kA + kStages * kABytes;
+  static constexpr uint32_t kBext = kAext + kUM * kExtRow;
+  static constexpr uint32_t kBar = kBext + kUN * kExtRow;
+  static constexpr uint32_t kBars = 2 * kStages + 2 + 4 + 1 + 4 + 2;
+  static constexpr uint32_t kTmem = kBar + kBars * 8;
+  static constexpr uint32_t kAbort = kTmem + 4;
+  static constexpr uint32_t kQidx = (kAbort + 4 + 15) & ~15u;
+  static constexpr uint32_t kQn2 = kQidx + kUN * 4;
+  static constexpr uint32_t kOkw = kQn2 + kUN * 4;
+  static constexpr uint32_t kItem = kOkw + 32;
+  static constexpr size_t kDyn = kItem + 8 + 1024;
+};
+static_assert(FilterLayout<true>::kDyn <= 232448 && FilterLayout<false>::kDyn <= 232448, "filter shared memory");
 
 // --- PTX wrappers -------------------------------------------------------------
 
@@ -254,17 +266,18 @@ __device__ __forceinline__ Item item_of(const BatchGemm& a, uint32_t w, uint32_t
 // kScreen: modes 1 and 3 (else 0 and 2); kResident: L <= 256, the query tile
 // stays in shared memory (else it is streamed with the row tiles).  The
 // launcher picks the instance, so the per-stage loops carry no mode tests.
-template <bool kScreen, bool kResident>
+template <bool kScreen, bool kResident, bool kBound>
 __global__ void __launch_bounds__(kThreads, 1)
     k_umma_filter(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmQ, BatchGemm a) {
+  using LY = FilterLayout<kBound>;
   extern __shared__ unsigned char umma_raw[];
   unsigned char* sm = umma_raw + ((1024 - (s2u(umma_raw) & 1023)) & 1023);
   const uint32_t base = s2u(sm);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t bar0 = base + kSmBar;
+  const uint32_t bar0 = base + LY::kBar;
   auto full_bar = [&](int s) { return bar0 + 8u * s; };
-  auto empty_bar = [&](int s) { return bar0 + 8u * (kAStages + s); };
-  const uint32_t qfull_bar = bar0 + 8u * (2 * kAStages);
+  auto empty_bar = [&](int s) { return bar0 + 8u * (LY::kStages + s); };
+  const uint32_t qfull_bar = bar0 + 8u * (2 * LY::kStages);
   const uint32_t qempty_bar = qfull_bar + 8;
   auto tfull_bar = [&](int b) { return qempty_bar + 8u + 8u * b; };
   auto tempty_bar = [&](int b) { return qempty_bar + 24u + 8u * b; };
@@ -273,16 +286,16 @@ __global__ void __launch_bounds__(kThreads, 1)
   auto iempty_bar = [&](int sl) { return done_bar + 24u + 8u * sl; };
   const uint32_t bfull_bar = done_bar + 40u;   // B_ext written for the item (epilogue -> MMA)
   const uint32_t bempty_bar = done_bar + 48u;  // the item's MMAs have read B_ext (MMA -> epilogue)
-  volatile uint32_t* s_item = reinterpret_cast<volatile uint32_t*>(sm + kSmItem);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + kSmAbort);
-  uint32_t* s_qidx = reinterpret_cast<uint32_t*>(sm + kSmQidx);
-  float* s_qn2 = reinterpret_cast<float*>(sm + kSmQn2);
-  volatile int* s_okw = reinterpret_cast<volatile int*>(sm + kSmOkw);
+  volatile uint32_t* s_item = reinterpret_cast<volatile uint32_t*>(sm + LY::kItem);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + LY::kAbort);
+  uint32_t* s_qidx = reinterpret_cast<uint32_t*>(sm + LY::kQidx);
+  float* s_qn2 = reinterpret_cast<float*>(sm + LY::kQn2);
+  volatile int* s_okw = reinterpret_cast<volatile int*>(sm + LY::kOkw);
 
   const uint64_t wns = a.wait_ns ? a.wait_ns : kWaitNs;  // every bounded wait gives up after this
   const int nkb = (a.L + kUK - 1) / kUK;
   constexpr bool resident = kResident;
-  constexpr uint32_t nst = resident ? kAStages : kResidentKB;  // streamed: one query slot per stage
+  constexpr uint32_t nst = resident ? LY::kStages : kResidentKB;  // streamed: one query slot per stage
   // query count (read on the device for rounds planned there) and queries
   // per tile (MMA N): 64 in the bound pass, else the launch's choice or, for
   // 0, the narrowest of 64 / 128 / 256 that holds the queries
@@ -297,7 +310,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t total = listed ? (a.nitems_dev ? min(a.nitems, *a.nitems_dev) : a.nitems) : nchunks * QT;
 
   if (tid == 0) {
-    for (int s = 0; s < kAStages; ++s) {
+    for (int s = 0; s < LY::kStages; ++s) {
       mbar_init(full_bar(s), 1);
       mbar_init(empty_bar(s), 1);
     }
@@ -321,21 +334,21 @@ __global__ void __launch_bounds__(kThreads, 1)
     // A_ext: every element 1 (BF16 0x3F80); B_ext: zero until an item's
     // thresholds are written.  Generic-proxy writes, made visible to the
     // tensor cores (async proxy) before the barrier below.
-    uint32_t* ae = reinterpret_cast<uint32_t*>(sm + kSmAext);
-    uint32_t* be = reinterpret_cast<uint32_t*>(sm + kSmBext);
+    uint32_t* ae = reinterpret_cast<uint32_t*>(sm + LY::kAext);
+    uint32_t* be = reinterpret_cast<uint32_t*>(sm + LY::kBext);
     for (int i = tid; i < (int)(kUM * kExtRow / 4); i += kThreads) ae[i] = 0x3F803F80u;
     for (int i = tid; i < (int)(kUN * kExtRow / 4); i += kThreads) be[i] = 0u;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 2) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(base + kSmTmem)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(base + LY::kTmem)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kSmTmem);
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + LY::kTmem);
 
   if (warp == 0) {
     // ---------------- TMA producer
@@ -357,9 +370,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (resident) {
           ok = mbar_wait(qempty_bar, (it_n & 1) ^ 1, abort_flag, a.err, wns);
           if (!ok) break;
-          mbar_expect_tx(qfull_bar, (uint32_t)nkb * kQBytes);
+          mbar_expect_tx(qfull_bar, (uint32_t)nkb * LY::kQBlk);
           for (int kb = 0; kb < nkb; ++kb)
-            tma_load_2d(base + kSmQ + kb * kQBytes, &tmQ, kb * kUK, (int)it.qoff, qfull_bar);
+            tma_load_2d(base + LY::kQ + kb * LY::kQBlk, &tmQ, kb * kUK, (int)it.qoff, qfull_bar);
           ++q_issued;
         }
         for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t) {
@@ -377,8 +390,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             // phase never completes and the MMA warp's bounded wait runs out
             if (a.withhold_first_copy && g == 0) continue;
             mbar_expect_tx(full_bar(s), resident ? kABytes : kABytes + kQBytes);
-            tma_load_2d(base + kSmA + s * kABytes, &tmA, kb * kUK, row0, full_bar(s));
-            if (!resident) tma_load_2d(base + kSmQ + s * kQBytes, &tmQ, kb * kUK, (int)it.qoff, full_bar(s));
+            tma_load_2d(base + LY::kA + s * kABytes, &tmA, kb * kUK, row0, full_bar(s));
+            if (!resident) tma_load_2d(base + LY::kQ + s * kQBytes, &tmQ, kb * kUK, (int)it.qoff, full_bar(s));
           }
         }
         if (!ok) break;
@@ -396,7 +409,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (lane == 0) {
       uint32_t g = 0, tcount = 0, it_n = 0;
       uint32_t s_cur = 0, ph = 0;  // stage g % nst and the parity of g / nst
-      const uint64_t dae = sw32_desc(base + kSmAext), dbe = sw32_desc(base + kSmBext);
+      const uint64_t dae = sw32_desc(base + LY::kAext), dbe = sw32_desc(base + LY::kBext);
       bool ok = true;
       for (; ok; ++it_n) {
         const int sl = (int)(it_n & 1);
@@ -437,8 +450,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (!ok) break;
             tc_fence_after();
             // K step k16 is 32 bytes on: 2 in the descriptors' address field
-            const uint64_t da = sw128_desc(base + kSmA + s * kABytes);
-            const uint64_t dq = sw128_desc(base + kSmQ + (resident ? kb : s) * kQBytes);
+            const uint64_t da = sw128_desc(base + LY::kA + s * kABytes);
+            const uint64_t dq = sw128_desc(base + LY::kQ + (resident ? (uint32_t)kb * LY::kQBlk : (uint32_t)s * kQBytes));
 #pragma unroll
             for (int k16 = 0; k16 < kUK / 16; ++k16)
               tc_mma(d, da + 2 * k16, dq + 2 * k16, idesc, (screen || kb || k16) ? 1u : 0u);
@@ -563,7 +576,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           tl = tv - th;  // exact: th is within a factor 2 of tv
         }
         const uint32_t row = (uint32_t)etid;
-        *reinterpret_cast<uint32_t*>(sm + kSmBext + row * kExtRow + (((row >> 2) & 1u) << 4)) =
+        *reinterpret_cast<uint32_t*>(sm + LY::kBext + row * kExtRow + (((row >> 2) & 1u) << 4)) =
             bf16_bits(-th) | (bf16_bits(-tl) << 16);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       }
@@ -1340,15 +1353,16 @@ cudaError_t launch_umma_pair(const CUtensorMap& rows_map, const CUtensorMap& q_h
   return cudaLaunchKernelEx(&cfg, k_umma_pair, rows_map, q_half_map, g);
 }
 
-size_t umma_filter_smem() { return kDynSmem; }
+size_t umma_filter_smem() { return FilterLayout<false>::kDyn; }
 
-template <bool kScreen, bool kResident>
+template <bool kScreen, bool kResident, bool kBound>
 static cudaError_t launch_filter_instance(const CUtensorMap& rows_map, const CUtensorMap& q_map, const BatchGemm& g,
                                           int grid, cudaStream_t s) {
+  constexpr int smem = (int)FilterLayout<kBound>::kDyn;
   static SmemLimit attr;
-  const cudaError_t ea = attr.ensure((const void*)k_umma_filter<kScreen, kResident>, (int)kDynSmem);
+  const cudaError_t ea = attr.ensure((const void*)k_umma_filter<kScreen, kResident, kBound>, smem);
   if (ea != cudaSuccess) return ea;
-  k_umma_filter<kScreen, kResident><<<grid, kThreads, kDynSmem, s>>>(rows_map, q_map, g);
+  k_umma_filter<kScreen, kResident, kBound><<<grid, kThreads, smem, s>>>(rows_map, q_map, g);
   return cudaGetLastError();
 }
 
@@ -1370,11 +1384,13 @@ cudaError_t launch_umma_filter(const CUtensorMap& rows_map, const CUtensorMap& q
   const bool screen = g.mode == 1 || g.mode == 3;
   const bool resident = (g.L + kUK - 1) / kUK <= kResidentKB;
   if (screen) {
-    return resident ? launch_filter_instance<true, true>(rows_map, q_map, g, grid, s)
-                    : launch_filter_instance<true, false>(rows_map, q_map, g, grid, s);
+    return resident ? launch_filter_instance<true, true, false>(rows_map, q_map, g, grid, s)
+                    : launch_filter_instance<true, false, false>(rows_map, q_map, g, grid, s);
   }
-  return resident ? launch_filter_instance<false, true>(rows_map, q_map, g, grid, s)
-                  : launch_filter_instance<false, false>(rows_map, q_map, g, grid, s);
+  // the bound pass with a resident query tile: q_map has 64-query boxes
+  if (g.mode == 0 && resident) return launch_filter_instance<false, true, true>(rows_map, q_map, g, grid, s);
+  return resident ? launch_filter_instance<false, true, false>(rows_map, q_map, g, grid, s)
+                  : launch_filter_instance<false, false, false>(rows_map, q_map, g, grid, s);
 }
 
 }  // namespace hg
