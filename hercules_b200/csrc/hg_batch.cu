@@ -49,10 +49,10 @@ constexpr int kBM = kBatchTileRows;
 __global__ void k_rows_to_bf16(const float* __restrict__ rows, const uint32_t* __restrict__ idx, uint64_t n,
                                const uint32_t* n_dev, int L, __nv_bfloat16* __restrict__ out,
                                float4* __restrict__ meta) {
-  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (n_dev) n = *n_dev;  // at most the n the grid was sized for
-  if (w >= n) return;
+  if (n_dev) n = min(n, (uint64_t)*n_dev);  // at most the n the launch was sized for
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += nw) {
   const uint64_t src = idx ? idx[w] : w;
   const float4* x = reinterpret_cast<const float4*>(rows + src * L);
   __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(out + w * L);
@@ -85,6 +85,7 @@ __global__ void k_rows_to_bf16(const float* __restrict__ rows, const uint32_t* _
     const double up = 1.0 + 1e-12;
     meta[src] = make_float4(__double2float_ru(a2 * up), __double2float_ru(sqrt(t2) * up),
                           __double2float_ru(sqrt(r2) * up), 0.0f);
+  }
   }
 }
 
@@ -159,9 +160,12 @@ __global__ void __launch_bounds__(kSelThreads) k_bound_select(BatchRank a) {
   // coalesced load), the chunk sums are added in chunk order
   // (ts_euclidean_distance_SIMD's order, no abandon)
   const int lane = tid & 31, nch = a.L >> 3;
+  // the 2k + 32 best slots by d~ (at most kMaxK) are ranked exactly: the k-th
+  // distinct exact distance among them bounds the query's k-th neighbour
+  const int nrank = min(kMaxK, 2 * k + 32);
   for (int i = tid >> 5; i < kWarpListCap; i += kSelThreads / 32) {
     unsigned long long v = ~0ull;
-    if (i < kMaxK && i < n && buf[i] != ~0ull) {  // uniform over the warp
+    if (i < nrank && i < n && buf[i] != ~0ull) {  // uniform over the warp
       const uint32_t row = (uint32_t)buf[i];
       const float* xr = a.rows + (uint64_t)row * a.L;
       float d = 0.0f;
@@ -738,7 +742,17 @@ static inline unsigned nblk(uint64_t n, int t) { return (unsigned)((n + t - 1) /
 cudaError_t launch_rows_to_bf16(const float* rows, const uint32_t* idx, uint64_t n, int L, void* out, float4* meta,
                                 cudaStream_t s, const uint32_t* n_dev) {
   if (!n) return cudaSuccess;
-  k_rows_to_bf16<<<nblk(n * 32, 256), 256, 0, s>>>(rows, idx, n, n_dev, L, static_cast<__nv_bfloat16*>(out), meta);
+  // a warp per row, grid-stride: a count read on the device (often far below
+  // n) costs no launch of n warps
+  uint64_t blocks = nblk(n * 32, 256);
+  if (n_dev) {
+    int dev = 0;
+    const cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t cap = 32ull * (uint64_t)sm_count(dev);
+    if (blocks > cap) blocks = cap;
+  }
+  k_rows_to_bf16<<<(unsigned)blocks, 256, 0, s>>>(rows, idx, n, n_dev, L, static_cast<__nv_bfloat16*>(out), meta);
   return cudaGetLastError();
 }
 
