@@ -649,46 +649,50 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc_wait_ld();
             if (a.mode == 0) {
               const int span = kUM / (int)it.sub;  // rows per slot: 8 .. 128
+              // 32-bit keys: the order-preserving bits of d~ with the low 7
+              // replaced by the row's index in its 128-row tile (a relative
+              // 2^-16 of d~; the exact ranking of the candidates decides)
+              const uint32_t rit = (uint32_t)(quarter * 32 + lane);
+              const uint64_t tile_row0 = it.rb + (uint64_t)t * kUM;
+              auto slot_key = [&](uint32_t k32) {
+                return ((unsigned long long)(k32 & ~0x7Fu) << 32) | (uint32_t)(tile_row0 + (k32 & 0x7Fu));
+              };
               if (span >= 32) {
                 // the warp's 32 rows lie in one slot: butterfly transpose-min,
                 // lane l ends with column c0 + l reduced over the 32 rows
-                unsigned long long v[32];
+                uint32_t v[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                   const float dd = xn2 + s_qn2[c0 + j] - 2.0f * __uint_as_float(r[j]);
-                  v[j] = row_ok ? (((unsigned long long)ordered_key(dd) << 32) | (uint32_t)row) : ~0ull;
+                  v[j] = row_ok ? ((ordered_key(dd) & ~0x7Fu) | rit) : 0xffffffffu;
                 }
 #pragma unroll
                 for (int o = 16; o >= 1; o >>= 1) {
                   const bool upper = (lane & o) != 0;
 #pragma unroll
                   for (int i = 0; i < o; ++i) {
-                    const unsigned long long send = upper ? v[i] : v[i + o];
-                    const unsigned long long keep = upper ? v[i + o] : v[i];
-                    const unsigned long long recv = __shfl_xor_sync(HG_FULL, send, o);
-                    v[i] = recv < keep ? recv : keep;
+                    const uint32_t send = upper ? v[i] : v[i + o];
+                    const uint32_t keep = upper ? v[i + o] : v[i];
+                    v[i] = min(keep, __shfl_xor_sync(HG_FULL, send, o));
                   }
                 }
                 const uint32_t slot = t * it.sub + (uint32_t)(quarter * 32 / span);
-                if (c0 + lane < c_hi && v[0] != ~0ull && slot < a.bm_cap)
-                  atomicMin(&a.bm[(uint64_t)s_qidx[c0 + lane] * a.bm_cap + slot], v[0]);
+                if (c0 + lane < c_hi && v[0] != 0xffffffffu && slot < a.bm_cap)
+                  atomicMin(&a.bm[(uint64_t)s_qidx[c0 + lane] * a.bm_cap + slot], slot_key(v[0]));
               } else {
                 const int grp = span;
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                   if (c0 + j >= c_hi) break;  // uniform over the warp
-                  unsigned long long key = ~0ull;
+                  uint32_t key = 0xffffffffu;
                   if (row_ok) {
                     const float dd = xn2 + s_qn2[c0 + j] - 2.0f * __uint_as_float(r[j]);
-                    key = ((unsigned long long)ordered_key(dd) << 32) | (uint32_t)row;
+                    key = (ordered_key(dd) & ~0x7Fu) | rit;
                   }
-                  for (int o = 1; o < grp; o <<= 1) {
-                    const unsigned long long w2 = __shfl_xor_sync(HG_FULL, key, o);
-                    key = w2 < key ? w2 : key;
-                  }
+                  for (int o = 1; o < grp; o <<= 1) key = min(key, __shfl_xor_sync(HG_FULL, key, o));
                   const uint32_t slot = t * it.sub + (uint32_t)((quarter * 32 + lane) / span);
-                  if ((lane & (grp - 1)) == 0 && key != ~0ull && slot < a.bm_cap)
-                    atomicMin(&a.bm[(uint64_t)s_qidx[c0 + j] * a.bm_cap + slot], key);
+                  if ((lane & (grp - 1)) == 0 && key != 0xffffffffu && slot < a.bm_cap)
+                    atomicMin(&a.bm[(uint64_t)s_qidx[c0 + j] * a.bm_cap + slot], slot_key(key));
                 }
               }
             } else if (row_ok) {
