@@ -220,6 +220,29 @@ __device__ __forceinline__ float fmax3(float a, float b, float c) {
   return r;
 }
 
+// Survivor mask of 32 accumulators against h (bit j: j < nv and v[j] >= h):
+// the maxima of four 8-column groups first (three-input max), then the
+// compares only in the groups whose maximum reaches h
+__device__ __forceinline__ uint32_t screen32(const float* v, float h, int nv) {
+  float g[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float* w = v + 8 * q;
+    g[q] = fmaxf(fmax3(fmax3(w[0], w[1], w[2]), w[3], w[4]), fmax3(w[5], w[6], w[7]));
+  }
+  uint32_t mask = 0;
+  if (fmax3(g[0], g[1], fmaxf(g[2], g[3])) >= h) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (g[q] >= h) {
+#pragma unroll
+        for (int j = 8 * q; j < 8 * q + 8; ++j) mask |= (j < nv && v[j] >= h) ? (1u << j) : 0u;
+      }
+    }
+  }
+  return mask;
+}
+
 __device__ __forceinline__ uint32_t ordered_key(float f) {
   const uint32_t b = __float_as_uint(f);
   return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
@@ -629,17 +652,7 @@ __global__ void __launch_bounds__(kThreads, 1)
               if (cb >= c_hi) break;  // uniform over the warp
               // the accumulators already hold acc_j - t_j: screen by their
               // maximum; columns past the item's queries never survive
-              const float* v = reinterpret_cast<const float*>(r[hh]);
-              float m = -inf;
-#pragma unroll
-              for (int j = 0; j < 32; j += 2) m = fmax3(m, v[j], v[j + 1]);
-              if (m >= h_row) {
-                const int nv = c_hi - cb;
-                uint32_t mask = 0;
-#pragma unroll
-                for (int j = 0; j < 32; ++j) mask |= (j < nv && v[j] >= h_row) ? (1u << j) : 0u;
-                masks[2 * i2 + hh] = mask;
-              }
+              masks[2 * i2 + hh] = screen32(reinterpret_cast<const float*>(r[hh]), h_row, c_hi - cb);
             }
           }
         } else {
@@ -1243,17 +1256,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           for (int hh = 0; hh < 2; ++hh) {
             const int cb = c0 + 32 * hh;
             if (cb >= c_hi) break;
-            const float* v = reinterpret_cast<const float*>(r[hh]);
-            float m = -inf;
-#pragma unroll
-            for (int jj = 0; jj < 32; jj += 2) m = fmax3(m, v[jj], v[jj + 1]);
-            if (m >= h_row) {
-              const int nv = c_hi - cb;
-              uint32_t mask = 0;
-#pragma unroll
-              for (int jj = 0; jj < 32; ++jj) mask |= (jj < nv && v[jj] >= h_row) ? (1u << jj) : 0u;
-              masks[2 * i2 + hh] = mask;
-            }
+            masks[2 * i2 + hh] = screen32(reinterpret_cast<const float*>(r[hh]), h_row, c_hi - cb);
           }
         }
         tc_fence_before();
