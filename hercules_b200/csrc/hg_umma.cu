@@ -318,7 +318,15 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint64_t wns = a.wait_ns ? a.wait_ns : kWaitNs;  // every bounded wait gives up after this
   const int nkb = (a.L + kUK - 1) / kUK;
   constexpr bool resident = kResident;
-  constexpr uint32_t nst = resident ? LY::kStages : kResidentKB;  // streamed: one query slot per stage
+  // A streamed query tile (L > 256) is shared by two row tiles: each stage
+  // holds one query K block and the same K block of two row tiles, whose
+  // products go to the two TMEM accumulators (the epilogue then takes both at
+  // once); three such stages of 64 KB fit.  A resident tile serves one row
+  // tile per accumulator, double-buffered.
+  constexpr uint32_t kGroup = resident ? 1u : 2u;                 // row tiles per MMA group
+  constexpr uint32_t nst = resident ? (uint32_t)LY::kStages : 3u;
+  constexpr uint32_t aBase = resident ? LY::kA : 3u * kQBytes;  // row stages (streamed: after the 3 query slots)
+  static_assert(resident || aBase + nst * kGroup * kABytes <= LY::kAext, "streamed stages");
   // query count (read on the device for rounds planned there) and queries
   // per tile (MMA N): 64 in the bound pass, else the launch's choice or, for
   // 0, the narrowest of 64 / 128 / 256 that holds the queries
@@ -398,8 +406,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             tma_load_2d(base + LY::kQ + kb * LY::kQBlk, &tmQ, kb * kUK, (int)it.qoff, qfull_bar);
           ++q_issued;
         }
-        for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t) {
-          const int row0 = (int)(it.rb + (uint64_t)t * kUM);
+        const uint32_t ngroups = it.t_hi > it.t_lo ? (it.t_hi - it.t_lo + kGroup - 1) / kGroup : 0u;
+        for (uint32_t jg = 0; ok && jg < ngroups; ++jg) {
+          const uint32_t t0 = it.t_lo + jg * kGroup;
           for (int kb = 0; kb < nkb; ++kb, ++g) {
             const int s = (int)s_cur;
             const uint32_t par = ph;
@@ -412,8 +421,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             // diagnostics: the first stage's copy withheld, so its barrier
             // phase never completes and the MMA warp's bounded wait runs out
             if (a.withhold_first_copy && g == 0) continue;
-            mbar_expect_tx(full_bar(s), resident ? kABytes : kABytes + kQBytes);
-            tma_load_2d(base + LY::kA + s * kABytes, &tmA, kb * kUK, row0, full_bar(s));
+            mbar_expect_tx(full_bar(s), kGroup * kABytes + (resident ? 0u : kQBytes));
+#pragma unroll
+            for (uint32_t gi = 0; gi < kGroup; ++gi)
+              tma_load_2d(base + aBase + (s * kGroup + gi) * kABytes, &tmA, kb * kUK,
+                          (int)(it.rb + (uint64_t)(t0 + gi) * kUM), full_bar(s));
             if (!resident) tma_load_2d(base + LY::kQ + s * kQBytes, &tmQ, kb * kUK, (int)it.qoff, full_bar(s));
           }
         }
@@ -454,14 +466,19 @@ __global__ void __launch_bounds__(kThreads, 1)
           tc_fence_after();
         }
         const uint32_t idesc = idesc_for(item_n(it.qcnt, qtile));
-        for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t, ++tcount) {
-          const int b = (int)(tcount & 1);
-          ok = mbar_wait(tempty_bar(b), ((tcount >> 1) & 1) ^ 1, abort_flag, a.err, wns);
+        const uint32_t ngroups = it.t_hi > it.t_lo ? (it.t_hi - it.t_lo + kGroup - 1) / kGroup : 0u;
+        for (uint32_t jg = 0; ok && jg < ngroups; ++jg, ++tcount) {
+          const int b = kGroup == 1 ? (int)(tcount & 1) : 0;
+          const uint32_t tph = kGroup == 1 ? ((tcount >> 1) & 1) : (tcount & 1);
+          ok = mbar_wait(tempty_bar(b), tph ^ 1, abort_flag, a.err, wns);
           if (!ok) break;
           tc_fence_after();
-          const uint32_t d = tmem + (uint32_t)b * kUN;
+          const uint32_t d = tmem + (uint32_t)b * kUN;  // + gi * kUN for the group's row tile gi
           // screening: the accumulator starts as -(t_hi + t_lo) of its column
-          if (screen) tc_mma(d, dae, dbe, idesc, 0u);
+          if (screen) {
+#pragma unroll
+            for (uint32_t gi = 0; gi < kGroup; ++gi) tc_mma(d + gi * kUN, dae, dbe, idesc, 0u);
+          }
           for (int kb = 0; kb < nkb; ++kb, ++g) {
             const int s = (int)s_cur;
             const uint32_t par = ph;
@@ -473,11 +490,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (!ok) break;
             tc_fence_after();
             // K step k16 is 32 bytes on: 2 in the descriptors' address field
-            const uint64_t da = sw128_desc(base + LY::kA + s * kABytes);
             const uint64_t dq = sw128_desc(base + LY::kQ + (resident ? (uint32_t)kb * LY::kQBlk : (uint32_t)s * kQBytes));
 #pragma unroll
-            for (int k16 = 0; k16 < kUK / 16; ++k16)
-              tc_mma(d, da + 2 * k16, dq + 2 * k16, idesc, (screen || kb || k16) ? 1u : 0u);
+            for (uint32_t gi = 0; gi < kGroup; ++gi) {
+              const uint64_t da = sw128_desc(base + aBase + (s * kGroup + gi) * kABytes);
+#pragma unroll
+              for (int k16 = 0; k16 < kUK / 16; ++k16)
+                tc_mma(d + gi * kUN, da + 2 * k16, dq + 2 * k16, idesc, (screen || kb || k16) ? 1u : 0u);
+            }
             tc_commit(empty_bar(s));
           }
           if (ok) tc_commit(tfull_bar(b));
@@ -609,34 +629,49 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int half_cols = min(qtile / 2, (int)((it.qcnt + 63u) / 64u) * 32);
       const int c_lo = half * half_cols;
       const int c_hi = min(c_lo + half_cols, (int)it.qcnt);
-      // the row's |x|^2, loaded one tile ahead
-      float xn_next = 0.0f;
-      auto prefetch = [&](uint32_t t) {
-        if (t >= it.t_hi) return;
-        const uint64_t rw = it.rb + (uint64_t)t * kUM + quarter * 32 + lane;
-        xn_next = (rw >= it.vb && rw < it.re && rw < a.nrows) ? a.xmeta[rw].x : 0.0f;
+      // the rows' |x|^2, loaded one group of row tiles ahead
+      float xn_next[kGroup];
+      auto prefetch = [&](uint32_t jg) {
+#pragma unroll
+        for (uint32_t gi = 0; gi < kGroup; ++gi) {
+          const uint32_t t = it.t_lo + jg * kGroup + gi;
+          const uint64_t rw = it.rb + (uint64_t)t * kUM + quarter * 32 + lane;
+          xn_next[gi] = (t < it.t_hi && rw >= it.vb && rw < it.re && rw < a.nrows) ? a.xmeta[rw].x : 0.0f;
+        }
       };
-      prefetch(it.t_lo);
-      for (uint32_t t = it.t_lo; ok && t < it.t_hi; ++t, ++tcount) {
-        const int b = (int)(tcount & 1);
-        const uint64_t row = it.rb + (uint64_t)t * kUM + quarter * 32 + lane;
-        const bool row_ok = row >= it.vb && row < it.re && row < a.nrows;
-        const float xn2 = xn_next;
-        prefetch(t + 1);
-        const float h_row = row_ok ? 0.5f * xn2 : inf;
+      const uint32_t ngroups = it.t_hi > it.t_lo ? (it.t_hi - it.t_lo + kGroup - 1) / kGroup : 0u;
+      prefetch(0);
+      for (uint32_t jg = 0; ok && jg < ngroups; ++jg, ++tcount) {
+        const int b = kGroup == 1 ? (int)(tcount & 1) : 0;
+        const uint32_t tph = kGroup == 1 ? ((tcount >> 1) & 1) : (tcount & 1);
+        float xn2s[kGroup];
+#pragma unroll
+        for (uint32_t gi = 0; gi < kGroup; ++gi) xn2s[gi] = xn_next[gi];
+        if (jg + 1 < ngroups) prefetch(jg + 1);
         // each warp waits for the accumulator itself (lane 0, result shared)
         int go = 0;
-        if (lane == 0) go = mbar_wait(tfull_bar(b), (tcount >> 1) & 1, abort_flag, a.err, wns) ? 1 : 0;
+        if (lane == 0) go = mbar_wait(tfull_bar(b), tph, abort_flag, a.err, wns) ? 1 : 0;
         go = __shfl_sync(HG_FULL, go, 0);
         if (!go) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)b * kUN;
-        // mode 1: survivor masks of the warp's (up to) four 32-column chunks;
-        // the buckets are written after the accumulator is handed back
-        uint32_t masks[4] = {0u, 0u, 0u, 0u};
+        // mode 1: survivor masks of the warp's (up to) four 32-column chunks
+        // per row tile; the buckets are written after the accumulator is
+        // handed back
+        uint32_t masks[kGroup][4];
+        uint64_t rows_g[kGroup];
+#pragma unroll
+        for (uint32_t gi = 0; gi < kGroup; ++gi) {
+        const uint32_t t = it.t_lo + jg * kGroup + gi;
+        const uint64_t row = it.rb + (uint64_t)t * kUM + quarter * 32 + lane;
+        const bool row_ok = t < it.t_hi && row >= it.vb && row < it.re && row < a.nrows;
+        rows_g[gi] = row;
+        const float xn2 = xn2s[gi];
+        const float h_row = row_ok ? 0.5f * xn2 : inf;
+        const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b + (int)gi) * kUN;
+        masks[gi][0] = masks[gi][1] = masks[gi][2] = masks[gi][3] = 0u;
         if (screen) {
 #pragma unroll
           for (int i2 = 0; i2 < 2; ++i2) {
@@ -652,7 +687,7 @@ __global__ void __launch_bounds__(kThreads, 1)
               if (cb >= c_hi) break;  // uniform over the warp
               // the accumulators already hold acc_j - t_j: screen by their
               // maximum; columns past the item's queries never survive
-              masks[2 * i2 + hh] = screen32(reinterpret_cast<const float*>(r[hh]), h_row, c_hi - cb);
+              masks[gi][2 * i2 + hh] = screen32(reinterpret_cast<const float*>(r[hh]), h_row, c_hi - cb);
             }
           }
         } else {
@@ -715,14 +750,18 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
           }
         }
+        }  // row tiles of the group
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(tempty_bar(b));
         // survivor pairs into the warp's reserved block of the pair list:
         // plain stores, one atomic per kPairBlock pairs
 #pragma unroll
+        for (uint32_t gi = 0; gi < kGroup; ++gi) {
+        const uint64_t row = rows_g[gi];
+#pragma unroll
         for (int ci = 0; ci < 4; ++ci) {
-          uint32_t mask = masks[ci];
+          uint32_t mask = masks[gi][ci];
           while (__any_sync(HG_FULL, mask != 0)) {
             const bool has = mask != 0;
             unsigned long long e = 0;
@@ -747,6 +786,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             pcur += n;
           }
         }
+        }  // row tiles of the group
       }
     }
     for (uint32_t i = pcur + lane; i < pend; i += 32) a.pairs[i] = ~0ull;  // close the last block
