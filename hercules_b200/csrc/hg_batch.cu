@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_merge(BatchRank a) {
   const float Tq = __uint_as_float(ld_volatile(&a.qbound[q]));
   const uint32_t p0 = a.seg_prefix[pos], p1 = a.seg_prefix[pos + 1];
   for (uint32_t p = p0; p < p1; ++p) {
-    const int pc = a.part_cnt[p];
+    const int pc = max(0, min(a.part_cnt[p], a.kmax));
     const unsigned long long* part = a.parts + (uint64_t)p * a.kmax;
     for (int base = 0; base < pc; base += 32) {
       const unsigned long long v = base + lane < pc ? part[base + lane] : ~0ull;
