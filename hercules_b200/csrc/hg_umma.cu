@@ -705,7 +705,33 @@ __global__ void __launch_bounds__(kThreads, 1)
               auto slot_key = [&](uint32_t k32) {
                 return ((unsigned long long)(k32 & ~0x7Fu) << 32) | (uint32_t)(tile_row0 + (k32 & 0x7Fu));
               };
-              if (span >= 32) {
+              if (span >= 32 && c_hi - c0 <= 16) {
+                // at most 16 columns (the usual bound-pass group): rows l and
+                // l + 16 combined first, then a 16-column butterfly
+                // transpose-min in each half, so lane l (< 16) ends with
+                // column c0 + l reduced over the 32 rows
+                uint32_t v[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                  const float dd = xn2 + s_qn2[c0 + j] - 2.0f * __uint_as_float(r[j]);
+                  v[j] = row_ok ? ((ordered_key(dd) & ~0x7Fu) | rit) : 0xffffffffu;
+                }
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = min(v[j], __shfl_xor_sync(HG_FULL, v[j], 16));
+#pragma unroll
+                for (int o = 8; o >= 1; o >>= 1) {
+                  const bool upper = (lane & o) != 0;
+#pragma unroll
+                  for (int i = 0; i < o; ++i) {
+                    const uint32_t send = upper ? v[i] : v[i + o];
+                    const uint32_t keep = upper ? v[i + o] : v[i];
+                    v[i] = min(keep, __shfl_xor_sync(HG_FULL, send, o));
+                  }
+                }
+                const uint32_t slot = t * it.sub + (uint32_t)(quarter * 32 / span);
+                if (lane < 16 && c0 + lane < c_hi && v[0] != 0xffffffffu && slot < a.bm_cap)
+                  atomicMin(&a.bm[(uint64_t)s_qidx[c0 + lane] * a.bm_cap + slot], slot_key(v[0]));
+              } else if (span >= 32) {
                 // the warp's 32 rows lie in one slot: butterfly transpose-min,
                 // lane l ends with column c0 + l reduced over the 32 rows
                 uint32_t v[32];
