@@ -629,6 +629,15 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int half_cols = min(qtile / 2, (int)((it.qcnt + 63u) / 64u) * 32);
       const int c_lo = half * half_cols;
       const int c_hi = min(c_lo + half_cols, (int)it.qcnt);
+      // the bound pass (64-query tiles: one 32-column chunk per warp): half
+      // the query norms of the warp's columns in registers; its keys order
+      // d~ / 2 = (|x|^2 + |q|^2) / 2 - q~.x~
+      static_assert(kBatchBoundQueries == 64, "one chunk per epilogue warp in the bound pass");
+      float gq[32];
+      if (!screen && a.mode == 0) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) gq[j] = 0.5f * s_qn2[(c_lo + j) & (kUN - 1)];
+      }
       // the rows' |x|^2, loaded one group of row tiles ahead
       float xn_next[kGroup];
       auto prefetch = [&](uint32_t jg) {
@@ -697,6 +706,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc_wait_ld();
             if (a.mode == 0) {
               const int span = kUM / (int)it.sub;  // rows per slot: 8 .. 128
+              const float h2 = 0.5f * xn2;
               // 32-bit keys: the order-preserving bits of d~ with the low 7
               // replaced by the row's index in its 128-row tile (a relative
               // 2^-16 of d~; the exact ranking of the candidates decides)
@@ -713,7 +723,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 uint32_t v[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                  const float dd = xn2 + s_qn2[c0 + j] - 2.0f * __uint_as_float(r[j]);
+                  const float dd = (h2 + gq[j]) - __uint_as_float(r[j]);
                   v[j] = row_ok ? ((ordered_key(dd) & ~0x7Fu) | rit) : 0xffffffffu;
                 }
 #pragma unroll
@@ -737,7 +747,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 uint32_t v[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
-                  const float dd = xn2 + s_qn2[c0 + j] - 2.0f * __uint_as_float(r[j]);
+                  const float dd = (h2 + gq[j]) - __uint_as_float(r[j]);
                   v[j] = row_ok ? ((ordered_key(dd) & ~0x7Fu) | rit) : 0xffffffffu;
                 }
 #pragma unroll
@@ -760,7 +770,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                   if (c0 + j >= c_hi) break;  // uniform over the warp
                   uint32_t key = 0xffffffffu;
                   if (row_ok) {
-                    const float dd = xn2 + s_qn2[c0 + j] - 2.0f * __uint_as_float(r[j]);
+                    const float dd = (h2 + gq[j]) - __uint_as_float(r[j]);
                     key = (ordered_key(dd) & ~0x7Fu) | rit;
                   }
                   for (int o = 1; o < grp; o <<= 1) key = min(key, __shfl_xor_sync(HG_FULL, key, o));
