@@ -117,5 +117,22 @@ __device__ __forceinline__ int unit_candidate(const uint32_t* unit_prefix, int n
   return lo;
 }
 
+// The same search by a whole warp (every lane calls it; all get the answer):
+// 32 probes per round narrow [lo, ncand - 1] 32-fold.  unit_prefix[lo] <=
+// unit must hold on entry.
+__device__ __forceinline__ int unit_candidate_warp(const uint32_t* unit_prefix, int ncand, int lo, uint32_t unit,
+                                                   int lane) {
+  int hi = ncand - 1;
+  while (true) {
+    const int step = hi - lo >= 32 ? (hi - lo + 32) / 32 : 1;  // probes lo, lo + step, ... cover [lo, hi]
+    const int p = lo + lane * step;
+    const uint32_t le = __ballot_sync(0xffffffffu, p <= hi && unit_prefix[p] <= unit);
+    const int j = le ? 31 - __clz(le) : 0;  // probes at or below `unit` form a prefix of the lanes
+    if (step == 1) return lo + j;
+    lo += j * step;
+    hi = min(hi, lo + step - 1);
+  }
+}
+
 
 }  // namespace hg

@@ -539,9 +539,12 @@ __global__ void k_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_pre
 // (255 / 254) (B (1 + 2^-10) + 1e-6): the reference's float LB_SAX exceeds
 // the bound with room to spare for its rounding, so every row this test
 // prunes is one the exact float test prunes too (never a true neighbour).
-// The 8-bit table is laid out lane-private -- word ((t * 256 + s) / 4) * 32
-// + lane holds the terms of symbols s..s+3 of segment t for that lane -- so
-// the 16 data-dependent lookups of a row never conflict on a bank.
+// The 8-bit table is laid out lane-private: byte b of word
+// ((h * 256 + s) * 2 + g) * 32 + lane holds that lane's term of symbol s for
+// segment t = 8 h + 4 g + b, so the byte of (t, s) sits at
+// (t / 8) * 65536 + ((t / 4) & 1) * 128 + (t & 3) + 256 s + 4 lane: the 16
+// data-dependent lookups of a row never conflict on a bank, and one byte
+// permute of the row's word and 4 lane gives each lookup's address.
 constexpr int kFiltConsumers = 20;                          // consumer warps
 constexpr int kFilterThreads = 32 * (kFiltConsumers + 1);   // + the producer warp
 constexpr int kUnitsPerWarp = 3;                            // units of a stage per consumer warp
@@ -552,7 +555,7 @@ constexpr uint32_t kStageBytes = kStageUnits * kUnitBytes;
 constexpr int kSaxTabWords = HG_PAA_SEGMENTS * HG_SAX_CARD / 4 * 32;  // 128 KB
 constexpr uint32_t kFiltSmStage = kSaxTabWords * 4;                     // stages after the table
 constexpr uint32_t kFiltSmBar = kFiltSmStage + kFiltStages * kStageBytes;  // 2 x kFiltStages mbarriers
-constexpr uint32_t kFiltSmMeta = kFiltSmBar + 2 * kFiltStages * 8;        // end unit, abort flag
+constexpr uint32_t kFiltSmMeta = kFiltSmBar + 2 * kFiltStages * 8;  // end unit, abort flag, first candidate
 constexpr uint64_t kFiltWaitNs = 2000000000ull;                           // 2 s per wait
 size_t lbsax_filter_smem() { return kFiltSmMeta + 16; }
 
@@ -617,46 +620,64 @@ __global__ void __launch_bounds__(kFilterThreads, 1) k_lbsax_filter(FilterArgs a
   const uint32_t per_block = (total + gridDim.x - 1) / gridDim.x;
   const uint32_t u0 = ubase + blockIdx.x * per_block;
   const uint32_t u1 = min(ubase + total, u0 + per_block);
-  if (threadIdx.x == 0) {
-    // the range ends at the first leaf whose LB exceeds the bound (LBs
-    // ascend along the list, so every later unit is past it too)
+  volatile int* s_c0 = reinterpret_cast<volatile int*>(fsm + kFiltSmMeta + 8);
+  if (wib == kFiltConsumers) {
+    // the producer warp finds the block's first candidate and where its
+    // range ends -- at the first leaf whose LB exceeds the bound (LBs ascend
+    // along the list, so every later unit is past it too) -- with 32-way
+    // searches, sets up the barriers and hands both to the consumers
+    // through named barrier 1, while they build the table
+    int c0 = clo;
     uint32_t ue = u0;
     if (u0 < u1) {
-      int c = unit_candidate(a.unit_prefix, ncand, clo, u0);
+      c0 = unit_candidate_warp(a.unit_prefix, ncand, clo, u0, lane);
       ue = u1;
-      for (; c < chi && a.unit_prefix[c] < u1; ++c)
-        if (a.cand_lb[c] > B) {
-          ue = max(u0, a.unit_prefix[c]);
+      for (int cb = c0; cb < chi; cb += 32) {
+        const int c = cb + lane;
+        const bool in_range = c < chi && a.unit_prefix[c] < u1;
+        const uint32_t past = __ballot_sync(HG_FULL, in_range && a.cand_lb[c] > B);
+        if (past) {
+          ue = max(u0, a.unit_prefix[cb + __ffs(past) - 1]);
           break;
         }
+        if (!__all_sync(HG_FULL, in_range)) break;
+      }
     }
-    *s_uend = ue;
-    *abort_flag = 0;
-    for (int st = 0; st < kFiltStages; ++st) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(full_bar(st)), "r"(1) : "memory");
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty_bar(st)), "r"(kFiltConsumers) : "memory");
+    if (lane == 0) {
+      *s_uend = ue;
+      *s_c0 = c0;
+      *abort_flag = 0;
+      for (int st = 0; st < kFiltStages; ++st) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(full_bar(st)), "r"(1) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty_bar(st)), "r"(kFiltConsumers) : "memory");
+      }
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (a.use_lbsax) {
+    __syncwarp();
+    asm volatile("bar.arrive 1, %0;" ::"r"(kFilterThreads) : "memory");
+  } else if (a.use_lbsax) {
     const float Bs = __fadd_rn(__fmul_rn(B, 1.0009765625f), 1e-6f);
     const float T = __fdiv_ru(Bs, (float)(a.L / HG_PAA_SEGMENTS));
     const float scale = __fdiv_rd(254.0f, T);  // 0 when the bound is +inf: nothing is pruned
-    for (int g = threadIdx.x; g < kSaxTabWords / 32; g += blockDim.x) {
-      const float4 v = reinterpret_cast<const float4*>(a.sax_tab)[g];
-      const uint32_t packed = sax_qterm(v.x, scale) | (sax_qterm(v.y, scale) << 8) |
-                              (sax_qterm(v.z, scale) << 16) | (sax_qterm(v.w, scale) << 24);
+    for (int g = threadIdx.x; g < kSaxTabWords / 32; g += 32 * kFiltConsumers) {
+      // the terms of symbol s for segments t0 .. t0 + 3
+      const int sym = (g >> 1) & (HG_SAX_CARD - 1), t0 = 8 * (g >> 9) + 4 * (g & 1);
+      const float* col = a.sax_tab + t0 * HG_SAX_CARD + sym;
+      const uint32_t packed = sax_qterm(col[0], scale) | (sax_qterm(col[HG_SAX_CARD], scale) << 8) |
+                              (sax_qterm(col[2 * HG_SAX_CARD], scale) << 16) |
+                              (sax_qterm(col[3 * HG_SAX_CARD], scale) << 24);
 #pragma unroll 8
       for (int r = 0; r < 32; ++r) qtab[g * 32 + ((r + lane) & 31)] = packed;
     }
   }
-  __syncthreads();
+  if (wib != kFiltConsumers) asm volatile("bar.sync 1, %0;" ::"r"(kFilterThreads) : "memory");
   const uint32_t uend = *s_uend;
+  const int c0 = *s_c0;
   const uint32_t nstages = (uend - u0 + kStageUnits - 1) / kStageUnits;  // 0 when u0 == uend
   if (wib == kFiltConsumers) {
     // ---------------- producer: bulk copies of whole units, leaf by leaf
     if (lane == 0 && nstages) {
-      int c = unit_candidate(a.unit_prefix, ncand, clo, u0);
+      int c = c0;
       uint32_t k = 0;
       bool ok = true;
       for (; k < nstages; ++k) {
@@ -693,9 +714,9 @@ __global__ void __launch_bounds__(kFilterThreads, 1) k_lbsax_filter(FilterArgs a
   } else {
     // ---------------- consumers: lane = row of a unit
     const unsigned char* tb = fsm;
-    const uint32_t lane2 = (uint32_t)(4 * lane) * 0x00010001u;  // 4 lane in both 16-bit halves
+    const uint32_t lanev = (uint32_t)(4 * lane);  // byte 0: 4 lane, bytes 1..3: zero
     const uint32_t lt = (1u << lane) - 1;
-    int c = nstages ? unit_candidate(a.unit_prefix, ncand, clo, u0 + wib * kUnitsPerWarp) : 0;
+    int c = c0;  // the body moves it forward to each unit's candidate
     uint32_t next_c = c + 1 < ncand ? a.unit_prefix[c + 1] : 0xffffffffu;
     int cur = -1;
     uint32_t lstart = 0, lend = 0, first_unit = 0;
@@ -732,22 +753,19 @@ __global__ void __launch_bounds__(kFilterThreads, 1) k_lbsax_filter(FilterArgs a
         bool pass = rr[i] >= lstart && rr[i] < lend;
         n_rows += (uint32_t)__popc(__ballot_sync(HG_FULL, pass));
         if (pass && a.use_lbsax) {
-          // byte (t, s) of this lane's table sits at t * 8192 + f(s) + 4 lane
-          // with f(s) = (s & 0xFC) * 32 + (s & 3) = (s & 0xFC) * 31 + s; the
-          // four symbols of a word get their offsets two at a time, in the
-          // 16-bit halves of one register (no carry: f(s) + 4 lane < 8192)
+          // byte j of word q is the symbol s of segment t = 4 q + j; the
+          // permute puts s in byte 1 and 4 lane in byte 0: 256 s + 4 lane,
+          // the lookup's offset from segment t's fixed base
           const uint4 w = stage[slot * 32 + lane];
           const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
           uint32_t sum = 0;
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            const uint32_t e = ws[q] & 0x00FF00FFu;         // symbols of segments 4q and 4q + 2
-            const uint32_t o = (ws[q] >> 8) & 0x00FF00FFu;  // 4q + 1 and 4q + 3
-            const uint32_t fe = (e & 0x00FC00FCu) * 31u + e + lane2;
-            const uint32_t fo = (o & 0x00FC00FCu) * 31u + o + lane2;
-            const int t0 = 4 * q;
-            sum += (uint32_t)tb[t0 * 8192 + (fe & 0xFFFFu)] + (uint32_t)tb[(t0 + 1) * 8192 + (fo & 0xFFFFu)] +
-                   (uint32_t)tb[(t0 + 2) * 8192 + (fe >> 16)] + (uint32_t)tb[(t0 + 3) * 8192 + (fo >> 16)];
+            const int tq = (q >> 1) * 65536 + (q & 1) * 128;
+            sum += (uint32_t)tb[tq + __byte_perm(ws[q], lanev, 0x5504)] +
+                   (uint32_t)tb[tq + 1 + __byte_perm(ws[q], lanev, 0x5514)] +
+                   (uint32_t)tb[tq + 2 + __byte_perm(ws[q], lanev, 0x5524)] +
+                   (uint32_t)tb[tq + 3 + __byte_perm(ws[q], lanev, 0x5534)];
           }
           pass = sum < 255u;
         }
