@@ -520,7 +520,8 @@ __global__ void k_pscan_prep(uint64_t nrows, int* cand_count, uint32_t* unit_pre
 // Stage 1.  Work: the candidate leaves in ascending LB_EAPCA order, cut into
 // 32-row units (32-aligned rows; a unit's rows outside its leaf are skipped).
 // One persistent block per SM owns a contiguous range of units, ending at the
-// first leaf whose LB exceeds the bound.  Its producer lane bulk-copies the
+// first leaf whose LB exceeds the bound (found by the producer warp while
+// the consumers build the table).  Its producer lane bulk-copies the
 // units' iSAX words (a leaf's units are contiguous in memory: one
 // cp.async.bulk per leaf run, 512 bytes per unit) into kFiltStages stages of
 // shared memory, each guarded by a full and an empty mbarrier; 20 consumer
