@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_rerank_part(BatchRank a) {
     const uint32_t seg = item - a.seg_prefix[lo];
     const uint32_t per = a.seg_rows[lo];
     const uint32_t first = seg * per;
-    const uint32_t last = min(a.bucket_cnt[q], first + per);
+    const uint32_t last = min(min(a.bucket_cnt[q], a.bucket_cap), first + per);  // an overflowed bucket holds bucket_cap rows
     const int k = (int)a.kq[q];
     const int c0 = a.init_cnt[q];
     for (int i = lane; i < kWarpListCap; i += 32) list[i] = i < c0 ? a.init[(uint64_t)q * kMaxK + i] : ~0ull;
