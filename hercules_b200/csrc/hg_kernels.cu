@@ -312,10 +312,11 @@ __global__ void k_query_segstats(const float* __restrict__ Q, int L, int nq, con
   }
 }
 
-// Leaves each query of a batch must filter: a warp per (query, leaf) sums
+// Leaves each query of a batch must filter: a thread per (query, leaf) sums
 // the LB_EAPCA terms of the leaf's segments in order (the plain path's
-// k_leaf_lb arithmetic, segment statistics from k_query_segstats) and keeps
-// the leaf when
+// k_leaf_lb arithmetic, segment statistics from k_query_segstats; the terms
+// are >= 0, so the sum stops once it exceeds the limit) and keeps the leaf
+// when
 //     LB <= B_q (1 + 2^-10) + L 2^-20,
 // B_q the query's bound (+inf keeps every leaf).  The plain path scans only
 // leaves with LB <= its running bound <= B_q, so the kept leaves include
@@ -323,39 +324,37 @@ __global__ void k_query_segstats(const float* __restrict__ Q, int L, int nq, con
 // Kept (leaf, query) pairs go to leaf_q[leaf * stride + i], counted in
 // leaf_cnt[leaf].
 // qlist (optional): the queries are qlist[0 .. *nq_dev) instead of 0 .. nq.
-// A warp per (query, leaf) pair, grid-stride.
+// A thread per (query, leaf) pair, grid-stride (a warp per pair, with the
+// sum's order kept through shuffles, made the bound phase 0.33 ms longer per
+// batch of 4,096 queries at 25M x 256).
 __global__ void k_leaf_keep(const float2* __restrict__ segstats, int nu, int L, int nq,
                             const int* __restrict__ seg_off, const short* __restrict__ points,
                             const int* __restrict__ seg_uid, const float* __restrict__ sk,
                             const uint32_t* __restrict__ leaf_size, int nleaves, const float* __restrict__ bound,
                             uint32_t* leaf_cnt, uint32_t* leaf_q, uint32_t stride, const uint32_t* qlist,
                             const uint32_t* nq_dev) {
-  const int lane = threadIdx.x & 31;
   const uint64_t n = (uint64_t)(nq_dev ? min((uint32_t)nq, *nq_dev) : (uint32_t)nq) * nleaves;
-  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gw < n; gw += nw) {
-  const int qi = (int)(gw / nleaves), w = (int)(gw % nleaves);
-  const int q = qlist ? (int)qlist[qi] : qi;
-  if (leaf_size[w] == 0) continue;
-  const float B = bound[q];
-  const float lim = B < __int_as_float(0x7f800000)
-                        ? __fadd_ru(__fmul_ru(B, 1.0f + 0x1p-10f), __fmul_ru((float)L, 0x1p-20f))
-                        : __int_as_float(0x7f800000);
-  const int off = seg_off[w], nseg = seg_off[w + 1] - off;
-  const float2* st = segstats + (uint64_t)q * nu;
-  float sum = 0.0f;
-  for (int s0 = 0; s0 < nseg && sum <= lim; s0 += 32) {
-    const int s = s0 + lane;
-    float term = 0.0f;
-    if (s < nseg) {
-      const int start = s == 0 ? 0 : points[off + s - 1], end = points[off + s];
+  const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += nt) {
+    const int qi = (int)(g / nleaves), w = (int)(g % nleaves);
+    const int q = qlist ? (int)qlist[qi] : qi;
+    if (leaf_size[w] == 0) continue;
+    const float B = bound[q];
+    const float lim = B < __int_as_float(0x7f800000)
+                          ? __fadd_ru(__fmul_ru(B, 1.0f + 0x1p-10f), __fmul_ru((float)L, 0x1p-20f))
+                          : __int_as_float(0x7f800000);
+    const int off = seg_off[w], nseg = seg_off[w + 1] - off;
+    const float2* st = segstats + (uint64_t)q * nu;
+    float sum = 0.0f;
+    int start = 0;
+    for (int s = 0; s < nseg; ++s) {
+      const int end = points[off + s];
       const float2 ms = st[seg_uid[off + s]];
-      term = hg_eapca_term(ms.x, ms.y, sk + 4 * (off + s), end - start);
+      sum = __fadd_rn(sum, hg_eapca_term(ms.x, ms.y, sk + 4 * (off + s), end - start));
+      start = end;
+      if (!(sum <= lim)) break;
     }
-    const int n = min(32, nseg - s0);
-    for (int j = 0; j < n; ++j) sum = __fadd_rn(sum, __shfl_sync(HG_FULL, term, j));
-  }
-  if (lane == 0 && sum <= lim) leaf_q[(uint64_t)w * stride + atomicAdd(&leaf_cnt[w], 1u)] = (uint32_t)q;
+    if (sum <= lim) leaf_q[(uint64_t)w * stride + atomicAdd(&leaf_cnt[w], 1u)] = (uint32_t)q;
   }
 }
 
@@ -1308,11 +1307,11 @@ cudaError_t launch_leaf_keep_list(const float2* segstats, int nu, int L, int nq,
                                   int nleaves, const float* bound, uint32_t* leaf_cnt, uint32_t* leaf_q,
                                   uint32_t stride, const uint32_t* qlist, const uint32_t* nq_dev, cudaStream_t s) {
   if (nq <= 0 || nleaves <= 0) return cudaSuccess;
-  // grid-stride over the (query, leaf) pairs: at most 64 blocks of 8 warps per SM
+  // grid-stride over the (query, leaf) pairs: at most 64 blocks of 256 threads per SM
   int dev = 0;
   const cudaError_t ed = cudaGetDevice(&dev);
   if (ed != cudaSuccess) return ed;
-  const uint64_t want = blocks_for((uint64_t)nq * nleaves * 32, 256);
+  const uint64_t want = blocks_for((uint64_t)nq * nleaves, 256);
   const uint64_t cap = 64ull * (uint64_t)sm_count(dev);
   k_leaf_keep<<<(unsigned)(want < cap ? want : cap), 256, 0, s>>>(
       segstats, nu, L, nq, seg_off, points, seg_uid, sk, leaf_size, nleaves, bound, leaf_cnt, leaf_q, stride, qlist,
